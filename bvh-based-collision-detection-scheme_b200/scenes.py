@@ -1,0 +1,156 @@
+"""Seeded synthetic frame generators for the collision workloads.
+
+The reference reads mesh sequences from disk through assimp
+(Mine/world/Scene.cpp:14-42) and hands the pipeline a ``SceneData{pos, fids}``
+(Mine/world/Scene.h:16-20): float3 positions and int3 faces, meshes
+concatenated with vertex offsets (Scene.cpp:31-40).  The benchmark datasets it
+was evaluated on are not available, so every workload here is generated from
+a fixed seed with the shapes, sizes and motion the workload names:
+
+* ``cloth_fold``      128x128 (or n x n) square cloth, analytic fold
+                      z = 0.3 sin(2 pi x t) cos(2 pi y t) + N(0, 1e-3),
+                      t = (f + 1) / frames.
+* ``cloth_over_sphere`` 512x512 cloth with a seeded damped-wave fold of
+                      amplitude 0.2 over a geodesic icosphere (frequency 45,
+                      40,500 triangles, radius 0.25); per-frame vertex motion
+                      at most 2% of an edge length.
+* ``stacked_layers``  four cloth layers 1e-3 apart with seeded in-plane shear.
+
+All arrays are float32 positions (V, 3) and int32 faces (T, 3).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def cloth_grid(n: int, size: float = 1.0):
+    """n x n vertex grid on [0, size]^2, two triangles per quad with a fixed
+    diagonal: T = 2 (n - 1)^2."""
+    xs = np.linspace(0.0, size, n, dtype=np.float64)
+    X, Y = np.meshgrid(xs, xs, indexing="xy")
+    idx = np.arange(n * n, dtype=np.int32).reshape(n, n)
+    a = idx[:-1, :-1].ravel()
+    b = idx[:-1, 1:].ravel()
+    c = idx[1:, :-1].ravel()
+    d = idx[1:, 1:].ravel()
+    f1 = np.stack([a, b, d], axis=1)
+    f2 = np.stack([a, d, c], axis=1)
+    faces = np.empty((2 * a.size, 3), dtype=np.int32)
+    faces[0::2] = f1
+    faces[1::2] = f2
+    return X.ravel(), Y.ravel(), faces
+
+
+def cloth_fold_frames(n: int = 128, frames: int = 20, seed: int = 1234,
+                      noise: float = 1e-3):
+    """Square cloth under the analytic fold; yields (frame, pos) with the
+    shared faces returned first.  Frame f uses t = (f + 1) / frames."""
+    x, y, faces = cloth_grid(n)
+    rng = np.random.default_rng(seed)
+    out = []
+    for f in range(frames):
+        t = (f + 1) / frames
+        z = 0.3 * np.sin(2 * np.pi * x * t) * np.cos(2 * np.pi * y * t)
+        z = z + rng.normal(0.0, noise, size=z.shape)
+        out.append(np.stack([x, y, z], axis=1).astype(np.float32))
+    return faces, out
+
+
+def icosphere(freq: int, radius: float = 1.0, center=(0.0, 0.0, 0.0)):
+    """Geodesic icosahedron of the given frequency: 20 freq^2 triangles,
+    10 freq^2 + 2 shared vertices, projected on a sphere."""
+    p = (1.0 + math.sqrt(5.0)) / 2.0
+    v = np.array([[-1, p, 0], [1, p, 0], [-1, -p, 0], [1, -p, 0],
+                  [0, -1, p], [0, 1, p], [0, -1, -p], [0, 1, -p],
+                  [p, 0, -1], [p, 0, 1], [-p, 0, -1], [-p, 0, 1]], dtype=np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    ico = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11),
+           (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6), (7, 1, 8),
+           (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9),
+           (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    keys = {}
+    verts = []
+
+    def vid(face, i, j):
+        # canonical key of the lattice point i*(B-A)/freq + j*(C-A)/freq + A on
+        # the face (A, B, C): weights on the sorted corner ids
+        a, b, c = face
+        w = {a: freq - i - j, b: i, c: j}
+        key = tuple(sorted((k, wt) for k, wt in w.items() if wt > 0))
+        if key not in keys:
+            pt = sum(v[k] * wt for k, wt in w.items()) / freq
+            keys[key] = len(verts)
+            verts.append(pt / np.linalg.norm(pt))
+        return keys[key]
+
+    faces = []
+    for face in ico:
+        grid = {}
+        for i in range(freq + 1):
+            for j in range(freq + 1 - i):
+                grid[(i, j)] = vid(face, i, j)
+        for i in range(freq):
+            for j in range(freq - i):
+                faces.append((grid[(i, j)], grid[(i + 1, j)], grid[(i, j + 1)]))
+                if i + j < freq - 1:
+                    faces.append((grid[(i + 1, j)], grid[(i + 1, j + 1)], grid[(i, j + 1)]))
+    verts = np.asarray(verts) * radius + np.asarray(center, dtype=np.float64)
+    return verts.astype(np.float64), np.asarray(faces, dtype=np.int32)
+
+
+def cloth_over_sphere_frames(n: int = 512, frames: int = 100, seed: int = 2024,
+                             sphere_freq: int = 45, amplitude: float = 0.2,
+                             height: float = 0.2, radius: float = 0.25,
+                             first_frame: int = 0):
+    """Cloth (n x n on [0,1]^2) folded by a seeded damped radial wave,
+    z = height + A e^{-lambda t} sin(k r - omega t + phi), over a static
+    icosphere centred under the cloth.  The step in t is chosen so that no
+    vertex moves more than 2% of an edge length (1/(n-1)) per frame.
+    Returns (faces, [pos per frame]) with the sphere appended after the cloth
+    (vertex ids offset by the cloth's vertex count)."""
+    x, y, cfaces = cloth_grid(n)
+    rng = np.random.default_rng(seed)
+    cx, cy = rng.uniform(0.3, 0.7, size=2)
+    phi = rng.uniform(0.0, 2 * np.pi)
+    k = 2 * np.pi * rng.uniform(2.0, 4.0)
+    lam, omega = 0.5, 2 * np.pi
+    edge = 1.0 / (n - 1)
+    dt = 0.02 * edge / (amplitude * (omega + lam)) * 0.999
+    r = np.hypot(x - cx, y - cy)
+    sv, sf = icosphere(sphere_freq, radius, (0.5, 0.5, 0.0))
+    faces = np.concatenate([cfaces, sf + x.size]).astype(np.int32)
+    out = []
+    prev = None
+    for f in range(first_frame, first_frame + frames):
+        t = f * dt
+        z = height + amplitude * math.exp(-lam * t) * np.sin(k * r - omega * t + phi)
+        cloth = np.stack([x, y, z], axis=1)
+        if prev is not None:
+            assert np.abs(cloth - prev).max() <= 0.02 * edge + 1e-12
+        prev = cloth
+        out.append(np.concatenate([cloth, sv]).astype(np.float32))
+    return faces, out
+
+
+def stacked_layers_frames(n: int = 512, layers: int = 4, frames: int = 50, seed: int = 77,
+                          gap: float = 1e-3, max_shear: float = 0.5):
+    """`layers` cloths at z = 0, gap, 2 gap, ... with a seeded in-plane shear
+    of up to +-max_shear edge lengths per frame per layer."""
+    x, y, cf = cloth_grid(n)
+    rng = np.random.default_rng(seed)
+    edge = 1.0 / (n - 1)
+    V = x.size
+    faces = np.concatenate([cf + l * V for l in range(layers)]).astype(np.int32)
+    shear = np.zeros((layers, 2))
+    out = []
+    for f in range(frames):
+        shear += rng.uniform(-max_shear, max_shear, size=(layers, 2)) * edge
+        pts = []
+        for l in range(layers):
+            sx = x + shear[l, 0] * y
+            sy = y + shear[l, 1] * x
+            pts.append(np.stack([sx, sy, np.full_like(x, l * gap)], axis=1))
+        out.append(np.concatenate(pts).astype(np.float32))
+    return faces, out

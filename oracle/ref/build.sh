@@ -1,0 +1,19 @@
+#!/bin/sh
+# Builds oracle/_ref/libref_tritri.so from the reference's gProximity header
+# where it lies in the reference tree (default /root/reference; override with
+# REF_ROOT).  Output goes to oracle/_ref/ only.  Skips quietly when the
+# reference tree is absent (the GPU box has only the prebuilt files).
+set -e
+HERE=$(cd "$(dirname "$0")" && pwd)
+REF_ROOT=${REF_ROOT:-/root/reference}
+OUT="$HERE/../_ref"
+GP="$REF_ROOT/Source/Externals/inc/gProximity"
+if [ ! -f "$GP/cuda_intersect_tritri.h" ]; then
+  echo "reference tree not found at $REF_ROOT; oracle/_ref not rebuilt"
+  exit 0
+fi
+mkdir -p "$OUT"
+CUDA_INC=${CUDA_HOME:-/usr/local/cuda}/include
+g++ -O2 -std=c++17 -fPIC -shared -ffp-contract=off -w \
+    -I"$GP" -I"$CUDA_INC" "$HERE/gproximity_tritri.cpp" -o "$OUT/libref_tritri.so"
+echo "built $OUT/libref_tritri.so"
