@@ -1,0 +1,336 @@
+"""Python mirror of the reference's collision module interface over the C ABI
+(include/bvhcd.h, libbvhcd.so built in this directory).
+
+``LBvh`` stands in for ``LBvhFixedDeformable`` and ``BvttFront`` for
+``BvttFrontLooseIntra`` (Mine/collision/lbvh/LBvhFixedDeformable.h:27-50,
+Mine/collision/bvtt_front/BvttFrontLooseIntra.h:27-36): same maintenance
+options, same meaning of the per-frame calls.  Inputs are numpy arrays (host,
+copied each call like the reference's SceneData upload) or CUDA tensors (read
+in place).  There is no fallback: the compiled library is required, and every
+error status raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbvhcd.so")
+
+BVH_BUILD, BVH_REFIT, BVH_UPDATE = 0, 1, 2
+FRONT_PURE_BVH_CD, FRONT_GENERATE, FRONT_UPDATE, FRONT_REORDER, FRONT_KEEP, FRONT_RESTRUCTURE = range(6)
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "capacity exceeded",
+          4: "CUDA error", 5: "timeout", 6: "not ready"}
+
+EXPORTED = [
+    "bvhcd_status_string", "bvhcd_device_check", "bvhcd_bvh_create", "bvhcd_bvh_destroy",
+    "bvhcd_bvh_maintain", "bvhcd_bvh_sizes", "bvhcd_bvh_opt_tag", "bvhcd_bvh_export",
+    "bvhcd_bvh_request_restructure",
+    "bvhcd_front_create", "bvhcd_front_destroy", "bvhcd_front_maintain", "bvhcd_front_stats_get",
+    "bvhcd_front_pairs", "bvhcd_front_device_results", "bvhcd_front_export",
+    "bvhcd_schedule_heuristic", "bvhcd_frame", "bvhcd_profile_enable", "bvhcd_profile_read",
+    "bvhcd_launch_count",
+]
+
+STAGES = ["bvh_build", "bvh_refit", "bvh_restructure", "front_generate", "front_update",
+          "front_keep", "front_balance", "front_reorder", "narrow", "quality", "pure_bvh_cd"]
+
+
+class BvhcdError(RuntimeError):
+    def __init__(self, status, what):
+        super().__init__(f"{what}: {STATUS.get(status, status)}")
+        self.status = status
+
+
+class BvhConfig(ctypes.Structure):
+    _fields_ = [("prim_capacity", ctypes.c_int32), ("vert_capacity", ctypes.c_int32),
+                ("enable_restr", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
+
+
+class FrontConfig(ctypes.Structure):
+    _fields_ = [("int_front_capacity", ctypes.c_int64), ("ext_front_capacity", ctypes.c_int64),
+                ("pair_capacity", ctypes.c_int64), ("cull_adjacent", ctypes.c_int32),
+                ("narrow_phase", ctypes.c_int32), ("auto_grow", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 5)]
+
+
+class Scene(ctypes.Structure):
+    _fields_ = [("pos", ctypes.c_void_p), ("faces", ctypes.c_void_p),
+                ("num_vertices", ctypes.c_int32), ("num_faces", ctypes.c_int32),
+                ("on_device", ctypes.c_int32), ("faces_static", ctypes.c_int32)]
+
+
+class FrontStats(ctypes.Structure):
+    _fields_ = [("int_front", ctypes.c_int64), ("ext_front", ctypes.c_int64),
+                ("broad_pairs", ctypes.c_int64), ("narrow_hits", ctypes.c_int64),
+                ("overflow", ctypes.c_int32), ("bvh_opt_tag", ctypes.c_int32),
+                ("front_op_run", ctypes.c_int32), ("restr_pending", ctypes.c_int32),
+                ("num_rt_subtrees", ctypes.c_int32), ("num_rt_int_nodes", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 6)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_LIB = None
+
+
+def build(force: bool = False):
+    """Compile libbvhcd.so in-tree (nvcc, sm_100a)."""
+    if force:
+        subprocess.run(["make", "-s", "-C", HERE, "clean"], check=True)
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    """The loaded C library.  Raises when it is missing: no fallback path."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing; run make in {HERE}")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+        sig = {
+            "bvhcd_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+            "bvhcd_device_check": (ctypes.c_int, [i32, ctypes.POINTER(i32)]),
+            "bvhcd_bvh_create": (ctypes.c_int, [ctypes.POINTER(BvhConfig), ctypes.POINTER(vp)]),
+            "bvhcd_bvh_destroy": (ctypes.c_int, [vp]),
+            "bvhcd_bvh_maintain": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(Scene), vp]),
+            "bvhcd_bvh_sizes": (ctypes.c_int, [vp, ctypes.POINTER(i32), ctypes.POINTER(i32),
+                                               ctypes.POINTER(i32)]),
+            "bvhcd_bvh_opt_tag": (ctypes.c_int, [vp, ctypes.POINTER(i32)]),
+            "bvhcd_bvh_export": (ctypes.c_int, [vp] + [vp] * 7 + [vp]),
+            "bvhcd_bvh_request_restructure": (ctypes.c_int, [vp, vp, i32, vp]),
+            "bvhcd_front_create": (ctypes.c_int, [vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
+            "bvhcd_front_destroy": (ctypes.c_int, [vp]),
+            "bvhcd_front_maintain": (ctypes.c_int, [vp, ctypes.c_int, vp]),
+            "bvhcd_front_stats_get": (ctypes.c_int, [vp, ctypes.POINTER(FrontStats), vp]),
+            "bvhcd_front_pairs": (ctypes.c_int, [vp, i32, vp, i64, ctypes.POINTER(i64), i32, vp]),
+            "bvhcd_front_device_results": (ctypes.c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp)]),
+            "bvhcd_front_export": (ctypes.c_int, [vp, i32, vp, i64, ctypes.POINTER(i64), vp]),
+            "bvhcd_schedule_heuristic": (ctypes.c_int, [i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
+            "bvhcd_frame": (ctypes.c_int, [vp, vp, i32, i32, ctypes.POINTER(Scene), vp]),
+            "bvhcd_profile_enable": (ctypes.c_int, [vp, i32]),
+            "bvhcd_profile_read": (ctypes.c_int, [vp, vp, vp, i32]),
+            "bvhcd_launch_count": (ctypes.c_int, [ctypes.POINTER(i64)]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def _check(status, what):
+    if status != 0:
+        raise BvhcdError(status, what)
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        except ImportError:
+            pass
+        return ctypes.c_void_p(0)
+    if isinstance(stream, int):
+        return ctypes.c_void_p(stream)
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def schedule(frame: int, start: int = 0):
+    """(bvh_op, front_op) of BenchmarkLogic::maintainScheme, STATIC_MANDATORY
+    with divergent marks (Mine/system/Logic/BenchmarkLogic.hpp:102-117)."""
+    b, f = ctypes.c_int32(), ctypes.c_int32()
+    _check(lib().bvhcd_schedule_heuristic(frame, start, ctypes.byref(b), ctypes.byref(f)), "schedule")
+    return b.value, f.value
+
+
+def launch_count() -> int:
+    n = ctypes.c_int64()
+    _check(lib().bvhcd_launch_count(ctypes.byref(n)), "launch count")
+    return n.value
+
+
+def device_check(device: int = 0) -> bool:
+    ok = ctypes.c_int32()
+    _check(lib().bvhcd_device_check(device, ctypes.byref(ok)), "device check")
+    return bool(ok.value)
+
+
+def _scene(pos, faces, faces_static=False):
+    """Scene struct plus the objects that keep its buffers alive."""
+    keep = []
+    try:
+        import torch
+        is_t = isinstance(pos, torch.Tensor)
+    except ImportError:
+        is_t = False
+    if is_t:
+        assert pos.is_cuda and faces.is_cuda, "tensors must live on the GPU"
+        assert pos.dtype == torch.float32 and faces.dtype == torch.int32
+        pos = pos.contiguous()
+        faces = faces.contiguous()
+        keep += [pos, faces]
+        sc = Scene(pos.data_ptr(), faces.data_ptr(), pos.shape[0], faces.shape[0], 1, int(faces_static))
+    else:
+        pos = np.ascontiguousarray(pos, dtype=np.float32)
+        faces = np.ascontiguousarray(faces, dtype=np.int32)
+        keep += [pos, faces]
+        sc = Scene(pos.ctypes.data, faces.ctypes.data, pos.shape[0], faces.shape[0], 0, int(faces_static))
+    return sc, keep
+
+
+class LBvh:
+    """LBvhFixedDeformable: maintain(BUILD | REFIT | UPDATE, scene) per frame."""
+
+    def __init__(self, prim_capacity: int, vert_capacity: int = 0, enable_restr: bool = True):
+        cfg = BvhConfig(int(prim_capacity), int(vert_capacity), int(enable_restr))
+        h = ctypes.c_void_p()
+        _check(lib().bvhcd_bvh_create(ctypes.byref(cfg), ctypes.byref(h)), "bvh create")
+        self._h = h
+        self._keep = []
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().bvhcd_bvh_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def maintain(self, op: int, pos, faces, stream=None, faces_static=False):
+        sc, keep = _scene(pos, faces, faces_static)
+        self._keep = keep
+        _check(lib().bvhcd_bvh_maintain(self._h, int(op), ctypes.byref(sc), _stream_ptr(stream)),
+               "bvh maintain")
+
+    def profile(self, on: bool = True):
+        """Record CUDA events around every stage (Logger::recordSection)."""
+        _check(lib().bvhcd_profile_enable(self._h, int(on)), "profile enable")
+
+    def stage_times(self, reset: bool = False) -> dict:
+        ms = np.zeros(len(STAGES), np.float64)
+        calls = np.zeros(len(STAGES), np.int64)
+        _check(lib().bvhcd_profile_read(self._h, ms.ctypes.data, calls.ctypes.data, int(reset)),
+               "profile read")
+        return {k: (float(ms[i]), int(calls[i])) for i, k in enumerate(STAGES)}
+
+    def sizes(self):
+        a, b, c = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().bvhcd_bvh_sizes(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "sizes")
+        return a.value, b.value, c.value
+
+    def opt_tag(self) -> int:
+        t = ctypes.c_int32()
+        _check(lib().bvhcd_bvh_opt_tag(self._h, ctypes.byref(t)), "opt tag")
+        return t.value
+
+    def request_restructure(self, roots, stream=None):
+        """Mark subtrees (DFS ids) as degraded; the next maintain restructures."""
+        r = np.ascontiguousarray(roots, dtype=np.int32)
+        _check(lib().bvhcd_bvh_request_restructure(self._h, r.ctypes.data, r.size, _stream_ptr(stream)),
+               "request restructure")
+
+    def export(self, stream=None):
+        T = self.sizes()[0]
+        I = max(T - 1, 0)
+        inode = np.zeros((max(I, 1), 6), np.int32)
+        ibox = np.zeros((max(I, 1), 6), np.float32)
+        leaf = np.zeros((max(T, 1), 4), np.int32)
+        lbox = np.zeros((max(T, 1), 6), np.float32)
+        lca = np.zeros(T + 1, np.int32)
+        codes = np.zeros(max(T, 1), np.uint32)
+        primmap = np.zeros(max(T, 1), np.int32)
+        _check(lib().bvhcd_bvh_export(self._h, inode.ctypes.data, ibox.ctypes.data, leaf.ctypes.data,
+                                      lbox.ctypes.data, lca.ctypes.data, codes.ctypes.data,
+                                      primmap.ctypes.data, _stream_ptr(stream)), "bvh export")
+        return dict(inode=inode[:I], ibox=ibox[:I], leaf=leaf[:T], lbox=lbox[:T], lca=lca,
+                    codes=codes[:T], primmap=primmap[:T])
+
+
+class BvttFront:
+    """BvttFrontLooseIntra over a borrowed LBvh: maintain(op) per frame."""
+
+    def __init__(self, bvh: LBvh, int_front_capacity: int = 2_300_000,
+                 ext_front_capacity: int = 2_300_000, pair_capacity: int = 1_600_000,
+                 cull_adjacent: bool = True, narrow_phase: bool = True, auto_grow: bool = False):
+        cfg = FrontConfig(int(int_front_capacity), int(ext_front_capacity), int(pair_capacity),
+                          int(cull_adjacent), int(narrow_phase), int(auto_grow))
+        h = ctypes.c_void_p()
+        _check(lib().bvhcd_front_create(bvh.handle, ctypes.byref(cfg), ctypes.byref(h)), "front create")
+        self._h = h
+        self._bvh = bvh
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().bvhcd_front_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def maintain(self, op: int, stream=None):
+        _check(lib().bvhcd_front_maintain(self._h, int(op), _stream_ptr(stream)), "front maintain")
+
+    def stats(self, stream=None) -> dict:
+        st = FrontStats()
+        _check(lib().bvhcd_front_stats_get(self._h, ctypes.byref(st), _stream_ptr(stream)), "stats")
+        return st.as_dict()
+
+    def pairs(self, narrow: bool = False, stream=None) -> np.ndarray:
+        """Broad-phase pairs (applyCpResults) or intersecting pairs, original ids."""
+        n = ctypes.c_int64()
+        st = lib().bvhcd_front_pairs(self._h, int(narrow), None, 0, ctypes.byref(n), 0, _stream_ptr(stream))
+        if st not in (0, 3):
+            _check(st, "pairs")
+        out = np.zeros((max(n.value, 1), 2), np.int32)
+        st = lib().bvhcd_front_pairs(self._h, int(narrow), out.ctypes.data, n.value, ctypes.byref(n), 0,
+                                     _stream_ptr(stream))
+        _check(st, "pairs")
+        return out[:n.value]
+
+    def export(self, which: int, stream=None) -> np.ndarray:
+        n = ctypes.c_int64()
+        st = lib().bvhcd_front_export(self._h, int(which), None, 0, ctypes.byref(n), _stream_ptr(stream))
+        if st not in (0, 3):
+            _check(st, "front export")
+        out = np.zeros((max(n.value, 1), 2), np.int32)
+        _check(lib().bvhcd_front_export(self._h, int(which), out.ctypes.data, n.value, ctypes.byref(n),
+                                        _stream_ptr(stream)), "front export")
+        return out[:n.value]
+
+    def device_results(self):
+        hits, counts = ctypes.c_void_p(), ctypes.c_void_p()
+        _check(lib().bvhcd_front_device_results(self._h, ctypes.byref(hits), ctypes.byref(counts)),
+               "device results")
+        return hits.value, counts.value
+
+
+def frame(bvh: LBvh, front: BvttFront, f: int, start: int, pos, faces, stream=None, faces_static=False):
+    """One frame of the reference app loop (CudaProjectApp.cpp:49-52)."""
+    sc, keep = _scene(pos, faces, faces_static)
+    _check(lib().bvhcd_frame(bvh.handle, front.handle, int(f), int(start), ctypes.byref(sc),
+                             _stream_ptr(stream)), "frame")
+    bvh._keep = keep

@@ -1,0 +1,195 @@
+// capi.cu -- extern "C" entry points declared in include/bvhcd.h.
+#include <new>
+
+#include "pipeline.h"
+
+struct bvhcd_bvh {
+    bvhcd::LBvh impl;
+    explicit bvhcd_bvh(const bvhcd_bvh_config &c) : impl(c) {}
+};
+struct bvhcd_front {
+    bvhcd::Front impl;
+    bvhcd_front(bvhcd::LBvh *b, const bvhcd_front_config &c) : impl(b, c) {}
+};
+
+namespace {
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+}  // namespace
+
+extern "C" {
+#pragma GCC visibility push(default)
+
+const char *bvhcd_status_string(bvhcd_status s) {
+    switch (s) {
+    case BVHCD_OK: return "ok";
+    case BVHCD_INVALID_ARG: return "invalid argument";
+    case BVHCD_OUT_OF_MEMORY: return "out of device memory";
+    case BVHCD_CAPACITY_EXCEEDED: return "capacity exceeded";
+    case BVHCD_CUDA_ERROR: return "CUDA error";
+    case BVHCD_TIMEOUT: return "timeout";
+    case BVHCD_NOT_READY: return "not ready";
+    }
+    return "unknown status";
+}
+
+bvhcd_status bvhcd_device_check(int32_t device, int32_t *ok) {
+    if (!ok) return BVHCD_INVALID_ARG;
+    *ok = 0;
+    cudaDeviceProp p;
+    cudaError_t e = cudaGetDeviceProperties(&p, device);
+    if (e != cudaSuccess) return bvhcd::cuda_status(e);
+    *ok = (p.major == 10 && p.minor == 0) ? 1 : 0;
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_bvh_create(const bvhcd_bvh_config *cfg, bvhcd_bvh **out) {
+    if (!cfg || !out) return BVHCD_INVALID_ARG;
+    *out = nullptr;
+    bvhcd_bvh *h = new (std::nothrow) bvhcd_bvh(*cfg);
+    if (!h) return BVHCD_OUT_OF_MEMORY;
+    bvhcd_status st = h->impl.init();
+    if (st != BVHCD_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_bvh_destroy(bvhcd_bvh *bvh) {
+    if (!bvh) return BVHCD_INVALID_ARG;
+    delete bvh;
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_bvh_maintain(bvhcd_bvh *bvh, bvhcd_bvh_op op, const bvhcd_scene *scene, void *stream) {
+    if (!bvh || !scene) return BVHCD_INVALID_ARG;
+    return bvh->impl.maintain(op, *scene, as_stream(stream));
+}
+
+bvhcd_status bvhcd_bvh_sizes(const bvhcd_bvh *bvh, int32_t *prims, int32_t *ext_nodes, int32_t *int_nodes) {
+    if (!bvh) return BVHCD_INVALID_ARG;
+    int T = bvh->impl.T();
+    if (prims) *prims = T;
+    if (ext_nodes) *ext_nodes = T;
+    if (int_nodes) *int_nodes = T > 0 ? T - 1 : 0;
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_bvh_opt_tag(const bvhcd_bvh *bvh, int32_t *tag) {
+    if (!bvh || !tag) return BVHCD_INVALID_ARG;
+    *tag = bvh->impl.opt_tag();
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_bvh_request_restructure(bvhcd_bvh *bvh, const int32_t *roots, int32_t n, void *stream) {
+    if (!bvh) return BVHCD_INVALID_ARG;
+    return bvh->impl.request_restructure(roots, n, as_stream(stream));
+}
+
+bvhcd_status bvhcd_bvh_export(const bvhcd_bvh *bvh, int32_t *inode, float *ibox, int32_t *leaf, float *lbox,
+                              int32_t *lca, uint32_t *codes, int32_t *primmap, void *stream) {
+    if (!bvh) return BVHCD_INVALID_ARG;
+    return bvh->impl.export_tree(inode, ibox, leaf, lbox, lca, codes, primmap, as_stream(stream));
+}
+
+bvhcd_status bvhcd_front_create(bvhcd_bvh *bvh, const bvhcd_front_config *cfg, bvhcd_front **out) {
+    if (!bvh || !cfg || !out) return BVHCD_INVALID_ARG;
+    *out = nullptr;
+    bvhcd_front *h = new (std::nothrow) bvhcd_front(&bvh->impl, *cfg);
+    if (!h) return BVHCD_OUT_OF_MEMORY;
+    bvhcd_status st = h->impl.init();
+    if (st != BVHCD_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_front_destroy(bvhcd_front *front) {
+    if (!front) return BVHCD_INVALID_ARG;
+    delete front;
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_front_maintain(bvhcd_front *front, bvhcd_front_op op, void *stream) {
+    if (!front) return BVHCD_INVALID_ARG;
+    return front->impl.maintain(op, as_stream(stream));
+}
+
+bvhcd_status bvhcd_front_stats_get(bvhcd_front *front, bvhcd_front_stats *stats, void *stream) {
+    if (!front || !stats) return BVHCD_INVALID_ARG;
+    return front->impl.stats(stats, as_stream(stream));
+}
+
+bvhcd_status bvhcd_front_pairs(bvhcd_front *front, int32_t which, int32_t *out, int64_t cap, int64_t *count,
+                               int32_t out_on_device, void *stream) {
+    if (!front || which < 0 || which > 1 || cap < 0) return BVHCD_INVALID_ARG;
+    return front->impl.pairs(which, out, cap, count, out_on_device != 0, as_stream(stream));
+}
+
+bvhcd_status bvhcd_front_device_results(bvhcd_front *front, const int32_t **hit_pairs, const int64_t **counts) {
+    if (!front) return BVHCD_INVALID_ARG;
+    return front->impl.device_results(hit_pairs, counts);
+}
+
+bvhcd_status bvhcd_front_export(bvhcd_front *front, int32_t which, int32_t *out, int64_t cap, int64_t *count,
+                                void *stream) {
+    if (!front || cap < 0) return BVHCD_INVALID_ARG;
+    return front->impl.export_front(which, out, cap, count, as_stream(stream));
+}
+
+bvhcd_status bvhcd_profile_enable(bvhcd_bvh *bvh, int32_t on) {
+    if (!bvh) return BVHCD_INVALID_ARG;
+    bvh->impl.profiler()->on = on != 0;
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_profile_read(bvhcd_bvh *bvh, double *ms, int64_t *calls, int32_t reset) {
+    if (!bvh) return BVHCD_INVALID_ARG;
+    return bvh->impl.profiler()->read(ms, calls, reset != 0);
+}
+
+// BenchmarkLogic::maintainScheme, STATIC_MANDATORY with divergent marks
+// (Mine/system/Logic/BenchmarkLogic.hpp:102-117): BVH cycle 12
+// (Mine/setting/BvhSettings.h:45), front cycle 6 (Mine/setting/BvttFrontSettings.h:49).
+bvhcd_status bvhcd_schedule_heuristic(int32_t frame, int32_t start_frame, int32_t *bvh_op, int32_t *front_op) {
+    if (!bvh_op || !front_op || frame < start_frame) return BVHCD_INVALID_ARG;
+    const int f = frame - start_frame;
+    int b = (f % 12) ? BVHCD_BVH_REFIT : BVHCD_BVH_BUILD;
+    int k = f % 6, fr;
+    if (k == 0) fr = (frame == start_frame) ? BVHCD_FRONT_GENERATE : BVHCD_FRONT_UPDATE;
+    else if (k == 5) fr = BVHCD_FRONT_REORDER;
+    else fr = BVHCD_FRONT_KEEP;
+    if (b == BVHCD_BVH_BUILD) fr = BVHCD_FRONT_GENERATE;
+    if ((f + 1) % 12 == 0) fr = BVHCD_FRONT_KEEP;
+    *bvh_op = b;
+    *front_op = fr;
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_frame(bvhcd_bvh *bvh, bvhcd_front *front, int32_t frame, int32_t start_frame,
+                         const bvhcd_scene *scene, void *stream) {
+    int32_t b, f;
+    bvhcd_status st = bvhcd_schedule_heuristic(frame, start_frame, &b, &f);
+    if (st != BVHCD_OK) return st;
+    st = bvhcd_bvh_maintain(bvh, (bvhcd_bvh_op)b, scene, stream);
+    if (st != BVHCD_OK) return st;
+    return bvhcd_front_maintain(front, (bvhcd_front_op)f, stream);
+}
+
+}  // extern "C"
+
+#include <atomic>
+namespace bvhcd {
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace bvhcd
+
+extern "C" __attribute__((visibility("default"))) bvhcd_status bvhcd_launch_count(int64_t *n) {
+    if (!n) return BVHCD_INVALID_ARG;
+    *n = bvhcd::launch_count();
+    return BVHCD_OK;
+}

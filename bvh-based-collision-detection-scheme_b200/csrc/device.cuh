@@ -1,0 +1,144 @@
+// device.cuh -- data layout in HBM and the device helpers shared by the
+// LBVH, front and narrow-phase kernels.
+//
+// Layout (T triangles, Morton-ordered "slots" s = 0..T-1, internal nodes in
+// DFS pre-order d = 0..T-2):
+//   lrec[2s], lrec[2s+1]  leaf record, one 32-byte sector:
+//                         {min.xyz, parent}, {max.xyz, escape}
+//                         parent = DFS id of the leaf's parent (for a left
+//                         child this is the bottom of the left chain that
+//                         starts at s); escape = lca[s+1], the next node in
+//                         DFS order after the leaf.
+//   nrec[2d], nrec[2d+1]  internal record, one 32-byte sector:
+//                         {min.xyz, rangex}, {max.xyz, escape}
+//                         escape = lca[rangey+1].
+//   sface[s]              int4 {v0, v1, v2, original triangle id}
+//   lca[0..T]             tagged DFS entry per leaf (node<<1, or leaf<<1|1),
+//                         lca[T] = -1, the reference's escape links
+//                         (Mine/collision/lbvh/LBvhBuildKernels.cu:187-200)
+//   topo[d]               int4 {lc, rc, par, mark}; mark bit0/bit1: left /
+//                         right child is a leaf, bit2: node is a right child
+//                         (LBvhBuildKernels.cu:147-148,168-169)
+// A traversal step therefore needs one internal sector per node on the left
+// spine and one leaf sector per chain; the integer fields ride in the .w lanes.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bvhcd {
+namespace cg = cooperative_groups;
+
+constexpr int kSms = 148;
+
+struct Tree {
+    float4 *nrec;      // 2 (T-1)
+    float4 *lrec;      // 2 T
+    int4 *topo;        // T-1
+    int2 *nrange;      // T-1 (rangex, rangey)
+    int *lca;          // T+1
+    int4 *sface;       // T
+    int *primmap;      // T (orig -> slot)
+    unsigned *code;    // T
+    int T;
+};
+
+struct FrontLog {      // FlOrderLog (Mine/collision/auxiliary/FlOrderLog.h:19-50)
+    unsigned *intcnt;  // T+1
+    unsigned *extcnt;  // T+1
+    unsigned *intbeg;  // T+1
+    unsigned *extbeg;  // T+1
+    unsigned *intback; // T+1
+    unsigned *extback; // T+1
+};
+
+// Counters kept on the device so no stage needs a host round trip.
+enum CounterSlot {
+    C_INT0 = 0, C_EXT0 = 1,   // front sizes, buffer set 0
+    C_INT1 = 2, C_EXT1 = 3,   // front sizes, buffer set 1
+    C_PAIRS = 4, C_HITS = 5,
+    C_OVERFLOW = 6,           // bit0 int front, bit1 ext front, bit2 pairs, bit3 hits
+    C_RT_SUBTREES = 7, C_RT_INTNODES = 8,
+    C_NUM = 16
+};
+
+__device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
+__device__ __forceinline__ float4 ldcg4(const float4 *p) { return __ldcg(p); }
+
+// AABB overlap, touching counts (BvhBvCompletePort::overlaps,
+// Mine/collision/lbvh/BvhBV.h:54-65).  n = node box, b = query box.
+__device__ __forceinline__ bool overlap(const float4 &nlo, const float4 &nhi, const float4 &blo,
+                                        const float4 &bhi) {
+    return !((blo.x > nhi.x) | (bhi.x < nlo.x) | (blo.y > nhi.y) | (bhi.y < nlo.y) |
+             (blo.z > nhi.z) | (bhi.z < nlo.z));
+}
+
+// covertex (Mine/utility/CudaDeviceUtils.cu:153-157)
+__device__ __forceinline__ bool covertex(const int4 &a, const int4 &b) {
+    return (a.x == b.x) | (a.x == b.y) | (a.x == b.z) | (a.y == b.x) | (a.y == b.y) |
+           (a.y == b.z) | (a.z == b.x) | (a.z == b.y) | (a.z == b.z);
+}
+
+__device__ __forceinline__ float3 load_vert(const float *v, int i) {
+    const float *p = v + 3 * (size_t)i;
+    return make_float3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
+}
+
+// Triangle box: AABB::empty then three combines (Mine/base/Bv.h:27-34,80-84).
+__device__ __forceinline__ void tri_box(const float3 &a, const float3 &b, const float3 &c,
+                                        float4 &lo, float4 &hi) {
+    lo.x = fminf(fminf(fminf(3.402823466e+38f, a.x), b.x), c.x);
+    lo.y = fminf(fminf(fminf(3.402823466e+38f, a.y), b.y), c.y);
+    lo.z = fminf(fminf(fminf(3.402823466e+38f, a.z), b.z), c.z);
+    hi.x = fmaxf(fmaxf(fmaxf(-3.402823466e+38f, a.x), b.x), c.x);
+    hi.y = fmaxf(fmaxf(fmaxf(-3.402823466e+38f, a.y), b.y), c.y);
+    hi.z = fmaxf(fmaxf(fmaxf(-3.402823466e+38f, a.z), b.z), c.z);
+}
+
+// 30-bit Morton code of a box centre normalised by the scene box
+// (calcMCs, LBvhBuildKernels.cu:76-91; morton3D/expandBits,
+// Mine/utility/CudaDeviceUtils.cu:82-130).  IEEE operations only, no
+// contraction, so the code is bit-identical to the reference's.
+__device__ __forceinline__ unsigned expand10(unsigned v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+__device__ __forceinline__ unsigned quant1024(float x) {
+    x = fminf(fmaxf(__fmul_rn(x, 1024.0f), 0.0f), 1023.0f);
+    return (unsigned)x;
+}
+__device__ __forceinline__ unsigned morton_box(const float4 &lo, const float4 &hi,
+                                               const float *scene) {
+    float cx = __fmul_rn(__fadd_rn(lo.x, hi.x), 0.5f);
+    float cy = __fmul_rn(__fadd_rn(lo.y, hi.y), 0.5f);
+    float cz = __fmul_rn(__fadd_rn(lo.z, hi.z), 0.5f);
+    float ox = __fsub_rn(cx, scene[0]), oy = __fsub_rn(cy, scene[1]), oz = __fsub_rn(cz, scene[2]);
+    float w = __fsub_rn(scene[3], scene[0]);
+    float h = __fsub_rn(scene[4], scene[1]);
+    float d = __fsub_rn(scene[5], scene[2]);
+    unsigned xx = expand10(quant1024(__fdiv_rn(ox, w)));
+    unsigned yy = expand10(quant1024(__fdiv_rn(oy, h)));
+    unsigned zz = expand10(quant1024(__fdiv_rn(oz, d)));
+    return xx * 4u + yy * 2u + zz;
+}
+
+// Warp-aggregated reservation: the converged threads that call it take
+// consecutive slots with one atomic.  Returns the slot; writes only when the
+// slot is below capacity, otherwise raises the overflow bit (the counter keeps
+// counting so the required size is known).
+template <typename T>
+__device__ __forceinline__ void emit(T *buf, unsigned *ctr, unsigned cap, const T &v,
+                                     unsigned *ovf, unsigned bit) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(ctr, (unsigned)g.size());
+    base = g.shfl(base, 0) + g.thread_rank();
+    if (base < cap) buf[base] = v;
+    else atomicOr(ovf, bit);
+}
+
+}  // namespace bvhcd

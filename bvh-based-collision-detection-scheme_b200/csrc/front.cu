@@ -1,0 +1,806 @@
+// front.cu -- BVTT front generation, maintenance (prune / sprout), keep,
+// ordering (counting sort by node) and balance, the front-quality metric, and
+// the triangle-triangle narrow phase.
+//
+// Every kernel reads its work size from a device counter and walks it with a
+// grid-stride loop, so a frame is a fixed launch sequence with no host round
+// trip.  Emission reserves slots with one atomic per converged warp group and
+// checks capacity before writing.
+#include <climits>
+
+#include "pipeline.h"
+#include "prims.cuh"
+
+namespace bvhcd {
+
+#define FR_TRY(x)                                        \
+    do {                                                 \
+        cudaError_t e__ = (x);                           \
+        if (e__ != cudaSuccess) return cuda_status(e__); \
+    } while (0)
+
+namespace {
+
+constexpr int kThreads = 256;
+// resident blocks for the grid-stride kernels: a multiple of the SM count
+constexpr int kFrontBlocks = kSms * 8;
+
+inline unsigned grid_for(int64_t n) {
+    int64_t g = (n + kThreads - 1) / kThreads;
+    if (g < 1) g = 1;
+    if (g > kFrontBlocks * 4) g = kFrontBlocks * 4;
+    return (unsigned)g;
+}
+
+struct FArgs {
+    const float4 *nrec, *lrec;
+    const int4 *topo;
+    const int *lca;
+    const int4 *sface;
+    FrontLog log;
+    unsigned *ctr;
+    const int2 *in_int, *in_ext;
+    int2 *out_int, *out_ext;
+    int in_int_slot, in_ext_slot, out_int_slot, out_ext_slot;
+    unsigned cap_int, cap_ext;
+    int2 *pairs;
+    unsigned cap_pairs;
+    int cull;
+    int T;
+};
+
+__device__ __forceinline__ void emit_int(const FArgs &a, int prim, int node) {
+    emit(a.out_int, a.ctr + a.out_int_slot, a.cap_int, make_int2(prim, node), a.ctr + C_OVERFLOW, 1u);
+    atomicAdd(a.log.intcnt + node, 1u);
+}
+__device__ __forceinline__ void emit_ext(const FArgs &a, int prim, int leaf) {
+    emit(a.out_ext, a.ctr + a.out_ext_slot, a.cap_ext, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 2u);
+    atomicAdd(a.log.extcnt + leaf, 1u);
+}
+__device__ __forceinline__ void emit_pair(const FArgs &a, int prim, const int4 &pf, int leaf) {
+    if (a.cull && covertex(pf, __ldg(&a.sface[leaf]))) return;
+    emit(a.pairs, a.ctr + C_PAIRS, a.cap_pairs, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 4u);
+}
+
+// Stackless traversal from tagged node `st` until tagged node `stop`
+// (the loop shared by genLooseIntraFrontsWithLog,
+// Mine/collision/bvtt_front/BvttFrontGenerateKernels.cu:65-88, the sprout
+// half of maintainIntLooseIntraFrontsWithLog,
+// BvttFrontPruneSproutKernels.cu:34-56, keepIntLooseIntraFronts,
+// BvttFrontKeepKernels.cu:26-42, and pureBvhSelfCD, BvhCDKernels.cu:30-47):
+// walk the left spine of an internal node by DFS id while the box overlaps,
+// up to the parent of its leftmost leaf; a node that stops overlapping is a
+// front node and is left through its escape link.
+template <bool kFront>
+__device__ __forceinline__ void traverse(const FArgs &a, int prim, const float4 &plo,
+                                         const float4 &phi, const int4 &pf, int st, int stop) {
+    while (st != stop) {
+        int leaf;
+        float4 llo, lhi;
+        if (st & 1) {
+            leaf = st >> 1;
+            llo = ldg4(a.lrec + 2 * leaf);
+            lhi = ldg4(a.lrec + 2 * leaf + 1);
+        } else {
+            int n = st >> 1;
+            float4 nlo = ldg4(a.nrec + 2 * n), nhi = ldg4(a.nrec + 2 * n + 1);
+            leaf = __float_as_int(nlo.w);
+            llo = ldg4(a.lrec + 2 * leaf);
+            lhi = ldg4(a.lrec + 2 * leaf + 1);
+            const int last = __float_as_int(llo.w);  // parent of the leftmost leaf
+            bool stopped = false;
+            while (true) {
+                if (!overlap(nlo, nhi, plo, phi)) { stopped = true; break; }
+                if (n == last) break;
+                ++n;
+                nlo = ldg4(a.nrec + 2 * n);
+                nhi = ldg4(a.nrec + 2 * n + 1);
+            }
+            if (stopped) {
+                if (kFront) emit_int(a, prim, n);
+                st = __float_as_int(nhi.w);
+                continue;
+            }
+        }
+        if (overlap(llo, lhi, plo, phi)) emit_pair(a, prim, pf, leaf);
+        if (kFront) emit_ext(a, prim, leaf);
+        st = __float_as_int(lhi.w);
+    }
+}
+
+// left child of internal node d, tagged, and its escape
+__device__ __forceinline__ int left_child_tagged(const FArgs &a, int d, const float4 &nlo) {
+    const int rx = __float_as_int(nlo.w);
+    const int last = __float_as_int(__ldg(reinterpret_cast<const float *>(a.lrec) + 8 * (size_t)rx + 3));
+    return last == d ? ((rx << 1) | 1) : ((d + 1) << 1);
+}
+
+__device__ __forceinline__ int4 prim_face(const FArgs &a, int prim) {
+    return a.cull ? __ldg(&a.sface[prim]) : make_int4(0, 0, 0, 0);
+}
+
+// genLooseIntraFrontsWithLog (BvttFrontGenerateKernels.cu:51-90) /
+// pureBvhSelfCD (BvhCDKernels.cu:17-49)
+template <bool kFront>
+__global__ void __launch_bounds__(kThreads) k_generate(FArgs a) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.T - 1; i += gridDim.x * blockDim.x) {
+        float4 plo = ldg4(a.lrec + 2 * i), phi = ldg4(a.lrec + 2 * i + 1);
+        traverse<kFront>(a, i, plo, phi, prim_face(a, i), __float_as_int(phi.w), -1);
+    }
+}
+
+// Walk up the left chain above node `n` (exclusive) while nodes do not
+// overlap; returns the node to emit or -1 to drop (prune half of
+// BvttFrontPruneSproutKernels.cu:24-30 and :76-82).
+__device__ __forceinline__ int prune_up(const FArgs &a, int n, int top, const float4 &plo,
+                                        const float4 &phi) {
+    for (; n >= top; --n) {
+        float4 lo = ldg4(a.nrec + 2 * n), hi = ldg4(a.nrec + 2 * n + 1);
+        if (overlap(lo, hi, plo, phi)) break;
+    }
+    if (n < top && n + 1 > 0) {
+        int p = __ldg(&a.topo[n + 1]).z;
+        float4 lo = ldg4(a.nrec + 2 * p), hi = ldg4(a.nrec + 2 * p + 1);
+        if (!overlap(lo, hi, plo, phi)) return -1;
+    }
+    return n + 1;
+}
+
+// maintainIntLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:12-57)
+__global__ void __launch_bounds__(kThreads) k_maintain_int(FArgs a) {
+    const unsigned n = min(a.ctr[a.in_int_slot], a.cap_int);
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        int2 e = a.in_int[q];
+        const int prim = e.x, st = e.y;
+        float4 plo = ldg4(a.lrec + 2 * prim), phi = ldg4(a.lrec + 2 * prim + 1);
+        float4 nlo = ldg4(a.nrec + 2 * st), nhi = ldg4(a.nrec + 2 * st + 1);
+        if (!overlap(nlo, nhi, plo, phi)) {
+            const int top = __ldg(&a.lca[__float_as_int(nlo.w)]) >> 1;
+            int k = prune_up(a, st - 1, top, plo, phi);
+            if (k >= 0) emit_int(a, prim, k);
+            continue;
+        }
+        traverse<true>(a, prim, plo, phi, prim_face(a, prim), left_child_tagged(a, st, nlo),
+                       __float_as_int(nhi.w));
+    }
+}
+
+// maintainExtLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:60-93)
+__global__ void __launch_bounds__(kThreads) k_maintain_ext(FArgs a) {
+    const unsigned n = min(a.ctr[a.in_ext_slot], a.cap_ext);
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        int2 e = a.in_ext[q];
+        const int prim = e.x, st = e.y;
+        float4 plo = ldg4(a.lrec + 2 * prim), phi = ldg4(a.lrec + 2 * prim + 1);
+        float4 llo = ldg4(a.lrec + 2 * st), lhi = ldg4(a.lrec + 2 * st + 1);
+        if (overlap(llo, lhi, plo, phi)) {
+            emit_ext(a, prim, st);
+            emit_pair(a, prim, prim_face(a, prim), st);
+            continue;
+        }
+        const int gfa = __float_as_int(llo.w);
+        float4 glo = ldg4(a.nrec + 2 * gfa), ghi = ldg4(a.nrec + 2 * gfa + 1);
+        if (overlap(glo, ghi, plo, phi)) {
+            emit_ext(a, prim, st);
+            continue;
+        }
+        const int l = __ldg(&a.lca[st]);
+        if (l & 1) continue;  // right child: the parent's left chain handles it
+        int k = prune_up(a, gfa - 1, l >> 1, plo, phi);
+        if (k >= 0) emit_int(a, prim, k);
+    }
+}
+
+// keepIntLooseIntraFronts / keepExtLooseIntraFronts (BvttFrontKeepKernels.cu:11-58)
+// in one index space: [0, F_int) internal entries, then external ones.
+__global__ void __launch_bounds__(kThreads) k_keep(FArgs a) {
+    const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
+    const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < ni + ne; q += gridDim.x * blockDim.x) {
+        if (q < ni) {
+            int2 e = a.in_int[q];
+            float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
+            float4 nlo = ldg4(a.nrec + 2 * e.y), nhi = ldg4(a.nrec + 2 * e.y + 1);
+            if (!overlap(nlo, nhi, plo, phi)) continue;
+            traverse<false>(a, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, nlo),
+                            __float_as_int(nhi.w));
+        } else {
+            int2 e = a.in_ext[q - ni];
+            float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
+            float4 llo = ldg4(a.lrec + 2 * e.y), lhi = ldg4(a.lrec + 2 * e.y + 1);
+            if (overlap(llo, lhi, plo, phi)) emit_pair(a, e.x, prim_face(a, e.x), e.y);
+        }
+    }
+}
+
+// balance: reorderIntLooseIntraFrontsWithLog (BvttFrontReorderKernels.cu:27-63)
+// + keepExtLooseIntraFronts for the external front.
+__global__ void __launch_bounds__(kThreads) k_balance(FArgs a) {
+    const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
+    const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[a.out_int_slot] = a.ctr[a.in_int_slot];
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < ni + ne; q += gridDim.x * blockDim.x) {
+        if (q < ni) {
+            int2 e = a.in_int[q];
+            float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
+            float4 nlo = ldg4(a.nrec + 2 * e.y), nhi = ldg4(a.nrec + 2 * e.y + 1);
+            if (!overlap(nlo, nhi, plo, phi)) {
+                unsigned pos = a.log.intbeg[e.y] + atomicAdd(a.log.intcnt + e.y, 1u);
+                if (pos < a.cap_int) a.out_int[pos] = e;
+                continue;
+            }
+            unsigned pos = a.log.intbeg[e.y + 1] - 1u - atomicAdd(a.log.intback + e.y, 1u);
+            if (pos < a.cap_int) a.out_int[pos] = e;
+            traverse<false>(a, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, nlo),
+                            __float_as_int(nhi.w));
+        } else {
+            int2 e = a.in_ext[q - ni];
+            float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
+            float4 llo = ldg4(a.lrec + 2 * e.y), lhi = ldg4(a.lrec + 2 * e.y + 1);
+            if (overlap(llo, lhi, plo, phi)) emit_pair(a, e.x, prim_face(a, e.x), e.y);
+        }
+    }
+}
+
+// pureReorderLooseFrontsWithLog (BvttFrontReorderKernels.cu:12-24): counting
+// sort scatter of both fronts by node id.
+__global__ void __launch_bounds__(kThreads) k_reorder(FArgs a) {
+    const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
+    const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.ctr[a.out_int_slot] = a.ctr[a.in_int_slot];
+        a.ctr[a.out_ext_slot] = a.ctr[a.in_ext_slot];
+    }
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < ni + ne; q += gridDim.x * blockDim.x) {
+        if (q < ni) {
+            int2 e = a.in_int[q];
+            unsigned pos = a.log.intbeg[e.y] + atomicAdd(a.log.intcnt + e.y, 1u);
+            if (pos < a.cap_int) a.out_int[pos] = e;
+        } else {
+            int2 e = a.in_ext[q - ni];
+            unsigned pos = a.log.extbeg[e.y] + atomicAdd(a.log.extcnt + e.y, 1u);
+            if (pos < a.cap_ext) a.out_ext[pos] = e;
+        }
+    }
+}
+
+// frontSnapshot (BvttFrontGenerateKernels.cu:26-32)
+__global__ void k_snapshot(int nint, const int2 *__restrict__ nrange, const unsigned *__restrict__ intbeg,
+                           const unsigned *__restrict__ extbeg, float *snap) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nint; i += gridDim.x * blockDim.x) {
+        int2 r = nrange[i];
+        unsigned ic = intbeg[i + r.y - r.x] - intbeg[i];
+        unsigned ec = extbeg[r.y + 1] - extbeg[r.x] + 1u;
+        snap[i] = __double2float_rn(__ddiv_rn(__dmul_rn(1.0, (double)ic), (double)ec));
+    }
+}
+
+__global__ void k_fill_i32(int n, int *p, int v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+// checkFrontQuality (BvttFrontGenerateKernels.cu:34-49): a subtree whose
+// internal/external front ratio grew past snapshot + 1 - 0.7 * share is
+// marked (+1/-1 range markers in DFS order and the shallowest root per
+// leftmost leaf).  Double precision, IEEE operations, as the reference.
+__global__ void k_check_quality(int nint, const int2 *__restrict__ nrange,
+                                const unsigned *__restrict__ intbeg, const unsigned *__restrict__ extbeg,
+                                const float *__restrict__ snap, int *intrange, int *rtroot) {
+    const unsigned total = intbeg[nint];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nint; i += gridDim.x * blockDim.x) {
+        int2 r = nrange[i];
+        int ic = (int)(intbeg[i + r.y - r.x] - intbeg[i]);
+        int ec = (int)(extbeg[r.y + 1] - extbeg[r.x]);
+        double lhs = __ddiv_rn((double)ic, (double)ec);
+        double rhs = __dsub_rn(__dadd_rn((double)snap[i], 1.0), __ddiv_rn(__dmul_rn(0.7, (double)ic), (double)total));
+        if (lhs > rhs) {
+            atomicAdd(intrange + i, 1);
+            atomicAdd(intrange + i + r.y - r.x, -1);
+            atomicMin(rtroot + r.x, i);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- narrow phase
+// FP32 17-axis separating-axis test (Gottschalk's triangle SAT as
+// gProximity's triangleIntersection2 applies it,
+// Source/Externals/inc/gProximity/cuda_intersect_tritri.h:247-266,349-433):
+// translate by P1, face normals, nine edge x edge axes, six in-plane edge
+// normals; intervals strictly apart separate.  Explicit round-to-nearest
+// intrinsics keep the compiler from contracting into FMAs, so the result is
+// bit-identical to the same sequence evaluated on the CPU.
+struct v3 { float x, y, z; };
+__device__ __forceinline__ v3 vsub(v3 a, v3 b) { return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)}; }
+__device__ __forceinline__ v3 vcross(v3 a, v3 b) {
+    return {__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
+            __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
+}
+__device__ __forceinline__ float vdot(v3 a, v3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ bool axis_overlap(v3 ax, v3 p2, v3 p3, v3 q1, v3 q2, v3 q3) {
+    const v3 p1 = {0.f, 0.f, 0.f};
+    float P1 = vdot(ax, p1), P2 = vdot(ax, p2), P3 = vdot(ax, p3);
+    float Q1 = vdot(ax, q1), Q2 = vdot(ax, q2), Q3 = vdot(ax, q3);
+    float mx1 = fmaxf(fmaxf(P1, P2), P3), mn1 = fminf(fminf(P1, P2), P3);
+    float mx2 = fmaxf(fmaxf(Q1, Q2), Q3), mn2 = fminf(fminf(Q1, Q2), Q3);
+    return !(mn1 > mx2) && !(mn2 > mx1);
+}
+__device__ bool tritri_sat32(v3 P1, v3 P2, v3 P3, v3 Q1, v3 Q2, v3 Q3) {
+    const v3 z = {0.f, 0.f, 0.f};
+    v3 p2 = vsub(P2, P1), p3 = vsub(P3, P1);
+    v3 q1 = vsub(Q1, P1), q2 = vsub(Q2, P1), q3 = vsub(Q3, P1);
+    v3 e0 = vsub(p2, z), e1 = vsub(p3, p2), e2 = vsub(z, p3);
+    v3 f0 = vsub(q2, q1), f1 = vsub(q3, q2), f2 = vsub(q1, q3);
+    v3 n = vcross(e0, e1), m = vcross(f0, f1);
+    if (!axis_overlap(n, p2, p3, q1, q2, q3)) return false;
+    if (!axis_overlap(m, p2, p3, q1, q2, q3)) return false;
+    const v3 e[3] = {e0, e1, e2}, f[3] = {f0, f1, f2};
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            if (!axis_overlap(vcross(e[i], f[j]), p2, p3, q1, q2, q3)) return false;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+        if (!axis_overlap(vcross(e[i], n), p2, p3, q1, q2, q3)) return false;
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+        if (!axis_overlap(vcross(f[j], m), p2, p3, q1, q2, q3)) return false;
+    return true;
+}
+
+__device__ __forceinline__ v3 vload(const float *v, int i) {
+    const float *p = v + 3 * (size_t)i;
+    return {__ldg(p), __ldg(p + 1), __ldg(p + 2)};
+}
+
+// simpleNarrowPhase (Mine/collision/narrow_phase/narrow_phase.cu:8-24):
+// keeps the pairs whose triangles intersect, as original triangle ids.
+__global__ void __launch_bounds__(kThreads) k_narrow(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
+                                                     const float *__restrict__ verts, unsigned *ctr,
+                                                     unsigned cap_pairs, int2 *hits, unsigned cap_hits) {
+    const unsigned n = min(ctr[C_PAIRS], cap_pairs);
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        int2 p = pairs[q];
+        int4 a = __ldg(&sface[p.x]), b = __ldg(&sface[p.y]);
+        if (tritri_sat32(vload(verts, a.x), vload(verts, a.y), vload(verts, a.z), vload(verts, b.x),
+                         vload(verts, b.y), vload(verts, b.z)))
+            emit(hits, ctr + C_HITS, cap_hits, make_int2(a.w, b.w), ctr + C_OVERFLOW, 8u);
+    }
+}
+
+// applyCpResults (BvttFrontLooseIntra.cu:63-67): broad pairs as original ids
+__global__ void k_pairs_to_orig(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
+                                const unsigned *__restrict__ ctr, unsigned cap_pairs, int2 *out) {
+    const unsigned n = min(ctr[C_PAIRS], cap_pairs);
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        int2 p = pairs[q];
+        out[q] = make_int2(__ldg(&sface[p.x]).w, __ldg(&sface[p.y]).w);
+    }
+}
+
+__global__ void k_counts64(const unsigned *__restrict__ ctr, unsigned cap_pairs, unsigned cap_hits,
+                           int64_t *out) {
+    if (threadIdx.x == 0) {
+        out[0] = min(ctr[C_PAIRS], cap_pairs);
+        out[1] = min(ctr[C_HITS], cap_hits);
+    }
+}
+
+}  // namespace
+
+// ====================================================================== host
+Front::~Front() {
+    for (auto &set : front_)
+        for (auto &b : set) b.release();
+    DBuf *bufs[] = {&pairs_, &hits_, &outbuf_, &intcnt_, &extcnt_, &intbeg_, &extbeg_, &intback_,
+                    &extback_, &snapshot_, &scratch_, &counts64_};
+    for (DBuf *b : bufs) b->release();
+}
+
+bvhcd_status Front::init() {
+    if (cfg_.int_front_capacity <= 0 || cfg_.ext_front_capacity <= 0 || cfg_.pair_capacity <= 0)
+        return BVHCD_INVALID_ARG;
+    if (cfg_.int_front_capacity > 0x7fffffffLL || cfg_.ext_front_capacity > 0x7fffffffLL ||
+        cfg_.pair_capacity > 0x7fffffffLL)
+        return BVHCD_INVALID_ARG;
+    fcap_[0] = cfg_.int_front_capacity;
+    fcap_[1] = cfg_.ext_front_capacity;
+    pcap_ = cfg_.pair_capacity;
+    for (int set = 0; set < 2; set++)
+        for (int k = 0; k < 2; k++) FR_TRY(front_[set][k].reserve(sizeof(int2) * (size_t)fcap_[k]));
+    FR_TRY(pairs_.reserve(sizeof(int2) * (size_t)pcap_));
+    FR_TRY(hits_.reserve(sizeof(int2) * (size_t)pcap_));
+    FR_TRY(counts64_.reserve(sizeof(int64_t) * 2));
+    return ensure_node_capacity(bvh_->T() > 0 ? bvh_->T() : 1);
+}
+
+bvhcd_status Front::ensure_node_capacity(int T) {
+    if (T <= capT_) return BVHCD_OK;
+    size_t n = (size_t)T + 2;
+    FR_TRY(intcnt_.reserve(sizeof(unsigned) * n));
+    FR_TRY(extcnt_.reserve(sizeof(unsigned) * n));
+    FR_TRY(intbeg_.reserve(sizeof(unsigned) * n));
+    FR_TRY(extbeg_.reserve(sizeof(unsigned) * n));
+    FR_TRY(intback_.reserve(sizeof(unsigned) * n));
+    FR_TRY(extback_.reserve(sizeof(unsigned) * n));
+    FR_TRY(snapshot_.reserve(sizeof(float) * n));
+    FR_TRY(scratch_.reserve(scan_scratch_bytes((int64_t)n)));
+    FR_TRY(cudaMemset(intcnt_.p, 0, sizeof(unsigned) * n));
+    FR_TRY(cudaMemset(extcnt_.p, 0, sizeof(unsigned) * n));
+    FR_TRY(cudaMemset(intbeg_.p, 0, sizeof(unsigned) * n));
+    FR_TRY(cudaMemset(extbeg_.p, 0, sizeof(unsigned) * n));
+    FR_TRY(cudaMemset(intback_.p, 0, sizeof(unsigned) * n));
+    FR_TRY(cudaMemset(extback_.p, 0, sizeof(unsigned) * n));
+    FR_TRY(cudaMemset(snapshot_.p, 0, sizeof(float) * n));
+    capT_ = T;
+    return BVHCD_OK;
+}
+
+FrontLog Front::log() const {
+    FrontLog l;
+    l.intcnt = intcnt_.as<unsigned>();
+    l.extcnt = extcnt_.as<unsigned>();
+    l.intbeg = intbeg_.as<unsigned>();
+    l.extbeg = extbeg_.as<unsigned>();
+    l.intback = intback_.as<unsigned>();
+    l.extback = extback_.as<unsigned>();
+    return l;
+}
+
+static FArgs make_args(const LBvh *bvh, const FrontLog &log, int cull) {
+    Tree t = bvh->tree();
+    FArgs a;
+    a.nrec = t.nrec; a.lrec = t.lrec; a.topo = t.topo; a.lca = t.lca; a.sface = t.sface;
+    a.log = log;
+    a.ctr = bvh->counters();
+    a.in_int = a.in_ext = nullptr;
+    a.out_int = a.out_ext = nullptr;
+    a.in_int_slot = C_INT0; a.in_ext_slot = C_EXT0; a.out_int_slot = C_INT1; a.out_ext_slot = C_EXT1;
+    a.cap_int = a.cap_ext = 0;
+    a.pairs = nullptr;
+    a.cap_pairs = 0;
+    a.cull = cull;
+    a.T = t.T;
+    return a;
+}
+
+// log clear (FlOrderLog.cpp clear): counts and back counts, T+1 entries
+static cudaError_t log_clear(const FrontLog &l, int T, cudaStream_t s) {
+    size_t n = sizeof(unsigned) * (size_t)(T + 1);
+    cudaError_t e = cudaMemsetAsync(l.intcnt, 0, n, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(l.extcnt, 0, n, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(l.intback, 0, n, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(l.extback, 0, n, s);
+    return e;
+}
+
+// FlOrderLog::prepare (FlOrderLog.cu:7-12): begins from counts
+static cudaError_t log_prepare(const FrontLog &l, int T, void *scratch, cudaStream_t s) {
+    cudaError_t e = scan_u32(l.intcnt, l.intbeg, T + 1, false, nullptr, scratch, s);
+    if (e == cudaSuccess) e = scan_u32(l.extcnt, l.extbeg, T + 1, false, nullptr, scratch, s);
+    return e;
+}
+
+bvhcd_status Front::reorder(cudaStream_t s) {
+    StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_REORDER, s);
+    const int T = bvh_->T();
+    FrontLog l = log();
+    FR_TRY(log_prepare(l, T, scratch_.p, s));
+    FR_TRY(log_clear(l, T, s));
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent);
+    const int nx = 1 - cur_;
+    a.in_int = front_[nx][0].as<int2>(); a.in_ext = front_[nx][1].as<int2>();
+    a.out_int = front_[cur_][0].as<int2>(); a.out_ext = front_[cur_][1].as<int2>();
+    a.in_int_slot = 2 * nx; a.in_ext_slot = 2 * nx + 1;
+    a.out_int_slot = 2 * cur_; a.out_ext_slot = 2 * cur_ + 1;
+    a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
+    k_reorder<<<kFrontBlocks, kThreads, 0, s>>>(a); note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+// Emission into the other buffer set; the caller reorders back.
+bvhcd_status Front::generate(cudaStream_t s, bool pure) {
+    const int T = bvh_->T();
+    unsigned *ctr = bvh_->counters();
+    FrontLog l = log();
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent);
+    a.pairs = pairs_.as<int2>();
+    a.cap_pairs = (unsigned)pcap_;
+    FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
+    if (pure) {
+        StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_PURE_BVH_CD, s);
+        k_generate<false><<<grid_for(T), kThreads, 0, s>>>(a); note_launch();
+        return cuda_status(cudaGetLastError());
+    }
+    FR_TRY(log_clear(l, T, s));
+    const int nx = 1 - cur_;
+    a.out_int = front_[nx][0].as<int2>(); a.out_ext = front_[nx][1].as<int2>();
+    a.out_int_slot = 2 * nx; a.out_ext_slot = 2 * nx + 1;
+    a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
+    FR_TRY(cudaMemsetAsync(ctr + 2 * nx, 0, 2 * sizeof(unsigned), s));
+    {
+        StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_GENERATE, s);
+        k_generate<true><<<grid_for(T), kThreads, 0, s>>>(a); note_launch();
+    }
+    FR_TRY(cudaGetLastError());
+    bvhcd_status st = reorder(s);
+    if (st != BVHCD_OK) return st;
+    has_front_ = true;
+    if (bvh_->restr_enabled()) return snapshot(s);
+    return BVHCD_OK;
+}
+
+bvhcd_status Front::snapshot(cudaStream_t s) {
+    const int T = bvh_->T();
+    Tree t = bvh_->tree();
+    k_snapshot<<<grid_for(T), kThreads, 0, s>>>(T - 1, t.nrange, intbeg_.as<unsigned>(), extbeg_.as<unsigned>(),
+                                                snapshot_.as<float>()); note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+bvhcd_status Front::check_quality(cudaStream_t s) {
+    StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_QUALITY, s);
+    const int T = bvh_->T();
+    Tree t = bvh_->tree();
+    k_fill_i32<<<grid_for(T), kThreads, 0, s>>>(T, bvh_->rtroot(), INT_MAX); note_launch();
+    FR_TRY(cudaMemsetAsync(bvh_->intrange(), 0, sizeof(int) * (size_t)T, s));
+    k_check_quality<<<grid_for(T), kThreads, 0, s>>>(T - 1, t.nrange, intbeg_.as<unsigned>(),
+                                                     extbeg_.as<unsigned>(), snapshot_.as<float>(),
+                                                     bvh_->intrange(), bvh_->rtroot()); note_launch();
+    FR_TRY(cudaGetLastError());
+    bvh_->set_updated(true);
+    return BVHCD_OK;
+}
+
+// pruneSprout (BvttFrontLooseIntra.cu:254-283)
+bvhcd_status Front::prune_sprout(cudaStream_t s) {
+    const int T = bvh_->T();
+    unsigned *ctr = bvh_->counters();
+    FrontLog l = log();
+    FR_TRY(log_clear(l, T, s));
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent);
+    const int nx = 1 - cur_;
+    a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
+    a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
+    a.out_int = front_[nx][0].as<int2>(); a.out_ext = front_[nx][1].as<int2>();
+    a.out_int_slot = 2 * nx; a.out_ext_slot = 2 * nx + 1;
+    a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
+    a.pairs = pairs_.as<int2>();
+    a.cap_pairs = (unsigned)pcap_;
+    FR_TRY(cudaMemsetAsync(ctr + 2 * nx, 0, 2 * sizeof(unsigned), s));
+    FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
+    {
+        StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_UPDATE, s);
+        k_maintain_int<<<kFrontBlocks, kThreads, 0, s>>>(a); note_launch();
+        k_maintain_ext<<<kFrontBlocks, kThreads, 0, s>>>(a); note_launch();
+    }
+    FR_TRY(cudaGetLastError());
+    if (bvh_->restr_enabled()) {
+        bvhcd_status st = check_quality(s);
+        if (st != BVHCD_OK) return st;
+    }
+    return reorder(s);
+}
+
+bvhcd_status Front::keep(cudaStream_t s) {
+    StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_KEEP, s);
+    unsigned *ctr = bvh_->counters();
+    FArgs a = make_args(bvh_, log(), cfg_.cull_adjacent);
+    a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
+    a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
+    a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
+    a.pairs = pairs_.as<int2>();
+    a.cap_pairs = (unsigned)pcap_;
+    FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
+    k_keep<<<kFrontBlocks, kThreads, 0, s>>>(a); note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+// balance (BvttFrontLooseIntra.cu:285-312).  The external front stays where
+// it is; only the internal front moves to the other buffer.
+bvhcd_status Front::balance(cudaStream_t s) {
+    StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_BALANCE, s);
+    const int T = bvh_->T();
+    unsigned *ctr = bvh_->counters();
+    FrontLog l = log();
+    FR_TRY(log_prepare(l, T, scratch_.p, s));
+    FR_TRY(log_clear(l, T, s));
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent);
+    const int nx = 1 - cur_;
+    a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
+    a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
+    a.out_int = front_[nx][0].as<int2>();
+    a.out_int_slot = 2 * nx;
+    a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
+    a.pairs = pairs_.as<int2>();
+    a.cap_pairs = (unsigned)pcap_;
+    FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
+    k_balance<<<kFrontBlocks, kThreads, 0, s>>>(a); note_launch();
+    FR_TRY(cudaGetLastError());
+    // swap the internal front buffers of the two sets, keep the external one
+    std::swap(front_[0][0], front_[1][0]);
+    FR_TRY(cudaMemcpyAsync(ctr + 2 * cur_, ctr + 2 * nx, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
+    return BVHCD_OK;
+}
+
+bvhcd_status Front::narrow(cudaStream_t s) {
+    StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_NARROW, s);
+    unsigned *ctr = bvh_->counters();
+    FR_TRY(cudaMemsetAsync(ctr + C_HITS, 0, sizeof(unsigned), s));
+    k_narrow<<<kFrontBlocks, kThreads, 0, s>>>(pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
+                                               (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_); note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+bvhcd_status Front::run(bvhcd_front_op op, cudaStream_t s) {
+    switch (op) {
+    case BVHCD_FRONT_PURE_BVH_CD: return generate(s, true);
+    case BVHCD_FRONT_GENERATE: return generate(s, false);
+    case BVHCD_FRONT_UPDATE: return prune_sprout(s);
+    case BVHCD_FRONT_REORDER: return balance(s);
+    case BVHCD_FRONT_KEEP: return keep(s);
+    default: return generate(s, false);
+    }
+}
+
+bvhcd_status Front::grow_and_check(cudaStream_t s, bool *overflowed) {
+    unsigned h[C_NUM];
+    FR_TRY(cudaMemcpyAsync(h, bvh_->counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaStreamSynchronize(s));
+    *overflowed = h[C_OVERFLOW] != 0;
+    if (!*overflowed) return BVHCD_OK;
+    int64_t need_int = (int64_t)(h[C_INT0] > h[C_INT1] ? h[C_INT0] : h[C_INT1]);
+    int64_t need_ext = (int64_t)(h[C_EXT0] > h[C_EXT1] ? h[C_EXT0] : h[C_EXT1]);
+    int64_t need_pairs = (int64_t)(h[C_PAIRS] > h[C_HITS] ? h[C_PAIRS] : h[C_HITS]);
+    auto grow = [](int64_t need, int64_t cur) {
+        int64_t g = need + need / 2 + 1024;
+        if (g > 0x7fffffffLL) g = 0x7fffffffLL;
+        return g > cur ? g : cur;
+    };
+    // the current front survives in set cur_: copy it into the grown buffers
+    int64_t nic = grow(need_int, fcap_[0]), nec = grow(need_ext, fcap_[1]), npc = grow(need_pairs, pcap_);
+    for (int k = 0; k < 2; k++) {
+        int64_t nc = k == 0 ? nic : nec;
+        if (nc == fcap_[k]) continue;
+        for (int set = 0; set < 2; set++) {
+            DBuf nb;
+            FR_TRY(nb.reserve(sizeof(int2) * (size_t)nc));
+            if (set == cur_) FR_TRY(cudaMemcpyAsync(nb.p, front_[set][k].p, sizeof(int2) * (size_t)fcap_[k],
+                                                    cudaMemcpyDeviceToDevice, s));
+            FR_TRY(cudaStreamSynchronize(s));
+            front_[set][k].release();
+            front_[set][k] = nb;
+        }
+        fcap_[k] = nc;
+    }
+    if (npc != pcap_) {
+        pairs_.release();
+        hits_.release();
+        FR_TRY(pairs_.reserve(sizeof(int2) * (size_t)npc));
+        FR_TRY(hits_.reserve(sizeof(int2) * (size_t)npc));
+        pcap_ = npc;
+    }
+    FR_TRY(cudaMemsetAsync(bvh_->counters() + C_OVERFLOW, 0, sizeof(unsigned), s));
+    return BVHCD_OK;
+}
+
+// BvttFrontLooseIntra::maintain (BvttFrontLooseIntra.cu:69-126)
+bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
+    if (op < BVHCD_FRONT_PURE_BVH_CD || op > BVHCD_FRONT_RESTRUCTURE) return BVHCD_INVALID_ARG;
+    if (!bvh_->built()) return BVHCD_NOT_READY;
+    const int T = bvh_->T();
+    bvhcd_status st = ensure_node_capacity(T);
+    if (st != BVHCD_OK) return st;
+    bvh_->set_updated(false);
+    bvhcd_front_op run_op = op;
+    // front override after a BVH build or restructure (:75-110): the front
+    // is regenerated in both cases
+    if (bvh_->restr_enabled() && (bvh_->opt_tag() == 2 || bvh_->opt_tag() == 1)) run_op = BVHCD_FRONT_GENERATE;
+    if (op == BVHCD_FRONT_RESTRUCTURE) run_op = BVHCD_FRONT_GENERATE;
+    // a front operation needs a front: the first one is generated
+    if (!has_front_ && (run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER || run_op == BVHCD_FRONT_KEEP))
+        run_op = BVHCD_FRONT_GENERATE;
+    unsigned *ctr = bvh_->counters();
+    FR_TRY(cudaMemsetAsync(ctr + C_OVERFLOW, 0, sizeof(unsigned), s));
+    if (T < 2) {
+        FR_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned) * 6, s));
+        last_op_ = run_op;
+        if (run_op != BVHCD_FRONT_PURE_BVH_CD) has_front_ = true;
+        return BVHCD_OK;
+    }
+    // With auto_grow the stage is replayed after growing the buffers.  The
+    // stage's input (the tree and the front in set cur_) is intact when an
+    // emission overflows because outputs go to the other set, except for the
+    // reorder scatter, which is checked before it runs.
+    for (int attempt = 0; attempt < 4; attempt++) {
+        st = run(run_op, s);
+        if (st != BVHCD_OK) return st;
+        if (cfg_.narrow_phase) {
+            st = narrow(s);
+            if (st != BVHCD_OK) return st;
+        }
+        if (!cfg_.auto_grow) break;
+        bool ovf = false;
+        st = grow_and_check(s, &ovf);
+        if (st != BVHCD_OK) return st;
+        if (!ovf) break;
+        // an UPDATE overwrote the front; start again from a generated front
+        if (run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER) run_op = BVHCD_FRONT_GENERATE;
+    }
+    last_op_ = run_op;
+    k_counts64<<<1, 32, 0, s>>>(ctr, (unsigned)pcap_, (unsigned)pcap_, counts64_.as<int64_t>()); note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+bvhcd_status Front::stats(bvhcd_front_stats *st, cudaStream_t s) {
+    unsigned h[C_NUM];
+    FR_TRY(cudaMemcpyAsync(h, bvh_->counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaStreamSynchronize(s));
+    *st = bvhcd_front_stats{};
+    st->int_front = h[2 * cur_];
+    st->ext_front = h[2 * cur_ + 1];
+    st->broad_pairs = h[C_PAIRS];
+    st->narrow_hits = h[C_HITS];
+    st->overflow = (int32_t)h[C_OVERFLOW];
+    st->bvh_opt_tag = bvh_->opt_tag();
+    st->front_op_run = last_op_;
+    st->restr_pending = bvh_->updated() ? 1 : 0;
+    st->num_rt_subtrees = bvh_->last_rt_subtrees();
+    st->num_rt_int_nodes = bvh_->last_rt_intnodes();
+    return BVHCD_OK;
+}
+
+bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, bool out_dev,
+                          cudaStream_t s) {
+    unsigned h[C_NUM];
+    FR_TRY(cudaMemcpyAsync(h, bvh_->counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaStreamSynchronize(s));
+    int64_t n = which ? (int64_t)h[C_HITS] : (int64_t)h[C_PAIRS];
+    if (n > pcap_) n = pcap_;
+    if (count) *count = n;
+    if (!out || cap <= 0) return n > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
+    int64_t m = n < cap ? n : cap;
+    const int2 *src;
+    if (which) {
+        src = hits_.as<int2>();
+    } else {
+        FR_TRY(outbuf_.reserve(sizeof(int2) * (size_t)(pcap_ > 0 ? pcap_ : 1)));
+        k_pairs_to_orig<<<kFrontBlocks, kThreads, 0, s>>>(pairs_.as<int2>(), bvh_->tree().sface,
+                                                          bvh_->counters(), (unsigned)pcap_, outbuf_.as<int2>()); note_launch();
+        FR_TRY(cudaGetLastError());
+        src = outbuf_.as<int2>();
+    }
+    if (m > 0)
+        FR_TRY(cudaMemcpyAsync(out, src, sizeof(int2) * (size_t)m,
+                               out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaStreamSynchronize(s));
+    if (h[C_OVERFLOW] & (which ? 8u : 4u)) return BVHCD_CAPACITY_EXCEEDED;
+    return n > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
+}
+
+bvhcd_status Front::export_front(int which, int32_t *out, int64_t cap, int64_t *count, cudaStream_t s) {
+    if (which < 0 || which > 1) return BVHCD_INVALID_ARG;
+    unsigned h[C_NUM];
+    FR_TRY(cudaMemcpyAsync(h, bvh_->counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaStreamSynchronize(s));
+    int64_t n = h[2 * cur_ + which];
+    if (n > fcap_[which]) n = fcap_[which];
+    if (count) *count = n;
+    int64_t m = n < cap ? n : cap;
+    if (out && m > 0) {
+        FR_TRY(cudaMemcpyAsync(out, front_[cur_][which].p, sizeof(int2) * (size_t)m, cudaMemcpyDeviceToHost, s));
+        FR_TRY(cudaStreamSynchronize(s));
+    }
+    return n > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
+}
+
+bvhcd_status Front::device_results(const int32_t **hits, const int64_t **counts) {
+    if (hits) *hits = hits_.as<int32_t>();
+    if (counts) *counts = counts64_.as<int64_t>();
+    return BVHCD_OK;
+}
+
+}  // namespace bvhcd

@@ -1,0 +1,883 @@
+// lbvh.cu -- LBVH build, refit and quality-triggered subtree restructuring.
+//
+// Build follows the reference's construction rule (Apetrei-style bottom-up
+// climb; a node covering leaves (l, r] is the right child of split l when
+// metric[l] < metric[r], else the left child of split r;
+// Mine/collision/lbvh/LBvhBuildKernels.cu:135-172) so the topology, the DFS
+// numbering and the escape links are the reference's.  The DFS ids are
+// computed without the reference's sequential chain walk
+// (calcIntNodeOrders, :174-185): every node records its distance from the
+// bottom of its left chain during the climb, the chain top records the chain
+// length, and one scan over chain lengths gives every id in parallel.
+#include <climits>
+#include <cstdio>
+#include <cstring>
+
+#include "pipeline.h"
+#include "prims.cuh"
+
+namespace bvhcd {
+
+bvhcd_status cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return BVHCD_OK;
+    if (e == cudaErrorMemoryAllocation) return BVHCD_OUT_OF_MEMORY;
+    return BVHCD_CUDA_ERROR;
+}
+
+#define BV_TRY(x)                                  \
+    do {                                           \
+        cudaError_t e__ = (x);                     \
+        if (e__ != cudaSuccess) return cuda_status(e__); \
+    } while (0)
+
+namespace {
+
+constexpr int kThreads = 256;
+inline unsigned grid_for(int64_t n, int per = kThreads) {
+    int64_t g = (n + per - 1) / per;
+    if (g < 1) g = 1;
+    if (g > 65535LL * 64) g = 65535LL * 64;
+    return (unsigned)g;
+}
+
+__device__ __forceinline__ int split_metric(unsigned a, unsigned b) {
+    return 32 - __clz(a ^ b);  // __clz(0) == 32 -> 0
+}
+
+// ---------------------------------------------------------------- scene box
+__global__ void __launch_bounds__(kThreads) k_box_partial(int T, const int *__restrict__ faces,
+                                                          const float *__restrict__ verts,
+                                                          float *partial) {
+    float mn[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+    float mx[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+        float3 a = load_vert(verts, __ldg(faces + 3 * (size_t)t));
+        float3 b = load_vert(verts, __ldg(faces + 3 * (size_t)t + 1));
+        float3 c = load_vert(verts, __ldg(faces + 3 * (size_t)t + 2));
+        float4 lo, hi;
+        tri_box(a, b, c, lo, hi);
+        mn[0] = fminf(mn[0], lo.x); mn[1] = fminf(mn[1], lo.y); mn[2] = fminf(mn[2], lo.z);
+        mx[0] = fmaxf(mx[0], hi.x); mx[1] = fmaxf(mx[1], hi.y); mx[2] = fmaxf(mx[2], hi.z);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+            mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+        }
+    __shared__ float s[kThreads / 32][6];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+        for (int k = 0; k < 3; k++) { s[w][k] = mn[k]; s[w][3 + k] = mx[k]; }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        float v = s[0][threadIdx.x];
+        for (int q = 1; q < kThreads / 32; q++)
+            v = threadIdx.x < 3 ? fminf(v, s[q][threadIdx.x]) : fmaxf(v, s[q][threadIdx.x]);
+        partial[6 * blockIdx.x + threadIdx.x] = v;
+    }
+}
+
+__global__ void k_box_final(int n, const float *partial, float *scene) {
+    if (threadIdx.x < 6) {
+        float v = threadIdx.x < 3 ? 3.402823466e+38f : -3.402823466e+38f;
+        for (int q = 0; q < n; q++)
+            v = threadIdx.x < 3 ? fminf(v, partial[6 * q + threadIdx.x])
+                                : fmaxf(v, partial[6 * q + threadIdx.x]);
+        scene[threadIdx.x] = v;
+    }
+}
+
+// ---------------------------------------------------------------- build
+__global__ void k_morton(int T, const int *__restrict__ faces, const float *__restrict__ verts,
+                         const float *__restrict__ scene, unsigned *keys, int *vals) {
+    __shared__ float s[6];
+    if (threadIdx.x < 6) s[threadIdx.x] = scene[threadIdx.x];
+    __syncthreads();
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+        float3 a = load_vert(verts, __ldg(faces + 3 * (size_t)t));
+        float3 b = load_vert(verts, __ldg(faces + 3 * (size_t)t + 1));
+        float3 c = load_vert(verts, __ldg(faces + 3 * (size_t)t + 2));
+        float4 lo, hi;
+        tri_box(a, b, c, lo, hi);
+        keys[t] = morton_box(lo, hi, s);
+        vals[t] = t;
+    }
+}
+
+// Morton-ordered primitives and leaves (calcInverseMapping,
+// Mine/utility/CudaKernelUtils.cu:28-32; buildPrimitives,
+// LBvhBuildKernels.cu:114-133, here storing the vertex ids too;
+// calcExtNodeSplitMetrics, Mine/collision/lbvh/BvhExtNode.cu:128-134).
+__global__ void k_leaves(int T, const unsigned *__restrict__ keys, const int *__restrict__ vals,
+                         const int *__restrict__ faces, const float *__restrict__ verts,
+                         int4 *sface, int *primmap, unsigned *code, int *metric, float4 *lrec) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) {
+        int t = vals[i];
+        int4 f = make_int4(__ldg(faces + 3 * (size_t)t), __ldg(faces + 3 * (size_t)t + 1),
+                           __ldg(faces + 3 * (size_t)t + 2), t);
+        sface[i] = f;
+        primmap[t] = i;
+        unsigned k = keys[i];
+        code[i] = k;
+        metric[i] = (i != T - 1) ? split_metric(k, keys[i + 1]) : 33;
+        float4 lo, hi;
+        tri_box(load_vert(verts, f.x), load_vert(verts, f.y), load_vert(verts, f.z), lo, hi);
+        lrec[2 * i] = lo;
+        lrec[2 * i + 1] = hi;
+    }
+}
+
+__global__ void k_single_leaf(int *lca, float4 *lrec) {
+    if (threadIdx.x == 0) {
+        lca[0] = 1;
+        lca[1] = -1;
+        lrec[0].w = __int_as_float(-1);
+        lrec[1].w = __int_as_float(-1);
+    }
+}
+
+__global__ void k_metrics(int T,const unsigned *__restrict__ code, int *metric) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x)
+        metric[i] = (i != T - 1) ? split_metric(code[i], code[i + 1]) : 33;
+}
+
+struct Climb {
+    int *ulc, *urc, *upar, *urx, *ury;
+    unsigned *umark;
+    float4 *ubox;
+    unsigned *uflag;
+    int *posb, *clen, *ulpar;
+};
+
+// Bottom-up construction (buildIntNodes, LBvhBuildKernels.cu:135-172; with
+// kSeg the confined rebuild of restrIntNodes,
+// Mine/collision/lbvh/LBvhRestructureKernels.cu:122-166).  Internal nodes are
+// indexed by split.  The second thread to reach a node merges the child
+// boxes, records posb = distance from the bottom of its left chain and, at a
+// chain top, the chain length of the chain's leftmost leaf.
+template <bool kSeg>
+__global__ void __launch_bounds__(kThreads) k_climb(int T, int n, const int *__restrict__ leaves,
+                                                    const int *__restrict__ seg,
+                                                    const int *__restrict__ metric,
+                                                    const float4 *__restrict__ lrec,
+                                                    const int4 *__restrict__ prev_topo, Climb c) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int idx = kSeg ? leaves[k] : k;
+        const int sub = kSeg ? seg[idx] : 0;
+        int l = idx - 1, r = idx, bd = 0;
+        bool mark;
+        if (kSeg) bd = ((l < 0 || seg[l] != sub) ? 2 : 0) | ((r == T - 1 || seg[r + 1] != sub) ? 1 : 0);
+        if (bd) mark = bd & 1;
+        else mark = (l >= 0) && (metric[l] < metric[r]);
+        int cur = mark ? l : r;
+        c.ulpar[idx] = cur;
+        if (mark) {
+            c.urc[cur] = idx;
+            c.ury[cur] = idx;
+            c.clen[idx] = 0;
+            __threadfence();
+            atomicOr(&c.umark[cur], 2u);
+        } else {
+            c.ulc[cur] = idx;
+            c.urx[cur] = idx;
+            __threadfence();
+            atomicOr(&c.umark[cur], 1u);
+        }
+        __threadfence();
+        while (atomicAdd(&c.uflag[cur], 1u) == 1u) {
+            __threadfence();
+            const unsigned m = __ldcg(&c.umark[cur]) & 3u;
+            const int lc = __ldcg(&c.ulc[cur]), rc = __ldcg(&c.urc[cur]);
+            const int rx = __ldcg(&c.urx[cur]), ry = __ldcg(&c.ury[cur]);
+            float4 alo, ahi, blo, bhi;
+            if (m & 1u) { alo = __ldcg(&lrec[2 * lc]); ahi = __ldcg(&lrec[2 * lc + 1]); }
+            else        { alo = __ldcg(&c.ubox[2 * lc]); ahi = __ldcg(&c.ubox[2 * lc + 1]); }
+            if (m & 2u) { blo = __ldcg(&lrec[2 * rc]); bhi = __ldcg(&lrec[2 * rc + 1]); }
+            else        { blo = __ldcg(&c.ubox[2 * rc]); bhi = __ldcg(&c.ubox[2 * rc + 1]); }
+            c.ubox[2 * cur] = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.f);
+            c.ubox[2 * cur + 1] = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.f);
+            const int pb = (m & 1u) ? 0 : __ldcg(&c.posb[lc]) + 1;
+            c.posb[cur] = pb;
+            l = rx - 1;
+            r = ry;
+            if (kSeg) bd = ((l < 0 || seg[l] != sub) ? 2 : 0) | ((r == T - 1 || seg[r + 1] != sub) ? 1 : 0);
+            const bool is_root = kSeg ? (bd == 3) : (l + 1 == 0 && r == T - 1);
+            if (is_root) {
+                c.upar[cur] = -1;
+                const bool right = kSeg ? ((prev_topo[sub].w & 4) != 0) : false;
+                c.umark[cur] = m | (right ? 4u : 0u);
+                c.clen[rx] = pb + 1;
+                break;
+            }
+            if (bd) mark = bd & 1;
+            else mark = (l >= 0) && (metric[l] < metric[r]);
+            const int par = mark ? l : r;
+            c.upar[cur] = par;
+            if (mark) {
+                c.urc[par] = cur;
+                c.ury[par] = r;
+                c.umark[cur] = m | 4u;
+                c.clen[rx] = pb + 1;
+                __threadfence();
+                atomicAnd(&c.umark[par], ~2u);
+            } else {
+                c.ulc[par] = cur;
+                c.urx[par] = l + 1;
+                c.umark[cur] = m;
+                __threadfence();
+                atomicAnd(&c.umark[par], ~1u);
+            }
+            __threadfence();
+            cur = par;
+        }
+    }
+}
+
+// DFS id of every internal node: chain offset of its leftmost leaf plus its
+// position from the chain top (calcIntNodeOrders, LBvhBuildKernels.cu:174-185).
+__global__ void k_dfs_ids(int nint, const int *__restrict__ urx, const int *__restrict__ posb,
+                          const unsigned *__restrict__ coff, const int *__restrict__ clen, int *dfs) {
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nint; u += gridDim.x * blockDim.x) {
+        int rx = urx[u];
+        dfs[u] = (int)coff[rx] + clen[rx] - 1 - posb[u];
+    }
+}
+
+__device__ __forceinline__ int lca_of(int s, int T, const unsigned *coff, const int *clen) {
+    if (s >= T) return -1;
+    return clen[s] > 0 ? (int)(coff[s] << 1) : ((s << 1) | 1);
+}
+
+// Escape links and leaf parents (updateBvhExtNodeLinks, LBvhBuildKernels.cu:187-200).
+__global__ void k_leaf_links(int T, const unsigned *__restrict__ coff, const int *__restrict__ clen,
+                             const int *__restrict__ ulpar, const int *__restrict__ dfs, int *lca,
+                             float4 *lrec) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x) {
+        lca[s] = lca_of(s, T, coff, clen);
+        if (s == 0) lca[T] = -1;
+        reinterpret_cast<float *>(lrec)[8 * (size_t)s + 3] = __int_as_float(dfs[ulpar[s]]);
+        reinterpret_cast<float *>(lrec)[8 * (size_t)s + 7] = __int_as_float(lca_of(s + 1, T, coff, clen));
+    }
+}
+
+// Internal nodes in DFS order (reorderIntNode, LBvhBuildKernels.cu:202-217).
+__global__ void k_write_nodes(int nint, int T, Climb c, const int *__restrict__ dfs,
+                              const unsigned *__restrict__ coff, const int *__restrict__ clen,
+                              float4 *nrec, int4 *topo, int2 *nrange) {
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nint; u += gridDim.x * blockDim.x) {
+        int d = dfs[u];
+        unsigned m = c.umark[u];
+        int lc = c.ulc[u], rc = c.urc[u], p = c.upar[u];
+        int rx = c.urx[u], ry = c.ury[u];
+        topo[d] = make_int4((m & 1u) ? lc : dfs[lc], (m & 2u) ? rc : dfs[rc], p < 0 ? -1 : dfs[p], (int)m);
+        nrange[d] = make_int2(rx, ry);
+        float4 lo = c.ubox[2 * u], hi = c.ubox[2 * u + 1];
+        lo.w = __int_as_float(rx);
+        hi.w = __int_as_float(lca_of(ry + 1, T, coff, clen));
+        nrec[2 * d] = lo;
+        nrec[2 * d + 1] = hi;
+    }
+}
+
+// ---------------------------------------------------------------- refit
+// refitExtNode (Mine/collision/lbvh/LBvhUpdateKernels.cu:35-61), by slot.
+__global__ void __launch_bounds__(kThreads) k_refit_leaves(int T, const int4 *__restrict__ sface,
+                                                           const float *__restrict__ verts,
+                                                           float4 *lrec) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x) {
+        int4 f = __ldg(&sface[s]);
+        float4 lo, hi;
+        tri_box(load_vert(verts, f.x), load_vert(verts, f.y), load_vert(verts, f.z), lo, hi);
+        float *p = reinterpret_cast<float *>(lrec + 2 * (size_t)s);
+        p[0] = lo.x; p[1] = lo.y; p[2] = lo.z;
+        p[4] = hi.x; p[5] = hi.y; p[6] = hi.z;
+    }
+}
+
+// refitIntNode (LBvhUpdateKernels.cu:63-74).  Each internal node receives
+// two arrivals per refit, so the flag's parity tells the second arrival
+// without clearing the flags between refits.
+__global__ void __launch_bounds__(kThreads) k_refit_internal(int T, const float4 *__restrict__ lrec,
+                                                             float4 *nrec, const int4 *__restrict__ topo,
+                                                             unsigned *flag) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x) {
+        int p = __float_as_int(__ldg(reinterpret_cast<const float *>(lrec) + 8 * (size_t)s + 3));
+        while (p >= 0) {
+            __threadfence();
+            if ((atomicAdd(&flag[p], 1u) & 1u) == 0u) break;
+            __threadfence();
+            int4 t = __ldg(&topo[p]);
+            float4 alo, ahi, blo, bhi;
+            if (t.w & 1) { alo = __ldg(&lrec[2 * t.x]); ahi = __ldg(&lrec[2 * t.x + 1]); }
+            else         { alo = __ldcg(&nrec[2 * t.x]); ahi = __ldcg(&nrec[2 * t.x + 1]); }
+            if (t.w & 2) { blo = __ldg(&lrec[2 * t.y]); bhi = __ldg(&lrec[2 * t.y + 1]); }
+            else         { blo = __ldcg(&nrec[2 * t.y]); bhi = __ldcg(&nrec[2 * t.y + 1]); }
+            float *q = reinterpret_cast<float *>(nrec + 2 * (size_t)p);
+            q[0] = fminf(alo.x, blo.x); q[1] = fminf(alo.y, blo.y); q[2] = fminf(alo.z, blo.z);
+            q[4] = fmaxf(ahi.x, bhi.x); q[5] = fmaxf(ahi.y, bhi.y); q[6] = fmaxf(ahi.z, bhi.z);
+            p = t.z;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- restructure
+// calibrateLeafRangeMarks (LBvhRestructureKernels.cu:9-17)
+__global__ void k_rs_leaf_marks(int T, const int *__restrict__ rtroot, const int *__restrict__ intmark,
+                                const int2 *__restrict__ nrange, int *extrange) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) {
+        int rt = rtroot[i];
+        if (rt != INT_MAX && intmark[rt] == 1) {
+            atomicAdd(extrange + i, 1);
+            atomicAdd(extrange + nrange[rt].y + 1, -1);
+        }
+    }
+}
+// calibrateRestrRoots (:19-35)
+__global__ void k_rs_roots(int T, const int *__restrict__ rtroot, const int *__restrict__ intmark,
+                           const int2 *__restrict__ nrange, int *rootmark, unsigned *ctr) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) {
+        int rt = rtroot[i];
+        if (rt != INT_MAX && intmark[rt] == 1) {
+            int2 rg = nrange[rt];
+            atomicAdd(rootmark + i, rt);
+            atomicAdd(rootmark + rg.y + 1, -rt);
+            atomicAdd(ctr + C_RT_INTNODES, (unsigned)(rg.y - rg.x));
+            atomicAdd(ctr + C_RT_SUBTREES, 1u);
+        }
+    }
+}
+__global__ void k_rs_flags(int T, const int *__restrict__ leafroot, unsigned *flag) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x)
+        flag[s] = leafroot[s] > 0 ? 1u : 0u;
+}
+// calcRestrMCs + selectPrimitives (:37-66): (subtree root, Morton) keys
+__global__ void k_rs_select(int T, const int *__restrict__ leafroot, const unsigned *__restrict__ pos,
+                            const int4 *__restrict__ sface, const float *__restrict__ verts,
+                            const float *__restrict__ scene, unsigned long long *keys, int *task,
+                            int *vals) {
+    __shared__ float sc[6];
+    if (threadIdx.x < 6) sc[threadIdx.x] = scene[threadIdx.x];
+    __syncthreads();
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x) {
+        int rt = leafroot[s];
+        if (rt > 0) {
+            int4 f = sface[s];
+            float4 lo, hi;
+            tri_box(load_vert(verts, f.x), load_vert(verts, f.y), load_vert(verts, f.z), lo, hi);
+            unsigned q = pos[s];
+            keys[q] = ((unsigned long long)(unsigned)rt << 32) | morton_box(lo, hi, sc);
+            task[q] = s;
+            vals[q] = s;
+        }
+    }
+}
+// updatePrimMap (:68-77), applying the sort permutation: slot task[k]
+// receives the primitive that sorts k-th inside its subtree.
+__global__ void k_rs_gather(int nr, const int *__restrict__ sorted, const int4 *__restrict__ sface,
+                            int4 *tmp) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nr; k += gridDim.x * blockDim.x)
+        tmp[k] = sface[sorted[k]];
+}
+__global__ void k_rs_scatter(int nr, const int *__restrict__ task, const int4 *__restrict__ tmp,
+                             const unsigned long long *__restrict__ keys, int4 *sface, int *primmap,
+                             unsigned *code) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nr; k += gridDim.x * blockDim.x) {
+        int s = task[k];
+        int4 f = tmp[k];
+        sface[s] = f;
+        primmap[f.w] = s;
+        code[s] = (unsigned)(keys[k] & 0xffffffffull);
+    }
+}
+// calcRestrIntNodeOrders (:168-195), ids part: DFS ids inside each subtree slot
+__global__ void k_rs_dfs(int nr, int T, const int *__restrict__ task, const int *__restrict__ leafroot,
+                         const int2 *__restrict__ nrange, const unsigned *__restrict__ coff,
+                         const int *__restrict__ clen, const int *__restrict__ posb,
+                         const int *__restrict__ urx, int *dfs) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nr; k += gridDim.x * blockDim.x) {
+        int s = task[k];
+        int root = leafroot[s];
+        if (s + 1 < T && leafroot[s + 1] == root) {
+            int rxr = nrange[root].x, rx = urx[s];
+            dfs[s] = root + (int)(coff[rx] - coff[rxr]) + clen[rx] - 1 - posb[s];
+        }
+    }
+}
+// calcRestrIntNodeOrders, link part: new escape links inside the subtrees.
+// The subtree root keeps its DFS id; when it is a left child the chain of
+// its leftmost leaf continues above it, so that leaf's link is unchanged.
+__global__ void k_rs_lca(int nr, const int *__restrict__ task, const int *__restrict__ leafroot,
+                         const int2 *__restrict__ nrange, const int4 *__restrict__ topo,
+                         const unsigned *__restrict__ coff, const int *__restrict__ clen, int *lca) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nr; k += gridDim.x * blockDim.x) {
+        int s = task[k];
+        int root = leafroot[s];
+        int rxr = nrange[root].x;
+        if (clen[s] > 0) {
+            bool keep = (s == rxr) && !(topo[root].w & 4);
+            if (!keep) lca[s] = (root + (int)(coff[s] - coff[rxr])) << 1;
+        } else {
+            lca[s] = (s << 1) | 1;
+        }
+    }
+}
+// reorderRestrIntNodes (:197-215) and the leaf links of restructured leaves
+__global__ void k_rs_write(int nr, int T, const int *__restrict__ task, const int *__restrict__ leafroot,
+                           Climb c, const int *__restrict__ dfs, const int *__restrict__ lca,
+                           float4 *nrec, int4 *topo, int2 *nrange, float4 *lrec) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nr; k += gridDim.x * blockDim.x) {
+        int s = task[k];
+        reinterpret_cast<float *>(lrec)[8 * (size_t)s + 3] = __int_as_float(dfs[c.ulpar[s]]);
+        reinterpret_cast<float *>(lrec)[8 * (size_t)s + 7] = __int_as_float(lca[s + 1]);
+        if (s + 1 < T && leafroot[s + 1] == leafroot[s]) {
+            int u = s, d = dfs[u];
+            unsigned m = c.umark[u];
+            int lc = c.ulc[u], rc = c.urc[u], p = c.upar[u];
+            int rx = c.urx[u], ry = c.ury[u];
+            int par = p < 0 ? topo[d].z : dfs[p];
+            topo[d] = make_int4((m & 1u) ? lc : dfs[lc], (m & 2u) ? rc : dfs[rc], par, (int)m);
+            nrange[d] = make_int2(rx, ry);
+            float4 lo = c.ubox[2 * u], hi = c.ubox[2 * u + 1];
+            lo.w = __int_as_float(rx);
+            hi.w = __int_as_float(lca[ry + 1]);
+            nrec[2 * d] = lo;
+            nrec[2 * d + 1] = hi;
+        }
+    }
+}
+
+// checkFrontQuality's marking step (BvttFrontGenerateKernels.cu:45-47) for
+// subtrees chosen by the caller
+__global__ void k_mark_roots(int n, int nint, const int *__restrict__ roots, const int2 *__restrict__ nrange,
+                             int *intrange, int *rtroot) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int i = roots[k];
+        if (i < 0 || i >= nint) continue;
+        int2 r = nrange[i];
+        atomicAdd(intrange + i, 1);
+        atomicAdd(intrange + i + r.y - r.x, -1);
+        atomicMin(rtroot + r.x, i);
+    }
+}
+__global__ void k_fill(int n, int *p, int v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+// Export helpers
+__global__ void k_export(int T, const float4 *__restrict__ nrec, const int4 *__restrict__ topo,
+                         const int2 *__restrict__ nrange, const float4 *__restrict__ lrec,
+                         const int4 *__restrict__ sface, const int *__restrict__ lca,
+                         int *inode, float *ibox, int *leaf, float *lbox) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) {
+        if (i < T - 1) {
+            int4 t = topo[i];
+            int2 r = nrange[i];
+            inode[6 * i + 0] = t.x; inode[6 * i + 1] = t.y; inode[6 * i + 2] = t.z;
+            inode[6 * i + 3] = t.w; inode[6 * i + 4] = r.x; inode[6 * i + 5] = r.y;
+            float4 lo = nrec[2 * i], hi = nrec[2 * i + 1];
+            ibox[6 * i + 0] = lo.x; ibox[6 * i + 1] = lo.y; ibox[6 * i + 2] = lo.z;
+            ibox[6 * i + 3] = hi.x; ibox[6 * i + 4] = hi.y; ibox[6 * i + 5] = hi.z;
+        }
+        float4 lo = lrec[2 * i], hi = lrec[2 * i + 1];
+        int l = lca[i];
+        leaf[4 * i + 0] = sface[i].w;
+        leaf[4 * i + 1] = __float_as_int(lo.w);
+        leaf[4 * i + 2] = (l & 1) ? 7 : 3;
+        leaf[4 * i + 3] = l;
+        lbox[6 * i + 0] = lo.x; lbox[6 * i + 1] = lo.y; lbox[6 * i + 2] = lo.z;
+        lbox[6 * i + 3] = hi.x; lbox[6 * i + 4] = hi.y; lbox[6 * i + 5] = hi.z;
+    }
+}
+
+}  // namespace
+
+// ====================================================================== host
+Profiler::~Profiler() {
+    for (auto &p : pending_) { pool_.push_back(p.a); pool_.push_back(p.b); }
+    for (cudaEvent_t e : open_) if (e) pool_.push_back(e);
+    for (cudaEvent_t e : pool_) cudaEventDestroy(e);
+}
+
+cudaEvent_t Profiler::get() {
+    if (!pool_.empty()) {
+        cudaEvent_t e = pool_.back();
+        pool_.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void Profiler::begin(int stage, cudaStream_t s) {
+    if (open_[stage]) pool_.push_back(open_[stage]);
+    open_[stage] = get();
+    cudaEventRecord(open_[stage], s);
+}
+
+void Profiler::end(int stage, cudaStream_t s) {
+    if (!open_[stage]) return;
+    cudaEvent_t b = get();
+    cudaEventRecord(b, s);
+    pending_.push_back({stage, open_[stage], b});
+    open_[stage] = nullptr;
+}
+
+bvhcd_status Profiler::read(double *ms, int64_t *calls, bool reset) {
+    for (auto &p : pending_) {
+        cudaError_t e = cudaEventSynchronize(p.b);
+        if (e != cudaSuccess) return cuda_status(e);
+        float t = 0.f;
+        e = cudaEventElapsedTime(&t, p.a, p.b);
+        if (e != cudaSuccess) return cuda_status(e);
+        ms_[p.stage] += t;
+        calls_[p.stage] += 1;
+        pool_.push_back(p.a);
+        pool_.push_back(p.b);
+    }
+    pending_.clear();
+    for (int i = 0; i < BVHCD_STAGE_COUNT; i++) {
+        if (ms) ms[i] = ms_[i];
+        if (calls) calls[i] = calls_[i];
+        if (reset) { ms_[i] = 0; calls_[i] = 0; }
+    }
+    return BVHCD_OK;
+}
+
+LBvh::~LBvh() {
+    DBuf *bufs[] = {&verts_, &faces_, &nrec_, &lrec_, &topo_, &nrange_, &lca_, &sface_, &primmap_,
+                    &code_, &refit_flag_, &keys_, &vals_, &keys2_, &vals2_, &k64_, &k64b_, &metric_,
+                    &ulc_, &urc_, &upar_, &urx_, &ury_, &umark_, &ubox_, &uflag_, &posb_, &clen_,
+                    &coff_, &dfs_, &ulpar_, &scene_, &partial_, &scratch_, &task_, &tmpface_,
+                    &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &flagbuf_,
+                    &ctr_};
+    for (DBuf *b : bufs) b->release();
+    if (h_ctr_) cudaFreeHost(h_ctr_);
+}
+
+bvhcd_status LBvh::init() {
+    if (cfg_.prim_capacity < 0 || cfg_.vert_capacity < 0) return BVHCD_INVALID_ARG;
+    BV_TRY(ctr_.reserve(sizeof(unsigned) * C_NUM));
+    BV_TRY(cudaMemset(ctr_.p, 0, sizeof(unsigned) * C_NUM));
+    BV_TRY(scene_.reserve(64));
+    BV_TRY(cudaMallocHost(&h_ctr_, sizeof(unsigned) * C_NUM));
+    int T = cfg_.prim_capacity > 0 ? cfg_.prim_capacity : 1;
+    int V = cfg_.vert_capacity > 0 ? cfg_.vert_capacity : 3 * T;
+    return ensure_capacity(T, V);
+}
+
+bvhcd_status LBvh::ensure_capacity(int T, int V) {
+    if (V > capV_) {
+        BV_TRY(verts_.reserve(sizeof(float) * 3 * (size_t)V));
+        capV_ = V;
+    }
+    if (T <= capT_) return BVHCD_OK;
+    size_t n = (size_t)T + 2;
+    BV_TRY(faces_.reserve(sizeof(int) * 3 * n));
+    BV_TRY(nrec_.reserve(sizeof(float4) * 2 * n));
+    BV_TRY(lrec_.reserve(sizeof(float4) * 2 * n));
+    BV_TRY(topo_.reserve(sizeof(int4) * n));
+    BV_TRY(nrange_.reserve(sizeof(int2) * n));
+    BV_TRY(lca_.reserve(sizeof(int) * (n + 1)));
+    BV_TRY(sface_.reserve(sizeof(int4) * n));
+    BV_TRY(primmap_.reserve(sizeof(int) * n));
+    BV_TRY(code_.reserve(sizeof(unsigned) * n));
+    BV_TRY(refit_flag_.reserve(sizeof(unsigned) * n));
+    BV_TRY(keys_.reserve(sizeof(unsigned) * n));
+    BV_TRY(vals_.reserve(sizeof(int) * n));
+    BV_TRY(keys2_.reserve(sizeof(unsigned) * n));
+    BV_TRY(vals2_.reserve(sizeof(int) * n));
+    BV_TRY(k64_.reserve(sizeof(unsigned long long) * n));
+    BV_TRY(k64b_.reserve(sizeof(unsigned long long) * n));
+    BV_TRY(metric_.reserve(sizeof(int) * n));
+    BV_TRY(ulc_.reserve(sizeof(int) * n));
+    BV_TRY(urc_.reserve(sizeof(int) * n));
+    BV_TRY(upar_.reserve(sizeof(int) * n));
+    BV_TRY(urx_.reserve(sizeof(int) * n));
+    BV_TRY(ury_.reserve(sizeof(int) * n));
+    BV_TRY(umark_.reserve(sizeof(unsigned) * n));
+    BV_TRY(ubox_.reserve(sizeof(float4) * 2 * n));
+    BV_TRY(uflag_.reserve(sizeof(unsigned) * n));
+    BV_TRY(posb_.reserve(sizeof(int) * n));
+    BV_TRY(clen_.reserve(sizeof(int) * (n + 1)));
+    BV_TRY(coff_.reserve(sizeof(unsigned) * (n + 1)));
+    BV_TRY(dfs_.reserve(sizeof(int) * n));
+    BV_TRY(ulpar_.reserve(sizeof(int) * n));
+    BV_TRY(partial_.reserve(sizeof(float) * 6 * 4096));
+    size_t scr = sort_scratch_bytes((int64_t)n);
+    size_t scr2 = scan_scratch_bytes((int64_t)n + 1);
+    BV_TRY(scratch_.reserve(scr > scr2 ? scr : scr2));
+    BV_TRY(task_.reserve(sizeof(int) * n));
+    BV_TRY(tmpface_.reserve(sizeof(int4) * n));
+    BV_TRY(intrange_.reserve(sizeof(int) * (n + 1)));
+    BV_TRY(rtroot_.reserve(sizeof(int) * (n + 1)));
+    BV_TRY(intmark_.reserve(sizeof(int) * (n + 1)));
+    BV_TRY(extrange_.reserve(sizeof(int) * (n + 1)));
+    BV_TRY(extmark_.reserve(sizeof(int) * (n + 1)));
+    BV_TRY(leafroot_.reserve(sizeof(int) * (n + 1)));
+    BV_TRY(flagbuf_.reserve(sizeof(unsigned) * (n + 1)));
+    capT_ = T;
+    return BVHCD_OK;
+}
+
+Tree LBvh::tree() const {
+    Tree t;
+    t.nrec = nrec_.as<float4>();
+    t.lrec = lrec_.as<float4>();
+    t.topo = topo_.as<int4>();
+    t.nrange = nrange_.as<int2>();
+    t.lca = lca_.as<int>();
+    t.sface = sface_.as<int4>();
+    t.primmap = primmap_.as<int>();
+    t.code = code_.as<unsigned>();
+    t.T = T_;
+    return t;
+}
+
+bvhcd_status LBvh::upload(const bvhcd_scene &sc, cudaStream_t s) {
+    if (sc.num_faces < 0 || sc.num_vertices < 0) return BVHCD_INVALID_ARG;
+    if (sc.num_faces > 0 && (!sc.pos || !sc.faces)) return BVHCD_INVALID_ARG;
+    bvhcd_status st = ensure_capacity(sc.num_faces, sc.num_vertices);
+    if (st != BVHCD_OK) return st;
+    if (sc.on_device) {
+        vptr_ = sc.pos;
+        fptr_ = sc.faces;
+    } else {
+        if (sc.num_vertices)
+            BV_TRY(cudaMemcpyAsync(verts_.p, sc.pos, sizeof(float) * 3 * (size_t)sc.num_vertices,
+                                   cudaMemcpyHostToDevice, s));
+        bool same = sc.faces_static && built_ && fptr_ == faces_.as<int>() && T_ == sc.num_faces;
+        if (!same && sc.num_faces)
+            BV_TRY(cudaMemcpyAsync(faces_.p, sc.faces, sizeof(int) * 3 * (size_t)sc.num_faces,
+                                   cudaMemcpyHostToDevice, s));
+        vptr_ = verts_.as<float>();
+        fptr_ = faces_.as<int>();
+    }
+    if (built_ && sc.num_faces != T_) built_ = false;
+    T_ = sc.num_faces;
+    V_ = sc.num_vertices;
+    return BVHCD_OK;
+}
+
+bvhcd_status LBvh::scene_box(cudaStream_t s) {
+    int g = (int)grid_for(T_);
+    if (g > 4096) g = 4096;
+    k_box_partial<<<g, kThreads, 0, s>>>(T_, fptr_, vptr_, partial_.as<float>()); note_launch();
+    k_box_final<<<1, 32, 0, s>>>(g, partial_.as<float>(), scene_.as<float>()); note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+static Climb make_climb(const DBuf &ulc, const DBuf &urc, const DBuf &upar, const DBuf &urx,
+                        const DBuf &ury, const DBuf &umark, const DBuf &ubox, const DBuf &uflag,
+                        const DBuf &posb, const DBuf &clen, const DBuf &ulpar) {
+    Climb c;
+    c.ulc = ulc.as<int>(); c.urc = urc.as<int>(); c.upar = upar.as<int>();
+    c.urx = urx.as<int>(); c.ury = ury.as<int>(); c.umark = umark.as<unsigned>();
+    c.ubox = ubox.as<float4>(); c.uflag = uflag.as<unsigned>(); c.posb = posb.as<int>();
+    c.clen = clen.as<int>(); c.ulpar = ulpar.as<int>();
+    return c;
+}
+
+bvhcd_status LBvh::build(cudaStream_t s) {
+    StageScope prof_scope(&prof_, BVHCD_STAGE_BVH_BUILD, s);
+    const int T = T_;
+    built_ = false;
+    if (T == 0) { built_ = true; return BVHCD_OK; }
+    bvhcd_status st = scene_box(s);
+    if (st != BVHCD_OK) return st;
+    k_morton<<<grid_for(T), kThreads, 0, s>>>(T, fptr_, vptr_, scene_.as<float>(), keys_.as<unsigned>(),
+                                              vals_.as<int>()); note_launch();
+    BV_TRY(radix_sort_u32(keys_.as<unsigned>(), vals_.as<int>(), keys2_.as<unsigned>(), vals2_.as<int>(),
+                          T, 30, scratch_.p, s));
+    k_leaves<<<grid_for(T), kThreads, 0, s>>>(T, keys_.as<unsigned>(), vals_.as<int>(), fptr_, vptr_,
+                                              sface_.as<int4>(), primmap_.as<int>(), code_.as<unsigned>(),
+                                              metric_.as<int>(), lrec_.as<float4>()); note_launch();
+    if (T == 1) {
+        // a single leaf: no internal node, lca = {leaf 0, end}, no parent
+        k_single_leaf<<<1, 32, 0, s>>>(lca_.as<int>(), lrec_.as<float4>()); note_launch();
+        BV_TRY(cudaGetLastError());
+        built_ = true;
+        return BVHCD_OK;
+    }
+    Climb c = make_climb(ulc_, urc_, upar_, urx_, ury_, umark_, ubox_, uflag_, posb_, clen_, ulpar_);
+    BV_TRY(cudaMemsetAsync(uflag_.p, 0, sizeof(unsigned) * (size_t)T, s));
+    BV_TRY(cudaMemsetAsync(clen_.as<int>() + T, 0, sizeof(int), s));
+    k_climb<false><<<grid_for(T), kThreads, 0, s>>>(T, T, nullptr, nullptr, metric_.as<int>(),
+                                                    lrec_.as<float4>(), nullptr, c); note_launch();
+    BV_TRY(scan_u32(clen_.as<unsigned>(), coff_.as<unsigned>(), T + 1, false, nullptr, scratch_.p, s));
+    k_dfs_ids<<<grid_for(T - 1), kThreads, 0, s>>>(T - 1, urx_.as<int>(), posb_.as<int>(),
+                                                   coff_.as<unsigned>(), clen_.as<int>(), dfs_.as<int>()); note_launch();
+    k_leaf_links<<<grid_for(T), kThreads, 0, s>>>(T, coff_.as<unsigned>(), clen_.as<int>(), ulpar_.as<int>(),
+                                                  dfs_.as<int>(), lca_.as<int>(), lrec_.as<float4>()); note_launch();
+    k_write_nodes<<<grid_for(T - 1), kThreads, 0, s>>>(T - 1, T, c, dfs_.as<int>(), coff_.as<unsigned>(),
+                                                       clen_.as<int>(), nrec_.as<float4>(), topo_.as<int4>(),
+                                                       nrange_.as<int2>()); note_launch();
+    BV_TRY(cudaMemsetAsync(refit_flag_.p, 0, sizeof(unsigned) * (size_t)T, s));
+    BV_TRY(cudaGetLastError());
+    built_ = true;
+    return BVHCD_OK;
+}
+
+bvhcd_status LBvh::refit(cudaStream_t s) {
+    StageScope prof_scope(&prof_, BVHCD_STAGE_BVH_REFIT, s);
+    const int T = T_;
+    if (T == 0) return BVHCD_OK;
+    k_refit_leaves<<<grid_for(T), kThreads, 0, s>>>(T, sface_.as<int4>(), vptr_, lrec_.as<float4>()); note_launch();
+    if (T >= 2)
+        k_refit_internal<<<grid_for(T), kThreads, 0, s>>>(T, lrec_.as<float4>(), nrec_.as<float4>(),
+                                                          topo_.as<int4>(), refit_flag_.as<unsigned>()); note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+// LBvhFixedDeformable::restructure (LBvhFixedDeformable.cu:210-352)
+bvhcd_status LBvh::restructure(cudaStream_t s) {
+    StageScope prof_scope(&prof_, BVHCD_STAGE_BVH_RESTRUCTURE, s);
+    const int T = T_, I = T - 1;
+    unsigned *ctr = ctr_.as<unsigned>();
+    // 1 int node marks, 2-3 leaf range marks, 4 subtree roots
+    BV_TRY(scan_i32(intrange_.as<int>(), intmark_.as<int>(), I, true, nullptr, scratch_.p, s));
+    BV_TRY(cudaMemsetAsync(extrange_.p, 0, sizeof(int) * (size_t)(T + 1), s));
+    k_rs_leaf_marks<<<grid_for(T), kThreads, 0, s>>>(T, rtroot_.as<int>(), intmark_.as<int>(),
+                                                     nrange_.as<int2>(), extrange_.as<int>()); note_launch();
+    BV_TRY(scan_i32(extrange_.as<int>(), extmark_.as<int>(), T + 1, true, nullptr, scratch_.p, s));
+    BV_TRY(cudaMemsetAsync(extrange_.p, 0, sizeof(int) * (size_t)(T + 1), s));
+    BV_TRY(cudaMemsetAsync(ctr + C_RT_SUBTREES, 0, sizeof(unsigned) * 2, s));
+    k_rs_roots<<<grid_for(T), kThreads, 0, s>>>(T, rtroot_.as<int>(), intmark_.as<int>(), nrange_.as<int2>(),
+                                                extrange_.as<int>(), ctr); note_launch();
+    BV_TRY(cudaMemcpyAsync(h_ctr_ + C_RT_SUBTREES, ctr + C_RT_SUBTREES, sizeof(unsigned) * 2,
+                           cudaMemcpyDeviceToHost, s));
+    BV_TRY(cudaStreamSynchronize(s));
+    rt_subtrees_ = (int)h_ctr_[C_RT_SUBTREES];
+    rt_intnodes_ = (int)h_ctr_[C_RT_INTNODES];
+    // the reference's thresholds (LBvhFixedDeformable.cu:245, :257)
+    if (rt_intnodes_ > (I >> 1)) {
+        bvhcd_status st = build(s);
+        opt_tag_ = 2;
+        return st;
+    }
+    if (rt_intnodes_ < (I >> 3)) {
+        opt_tag_ = 0;
+        return refit(s);
+    }
+    // 5 per-leaf subtree root
+    BV_TRY(scan_i32(extrange_.as<int>(), leafroot_.as<int>(), T + 1, true, nullptr, scratch_.p, s));
+    // 6-7 keys of the restructured primitives
+    bvhcd_status st = scene_box(s);
+    if (st != BVHCD_OK) return st;
+    unsigned *flag = flagbuf_.as<unsigned>();
+    unsigned *pos = keys2_.as<unsigned>();
+    k_rs_flags<<<grid_for(T), kThreads, 0, s>>>(T, leafroot_.as<int>(), flag); note_launch();
+    BV_TRY(scan_u32(flag, pos, T, false, ctr + C_RT_SUBTREES + 2, scratch_.p, s));
+    k_rs_select<<<grid_for(T), kThreads, 0, s>>>(T, leafroot_.as<int>(), pos, sface_.as<int4>(), vptr_,
+                                                 scene_.as<float>(), k64_.as<unsigned long long>(),
+                                                 task_.as<int>(), vals_.as<int>()); note_launch();
+    const int nr = rt_intnodes_ + rt_subtrees_;  // leaves = internal nodes + subtrees
+    int bits = 32;
+    while ((1LL << (bits - 32)) <= (long long)T && bits < 64) bits++;
+    BV_TRY(radix_sort_u64(k64_.as<unsigned long long>(), vals_.as<int>(), k64b_.as<unsigned long long>(),
+                          vals2_.as<int>(), nr, bits, scratch_.p, s));
+    // 8 permutation
+    k_rs_gather<<<grid_for(nr), kThreads, 0, s>>>(nr, vals_.as<int>(), sface_.as<int4>(), tmpface_.as<int4>()); note_launch();
+    k_rs_scatter<<<grid_for(nr), kThreads, 0, s>>>(nr, task_.as<int>(), tmpface_.as<int4>(),
+                                                   k64_.as<unsigned long long>(), sface_.as<int4>(),
+                                                   primmap_.as<int>(), code_.as<unsigned>()); note_launch();
+    // 9 boxes + refit with the old topology
+    st = refit(s);
+    if (st != BVHCD_OK) return st;
+    // 10 confined rebuild
+    k_metrics<<<grid_for(T), kThreads, 0, s>>>(T, code_.as<unsigned>(), metric_.as<int>()); note_launch();
+    Climb c = make_climb(ulc_, urc_, upar_, urx_, ury_, umark_, ubox_, uflag_, posb_, clen_, ulpar_);
+    BV_TRY(cudaMemsetAsync(uflag_.p, 0, sizeof(unsigned) * (size_t)T, s));
+    BV_TRY(cudaMemsetAsync(clen_.p, 0, sizeof(int) * (size_t)(T + 1), s));
+    k_climb<true><<<grid_for(nr), kThreads, 0, s>>>(T, nr, task_.as<int>(), leafroot_.as<int>(),
+                                                    metric_.as<int>(), lrec_.as<float4>(), topo_.as<int4>(), c); note_launch();
+    BV_TRY(scan_u32(clen_.as<unsigned>(), coff_.as<unsigned>(), T + 1, false, nullptr, scratch_.p, s));
+    k_rs_dfs<<<grid_for(nr), kThreads, 0, s>>>(nr, T, task_.as<int>(), leafroot_.as<int>(), nrange_.as<int2>(),
+                                               coff_.as<unsigned>(), clen_.as<int>(), posb_.as<int>(),
+                                               urx_.as<int>(), dfs_.as<int>()); note_launch();
+    k_rs_lca<<<grid_for(nr), kThreads, 0, s>>>(nr, task_.as<int>(), leafroot_.as<int>(), nrange_.as<int2>(),
+                                               topo_.as<int4>(), coff_.as<unsigned>(), clen_.as<int>(),
+                                               lca_.as<int>()); note_launch();
+    k_rs_write<<<grid_for(nr), kThreads, 0, s>>>(nr, T, task_.as<int>(), leafroot_.as<int>(), c, dfs_.as<int>(),
+                                                 lca_.as<int>(), nrec_.as<float4>(), topo_.as<int4>(),
+                                                 nrange_.as<int2>(), lrec_.as<float4>()); note_launch();
+    BV_TRY(cudaGetLastError());
+    opt_tag_ = 1;
+    return BVHCD_OK;
+}
+
+// LBvhFixedDeformable::maintain (LBvhFixedDeformable.cu:68-87)
+bvhcd_status LBvh::maintain(bvhcd_bvh_op op, const bvhcd_scene &scene, cudaStream_t s) {
+    if (op < BVHCD_BVH_BUILD || op > BVHCD_BVH_UPDATE) return BVHCD_INVALID_ARG;
+    int prevT = T_;
+    bool was_built = built_;
+    bvhcd_status st = upload(scene, s);
+    if (st != BVHCD_OK) return st;
+    opt_tag_ = 0;
+    if (cfg_.enable_restr && updated_ && was_built && built_ && prevT == T_ && T_ >= 2)
+        return restructure(s);
+    if (op == BVHCD_BVH_BUILD || !built_) return build(s);
+    return refit(s);  // UPDATE is refit: the reference marks updateIntNode deprecated (LBvhUpdateKernels.cu:88)
+}
+
+bvhcd_status LBvh::request_restructure(const int32_t *roots, int32_t n, cudaStream_t s) {
+    if (n < 0 || (n > 0 && !roots)) return BVHCD_INVALID_ARG;
+    if (!built_) return BVHCD_NOT_READY;
+    if (!cfg_.enable_restr || T_ < 2 || n == 0) return BVHCD_OK;
+    const int T = T_;
+    if (!updated_) {
+        k_fill<<<grid_for(T), kThreads, 0, s>>>(T, rtroot_.as<int>(), INT_MAX); note_launch();
+        BV_TRY(cudaMemsetAsync(intrange_.p, 0, sizeof(int) * (size_t)T, s));
+    }
+    DBuf tmp;
+    BV_TRY(tmp.reserve(sizeof(int) * (size_t)n));
+    BV_TRY(cudaMemcpyAsync(tmp.p, roots, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+    k_mark_roots<<<grid_for(n), kThreads, 0, s>>>(n, T - 1, tmp.as<int>(), nrange_.as<int2>(), intrange_.as<int>(),
+                                                  rtroot_.as<int>()); note_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    tmp.release();
+    BV_TRY(e);
+    updated_ = true;
+    return BVHCD_OK;
+}
+
+bvhcd_status LBvh::export_tree(int32_t *inode, float *ibox, int32_t *leaf, float *lbox, int32_t *lca,
+                               uint32_t *codes, int32_t *primmap, cudaStream_t s) const {
+    const int T = T_;
+    if (!built_) return BVHCD_NOT_READY;
+    if (T == 0) return BVHCD_OK;
+    DBuf tmp;
+    size_t nb = sizeof(int) * 6 * (size_t)T * 2 + sizeof(int) * 4 * (size_t)T + sizeof(float) * 6 * (size_t)T;
+    BV_TRY(tmp.reserve(nb));
+    int *d_inode = tmp.as<int>();
+    float *d_ibox = reinterpret_cast<float *>(d_inode + 6 * (size_t)T);
+    int *d_leaf = reinterpret_cast<int *>(d_ibox + 6 * (size_t)T);
+    float *d_lbox = reinterpret_cast<float *>(d_leaf + 4 * (size_t)T);
+    k_export<<<grid_for(T), kThreads, 0, s>>>(T, nrec_.as<float4>(), topo_.as<int4>(), nrange_.as<int2>(),
+                                              lrec_.as<float4>(), sface_.as<int4>(), lca_.as<int>(), d_inode,
+                                              d_ibox, d_leaf, d_lbox); note_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && inode && T > 1)
+        e = cudaMemcpyAsync(inode, d_inode, sizeof(int) * 6 * (size_t)(T - 1), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && ibox && T > 1)
+        e = cudaMemcpyAsync(ibox, d_ibox, sizeof(float) * 6 * (size_t)(T - 1), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && leaf)
+        e = cudaMemcpyAsync(leaf, d_leaf, sizeof(int) * 4 * (size_t)T, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && lbox)
+        e = cudaMemcpyAsync(lbox, d_lbox, sizeof(float) * 6 * (size_t)T, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && lca)
+        e = cudaMemcpyAsync(lca, lca_.p, sizeof(int) * (size_t)(T + 1), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && codes)
+        e = cudaMemcpyAsync(codes, code_.p, sizeof(unsigned) * (size_t)T, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && primmap)
+        e = cudaMemcpyAsync(primmap, primmap_.p, sizeof(int) * (size_t)T, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    DBuf &t = const_cast<DBuf &>(tmp);
+    t.release();
+    return cuda_status(e);
+}
+
+}  // namespace bvhcd

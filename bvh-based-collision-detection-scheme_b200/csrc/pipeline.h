@@ -1,0 +1,172 @@
+// pipeline.h -- host classes behind the C ABI.  LBvh mirrors
+// LBvhFixedDeformable (Mine/collision/lbvh/LBvhFixedDeformable.h:27-108) and
+// Front mirrors BvttFrontLooseIntra (Mine/collision/bvtt_front/BvttFrontLooseIntra.h:27-80):
+// same maintenance options, same per-frame state machine, but every size
+// stays on the device and every call only enqueues work on a stream.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "../../include/bvhcd.h"
+#include "device.cuh"
+
+namespace bvhcd {
+
+// Device buffer owned by a handle.
+struct DBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t n) {
+        if (n <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T>
+    T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+bvhcd_status cuda_status(cudaError_t e);
+
+// Stage timer: CUDA event pairs recorded on the work stream, resolved when
+// read (the reference's Logger::recordSection, Mine/utility/CudaTimer.hpp:43-53).
+class Profiler {
+  public:
+    ~Profiler();
+    bool on = false;
+    void begin(int stage, cudaStream_t s);
+    void end(int stage, cudaStream_t s);
+    bvhcd_status read(double *ms, int64_t *calls, bool reset);
+
+  private:
+    struct Pending { int stage; cudaEvent_t a, b; };
+    cudaEvent_t get();
+    std::vector<cudaEvent_t> pool_;
+    std::vector<Pending> pending_;
+    cudaEvent_t open_[BVHCD_STAGE_COUNT] = {};
+    double ms_[BVHCD_STAGE_COUNT] = {};
+    int64_t calls_[BVHCD_STAGE_COUNT] = {};
+};
+
+// RAII stage scope
+struct StageScope {
+    Profiler *p;
+    int stage;
+    cudaStream_t s;
+    StageScope(Profiler *p_, int st, cudaStream_t s_) : p(p_), stage(st), s(s_) {
+        if (p->on) p->begin(stage, s);
+    }
+    ~StageScope() {
+        if (p->on) p->end(stage, s);
+    }
+};
+
+class LBvh {
+  public:
+    explicit LBvh(const bvhcd_bvh_config &cfg) : cfg_(cfg) {}
+    ~LBvh();
+    bvhcd_status init();
+    bvhcd_status maintain(bvhcd_bvh_op op, const bvhcd_scene &scene, cudaStream_t s);
+    bvhcd_status export_tree(int32_t *inode, float *ibox, int32_t *leaf, float *lbox, int32_t *lca,
+                             uint32_t *codes, int32_t *primmap, cudaStream_t s) const;
+    bvhcd_status request_restructure(const int32_t *roots, int32_t n, cudaStream_t s);
+
+    Tree tree() const;
+    int T() const { return T_; }
+    int V() const { return V_; }
+    bool built() const { return built_; }
+    int opt_tag() const { return opt_tag_; }
+    const float *verts() const { return vptr_; }
+    bool restr_enabled() const { return cfg_.enable_restr != 0; }
+
+    // BvhRestrLog (Mine/collision/auxiliary/BvhRestrLog.h:57-80): written by
+    // the front's quality check, consumed by the next maintain.
+    int *intrange() const { return intrange_.as<int>(); }
+    int *rtroot() const { return rtroot_.as<int>(); }
+    void set_updated(bool u) { updated_ = u; }
+    bool updated() const { return updated_; }
+    unsigned *counters() const { return ctr_.as<unsigned>(); }
+    int last_rt_subtrees() const { return rt_subtrees_; }
+    int last_rt_intnodes() const { return rt_intnodes_; }
+    Profiler *profiler() { return &prof_; }
+
+  private:
+    bvhcd_status ensure_capacity(int T, int V);
+    bvhcd_status upload(const bvhcd_scene &scene, cudaStream_t s);
+    bvhcd_status build(cudaStream_t s);
+    bvhcd_status refit(cudaStream_t s);
+    bvhcd_status restructure(cudaStream_t s);
+    bvhcd_status scene_box(cudaStream_t s);
+    bvhcd_status climb_and_order(cudaStream_t s);
+
+    bvhcd_bvh_config cfg_;
+    int T_ = 0, V_ = 0, capT_ = 0, capV_ = 0;
+    bool built_ = false, updated_ = false;
+    int opt_tag_ = 0, rt_subtrees_ = 0, rt_intnodes_ = 0;
+    const float *vptr_ = nullptr;
+    const int *fptr_ = nullptr;
+    // owned copies of host input
+    DBuf verts_, faces_;
+    // tree
+    DBuf nrec_, lrec_, topo_, nrange_, lca_, sface_, primmap_, code_, refit_flag_;
+    // build scratch
+    DBuf keys_, vals_, keys2_, vals2_, k64_, k64b_, metric_, ulc_, urc_, upar_, urx_, ury_, umark_,
+        ubox_, uflag_, posb_, clen_, coff_, dfs_, ulpar_, scene_, partial_, scratch_, task_, tmpface_;
+    // restructure log
+    DBuf intrange_, rtroot_, intmark_, extrange_, extmark_, leafroot_, flagbuf_;
+    DBuf ctr_;
+    unsigned *h_ctr_ = nullptr;  // pinned
+    Profiler prof_;
+};
+
+class Front {
+  public:
+    Front(LBvh *bvh, const bvhcd_front_config &cfg) : bvh_(bvh), cfg_(cfg) {}
+    ~Front();
+    bvhcd_status init();
+    bvhcd_status maintain(bvhcd_front_op op, cudaStream_t s);
+    bvhcd_status stats(bvhcd_front_stats *st, cudaStream_t s);
+    bvhcd_status pairs(int which, int32_t *out, int64_t cap, int64_t *count, bool out_dev,
+                       cudaStream_t s);
+    bvhcd_status export_front(int which, int32_t *out, int64_t cap, int64_t *count, cudaStream_t s);
+    bvhcd_status device_results(const int32_t **hits, const int64_t **counts);
+
+  private:
+    bvhcd_status ensure_node_capacity(int T);
+    bvhcd_status run(bvhcd_front_op op, cudaStream_t s);
+    bvhcd_status generate(cudaStream_t s, bool pure);
+    bvhcd_status prune_sprout(cudaStream_t s);
+    bvhcd_status keep(cudaStream_t s);
+    bvhcd_status balance(cudaStream_t s);
+    bvhcd_status reorder(cudaStream_t s);
+    bvhcd_status narrow(cudaStream_t s);
+    bvhcd_status check_quality(cudaStream_t s);
+    bvhcd_status snapshot(cudaStream_t s);
+    bvhcd_status grow_and_check(cudaStream_t s, bool *overflowed);
+    FrontLog log() const;
+
+    LBvh *bvh_;
+    bvhcd_front_config cfg_;
+    int capT_ = 0;
+    int cur_ = 0;  // which buffer set holds the current front
+    int last_op_ = -1;
+    bool has_front_ = false;
+    DBuf front_[2][2];  // [set][0 int, 1 ext] int2 entries
+    int64_t fcap_[2] = {0, 0};
+    DBuf pairs_, hits_, outbuf_;
+    int64_t pcap_ = 0;
+    DBuf intcnt_, extcnt_, intbeg_, extbeg_, intback_, extback_, snapshot_, scratch_, counts64_;
+};
+
+}  // namespace bvhcd

@@ -1,0 +1,209 @@
+/*
+ * bvhcd.h -- C ABI of the B200 collision pipeline (LBVH + BVTT front +
+ * triangle-triangle narrow phase).
+ *
+ * The entry points replace the reference's two module classes and its
+ * scheduler; each declaration names the reference interface it stands in for
+ * (paths inside littlemine/BVH-based-Collision-Detection-Scheme,
+ * Mine/ = Source/Project/Mine/).  Plain pointers and sizes only: positions
+ * are float[3] per vertex, faces int[3] per triangle, pairs int[2].  Streams
+ * are cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Every function returns a bvhcd_status; nothing prints or exits.  Work is
+ * enqueued asynchronously on the given stream; functions that return counts
+ * to the host synchronise that stream and say so.
+ */
+#ifndef BVHCD_H_
+#define BVHCD_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    BVHCD_OK = 0,
+    BVHCD_INVALID_ARG = 1,
+    BVHCD_OUT_OF_MEMORY = 2,
+    BVHCD_CAPACITY_EXCEEDED = 3, /* a front / pair buffer overflowed; see stats */
+    BVHCD_CUDA_ERROR = 4,
+    BVHCD_TIMEOUT = 5,
+    BVHCD_NOT_READY = 6          /* e.g. front maintained before any BVH build */
+} bvhcd_status;
+
+/* LBvhFixedDeformableMaintenance {BUILD, REFIT, UPDATE}
+ * (Mine/collision/lbvh/LBvhFixedDeformable.h:20-21). */
+typedef enum { BVHCD_BVH_BUILD = 0, BVHCD_BVH_REFIT = 1, BVHCD_BVH_UPDATE = 2 } bvhcd_bvh_op;
+
+/* BvttFrontLooseIntraMaintenance {PURE_BVH_CD, GENERATE, UPDATE, REORDER,
+ * KEEP, RESTRUCTURE} (Mine/collision/bvtt_front/BvttFrontLooseIntra.h:20-22). */
+typedef enum {
+    BVHCD_FRONT_PURE_BVH_CD = 0,
+    BVHCD_FRONT_GENERATE = 1,
+    BVHCD_FRONT_UPDATE = 2,
+    BVHCD_FRONT_REORDER = 3,
+    BVHCD_FRONT_KEEP = 4,
+    BVHCD_FRONT_RESTRUCTURE = 5
+} bvhcd_front_op;
+
+/* LBvhBuildConfig{primSize, extSize, intSize} (Mine/setting/BvhSettings.h:49-54)
+ * plus the CDBenchmarkSettings switches (Mine/setting/CDBenchmarkSettings.h:33-35). */
+typedef struct {
+    int32_t prim_capacity;   /* max triangles (reference default 150000) */
+    int32_t vert_capacity;   /* max vertices */
+    int32_t enable_restr;    /* quality-triggered restructuring (reference: on) */
+    int32_t reserved[5];
+} bvhcd_bvh_config;
+
+/* BvttFrontIntraBuildConfig{intFrontSize, extFrontSize, cpNum}
+ * (Mine/setting/BvttFrontSettings.h:52-63). */
+typedef struct {
+    int64_t int_front_capacity;  /* reference default 2,300,000 */
+    int64_t ext_front_capacity;  /* reference default 2,300,000 */
+    int64_t pair_capacity;       /* reference default 1,600,000 */
+    int32_t cull_adjacent;       /* drop pairs sharing a vertex id (covertex) */
+    int32_t narrow_phase;        /* run the tri-tri test after the broad phase */
+    int32_t auto_grow;           /* on overflow: grow buffers and replay (syncs) */
+    int32_t reserved[5];
+} bvhcd_front_config;
+
+/* SceneData{pos, fids} (Mine/world/Scene.h:16-20). */
+typedef struct {
+    const float *pos;      /* V x 3 */
+    const int32_t *faces;  /* T x 3 vertex ids */
+    int32_t num_vertices;
+    int32_t num_faces;
+    int32_t on_device;     /* 1: device pointers, read in place; 0: host pointers, copied */
+    int32_t faces_static;  /* 1: faces unchanged since the last call (skip their copy) */
+} bvhcd_scene;
+
+/* Stats the reference logs per frame in inspectResults
+ * (Mine/collision/bvtt_front/BvttFrontLooseIntra.cu:50-61). */
+typedef struct {
+    int64_t int_front;       /* F_int */
+    int64_t ext_front;       /* F_ext */
+    int64_t broad_pairs;     /* cpNum */
+    int64_t narrow_hits;     /* actualCpNum */
+    int32_t overflow;        /* bit0 int front, bit1 ext front, bit2 pairs */
+    int32_t bvh_opt_tag;     /* 0 refit, 1 restructure, 2 build (BvhRestrLog.h:59) */
+    int32_t front_op_run;    /* the front operation that actually ran */
+    int32_t restr_pending;   /* quality check marked the BVH for restructuring */
+    int32_t num_rt_subtrees; /* restructure decision inputs (LBvhFixedDeformable.cu:240-241) */
+    int32_t num_rt_int_nodes;
+    int32_t reserved[6];
+} bvhcd_front_stats;
+
+typedef struct bvhcd_bvh bvhcd_bvh;
+typedef struct bvhcd_front bvhcd_front;
+
+const char *bvhcd_status_string(bvhcd_status s);
+/* 1 when the library was built with device code for this device. */
+bvhcd_status bvhcd_device_check(int32_t device, int32_t *ok);
+
+/* ---- BVH module: replaces LBvhFixedDeformable
+ * ctor  (Mine/collision/lbvh/LBvhFixedDeformable.cu:20-55, .h:30),
+ * dtor  (.cu:57-66),
+ * maintain(scheme, SceneData) (.cu:68-87),
+ * getPrimNodeSize/getExtNodeSize/getIntNodeSize, bvhOptTag (.h:37-50). */
+bvhcd_status bvhcd_bvh_create(const bvhcd_bvh_config *cfg, bvhcd_bvh **out);
+bvhcd_status bvhcd_bvh_destroy(bvhcd_bvh *bvh);
+bvhcd_status bvhcd_bvh_maintain(bvhcd_bvh *bvh, bvhcd_bvh_op op, const bvhcd_scene *scene,
+                                void *stream);
+bvhcd_status bvhcd_bvh_sizes(const bvhcd_bvh *bvh, int32_t *prims, int32_t *ext_nodes,
+                             int32_t *int_nodes);
+bvhcd_status bvhcd_bvh_opt_tag(const bvhcd_bvh *bvh, int32_t *tag);
+/* Marks subtrees (internal nodes by DFS id, host array) as degraded, the
+ * marks the front-quality check leaves in BvhRestrLog
+ * (Mine/collision/bvtt_front/BvttFrontGenerateKernels.cu:45-47); the next
+ * bvhcd_bvh_maintain applies the reference's restructure decision
+ * (Mine/collision/lbvh/LBvhFixedDeformable.cu:210-352) to them.  Used by
+ * schedulers that pick subtrees themselves.  Ignored when enable_restr = 0. */
+bvhcd_status bvhcd_bvh_request_restructure(bvhcd_bvh *bvh, const int32_t *roots, int32_t n,
+                                           void *stream);
+/* Copies the tree to host arrays for invariant checks (the reference's
+ * debug kernels checkBVHIntegrity / checkPrimmap,
+ * Mine/collision/lbvh/LBvhBuildKernels.cu:228-293).  Synchronises `stream`.
+ * inode: 6 ints per internal node in DFS order (lc, rc, par, mark, rangex,
+ * rangey); ibox, lbox: 6 floats per node; leaf: 4 ints per Morton slot (orig
+ * triangle id, parent, mark, lca); lca: T+1 ints; codes: T; primmap: T.
+ * Any pointer may be NULL. */
+bvhcd_status bvhcd_bvh_export(const bvhcd_bvh *bvh, int32_t *inode, float *ibox, int32_t *leaf,
+                              float *lbox, int32_t *lca, uint32_t *codes, int32_t *primmap,
+                              void *stream);
+
+/* ---- Front module: replaces BvttFrontLooseIntra
+ * ctor  (Mine/collision/bvtt_front/BvttFrontLooseIntra.cu:16-38), borrows the BVH,
+ * dtor  (:40-48),
+ * maintain(scheme) (:69-126),
+ * inspectResults (:50-61) -> bvhcd_front_stats,
+ * applyCpResults(uint*, uint2*) (:63-67) -> bvhcd_front_pairs(which = 0). */
+bvhcd_status bvhcd_front_create(bvhcd_bvh *bvh, const bvhcd_front_config *cfg,
+                                bvhcd_front **out);
+bvhcd_status bvhcd_front_destroy(bvhcd_front *front);
+bvhcd_status bvhcd_front_maintain(bvhcd_front *front, bvhcd_front_op op, void *stream);
+/* Synchronises `stream`. */
+bvhcd_status bvhcd_front_stats_get(bvhcd_front *front, bvhcd_front_stats *stats, void *stream);
+/* Copies pairs of original triangle ids.  which = 0: broad-phase candidate
+ * pairs (applyCpResults); 1: pairs whose triangles intersect (the narrow
+ * result the reference keeps in d_orderedCdpairs).  out_on_device selects a
+ * device or host destination.  *count receives the full count even when it
+ * exceeds cap (then only cap pairs are written and CAPACITY_EXCEEDED is
+ * returned).  Synchronises `stream`. */
+bvhcd_status bvhcd_front_pairs(bvhcd_front *front, int32_t which, int32_t *out, int64_t cap,
+                               int64_t *count, int32_t out_on_device, void *stream);
+/* Device pointer of the current hit list (pairs of original triangle ids)
+ * and of two device-side int64 counts {broad pairs, hits}, both written by
+ * the last maintain on its stream; valid until the next maintain.  No sync. */
+bvhcd_status bvhcd_front_device_results(bvhcd_front *front, const int32_t **hit_pairs,
+                                        const int64_t **counts);
+/* Copies the current front (sorted-prim, node) entries; which = 0 internal,
+ * 1 external.  Synchronises `stream`. */
+bvhcd_status bvhcd_front_export(bvhcd_front *front, int32_t which, int32_t *out, int64_t cap,
+                                int64_t *count, void *stream);
+
+/* ---- Stage timing: the reference's Logger::recordSection GPU sections
+ * (Mine/utility/CudaTimer.hpp:43-53, e.g. "refit_bvh", "broad_phase_cd_update",
+ * "narrow_phase").  When enabled, the library records a CUDA event pair on
+ * the work stream around each stage (no synchronisation); reading the times
+ * synchronises the events and accumulates them per stage. */
+typedef enum {
+    BVHCD_STAGE_BVH_BUILD = 0,
+    BVHCD_STAGE_BVH_REFIT = 1,
+    BVHCD_STAGE_BVH_RESTRUCTURE = 2,
+    BVHCD_STAGE_FRONT_GENERATE = 3,
+    BVHCD_STAGE_FRONT_UPDATE = 4,
+    BVHCD_STAGE_FRONT_KEEP = 5,
+    BVHCD_STAGE_FRONT_BALANCE = 6,
+    BVHCD_STAGE_FRONT_REORDER = 7,
+    BVHCD_STAGE_NARROW = 8,
+    BVHCD_STAGE_QUALITY = 9,
+    BVHCD_STAGE_PURE_BVH_CD = 10,
+    BVHCD_STAGE_COUNT = 11
+} bvhcd_stage;
+
+bvhcd_status bvhcd_profile_enable(bvhcd_bvh *bvh, int32_t on);
+/* ms[i] = summed milliseconds of stage i since the last reset, calls[i] =
+ * number of timed calls.  reset != 0 clears the sums after reading. */
+bvhcd_status bvhcd_profile_read(bvhcd_bvh *bvh, double *ms, int64_t *calls, int32_t reset);
+
+/* Number of kernels this library has launched in this process (a counter
+ * for benchmarks; no reference counterpart beyond the per-kernel timers of
+ * Mine/system/CudaDevice/CudaKernelLauncher.cu:54-69). */
+bvhcd_status bvhcd_launch_count(int64_t *n);
+
+/* ---- Scheduler: BenchmarkLogic::maintainScheme, STATIC_MANDATORY with
+ * divergent marks (Mine/system/Logic/BenchmarkLogic.hpp:90-156). */
+bvhcd_status bvhcd_schedule_heuristic(int32_t frame, int32_t start_frame, int32_t *bvh_op,
+                                      int32_t *front_op);
+
+/* ---- One-call frame: schedule + BVH maintain + front maintain, the body of
+ * CudaProjectApp::Main's loop (Mine/Frameworks/CudaProject/CudaProjectApp.cpp:49-52). */
+bvhcd_status bvhcd_frame(bvhcd_bvh *bvh, bvhcd_front *front, int32_t frame, int32_t start_frame,
+                         const bvhcd_scene *scene, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

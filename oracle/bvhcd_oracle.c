@@ -413,7 +413,7 @@ static void orc_build(orc_pipe *p) {
     for (int i = 0; i < T; i++) p->metric[i] = (i != T - 1) ? split_metric(p->code[i], p->code[i + 1]) : 33;
     p->lca[T] = -1;
     if (T < 2) {
-        if (T == 1) { p->lca[0] = 1; p->lpar[0] = -1; p->lmark[0] = 3; }
+        if (T == 1) { p->lca[0] = 1; p->lpar[0] = -1; p->lmark[0] = 7; }
         p->built = 1;
         return;
     }
@@ -982,6 +982,26 @@ int orc_pipe_frame(orc_pipe *p, int T, const int *faces, int V, const float *ver
     orc_bvh_maintain(p, bvh_op);
     orc_front_maintain(p, front_op);
     return 0;
+}
+
+/* Marks subtrees (DFS roots) as degraded exactly as checkFrontQuality does
+ * (BvttFrontGenerateKernels.cu:45-47); the next BVH maintain restructures. */
+void orc_pipe_mark_restructure(orc_pipe *p, const int *roots, int n) {
+    const int T = p->T;
+    if (T < 2) return;
+    if (!p->updated) {
+        for (int i = 0; i < T; i++) p->rtroot[i] = INT_MAX;
+        memset(p->intrange, 0, sizeof(int) * (size_t)T);
+    }
+    for (int k = 0; k < n; k++) {
+        int i = roots[k];
+        if (i < 0 || i >= T - 1) continue;
+        int x = p->rx[i], y = p->ry[i];
+        p->intrange[i] += 1;
+        p->intrange[i + y - x] -= 1;
+        if (i < p->rtroot[x]) p->rtroot[x] = i;
+    }
+    p->updated = 1;
 }
 
 void orc_pipe_info(const orc_pipe *p, int64_t *info) {

@@ -58,6 +58,7 @@ int orc_pipe_tree(const orc_pipe *p, int *inode, float *ibox, int *leaf,
 int orc_pipe_log(const orc_pipe *p, unsigned *intcnt, unsigned *extcnt,
                  unsigned *intbeg, unsigned *extbeg);
 void orc_set_threads(int n);
+void orc_pipe_mark_restructure(orc_pipe *p, const int *roots, int n);
 
 /* Standalone stages. */
 void orc_scene_box(int T, const int *faces, const float *verts, float *box6);

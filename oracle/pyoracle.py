@@ -53,6 +53,7 @@ def lib():
         L.orc_pipe_log.restype = ctypes.c_int
         L.orc_pipe_log.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4
         L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_pipe_mark_restructure.argtypes = [ctypes.c_void_p, _i32p, ctypes.c_int]
         L.orc_scene_box.argtypes = [ctypes.c_int, _i32p, _f32p, _f32p]
         L.orc_morton_codes.argtypes = [ctypes.c_int, _i32p, _f32p, _f32p, _u32p]
         L.orc_brute_pairs.restype = ctypes.c_int64
@@ -162,6 +163,10 @@ class Pipeline:
                                   self._pos.shape[0], self._pos, int(bvh_op), int(front_op))
         if rc != 0:
             raise RuntimeError("oracle frame failed")
+
+    def mark_restructure(self, roots):
+        r = np.ascontiguousarray(roots, dtype=np.int32)
+        lib().orc_pipe_mark_restructure(self._p, r, r.size)
 
     def info(self):
         a = np.zeros(16, dtype=np.int64)

@@ -1,0 +1,241 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Integer and index results (tree topology, DFS ids, escape links, Morton
+codes, fronts as multisets, pair sets) must be bit-exact; so must the FP32
+boxes, which are exact min/max of FP32 inputs.  The narrow phase is an FP32
+predicate evaluated in the same operation order without contraction on both
+sides, so its hit set must match exactly too.
+"""
+import numpy as np
+import pytest
+
+from treecheck import check_tree
+
+pytestmark = pytest.mark.gpu
+
+CAPS = dict(int_front_capacity=4_000_000, ext_front_capacity=4_000_000, pair_capacity=2_000_000)
+
+
+def canon(p):
+    import pyoracle
+    return pyoracle.canon_pairs(p)
+
+
+def sorted_rows(a):
+    a = np.asarray(a).reshape(-1, 2)
+    if a.size == 0:
+        return a
+    return a[np.lexsort((a[:, 1], a[:, 0]))]
+
+
+def _new(bvhcd, T, V, restr=True, cull=True, narrow=True, auto_grow=False, caps=None):
+    bvh = bvhcd.LBvh(max(T, 1), max(V, 1), enable_restr=restr)
+    front = bvhcd.BvttFront(bvh, cull_adjacent=cull, narrow_phase=narrow, auto_grow=auto_grow,
+                            **(caps or CAPS))
+    return bvh, front
+
+
+def _tree_equal(a, b):
+    for k in ("inode", "ibox", "leaf", "lbox", "lca", "codes", "primmap"):
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
+
+
+def test_build_and_refit_bit_exact(cuda, lib_built, oracle, cloth_c1):
+    faces, frames = cloth_c1
+    T, V = faces.shape[0], frames[0].shape[0]
+    bvh, front = _new(lib_built, T, V)
+    p = oracle.Pipeline(True, True, True)
+    bvh.maintain(lib_built.BVH_BUILD, frames[0], faces)
+    p.frame(faces, frames[0], 0, 1)
+    g, o = bvh.export(), p.tree()
+    _tree_equal(g, o)
+    assert not check_tree(g, T)
+    front.maintain(lib_built.FRONT_GENERATE)
+    bvh.maintain(lib_built.BVH_REFIT, frames[1], faces)
+    p.frame(faces, frames[1], 1, 4)
+    _tree_equal(bvh.export(), p.tree())
+
+
+@pytest.mark.parametrize("cull", [1, 0])
+def test_pipeline_parity_over_schedule(cuda, lib_built, oracle, cloth_c1, cull):
+    faces, frames = cloth_c1
+    T, V = faces.shape[0], frames[0].shape[0]
+    bvh, front = _new(lib_built, T, V, cull=bool(cull))
+    p = oracle.Pipeline(True, bool(cull), True)
+    for f, pos in enumerate(frames):
+        b, fr = lib_built.schedule(f)
+        bvh.maintain(b, pos, faces)
+        front.maintain(fr)
+        p.frame(faces, pos, b, fr)
+        st, info = front.stats(), p.info()
+        assert st["overflow"] == 0
+        assert st["front_op_run"] == info["front_op"], f
+        assert st["bvh_opt_tag"] == info["opt_tag"], f
+        assert (st["int_front"], st["ext_front"]) == (info["F_int"], info["F_ext"]), f
+        assert (st["broad_pairs"], st["narrow_hits"]) == (info["P"], info["H"]), f
+        assert np.array_equal(canon(front.pairs()), canon(p.pairs())), f
+        assert np.array_equal(canon(front.pairs(narrow=True)), canon(p.pairs(narrow=True))), f
+        if f in (0, 6, 7, 12, 18):
+            assert np.array_equal(canon(front.pairs()), oracle.brute_pairs(faces, pos, cull)), f
+            for which in (0, 1):
+                assert np.array_equal(sorted_rows(front.export(which)), sorted_rows(p.front(which))), (f, which)
+
+
+def test_front_is_node_ordered(cuda, lib_built, cloth_c1):
+    faces, frames = cloth_c1
+    bvh, front = _new(lib_built, faces.shape[0], frames[0].shape[0])
+    bvh.maintain(lib_built.BVH_BUILD, frames[0], faces)
+    front.maintain(lib_built.FRONT_GENERATE)
+    for which in (0, 1):
+        nodes = front.export(which)[:, 1]
+        assert np.all(np.diff(nodes) >= 0), "counting sort must order entries by node"
+
+
+def _pick_roots(tree, frac=0.25, lo=16, hi=512):
+    inode = tree["inode"]
+    size = inode[:, 5] - inode[:, 4] + 1
+    covered = np.zeros(inode.shape[0] + 1, bool)
+    chosen, total = [], 0
+    for d in range(inode.shape[0]):
+        if lo <= size[d] <= hi and not covered[d]:
+            chosen.append(d)
+            covered[d:d + size[d] - 1] = True
+            total += size[d] - 1
+            if total >= frac * inode.shape[0]:
+                break
+    return np.array(chosen, np.int32)
+
+
+def test_restructure_parity(cuda, lib_built, oracle, cloth_c1):
+    faces, frames = cloth_c1
+    T, V = faces.shape[0], frames[0].shape[0]
+    bvh, front = _new(lib_built, T, V)
+    p = oracle.Pipeline(True, True, True)
+    for f in range(8):
+        pos = frames[f]
+        b, fr = lib_built.schedule(f)
+        bvh.maintain(b, pos, faces)
+        front.maintain(fr)
+        p.frame(faces, pos, b, fr)
+        assert bvh.opt_tag() == p.info()["opt_tag"], f
+        _tree_equal(bvh.export(), p.tree())
+        assert not check_tree(bvh.export(), T)
+        assert np.array_equal(canon(front.pairs()), canon(p.pairs())), f
+        if f == 2:
+            roots = _pick_roots(p.tree())
+            bvh.request_restructure(roots)
+            p.mark_restructure(roots)
+        if f == 3:
+            assert bvh.opt_tag() == 1
+            st = front.stats()
+            assert st["num_rt_int_nodes"] == p.info()["num_rt_int"]
+
+
+def test_pure_bvh_cd(cuda, lib_built, oracle, cloth_c1):
+    faces, frames = cloth_c1
+    bvh, front = _new(lib_built, faces.shape[0], frames[0].shape[0])
+    for f in (0, 5, 11):
+        bvh.maintain(lib_built.BVH_BUILD if f == 0 else lib_built.BVH_REFIT, frames[f], faces)
+        front.maintain(lib_built.FRONT_PURE_BVH_CD)
+        assert np.array_equal(canon(front.pairs()), oracle.brute_pairs(faces, frames[f], 1))
+
+
+def _edge_scene(kind):
+    if kind == "empty":
+        return np.zeros((0, 3), np.int32), np.zeros((0, 3), np.float32)
+    if kind == "one":
+        return np.array([[0, 1, 2]], np.int32), np.eye(3, dtype=np.float32)
+    if kind == "two":
+        return np.array([[0, 1, 2], [3, 4, 5]], np.int32), np.concatenate([np.eye(3), np.eye(3) + 0.5]).astype(np.float32)
+    if kind == "three":
+        v = np.random.default_rng(3).uniform(0, 1, (9, 3)).astype(np.float32)
+        return np.arange(9, dtype=np.int32).reshape(3, 3), v
+    if kind == "identical":  # all Morton codes equal
+        v = np.tile(np.eye(3, dtype=np.float32), (200, 1))
+        return np.arange(600, dtype=np.int32).reshape(200, 3), v
+    if kind == "degenerate":  # zero-area triangles and a flat scene (zero z extent)
+        rng = np.random.default_rng(9)
+        v = rng.uniform(0, 1, (300, 3)).astype(np.float32)
+        v[:, 2] = 0.0
+        f = rng.integers(0, 300, (500, 3)).astype(np.int32)
+        f[:50, 1] = f[:50, 0]
+        return f, v
+    raise KeyError(kind)
+
+
+@pytest.mark.parametrize("kind", ["empty", "one", "two", "three", "identical", "degenerate"])
+def test_edge_cases(cuda, lib_built, oracle, kind):
+    faces, verts = _edge_scene(kind)
+    T = faces.shape[0]
+    bvh, front = _new(lib_built, T, verts.shape[0], cull=False)
+    p = oracle.Pipeline(True, False, True)
+    for f, op in enumerate([(0, 1), (1, 4), (1, 2), (1, 3), (0, 1)]):
+        bvh.maintain(op[0], verts, faces)
+        front.maintain(op[1])
+        p.frame(faces, verts, *op)
+        assert np.array_equal(canon(front.pairs()), canon(p.pairs())), (kind, f)
+        assert np.array_equal(canon(front.pairs(narrow=True)), canon(p.pairs(narrow=True))), (kind, f)
+        if T >= 1:
+            _tree_equal(bvh.export(), p.tree())
+    assert np.array_equal(canon(front.pairs()), oracle.brute_pairs(faces, verts, 0))
+
+
+def test_overflow_is_reported_and_auto_grow_recovers(cuda, lib_built, oracle, cloth_c1):
+    faces, frames = cloth_c1
+    T, V = faces.shape[0], frames[0].shape[0]
+    small = dict(int_front_capacity=1000, ext_front_capacity=1000, pair_capacity=1000)
+    bvh, front = _new(lib_built, T, V, caps=small)
+    bvh.maintain(0, frames[0], faces)
+    front.maintain(1)
+    st = front.stats()
+    assert st["overflow"] & 1 and st["overflow"] & 2 and st["overflow"] & 4
+    with pytest.raises(lib_built.BvhcdError):
+        front.pairs()
+    bvh2, front2 = _new(lib_built, T, V, caps=small, auto_grow=True)
+    for f in range(8):
+        b, fr = lib_built.schedule(f)
+        bvh2.maintain(b, frames[f], faces)
+        front2.maintain(fr)
+        assert front2.stats()["overflow"] == 0
+        assert np.array_equal(canon(front2.pairs()), oracle.brute_pairs(faces, frames[f], 1)), f
+
+
+def test_device_resident_input(cuda, lib_built, cloth_c1):
+    torch = cuda
+    faces, frames = cloth_c1
+    T, V = faces.shape[0], frames[0].shape[0]
+    b1, f1 = _new(lib_built, T, V)
+    b2, f2 = _new(lib_built, T, V)
+    df = torch.from_numpy(faces).cuda()
+    for f in range(7):
+        b, fr = lib_built.schedule(f)
+        b1.maintain(b, frames[f], faces)
+        f1.maintain(fr)
+        b2.maintain(b, torch.from_numpy(frames[f]).cuda(), df)
+        f2.maintain(fr)
+        assert np.array_equal(canon(f1.pairs(True)), canon(f2.pairs(True)))
+        assert np.array_equal(canon(f1.pairs()), canon(f2.pairs()))
+    hits, counts = f2.device_results()
+    assert hits and counts
+
+
+def test_cloth_over_sphere_full_size(cuda, lib_built, oracle):
+    import scenes
+    faces, frames = scenes.cloth_over_sphere_frames(512, 3)
+    T, V = faces.shape[0], frames[0].shape[0]
+    assert T == 522242 + 40500
+    caps = dict(int_front_capacity=40_000_000, ext_front_capacity=40_000_000, pair_capacity=8_000_000)
+    bvh, front = _new(lib_built, T, V, caps=caps)
+    for f in range(3):
+        b, fr = lib_built.schedule(f)
+        bvh.maintain(b, frames[f], faces)
+        front.maintain(fr)
+        st = front.stats()
+        assert st["overflow"] == 0
+        pairs = canon(front.pairs())
+        assert np.array_equal(pairs, oracle.brute_pairs(faces, frames[f], 1)), f
+        hits = canon(front.pairs(narrow=True))
+        keep = oracle.narrow(pairs, faces, frames[f]).astype(bool)
+        assert np.array_equal(hits, pairs[keep]), f
+        assert len(hits) > 0, "the cloth must cut the sphere"
+    assert not check_tree(bvh.export(), T)
