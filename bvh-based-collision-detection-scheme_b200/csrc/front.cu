@@ -74,7 +74,14 @@ __device__ __forceinline__ void emit_pair(const FArgs &a, int prim, const int4 &
 template <bool kFront>
 __device__ __forceinline__ void traverse(const FArgs &a, int prim, const float4 &plo,
                                          const float4 &phi, const int4 &pf, int st, int stop) {
+    // a valid tree is left after at most 2T - 1 visits; the bound only turns
+    // a corrupted tree into an error flag instead of an endless loop
+    int guard = 2 * a.T + 2;
     while (st != stop) {
+        if (--guard < 0) {
+            atomicOr(a.ctr + C_OVERFLOW, 16u);
+            return;
+        }
         int leaf;
         float4 llo, lhi;
         if (st & 1) {
@@ -91,7 +98,7 @@ __device__ __forceinline__ void traverse(const FArgs &a, int prim, const float4 
             bool stopped = false;
             while (true) {
                 if (!overlap(nlo, nhi, plo, phi)) { stopped = true; break; }
-                if (n == last) break;
+                if (n >= last) break;
                 ++n;
                 nlo = ldg4(a.nrec + 2 * n);
                 nhi = ldg4(a.nrec + 2 * n + 1);

@@ -304,7 +304,8 @@ __global__ void __launch_bounds__(kThreads) k_refit_internal(int T, const float4
                                                              unsigned *flag) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x) {
         int p = __float_as_int(__ldg(reinterpret_cast<const float *>(lrec) + 8 * (size_t)s + 3));
-        while (p >= 0) {
+        // at most T - 1 ancestors; the bound keeps a corrupted tree from looping
+        for (int guard = T; p >= 0 && guard > 0; --guard) {
             __threadfence();
             if ((atomicAdd(&flag[p], 1u) & 1u) == 0u) break;
             __threadfence();
