@@ -36,7 +36,7 @@ sys.path.insert(0, PKG)
 
 WORKLOAD = "cloth512_over_icosphere45"
 METRIC = "ms_per_frame_cloth512_over_sphere"
-CAPS = dict(int_front_capacity=48_000_000, ext_front_capacity=48_000_000, pair_capacity=12_000_000)
+CAPS = dict(int_front_capacity=16_000_000, ext_front_capacity=16_000_000, pair_capacity=4_000_000)
 
 
 def _peaks():
@@ -171,40 +171,11 @@ def run_ours(args):
         dist.barrier()
     value = dev_ms / (K * world)
 
-    # ---- e2e: host buffers through the public API, upload + read-back timed
-    bvh2, front2 = pipeline()
-    for f in range(W):
-        bvhcd.frame(bvh2, front2, f, 0, host[f].numpy(), faces, stream=stream, faces_static=f > 0)
-        front2.pairs(narrow=True, stream=stream)
-    torch.cuda.synchronize()
-    e_starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
-    e_ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
-    d2h = 0
-    L = bvhcd.lib()
-    import ctypes
-    for i in range(K):
-        f = W + i
-        flush.zero_()
-        e_starts[i].record(stream)
-        bvhcd.frame(bvh2, front2, f, 0, host[f].numpy(), faces, stream=stream, faces_static=True)
-        n = ctypes.c_int64()
-        st2 = L.bvhcd_front_pairs(front2.handle, 1, ctypes.c_void_p(hits_host.data_ptr()),
-                                  hits_host.shape[0], ctypes.byref(n), 0, ctypes.c_void_p(stream.cuda_stream))
-        if st2 != 0:
-            raise RuntimeError(f"pairs read-back failed: {st2}")
-        e_ends[i].record(stream)
-        d2h += 8 * int(n.value) + 4 * 16
-    torch.cuda.synchronize()
-    e2e_ms = float(sum(s.elapsed_time(e) for s, e in zip(e_starts, e_ends)))
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": e2e_ms / (K * world), "unit": "ms/frame", "h2d_bytes_per_step": int(V * 12),
-           "d2h_bytes_per_step": int(d2h // K)}
-
-    # ---- roofline of the dominant stage, from a stage-timed replay
-    roof = roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
+    e2e = roof = None
+    if not args.only_value:
+        e2e = e2e_pass(bvhcd, torch, pipeline, host, faces, flush, hits_host, stream, W, K, V, world)
+        # roofline of the dominant stage, from a stage-timed replay
+        roof = roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
 
     out = None
     if rank == 0:
@@ -235,6 +206,43 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+def e2e_pass(bvhcd, torch, pipeline, host, faces, flush, hits_host, stream, W, K, V, world):
+    """Same frames through the public API with host buffers: the vertex
+    upload (pinned host -> HBM) and the read-back of the contact pairs are
+    inside each frame's events."""
+    import torch.distributed as dist
+    bvh2, front2 = pipeline()
+    for f in range(W):
+        bvhcd.frame(bvh2, front2, f, 0, host[f].numpy(), faces, stream=stream, faces_static=f > 0)
+        front2.pairs(narrow=True, stream=stream)
+    torch.cuda.synchronize()
+    e_starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    e_ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    d2h = 0
+    L = bvhcd.lib()
+    import ctypes
+    for i in range(K):
+        f = W + i
+        flush.zero_()
+        e_starts[i].record(stream)
+        bvhcd.frame(bvh2, front2, f, 0, host[f].numpy(), faces, stream=stream, faces_static=True)
+        n = ctypes.c_int64()
+        st2 = L.bvhcd_front_pairs(front2.handle, 1, ctypes.c_void_p(hits_host.data_ptr()),
+                                  hits_host.shape[0], ctypes.byref(n), 0, ctypes.c_void_p(stream.cuda_stream))
+        if st2 != 0:
+            raise RuntimeError(f"pairs read-back failed: {st2}")
+        e_ends[i].record(stream)
+        d2h += 8 * int(n.value) + 4 * 16
+    torch.cuda.synchronize()
+    e2e_ms = float(sum(s.elapsed_time(e) for s, e in zip(e_starts, e_ends)))
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    return {"value": e2e_ms / (K * world), "unit": "ms/frame", "h2d_bytes_per_step": int(V * 12),
+            "d2h_bytes_per_step": int(d2h // K)}
 
 
 def front_bytes(st_prev, st, T, uniq_nodes):
@@ -352,6 +360,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only-value", action="store_true",
+                    help="time the device-resident frames only (no e2e / roofline replay); for profiling")
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
     args = ap.parse_args()
     if args.warmup < 3:

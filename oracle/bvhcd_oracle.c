@@ -252,7 +252,7 @@ struct orc_pipe {
 static void *xcalloc(size_t n, size_t s) { return calloc(n ? n : 1, s); }
 
 static void pipe_alloc(orc_pipe *p, int T) {
-    if (T <= p->cap) return;
+    if (p->lbox && T + 2 <= p->cap) return;
     int c = T + 2;
 #define RE(ptr, type, n) ptr = (type *)realloc(ptr, sizeof(type) * (size_t)(n))
     RE(p->lbox, obox, c); RE(p->lidx, int, c); RE(p->lvid, int, 3 * c); RE(p->lpar, int, c);
