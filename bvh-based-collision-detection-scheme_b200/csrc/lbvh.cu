@@ -282,42 +282,44 @@ __global__ void k_write_nodes(int nint, int T, Climb c, const int *__restrict__ 
 }
 
 // ---------------------------------------------------------------- refit
-// refitExtNode (Mine/collision/lbvh/LBvhUpdateKernels.cu:35-61), by slot.
-__global__ void __launch_bounds__(kThreads) k_refit_leaves(int T, const int4 *__restrict__ sface,
-                                                           const float *__restrict__ verts,
-                                                           float4 *lrec) {
+// refitExtNode + refitIntNode (Mine/collision/lbvh/LBvhUpdateKernels.cu:35-74)
+// fused: each slot's thread computes its leaf box from the three vertices,
+// then climbs.  A node receives two arrivals per refit, so the parity of its
+// flag tells the second arrival without clearing flags between refits.  The
+// climbing thread keeps its own child's box in registers and loads only the
+// sibling's; the parent's topology (static) is requested before the atomic so
+// one level costs one atomic round trip plus one sibling load.
+__global__ void __launch_bounds__(kThreads) k_refit(int T, const int4 *__restrict__ sface,
+                                                    const float *__restrict__ verts, float4 *lrec,
+                                                    float4 *nrec, const int4 *__restrict__ topo,
+                                                    unsigned *flag) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x) {
-        int4 f = __ldg(&sface[s]);
+        const int4 f = __ldg(&sface[s]);
+        int p = __float_as_int(reinterpret_cast<const float *>(lrec)[8 * (size_t)s + 3]);
         float4 lo, hi;
         tri_box(load_vert(verts, f.x), load_vert(verts, f.y), load_vert(verts, f.z), lo, hi);
-        float *p = reinterpret_cast<float *>(lrec + 2 * (size_t)s);
-        p[0] = lo.x; p[1] = lo.y; p[2] = lo.z;
-        p[4] = hi.x; p[5] = hi.y; p[6] = hi.z;
-    }
-}
-
-// refitIntNode (LBvhUpdateKernels.cu:63-74).  Each internal node receives
-// two arrivals per refit, so the flag's parity tells the second arrival
-// without clearing the flags between refits.
-__global__ void __launch_bounds__(kThreads) k_refit_internal(int T, const float4 *__restrict__ lrec,
-                                                             float4 *nrec, const int4 *__restrict__ topo,
-                                                             unsigned *flag) {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x) {
-        int p = __float_as_int(__ldg(reinterpret_cast<const float *>(lrec) + 8 * (size_t)s + 3));
+        float *w = reinterpret_cast<float *>(lrec + 2 * (size_t)s);
+        w[0] = lo.x; w[1] = lo.y; w[2] = lo.z;
+        w[4] = hi.x; w[5] = hi.y; w[6] = hi.z;
+        int child = s;
+        bool child_leaf = true;
         // at most T - 1 ancestors; the bound keeps a corrupted tree from looping
         for (int guard = T; p >= 0 && guard > 0; --guard) {
-            __threadfence();
-            if ((atomicAdd(&flag[p], 1u) & 1u) == 0u) break;
-            __threadfence();
-            int4 t = __ldg(&topo[p]);
-            float4 alo, ahi, blo, bhi;
-            if (t.w & 1) { alo = __ldg(&lrec[2 * t.x]); ahi = __ldg(&lrec[2 * t.x + 1]); }
-            else         { alo = __ldcg(&nrec[2 * t.x]); ahi = __ldcg(&nrec[2 * t.x + 1]); }
-            if (t.w & 2) { blo = __ldg(&lrec[2 * t.y]); bhi = __ldg(&lrec[2 * t.y + 1]); }
-            else         { blo = __ldcg(&nrec[2 * t.y]); bhi = __ldcg(&nrec[2 * t.y + 1]); }
+            const int4 t = __ldg(&topo[p]);
+            cuda::atomic_ref<unsigned, cuda::thread_scope_device> fl(flag[p]);
+            if ((fl.fetch_add(1u, cuda::memory_order_acq_rel) & 1u) == 0u) break;
+            const bool from_left = (child == t.x) && (((t.w & 1) != 0) == child_leaf);
+            const int sib = from_left ? t.y : t.x;
+            const bool sib_leaf = from_left ? (t.w & 2) != 0 : (t.w & 1) != 0;
+            const float4 *src = sib_leaf ? lrec : nrec;
+            const float4 slo = __ldcg(src + 2 * (size_t)sib), shi = __ldcg(src + 2 * (size_t)sib + 1);
+            lo.x = fminf(lo.x, slo.x); lo.y = fminf(lo.y, slo.y); lo.z = fminf(lo.z, slo.z);
+            hi.x = fmaxf(hi.x, shi.x); hi.y = fmaxf(hi.y, shi.y); hi.z = fmaxf(hi.z, shi.z);
             float *q = reinterpret_cast<float *>(nrec + 2 * (size_t)p);
-            q[0] = fminf(alo.x, blo.x); q[1] = fminf(alo.y, blo.y); q[2] = fminf(alo.z, blo.z);
-            q[4] = fmaxf(ahi.x, bhi.x); q[5] = fmaxf(ahi.y, bhi.y); q[6] = fmaxf(ahi.z, bhi.z);
+            q[0] = lo.x; q[1] = lo.y; q[2] = lo.z;
+            q[4] = hi.x; q[5] = hi.y; q[6] = hi.z;
+            child = p;
+            child_leaf = false;
             p = t.z;
         }
     }
@@ -725,10 +727,8 @@ bvhcd_status LBvh::refit(cudaStream_t s) {
     StageScope prof_scope(&prof_, BVHCD_STAGE_BVH_REFIT, s);
     const int T = T_;
     if (T == 0) return BVHCD_OK;
-    k_refit_leaves<<<grid_for(T), kThreads, 0, s>>>(T, sface_.as<int4>(), vptr_, lrec_.as<float4>()); note_launch();
-    if (T >= 2)
-        k_refit_internal<<<grid_for(T), kThreads, 0, s>>>(T, lrec_.as<float4>(), nrec_.as<float4>(),
-                                                          topo_.as<int4>(), refit_flag_.as<unsigned>()); note_launch();
+    k_refit<<<grid_for(T), kThreads, 0, s>>>(T, sface_.as<int4>(), vptr_, lrec_.as<float4>(), nrec_.as<float4>(),
+                                             topo_.as<int4>(), refit_flag_.as<unsigned>()); note_launch();
     return cuda_status(cudaGetLastError());
 }
 
