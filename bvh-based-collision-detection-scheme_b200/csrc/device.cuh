@@ -59,8 +59,10 @@ enum CounterSlot {
     C_INT0 = 0, C_EXT0 = 1,   // front sizes, buffer set 0
     C_INT1 = 2, C_EXT1 = 3,   // front sizes, buffer set 1
     C_PAIRS = 4, C_HITS = 5,
-    C_OVERFLOW = 6,           // bit0 int front, bit1 ext front, bit2 pairs, bit3 hits
+    C_OVERFLOW = 6,           // bit0 int front, bit1 ext front, bit2 pairs, bit3 hits,
+                              // bit4 traversal bound hit, bit5 sprout work list
     C_RT_SUBTREES = 7, C_RT_INTNODES = 8,
+    C_WORK = 10,              // overlapping internal entries queued for traversal
     C_NUM = 16
 };
 

@@ -7,6 +7,7 @@
 // trip.  Emission reserves slots with one atomic per converged warp group and
 // checks capacity before writing.
 #include <climits>
+#include <cstdlib>
 
 #include "pipeline.h"
 #include "prims.cuh"
@@ -45,6 +46,8 @@ struct FArgs {
     unsigned cap_int, cap_ext;
     int2 *pairs;
     unsigned cap_pairs;
+    int2 *work;
+    unsigned cap_work;
     int cull;
     int T;
 };
@@ -153,98 +156,163 @@ __device__ __forceinline__ int prune_up(const FArgs &a, int n, int top, const fl
     return n + 1;
 }
 
-// maintainIntLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:12-57)
-__global__ void __launch_bounds__(kThreads) k_maintain_int(FArgs a) {
-    const unsigned n = min(a.ctr[a.in_int_slot], a.cap_int);
+// Batched front scans.  The common case of every front operation is a test
+// of one front entry (primitive record against node record) that ends the
+// entry's work; the rare overlapping internal entry needs a traversal below
+// its node.  The scans below test kU entries per thread per step with all
+// their loads issued together (memory-level parallelism instead of one
+// dependent chain per entry), keep the register count low, and append the
+// overlapping internal entries to a work list that k_sprout traverses.
+template <int kU>
+struct Batch {
+    int2 e[kU];
+    bool v[kU], in_int[kU];
+    float4 plo[kU], phi[kU], nlo[kU], nhi[kU];
+};
+
+// loads entries q0 + k*stride (internal ones first in the index space,
+// then external ones) and their primitive and node records
+template <int kU>
+__device__ __forceinline__ void load_batch(const FArgs &a, unsigned q0, unsigned stride, unsigned ni,
+                                           unsigned total, Batch<kU> &b) {
+#pragma unroll
+    for (int k = 0; k < kU; k++) {
+        const unsigned q = q0 + k * stride;
+        b.v[k] = q < total;
+        b.in_int[k] = q < ni;
+        b.e[k] = b.v[k] ? (b.in_int[k] ? a.in_int[q] : a.in_ext[q - ni]) : make_int2(0, 0);
+    }
+#pragma unroll
+    for (int k = 0; k < kU; k++) {
+        if (!b.v[k]) continue;
+        b.plo[k] = ldg4(a.lrec + 2 * b.e[k].x);
+        b.phi[k] = ldg4(a.lrec + 2 * b.e[k].x + 1);
+        const float4 *nb = b.in_int[k] ? a.nrec : a.lrec;
+        b.nlo[k] = ldg4(nb + 2 * b.e[k].y);
+        b.nhi[k] = ldg4(nb + 2 * b.e[k].y + 1);
+    }
+}
+
+__device__ __forceinline__ void emit_work(const FArgs &a, const int2 &e) {
+    emit(a.work, a.ctr + C_WORK, a.cap_work, e, a.ctr + C_OVERFLOW, 32u);
+}
+
+// Traversal below overlapping internal front nodes (the sprout half of
+// maintainIntLooseIntraFrontsWithLog, BvttFrontPruneSproutKernels.cu:32-56,
+// with kFront; keepIntLooseIntraFronts, BvttFrontKeepKernels.cu:21-42, and the
+// overlap half of reorderIntLooseIntraFrontsWithLog,
+// BvttFrontReorderKernels.cu:43-62, without).
+template <bool kFront>
+__global__ void __launch_bounds__(kThreads) k_sprout(FArgs a) {
+    const unsigned n = min(a.ctr[C_WORK], a.cap_work);
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        int2 e = a.in_int[q];
-        const int prim = e.x, st = e.y;
-        float4 plo = ldg4(a.lrec + 2 * prim), phi = ldg4(a.lrec + 2 * prim + 1);
-        float4 nlo = ldg4(a.nrec + 2 * st), nhi = ldg4(a.nrec + 2 * st + 1);
-        if (!overlap(nlo, nhi, plo, phi)) {
-            const int top = __ldg(&a.lca[__float_as_int(nlo.w)]) >> 1;
-            int k = prune_up(a, st - 1, top, plo, phi);
-            if (k >= 0) emit_int(a, prim, k);
-            continue;
+        const int2 e = a.work[q];
+        const float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
+        const float4 nlo = ldg4(a.nrec + 2 * e.y), nhi = ldg4(a.nrec + 2 * e.y + 1);
+        traverse<kFront>(a, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, nlo),
+                         __float_as_int(nhi.w));
+    }
+}
+
+// maintainIntLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:12-57):
+// non-overlapping entries are pruned here, overlapping ones go to k_sprout<true>.
+template <int kU>
+__global__ void __launch_bounds__(kThreads) k_maintain_int_scan(FArgs a) {
+    const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
+    const unsigned stride = gridDim.x * blockDim.x;
+    for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < ni; q0 += kU * stride) {
+        Batch<kU> b;
+        load_batch(a, q0, stride, ni, ni, b);
+#pragma unroll
+        for (int k = 0; k < kU; k++) {
+            if (!b.v[k]) continue;
+            if (overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k])) {
+                emit_work(a, b.e[k]);
+                continue;
+            }
+            const int top = __ldg(&a.lca[__float_as_int(b.nlo[k].w)]) >> 1;
+            const int m = prune_up(a, b.e[k].y - 1, top, b.plo[k], b.phi[k]);
+            if (m >= 0) emit_int(a, b.e[k].x, m);
         }
-        traverse<true>(a, prim, plo, phi, prim_face(a, prim), left_child_tagged(a, st, nlo),
-                       __float_as_int(nhi.w));
     }
 }
 
 // maintainExtLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:60-93)
+template <int kU>
 __global__ void __launch_bounds__(kThreads) k_maintain_ext(FArgs a) {
-    const unsigned n = min(a.ctr[a.in_ext_slot], a.cap_ext);
-    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        int2 e = a.in_ext[q];
-        const int prim = e.x, st = e.y;
-        float4 plo = ldg4(a.lrec + 2 * prim), phi = ldg4(a.lrec + 2 * prim + 1);
-        float4 llo = ldg4(a.lrec + 2 * st), lhi = ldg4(a.lrec + 2 * st + 1);
-        if (overlap(llo, lhi, plo, phi)) {
-            emit_ext(a, prim, st);
-            emit_pair(a, prim, prim_face(a, prim), st);
-            continue;
+    const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
+    const unsigned stride = gridDim.x * blockDim.x;
+    for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < ne; q0 += kU * stride) {
+        Batch<kU> b;
+        load_batch(a, q0, stride, 0, ne, b);
+#pragma unroll
+        for (int k = 0; k < kU; k++) {
+            if (!b.v[k]) continue;
+            const int prim = b.e[k].x, st = b.e[k].y;
+            if (overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k])) {
+                emit_ext(a, prim, st);
+                emit_pair(a, prim, prim_face(a, prim), st);
+                continue;
+            }
+            const int gfa = __float_as_int(b.nlo[k].w);
+            const float4 glo = ldg4(a.nrec + 2 * gfa), ghi = ldg4(a.nrec + 2 * gfa + 1);
+            if (overlap(glo, ghi, b.plo[k], b.phi[k])) {
+                emit_ext(a, prim, st);
+                continue;
+            }
+            const int l = __ldg(&a.lca[st]);
+            if (l & 1) continue;  // right child: the parent's left chain handles it
+            const int m = prune_up(a, gfa - 1, l >> 1, b.plo[k], b.phi[k]);
+            if (m >= 0) emit_int(a, prim, m);
         }
-        const int gfa = __float_as_int(llo.w);
-        float4 glo = ldg4(a.nrec + 2 * gfa), ghi = ldg4(a.nrec + 2 * gfa + 1);
-        if (overlap(glo, ghi, plo, phi)) {
-            emit_ext(a, prim, st);
-            continue;
-        }
-        const int l = __ldg(&a.lca[st]);
-        if (l & 1) continue;  // right child: the parent's left chain handles it
-        int k = prune_up(a, gfa - 1, l >> 1, plo, phi);
-        if (k >= 0) emit_int(a, prim, k);
     }
 }
 
 // keepIntLooseIntraFronts / keepExtLooseIntraFronts (BvttFrontKeepKernels.cu:11-58)
 // in one index space: [0, F_int) internal entries, then external ones.
-__global__ void __launch_bounds__(kThreads) k_keep(FArgs a) {
+template <int kU>
+__global__ void __launch_bounds__(kThreads) k_keep_scan(FArgs a) {
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
-    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < ni + ne; q += gridDim.x * blockDim.x) {
-        if (q < ni) {
-            int2 e = a.in_int[q];
-            float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
-            float4 nlo = ldg4(a.nrec + 2 * e.y), nhi = ldg4(a.nrec + 2 * e.y + 1);
-            if (!overlap(nlo, nhi, plo, phi)) continue;
-            traverse<false>(a, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, nlo),
-                            __float_as_int(nhi.w));
-        } else {
-            int2 e = a.in_ext[q - ni];
-            float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
-            float4 llo = ldg4(a.lrec + 2 * e.y), lhi = ldg4(a.lrec + 2 * e.y + 1);
-            if (overlap(llo, lhi, plo, phi)) emit_pair(a, e.x, prim_face(a, e.x), e.y);
+    const unsigned stride = gridDim.x * blockDim.x;
+    for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < ni + ne; q0 += kU * stride) {
+        Batch<kU> b;
+        load_batch(a, q0, stride, ni, ni + ne, b);
+#pragma unroll
+        for (int k = 0; k < kU; k++) {
+            if (!b.v[k] || !overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k])) continue;
+            if (b.in_int[k]) emit_work(a, b.e[k]);
+            else emit_pair(a, b.e[k].x, prim_face(a, b.e[k].x), b.e[k].y);
         }
     }
 }
 
 // balance: reorderIntLooseIntraFrontsWithLog (BvttFrontReorderKernels.cu:27-63)
-// + keepExtLooseIntraFronts for the external front.
-__global__ void __launch_bounds__(kThreads) k_balance(FArgs a) {
+// + keepExtLooseIntraFronts for the external front.  Non-overlapping entries
+// fill their node's bucket from the front, overlapping ones from the back
+// and are traversed by k_sprout<false>.
+template <int kU>
+__global__ void __launch_bounds__(kThreads) k_balance_scan(FArgs a) {
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
+    const unsigned stride = gridDim.x * blockDim.x;
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[a.out_int_slot] = a.ctr[a.in_int_slot];
-    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < ni + ne; q += gridDim.x * blockDim.x) {
-        if (q < ni) {
-            int2 e = a.in_int[q];
-            float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
-            float4 nlo = ldg4(a.nrec + 2 * e.y), nhi = ldg4(a.nrec + 2 * e.y + 1);
-            if (!overlap(nlo, nhi, plo, phi)) {
-                unsigned pos = a.log.intbeg[e.y] + atomicAdd(a.log.intcnt + e.y, 1u);
+    for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < ni + ne; q0 += kU * stride) {
+        Batch<kU> b;
+        load_batch(a, q0, stride, ni, ni + ne, b);
+#pragma unroll
+        for (int k = 0; k < kU; k++) {
+            if (!b.v[k]) continue;
+            const int2 e = b.e[k];
+            const bool ov = overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k]);
+            if (b.in_int[k]) {
+                unsigned pos = ov ? a.log.intbeg[e.y + 1] - 1u - atomicAdd(a.log.intback + e.y, 1u)
+                                  : a.log.intbeg[e.y] + atomicAdd(a.log.intcnt + e.y, 1u);
                 if (pos < a.cap_int) a.out_int[pos] = e;
-                continue;
+                if (ov) emit_work(a, e);
+            } else if (ov) {
+                emit_pair(a, e.x, prim_face(a, e.x), e.y);
             }
-            unsigned pos = a.log.intbeg[e.y + 1] - 1u - atomicAdd(a.log.intback + e.y, 1u);
-            if (pos < a.cap_int) a.out_int[pos] = e;
-            traverse<false>(a, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, nlo),
-                            __float_as_int(nhi.w));
-        } else {
-            int2 e = a.in_ext[q - ni];
-            float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
-            float4 llo = ldg4(a.lrec + 2 * e.y), lhi = ldg4(a.lrec + 2 * e.y + 1);
-            if (overlap(llo, lhi, plo, phi)) emit_pair(a, e.x, prim_face(a, e.x), e.y);
         }
     }
 }
@@ -396,18 +464,39 @@ __global__ void k_counts64(const unsigned *__restrict__ ctr, unsigned cap_pairs,
     }
 }
 
+unsigned resident_blocks(const void *kernel) {
+    int nb = 0, dev = 0, sms = kSms;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kThreads, 0);
+    return (unsigned)((nb > 0 ? nb : 1) * sms);
+}
+
 }  // namespace
+
+// One resident wave of blocks (blocks per SM at this kernel's occupancy x SM
+// count): the grid-stride kernels then run without a tail wave.
+#define RESIDENT(K) ([]() { static unsigned g_ = 0; if (!g_) g_ = resident_blocks((const void *)(K)); return g_; }())
+// Batched scans come in entry batches of 1, 2 or 4 per thread step.
+#define LAUNCH_U(KERNEL, U, S, ARG)                                                  \
+    do {                                                                             \
+        if ((U) == 1) KERNEL<1><<<RESIDENT(KERNEL<1>), kThreads, 0, S>>>(ARG);       \
+        else if ((U) == 4) KERNEL<4><<<RESIDENT(KERNEL<4>), kThreads, 0, S>>>(ARG);  \
+        else KERNEL<2><<<RESIDENT(KERNEL<2>), kThreads, 0, S>>>(ARG);                \
+        note_launch();                                                               \
+    } while (0)
 
 // ====================================================================== host
 Front::~Front() {
     for (auto &set : front_)
         for (auto &b : set) b.release();
-    DBuf *bufs[] = {&pairs_, &hits_, &outbuf_, &intcnt_, &extcnt_, &intbeg_, &extbeg_, &intback_,
+    DBuf *bufs[] = {&pairs_, &hits_, &outbuf_, &work_, &intcnt_, &extcnt_, &intbeg_, &extbeg_, &intback_,
                     &extback_, &snapshot_, &scratch_, &counts64_};
     for (DBuf *b : bufs) b->release();
 }
 
 bvhcd_status Front::init() {
+    if (const char *u = getenv("BVHCD_FRONT_UNROLL")) unroll_ = atoi(u);
     if (cfg_.int_front_capacity <= 0 || cfg_.ext_front_capacity <= 0 || cfg_.pair_capacity <= 0)
         return BVHCD_INVALID_ARG;
     if (cfg_.int_front_capacity > 0x7fffffffLL || cfg_.ext_front_capacity > 0x7fffffffLL ||
@@ -420,6 +509,7 @@ bvhcd_status Front::init() {
         for (int k = 0; k < 2; k++) FR_TRY(front_[set][k].reserve(sizeof(int2) * (size_t)fcap_[k]));
     FR_TRY(pairs_.reserve(sizeof(int2) * (size_t)pcap_));
     FR_TRY(hits_.reserve(sizeof(int2) * (size_t)pcap_));
+    FR_TRY(work_.reserve(sizeof(int2) * (size_t)fcap_[0]));
     FR_TRY(counts64_.reserve(sizeof(int64_t) * 2));
     return ensure_node_capacity(bvh_->T() > 0 ? bvh_->T() : 1);
 }
@@ -457,7 +547,7 @@ FrontLog Front::log() const {
     return l;
 }
 
-static FArgs make_args(const LBvh *bvh, const FrontLog &log, int cull) {
+static FArgs make_args(const LBvh *bvh, const FrontLog &log, int cull, const DBuf &work, int64_t cap_work) {
     Tree t = bvh->tree();
     FArgs a;
     a.nrec = t.nrec; a.lrec = t.lrec; a.topo = t.topo; a.lca = t.lca; a.sface = t.sface;
@@ -469,6 +559,8 @@ static FArgs make_args(const LBvh *bvh, const FrontLog &log, int cull) {
     a.cap_int = a.cap_ext = 0;
     a.pairs = nullptr;
     a.cap_pairs = 0;
+    a.work = work.as<int2>();
+    a.cap_work = (unsigned)cap_work;
     a.cull = cull;
     a.T = t.T;
     return a;
@@ -497,14 +589,14 @@ bvhcd_status Front::reorder(cudaStream_t s) {
     FrontLog l = log();
     FR_TRY(log_prepare(l, T, scratch_.p, s));
     FR_TRY(log_clear(l, T, s));
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent);
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_, fcap_[0]);
     const int nx = 1 - cur_;
     a.in_int = front_[nx][0].as<int2>(); a.in_ext = front_[nx][1].as<int2>();
     a.out_int = front_[cur_][0].as<int2>(); a.out_ext = front_[cur_][1].as<int2>();
     a.in_int_slot = 2 * nx; a.in_ext_slot = 2 * nx + 1;
     a.out_int_slot = 2 * cur_; a.out_ext_slot = 2 * cur_ + 1;
     a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
-    k_reorder<<<kFrontBlocks, kThreads, 0, s>>>(a); note_launch();
+    k_reorder<<<RESIDENT(k_reorder), kThreads, 0, s>>>(a); note_launch();
     return cuda_status(cudaGetLastError());
 }
 
@@ -513,7 +605,7 @@ bvhcd_status Front::generate(cudaStream_t s, bool pure) {
     const int T = bvh_->T();
     unsigned *ctr = bvh_->counters();
     FrontLog l = log();
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent);
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_, fcap_[0]);
     a.pairs = pairs_.as<int2>();
     a.cap_pairs = (unsigned)pcap_;
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
@@ -568,7 +660,7 @@ bvhcd_status Front::prune_sprout(cudaStream_t s) {
     unsigned *ctr = bvh_->counters();
     FrontLog l = log();
     FR_TRY(log_clear(l, T, s));
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent);
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_, fcap_[0]);
     const int nx = 1 - cur_;
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
     a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
@@ -579,10 +671,12 @@ bvhcd_status Front::prune_sprout(cudaStream_t s) {
     a.cap_pairs = (unsigned)pcap_;
     FR_TRY(cudaMemsetAsync(ctr + 2 * nx, 0, 2 * sizeof(unsigned), s));
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
+    FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
     {
         StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_UPDATE, s);
-        k_maintain_int<<<kFrontBlocks, kThreads, 0, s>>>(a); note_launch();
-        k_maintain_ext<<<kFrontBlocks, kThreads, 0, s>>>(a); note_launch();
+        LAUNCH_U(k_maintain_int_scan, unroll_, s, a);
+        LAUNCH_U(k_maintain_ext, unroll_, s, a);
+        k_sprout<true><<<RESIDENT(k_sprout<true>), kThreads, 0, s>>>(a); note_launch();
     }
     FR_TRY(cudaGetLastError());
     if (bvh_->restr_enabled()) {
@@ -595,14 +689,16 @@ bvhcd_status Front::prune_sprout(cudaStream_t s) {
 bvhcd_status Front::keep(cudaStream_t s) {
     StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_KEEP, s);
     unsigned *ctr = bvh_->counters();
-    FArgs a = make_args(bvh_, log(), cfg_.cull_adjacent);
+    FArgs a = make_args(bvh_, log(), cfg_.cull_adjacent, work_, fcap_[0]);
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
     a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
     a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
     a.pairs = pairs_.as<int2>();
     a.cap_pairs = (unsigned)pcap_;
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
-    k_keep<<<kFrontBlocks, kThreads, 0, s>>>(a); note_launch();
+    FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
+    LAUNCH_U(k_keep_scan, unroll_, s, a);
+    k_sprout<false><<<RESIDENT(k_sprout<false>), kThreads, 0, s>>>(a); note_launch();
     return cuda_status(cudaGetLastError());
 }
 
@@ -615,7 +711,7 @@ bvhcd_status Front::balance(cudaStream_t s) {
     FrontLog l = log();
     FR_TRY(log_prepare(l, T, scratch_.p, s));
     FR_TRY(log_clear(l, T, s));
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent);
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_, fcap_[0]);
     const int nx = 1 - cur_;
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
     a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
@@ -625,7 +721,9 @@ bvhcd_status Front::balance(cudaStream_t s) {
     a.pairs = pairs_.as<int2>();
     a.cap_pairs = (unsigned)pcap_;
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
-    k_balance<<<kFrontBlocks, kThreads, 0, s>>>(a); note_launch();
+    FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
+    LAUNCH_U(k_balance_scan, unroll_, s, a);
+    k_sprout<false><<<RESIDENT(k_sprout<false>), kThreads, 0, s>>>(a); note_launch();
     FR_TRY(cudaGetLastError());
     // swap the internal front buffers of the two sets, keep the external one
     std::swap(front_[0][0], front_[1][0]);
@@ -637,7 +735,7 @@ bvhcd_status Front::narrow(cudaStream_t s) {
     StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_NARROW, s);
     unsigned *ctr = bvh_->counters();
     FR_TRY(cudaMemsetAsync(ctr + C_HITS, 0, sizeof(unsigned), s));
-    k_narrow<<<kFrontBlocks, kThreads, 0, s>>>(pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
+    k_narrow<<<RESIDENT(k_narrow), kThreads, 0, s>>>(pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
                                                (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_); note_launch();
     return cuda_status(cudaGetLastError());
 }

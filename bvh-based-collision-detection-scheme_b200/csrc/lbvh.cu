@@ -79,12 +79,30 @@ __global__ void __launch_bounds__(kThreads) k_box_partial(int T, const int *__re
     }
 }
 
-__global__ void k_box_final(int n, const float *partial, float *scene) {
+__global__ void __launch_bounds__(kThreads) k_box_final(int n, const float *partial, float *scene) {
+    float mn[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+    float mx[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+    for (int q = threadIdx.x; q < n; q += blockDim.x)
+        for (int k = 0; k < 3; k++) {
+            mn[k] = fminf(mn[k], partial[6 * q + k]);
+            mx[k] = fmaxf(mx[k], partial[6 * q + 3 + k]);
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+            mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+        }
+    __shared__ float s[kThreads / 32][6];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+        for (int k = 0; k < 3; k++) { s[w][k] = mn[k]; s[w][3 + k] = mx[k]; }
+    __syncthreads();
     if (threadIdx.x < 6) {
-        float v = threadIdx.x < 3 ? 3.402823466e+38f : -3.402823466e+38f;
-        for (int q = 0; q < n; q++)
-            v = threadIdx.x < 3 ? fminf(v, partial[6 * q + threadIdx.x])
-                                : fmaxf(v, partial[6 * q + threadIdx.x]);
+        float v = s[0][threadIdx.x];
+        for (int q = 1; q < kThreads / 32; q++)
+            v = threadIdx.x < 3 ? fminf(v, s[q][threadIdx.x]) : fmaxf(v, s[q][threadIdx.x]);
         scene[threadIdx.x] = v;
     }
 }
@@ -668,7 +686,7 @@ bvhcd_status LBvh::scene_box(cudaStream_t s) {
     int g = (int)grid_for(T_);
     if (g > 4096) g = 4096;
     k_box_partial<<<g, kThreads, 0, s>>>(T_, fptr_, vptr_, partial_.as<float>()); note_launch();
-    k_box_final<<<1, 32, 0, s>>>(g, partial_.as<float>(), scene_.as<float>()); note_launch();
+    k_box_final<<<1, kThreads, 0, s>>>(g, partial_.as<float>(), scene_.as<float>()); note_launch();
     return cuda_status(cudaGetLastError());
 }
 

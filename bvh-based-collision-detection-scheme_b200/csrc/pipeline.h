@@ -161,10 +161,11 @@ class Front {
     int capT_ = 0;
     int cur_ = 0;  // which buffer set holds the current front
     int last_op_ = -1;
+    int unroll_ = 2;  // entries per thread step in the batched front scans (1, 2 or 4)
     bool has_front_ = false;
     DBuf front_[2][2];  // [set][0 int, 1 ext] int2 entries
     int64_t fcap_[2] = {0, 0};
-    DBuf pairs_, hits_, outbuf_;
+    DBuf pairs_, hits_, outbuf_, work_;
     int64_t pcap_ = 0;
     DBuf intcnt_, extcnt_, intbeg_, extbeg_, intback_, extback_, snapshot_, scratch_, counts64_;
 };
