@@ -52,13 +52,30 @@ struct FArgs {
     int T;
 };
 
+// Per-node counter increment aggregated over the converged lanes of a warp
+// that hit the same node: one atomic per distinct node instead of one per
+// entry.  Nodes near the root sit in the fronts of a large share of all
+// primitives, so unaggregated increments serialise on a few L2 addresses.
+// Returns this lane's rank among the increments of its node (old value +
+// rank within the group).
+__device__ __forceinline__ unsigned node_add(unsigned *cnt, unsigned key, int node) {
+    const unsigned mask = __activemask();
+    const unsigned peers = __match_any_sync(mask, key);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(cnt + node, (unsigned)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
+}
+
 __device__ __forceinline__ void emit_int(const FArgs &a, int prim, int node) {
     emit(a.out_int, a.ctr + a.out_int_slot, a.cap_int, make_int2(prim, node), a.ctr + C_OVERFLOW, 1u);
-    atomicAdd(a.log.intcnt + node, 1u);
+    node_add(a.log.intcnt, (unsigned)node, node);
 }
 __device__ __forceinline__ void emit_ext(const FArgs &a, int prim, int leaf) {
     emit(a.out_ext, a.ctr + a.out_ext_slot, a.cap_ext, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 2u);
-    atomicAdd(a.log.extcnt + leaf, 1u);
+    node_add(a.log.extcnt, (unsigned)leaf, leaf);
 }
 __device__ __forceinline__ void emit_pair(const FArgs &a, int prim, const int4 &pf, int leaf) {
     if (a.cull && covertex(pf, __ldg(&a.sface[leaf]))) return;
@@ -306,8 +323,9 @@ __global__ void __launch_bounds__(kThreads) k_balance_scan(FArgs a) {
             const int2 e = b.e[k];
             const bool ov = overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k]);
             if (b.in_int[k]) {
-                unsigned pos = ov ? a.log.intbeg[e.y + 1] - 1u - atomicAdd(a.log.intback + e.y, 1u)
-                                  : a.log.intbeg[e.y] + atomicAdd(a.log.intcnt + e.y, 1u);
+                const unsigned key = ((unsigned)e.y << 1) | (ov ? 1u : 0u);
+                unsigned pos = ov ? a.log.intbeg[e.y + 1] - 1u - node_add(a.log.intback, key, e.y)
+                                  : a.log.intbeg[e.y] + node_add(a.log.intcnt, key, e.y);
                 if (pos < a.cap_int) a.out_int[pos] = e;
                 if (ov) emit_work(a, e);
             } else if (ov) {
@@ -327,13 +345,14 @@ __global__ void __launch_bounds__(kThreads) k_reorder(FArgs a) {
         a.ctr[a.out_ext_slot] = a.ctr[a.in_ext_slot];
     }
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < ni + ne; q += gridDim.x * blockDim.x) {
-        if (q < ni) {
-            int2 e = a.in_int[q];
-            unsigned pos = a.log.intbeg[e.y] + atomicAdd(a.log.intcnt + e.y, 1u);
+        const bool is_int = q < ni;
+        const int2 e = is_int ? a.in_int[q] : a.in_ext[q - ni];
+        const unsigned key = ((unsigned)e.y << 1) | (is_int ? 0u : 1u);
+        if (is_int) {
+            unsigned pos = a.log.intbeg[e.y] + node_add(a.log.intcnt, key, e.y);
             if (pos < a.cap_int) a.out_int[pos] = e;
         } else {
-            int2 e = a.in_ext[q - ni];
-            unsigned pos = a.log.extbeg[e.y] + atomicAdd(a.log.extcnt + e.y, 1u);
+            unsigned pos = a.log.extbeg[e.y] + node_add(a.log.extcnt, key, e.y);
             if (pos < a.cap_ext) a.out_ext[pos] = e;
         }
     }
