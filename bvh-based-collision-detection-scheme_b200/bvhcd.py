@@ -33,7 +33,7 @@ EXPORTED = [
     "bvhcd_front_create", "bvhcd_front_destroy", "bvhcd_front_maintain", "bvhcd_front_stats_get",
     "bvhcd_front_pairs", "bvhcd_front_device_results", "bvhcd_front_export",
     "bvhcd_schedule_heuristic", "bvhcd_frame", "bvhcd_profile_enable", "bvhcd_profile_read",
-    "bvhcd_launch_count",
+    "bvhcd_launch_count", "bvhcd_morton_order_noalloc",
 ]
 
 STAGES = ["bvh_build", "bvh_refit", "bvh_restructure", "front_generate", "front_update",
@@ -117,6 +117,7 @@ def lib():
             "bvhcd_profile_enable": (ctypes.c_int, [vp, i32]),
             "bvhcd_profile_read": (ctypes.c_int, [vp, vp, vp, i32]),
             "bvhcd_launch_count": (ctypes.c_int, [ctypes.POINTER(i64)]),
+            "bvhcd_morton_order_noalloc": (ctypes.c_int, [vp, vp, i32, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -151,6 +151,11 @@ bvhcd_status bvhcd_profile_read(bvhcd_bvh *bvh, double *ms, int64_t *calls, int3
     return bvh->impl.profiler()->read(ms, calls, reset != 0);
 }
 
+bvhcd_status bvhcd_morton_order_noalloc(const float *pos, const int32_t *faces, int32_t num_faces, uint32_t *codes,
+                                        int32_t *order, void *stream) {
+    return bvhcd::morton_order_noalloc(pos, faces, num_faces, codes, order, as_stream(stream));
+}
+
 // BenchmarkLogic::maintainScheme, STATIC_MANDATORY with divergent marks
 // (Mine/system/Logic/BenchmarkLogic.hpp:102-117): BVH cycle 12
 // (Mine/setting/BvhSettings.h:45), front cycle 6 (Mine/setting/BvttFrontSettings.h:49).

@@ -12,6 +12,7 @@
 #include <climits>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "pipeline.h"
 #include "prims.cuh"
@@ -897,6 +898,68 @@ bvhcd_status LBvh::export_tree(int32_t *inode, float *ibox, int32_t *leaf, float
     DBuf &t = const_cast<DBuf &>(tmp);
     t.release();
     return cuda_status(e);
+}
+
+// ---------------------------------------------------------------- Morton order
+// without allocation.  Same kernels as the build's first half (scene box,
+// Morton codes, stable radix sort), for callers that may not allocate device
+// memory: the temporaries live in one fixed file-scope device array.
+namespace {
+constexpr size_t kNaPartialBytes = 4096 * 6 * sizeof(float);  // box partials, one per block
+constexpr size_t kNaSceneBytes = 256;                          // scene box
+constexpr size_t kNaKeysBytes = sizeof(unsigned) * BVHCD_NOALLOC_MAX_FACES;  // sort ping-pong keys
+constexpr size_t kNaValsBytes = sizeof(int) * BVHCD_NOALLOC_MAX_FACES;       // sort ping-pong values
+constexpr size_t kNaSortBytes = 1u << 20;                      // histograms + scan sums
+constexpr size_t kNaTotal = kNaPartialBytes + kNaSceneBytes + kNaKeysBytes + kNaValsBytes + kNaSortBytes;
+}  // namespace
+
+// Loaded into every device context that uses this library and held there
+// until the process exits (about 9.2 MB).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaTotal];
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[256] = {};
+
+// The symbol's device address for the current device, looked up once per
+// device.  In host code the array's name only stands in for the symbol.
+static cudaError_t noalloc_scratch(unsigned char **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = static_cast<unsigned char *>(g_noalloc_ptr[dev]);
+    return cudaSuccess;
+}
+
+bvhcd_status morton_order_noalloc(const float *verts, const int *faces, int T, unsigned *codes, int *order,
+                                  cudaStream_t s) {
+    if (T < 0 || (T > 0 && (!verts || !faces || !codes || !order))) return BVHCD_INVALID_ARG;
+    if ((int64_t)T > (int64_t)BVHCD_NOALLOC_MAX_FACES || sort_scratch_bytes(T) > kNaSortBytes)
+        return BVHCD_CAPACITY_EXCEEDED;
+    if (T == 0) return BVHCD_OK;
+    unsigned char *base = nullptr;
+    BV_TRY(noalloc_scratch(&base));
+    float *partial = reinterpret_cast<float *>(base);
+    float *scene = reinterpret_cast<float *>(base + kNaPartialBytes);
+    unsigned *keys_alt = reinterpret_cast<unsigned *>(base + kNaPartialBytes + kNaSceneBytes);
+    int *vals_alt = reinterpret_cast<int *>(base + kNaPartialBytes + kNaSceneBytes + kNaKeysBytes);
+    void *sort_scratch = base + kNaPartialBytes + kNaSceneBytes + kNaKeysBytes + kNaValsBytes;
+    // every scratch word read below is written earlier in the same call
+    int g = (int)grid_for(T);
+    if (g > 4096) g = 4096;
+    k_box_partial<<<g, kThreads, 0, s>>>(T, faces, verts, partial); note_launch();
+    k_box_final<<<1, kThreads, 0, s>>>(g, partial, scene); note_launch();
+    k_morton<<<grid_for(T), kThreads, 0, s>>>(T, faces, verts, scene, codes, order); note_launch();
+    BV_TRY(cudaGetLastError());
+    BV_TRY(radix_sort_u32(codes, order, keys_alt, vals_alt, T, 30, sort_scratch, s));
+    return BVHCD_OK;
 }
 
 }  // namespace bvhcd

@@ -38,6 +38,8 @@ struct DBuf {
 };
 
 bvhcd_status cuda_status(cudaError_t e);
+bvhcd_status morton_order_noalloc(const float *verts, const int *faces, int T, unsigned *codes, int *order,
+                                  cudaStream_t s);
 
 // Stage timer: CUDA event pairs recorded on the work stream, resolved when
 // read (the reference's Logger::recordSection, Mine/utility/CudaTimer.hpp:43-53).

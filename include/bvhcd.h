@@ -193,6 +193,28 @@ bvhcd_status bvhcd_profile_read(bvhcd_bvh *bvh, double *ms, int64_t *calls, int3
  * Mine/system/CudaDevice/CudaKernelLauncher.cu:54-69). */
 bvhcd_status bvhcd_launch_count(int64_t *n);
 
+/* ---- Morton order without device allocation.  No counterpart in the
+ * reference.  For callers that may not allocate device memory once they are
+ * running -- a simulator that hands the whole device to its own memory pool,
+ * or a real-time loop in which cudaMalloc's implicit device synchronisation
+ * is not allowed -- this computes what a BVH build starts with: the scene
+ * box, the 30-bit Morton code of every triangle and the stable sort by code.
+ * codes[s] receives the s-th smallest code, order[s] the original triangle
+ * id in Morton slot s (ties keep the original order), the same codes and
+ * order bvhcd_bvh_maintain(BUILD) produces.  All pointers are device
+ * pointers the caller owns; the temporaries live in one fixed device array of
+ * the library (about 9.2 MB, present on every GPU that loads the library
+ * until the process exits), so num_faces is limited to
+ * BVHCD_NOALLOC_MAX_FACES; larger requests return BVHCD_CAPACITY_EXCEEDED
+ * without touching the GPU.  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  Calls share the array: two calls whose work overlaps on
+ * the GPU (different streams, or different host threads) race and must be
+ * serialised by the caller.  Asynchronous on `stream`. */
+#define BVHCD_NOALLOC_MAX_FACES 1048576
+bvhcd_status bvhcd_morton_order_noalloc(const float *pos, const int32_t *faces, int32_t num_faces,
+                                        uint32_t *codes, int32_t *order, void *stream);
+
 /* ---- Scheduler: BenchmarkLogic::maintainScheme, STATIC_MANDATORY with
  * divergent marks (Mine/system/Logic/BenchmarkLogic.hpp:90-156). */
 bvhcd_status bvhcd_schedule_heuristic(int32_t frame, int32_t start_frame, int32_t *bvh_op,
