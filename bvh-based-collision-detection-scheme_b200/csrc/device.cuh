@@ -63,6 +63,8 @@ enum CounterSlot {
                               // bit4 traversal bound hit, bit5 sprout work list
     C_RT_SUBTREES = 7, C_RT_INTNODES = 8,
     C_WORK = 10,              // overlapping internal entries queued for traversal
+    C_PAIRS_VALID = 11,       // broad-phase pairs (C_PAIRS counts reserved slots, holes included)
+    C_COMPACT = 12,           // compaction cursor of the pair export
     C_NUM = 16
 };
 

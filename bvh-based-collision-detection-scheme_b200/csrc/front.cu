@@ -4,8 +4,8 @@
 //
 // Every kernel reads its work size from a device counter and walks it with a
 // grid-stride loop, so a frame is a fixed launch sequence with no host round
-// trip.  Emission reserves slots with one atomic per converged warp group and
-// checks capacity before writing.
+// trip.  Emission reserves output slots in per-thread chunks and checks
+// capacity before writing.
 #include <climits>
 #include <cstdlib>
 
@@ -69,17 +69,63 @@ __device__ __forceinline__ unsigned node_add(unsigned *cnt, unsigned key, int no
     return base + __popc(peers & ((1u << lane) - 1u));
 }
 
-__device__ __forceinline__ void emit_int(const FArgs &a, int prim, int node) {
-    emit(a.out_int, a.ctr + a.out_int_slot, a.cap_int, make_int2(prim, node), a.ctr + C_OVERFLOW, 1u);
+// Output slots are handed out in per-thread chunks: a thread reserves kChunk
+// consecutive slots of a stream with one atomic (shared by the converged
+// lanes that need a chunk at the same time) and fills them as it emits.  The
+// slots it has not filled when it finishes are closed with the hole marker
+// (-1, -1), which every consumer skips.  Without chunks the traversal kernels
+// serialise on the one counter per stream.  The stream counters therefore
+// count reserved slots; true sizes come from the per-node counts (fronts) and
+// from the narrow phase's count of valid pairs.
+constexpr unsigned kChunk = 8;
+struct Chunk {
+    unsigned base = 0, left = 0;
+};
+struct Em {
+    Chunk fi, fe, pr, wk;  // internal front, external front, pairs, sprout work
+};
+
+__device__ __forceinline__ void chunk_put(int2 *buf, unsigned *ctr, unsigned cap, Chunk &c, const int2 &v,
+                                          unsigned *ovf, unsigned bit) {
+    if (c.left == 0) {
+        cg::coalesced_group g = cg::coalesced_threads();
+        unsigned b = 0;
+        if (g.thread_rank() == 0) b = atomicAdd(ctr, kChunk * g.size());
+        c.base = g.shfl(b, 0) + kChunk * g.thread_rank();
+        c.left = kChunk;
+    }
+    const unsigned slot = c.base++;
+    --c.left;
+    if (slot < cap) buf[slot] = v;
+    else atomicOr(ovf, bit);
+}
+__device__ __forceinline__ void chunk_close(int2 *buf, unsigned cap, Chunk &c) {
+    for (; c.left > 0; --c.left) {
+        const unsigned slot = c.base++;
+        if (slot < cap) buf[slot] = make_int2(-1, -1);
+    }
+}
+
+__device__ __forceinline__ void emit_int(const FArgs &a, Em &em, int prim, int node) {
+    chunk_put(a.out_int, a.ctr + a.out_int_slot, a.cap_int, em.fi, make_int2(prim, node), a.ctr + C_OVERFLOW, 1u);
     node_add(a.log.intcnt, (unsigned)node, node);
 }
-__device__ __forceinline__ void emit_ext(const FArgs &a, int prim, int leaf) {
-    emit(a.out_ext, a.ctr + a.out_ext_slot, a.cap_ext, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 2u);
+__device__ __forceinline__ void emit_ext(const FArgs &a, Em &em, int prim, int leaf) {
+    chunk_put(a.out_ext, a.ctr + a.out_ext_slot, a.cap_ext, em.fe, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 2u);
     node_add(a.log.extcnt, (unsigned)leaf, leaf);
 }
-__device__ __forceinline__ void emit_pair(const FArgs &a, int prim, const int4 &pf, int leaf) {
+__device__ __forceinline__ void emit_pair(const FArgs &a, Em &em, int prim, const int4 &pf, int leaf) {
     if (a.cull && covertex(pf, __ldg(&a.sface[leaf]))) return;
-    emit(a.pairs, a.ctr + C_PAIRS, a.cap_pairs, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 4u);
+    chunk_put(a.pairs, a.ctr + C_PAIRS, a.cap_pairs, em.pr, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 4u);
+}
+__device__ __forceinline__ void emit_work(const FArgs &a, Em &em, const int2 &e) {
+    chunk_put(a.work, a.ctr + C_WORK, a.cap_work, em.wk, e, a.ctr + C_OVERFLOW, 32u);
+}
+__device__ __forceinline__ void em_close(const FArgs &a, Em &em) {
+    if (a.out_int) chunk_close(a.out_int, a.cap_int, em.fi);
+    if (a.out_ext) chunk_close(a.out_ext, a.cap_ext, em.fe);
+    if (a.pairs) chunk_close(a.pairs, a.cap_pairs, em.pr);
+    if (a.work) chunk_close(a.work, a.cap_work, em.wk);
 }
 
 // Stackless traversal from tagged node `st` until tagged node `stop`
@@ -92,7 +138,7 @@ __device__ __forceinline__ void emit_pair(const FArgs &a, int prim, const int4 &
 // up to the parent of its leftmost leaf; a node that stops overlapping is a
 // front node and is left through its escape link.
 template <bool kFront>
-__device__ __forceinline__ void traverse(const FArgs &a, int prim, const float4 &plo,
+__device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const float4 &plo,
                                          const float4 &phi, const int4 &pf, int st, int stop) {
     // a valid tree is left after at most 2T - 1 visits; the bound only turns
     // a corrupted tree into an error flag instead of an endless loop
@@ -124,13 +170,13 @@ __device__ __forceinline__ void traverse(const FArgs &a, int prim, const float4 
                 nhi = ldg4(a.nrec + 2 * n + 1);
             }
             if (stopped) {
-                if (kFront) emit_int(a, prim, n);
+                if (kFront) emit_int(a, em, prim, n);
                 st = __float_as_int(nhi.w);
                 continue;
             }
         }
-        if (overlap(llo, lhi, plo, phi)) emit_pair(a, prim, pf, leaf);
-        if (kFront) emit_ext(a, prim, leaf);
+        if (overlap(llo, lhi, plo, phi)) emit_pair(a, em, prim, pf, leaf);
+        if (kFront) emit_ext(a, em, prim, leaf);
         st = __float_as_int(lhi.w);
     }
 }
@@ -150,10 +196,12 @@ __device__ __forceinline__ int4 prim_face(const FArgs &a, int prim) {
 // pureBvhSelfCD (BvhCDKernels.cu:17-49)
 template <bool kFront>
 __global__ void __launch_bounds__(kThreads) k_generate(FArgs a) {
+    Em em;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.T - 1; i += gridDim.x * blockDim.x) {
         float4 plo = ldg4(a.lrec + 2 * i), phi = ldg4(a.lrec + 2 * i + 1);
-        traverse<kFront>(a, i, plo, phi, prim_face(a, i), __float_as_int(phi.w), -1);
+        traverse<kFront>(a, em, i, plo, phi, prim_face(a, i), __float_as_int(phi.w), -1);
     }
+    em_close(a, em);
 }
 
 // Walk up the left chain above node `n` (exclusive) while nodes do not
@@ -210,9 +258,6 @@ __device__ __forceinline__ void load_batch(const FArgs &a, unsigned q0, unsigned
     }
 }
 
-__device__ __forceinline__ void emit_work(const FArgs &a, const int2 &e) {
-    emit(a.work, a.ctr + C_WORK, a.cap_work, e, a.ctr + C_OVERFLOW, 32u);
-}
 
 // Traversal below overlapping internal front nodes (the sprout half of
 // maintainIntLooseIntraFrontsWithLog, BvttFrontPruneSproutKernels.cu:32-56,
@@ -221,20 +266,24 @@ __device__ __forceinline__ void emit_work(const FArgs &a, const int2 &e) {
 // BvttFrontReorderKernels.cu:43-62, without).
 template <bool kFront>
 __global__ void __launch_bounds__(kThreads) k_sprout(FArgs a) {
+    Em em;
     const unsigned n = min(a.ctr[C_WORK], a.cap_work);
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const int2 e = a.work[q];
+        if (e.x < 0) continue;  // hole
         const float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
         const float4 nlo = ldg4(a.nrec + 2 * e.y), nhi = ldg4(a.nrec + 2 * e.y + 1);
-        traverse<kFront>(a, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, nlo),
+        traverse<kFront>(a, em, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, nlo),
                          __float_as_int(nhi.w));
     }
+    em_close(a, em);
 }
 
 // maintainIntLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:12-57):
 // non-overlapping entries are pruned here, overlapping ones go to k_sprout<true>.
 template <int kU>
 __global__ void __launch_bounds__(kThreads) k_maintain_int_scan(FArgs a) {
+    Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned stride = gridDim.x * blockDim.x;
     for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < ni; q0 += kU * stride) {
@@ -244,19 +293,21 @@ __global__ void __launch_bounds__(kThreads) k_maintain_int_scan(FArgs a) {
         for (int k = 0; k < kU; k++) {
             if (!b.v[k]) continue;
             if (overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k])) {
-                emit_work(a, b.e[k]);
+                emit_work(a, em, b.e[k]);
                 continue;
             }
             const int top = __ldg(&a.lca[__float_as_int(b.nlo[k].w)]) >> 1;
             const int m = prune_up(a, b.e[k].y - 1, top, b.plo[k], b.phi[k]);
-            if (m >= 0) emit_int(a, b.e[k].x, m);
+            if (m >= 0) emit_int(a, em, b.e[k].x, m);
         }
     }
+    em_close(a, em);
 }
 
 // maintainExtLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:60-93)
 template <int kU>
 __global__ void __launch_bounds__(kThreads) k_maintain_ext(FArgs a) {
+    Em em;
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     const unsigned stride = gridDim.x * blockDim.x;
     for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < ne; q0 += kU * stride) {
@@ -267,28 +318,30 @@ __global__ void __launch_bounds__(kThreads) k_maintain_ext(FArgs a) {
             if (!b.v[k]) continue;
             const int prim = b.e[k].x, st = b.e[k].y;
             if (overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k])) {
-                emit_ext(a, prim, st);
-                emit_pair(a, prim, prim_face(a, prim), st);
+                emit_ext(a, em, prim, st);
+                emit_pair(a, em, prim, prim_face(a, prim), st);
                 continue;
             }
             const int gfa = __float_as_int(b.nlo[k].w);
             const float4 glo = ldg4(a.nrec + 2 * gfa), ghi = ldg4(a.nrec + 2 * gfa + 1);
             if (overlap(glo, ghi, b.plo[k], b.phi[k])) {
-                emit_ext(a, prim, st);
+                emit_ext(a, em, prim, st);
                 continue;
             }
             const int l = __ldg(&a.lca[st]);
             if (l & 1) continue;  // right child: the parent's left chain handles it
             const int m = prune_up(a, gfa - 1, l >> 1, b.plo[k], b.phi[k]);
-            if (m >= 0) emit_int(a, prim, m);
+            if (m >= 0) emit_int(a, em, prim, m);
         }
     }
+    em_close(a, em);
 }
 
 // keepIntLooseIntraFronts / keepExtLooseIntraFronts (BvttFrontKeepKernels.cu:11-58)
 // in one index space: [0, F_int) internal entries, then external ones.
 template <int kU>
 __global__ void __launch_bounds__(kThreads) k_keep_scan(FArgs a) {
+    Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     const unsigned stride = gridDim.x * blockDim.x;
@@ -298,10 +351,11 @@ __global__ void __launch_bounds__(kThreads) k_keep_scan(FArgs a) {
 #pragma unroll
         for (int k = 0; k < kU; k++) {
             if (!b.v[k] || !overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k])) continue;
-            if (b.in_int[k]) emit_work(a, b.e[k]);
-            else emit_pair(a, b.e[k].x, prim_face(a, b.e[k].x), b.e[k].y);
+            if (b.in_int[k]) emit_work(a, em, b.e[k]);
+            else emit_pair(a, em, b.e[k].x, prim_face(a, b.e[k].x), b.e[k].y);
         }
     }
+    em_close(a, em);
 }
 
 // balance: reorderIntLooseIntraFrontsWithLog (BvttFrontReorderKernels.cu:27-63)
@@ -310,6 +364,7 @@ __global__ void __launch_bounds__(kThreads) k_keep_scan(FArgs a) {
 // and are traversed by k_sprout<false>.
 template <int kU>
 __global__ void __launch_bounds__(kThreads) k_balance_scan(FArgs a) {
+    Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     const unsigned stride = gridDim.x * blockDim.x;
@@ -327,26 +382,29 @@ __global__ void __launch_bounds__(kThreads) k_balance_scan(FArgs a) {
                 unsigned pos = ov ? a.log.intbeg[e.y + 1] - 1u - node_add(a.log.intback, key, e.y)
                                   : a.log.intbeg[e.y] + node_add(a.log.intcnt, key, e.y);
                 if (pos < a.cap_int) a.out_int[pos] = e;
-                if (ov) emit_work(a, e);
+                if (ov) emit_work(a, em, e);
             } else if (ov) {
-                emit_pair(a, e.x, prim_face(a, e.x), e.y);
+                emit_pair(a, em, e.x, prim_face(a, e.x), e.y);
             }
         }
     }
+    em_close(a, em);
 }
 
 // pureReorderLooseFrontsWithLog (BvttFrontReorderKernels.cu:12-24): counting
-// sort scatter of both fronts by node id.
+// sort scatter of both fronts by node id.  Holes left by chunked emission are
+// skipped; the sorted fronts' sizes are the per-node count totals.
 __global__ void __launch_bounds__(kThreads) k_reorder(FArgs a) {
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        a.ctr[a.out_int_slot] = a.ctr[a.in_int_slot];
-        a.ctr[a.out_ext_slot] = a.ctr[a.in_ext_slot];
+        a.ctr[a.out_int_slot] = a.log.intbeg[a.T];
+        a.ctr[a.out_ext_slot] = a.log.extbeg[a.T];
     }
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < ni + ne; q += gridDim.x * blockDim.x) {
         const bool is_int = q < ni;
         const int2 e = is_int ? a.in_int[q] : a.in_ext[q - ni];
+        if (e.x < 0) continue;  // hole
         const unsigned key = ((unsigned)e.y << 1) | (is_int ? 0u : 1u);
         if (is_int) {
             unsigned pos = a.log.intbeg[e.y] + node_add(a.log.intcnt, key, e.y);
@@ -451,34 +509,47 @@ __device__ __forceinline__ v3 vload(const float *v, int i) {
 }
 
 // simpleNarrowPhase (Mine/collision/narrow_phase/narrow_phase.cu:8-24):
-// keeps the pairs whose triangles intersect, as original triangle ids.
+// keeps the pairs whose triangles intersect, as original triangle ids, and
+// counts the valid broad-phase pairs (the pair list has holes).  Without
+// kTest it only counts.
+template <bool kTest>
 __global__ void __launch_bounds__(kThreads) k_narrow(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
                                                      const float *__restrict__ verts, unsigned *ctr,
                                                      unsigned cap_pairs, int2 *hits, unsigned cap_hits) {
     const unsigned n = min(ctr[C_PAIRS], cap_pairs);
+    unsigned valid = 0;
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         int2 p = pairs[q];
+        if (p.x < 0) continue;  // hole
+        ++valid;
+        if (!kTest) continue;
         int4 a = __ldg(&sface[p.x]), b = __ldg(&sface[p.y]);
         if (tritri_sat32(vload(verts, a.x), vload(verts, a.y), vload(verts, a.z), vload(verts, b.x),
                          vload(verts, b.y), vload(verts, b.z)))
             emit(hits, ctr + C_HITS, cap_hits, make_int2(a.w, b.w), ctr + C_OVERFLOW, 8u);
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) valid += __shfl_xor_sync(0xffffffffu, valid, o);
+    if ((threadIdx.x & 31) == 0 && valid) atomicAdd(ctr + C_PAIRS_VALID, valid);
 }
 
-// applyCpResults (BvttFrontLooseIntra.cu:63-67): broad pairs as original ids
+// applyCpResults (BvttFrontLooseIntra.cu:63-67): broad pairs as original ids,
+// compacted past the holes
 __global__ void k_pairs_to_orig(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
-                                const unsigned *__restrict__ ctr, unsigned cap_pairs, int2 *out) {
+                                unsigned *ctr, unsigned cap_pairs, int2 *out) {
     const unsigned n = min(ctr[C_PAIRS], cap_pairs);
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         int2 p = pairs[q];
-        out[q] = make_int2(__ldg(&sface[p.x]).w, __ldg(&sface[p.y]).w);
+        if (p.x < 0) continue;
+        emit(out, ctr + C_COMPACT, cap_pairs, make_int2(__ldg(&sface[p.x]).w, __ldg(&sface[p.y]).w),
+             ctr + C_OVERFLOW, 4u);
     }
 }
 
 __global__ void k_counts64(const unsigned *__restrict__ ctr, unsigned cap_pairs, unsigned cap_hits,
                            int64_t *out) {
     if (threadIdx.x == 0) {
-        out[0] = min(ctr[C_PAIRS], cap_pairs);
+        out[0] = min(ctr[C_PAIRS_VALID], cap_pairs);
         out[1] = min(ctr[C_HITS], cap_hits);
     }
 }
@@ -750,12 +821,20 @@ bvhcd_status Front::balance(cudaStream_t s) {
     return BVHCD_OK;
 }
 
-bvhcd_status Front::narrow(cudaStream_t s) {
+bvhcd_status Front::narrow(cudaStream_t s, bool test) {
     StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_NARROW, s);
     unsigned *ctr = bvh_->counters();
     FR_TRY(cudaMemsetAsync(ctr + C_HITS, 0, sizeof(unsigned), s));
-    k_narrow<<<RESIDENT(k_narrow), kThreads, 0, s>>>(pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
-                                               (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_); note_launch();
+    FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));
+    if (test)
+        k_narrow<true><<<RESIDENT(k_narrow<true>), kThreads, 0, s>>>(
+            pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr, (unsigned)pcap_, hits_.as<int2>(),
+            (unsigned)pcap_);
+    else
+        k_narrow<false><<<RESIDENT(k_narrow<false>), kThreads, 0, s>>>(
+            pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr, (unsigned)pcap_, hits_.as<int2>(),
+            (unsigned)pcap_);
+    note_launch();
     return cuda_status(cudaGetLastError());
 }
 
@@ -831,6 +910,7 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     FR_TRY(cudaMemsetAsync(ctr + C_OVERFLOW, 0, sizeof(unsigned), s));
     if (T < 2) {
         FR_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned) * 6, s));
+        FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));
         last_op_ = run_op;
         if (run_op != BVHCD_FRONT_PURE_BVH_CD) has_front_ = true;
         return BVHCD_OK;
@@ -842,10 +922,8 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     for (int attempt = 0; attempt < 4; attempt++) {
         st = run(run_op, s);
         if (st != BVHCD_OK) return st;
-        if (cfg_.narrow_phase) {
-            st = narrow(s);
-            if (st != BVHCD_OK) return st;
-        }
+        st = narrow(s, cfg_.narrow_phase != 0);  // without the test it only counts the pairs
+        if (st != BVHCD_OK) return st;
         if (!cfg_.auto_grow) break;
         bool ovf = false;
         st = grow_and_check(s, &ovf);
@@ -866,7 +944,7 @@ bvhcd_status Front::stats(bvhcd_front_stats *st, cudaStream_t s) {
     *st = bvhcd_front_stats{};
     st->int_front = h[2 * cur_];
     st->ext_front = h[2 * cur_ + 1];
-    st->broad_pairs = h[C_PAIRS];
+    st->broad_pairs = h[C_PAIRS_VALID];
     st->narrow_hits = h[C_HITS];
     st->overflow = (int32_t)h[C_OVERFLOW];
     st->bvh_opt_tag = bvh_->opt_tag();
@@ -879,24 +957,24 @@ bvhcd_status Front::stats(bvhcd_front_stats *st, cudaStream_t s) {
 
 bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, bool out_dev,
                           cudaStream_t s) {
-    unsigned h[C_NUM];
-    FR_TRY(cudaMemcpyAsync(h, bvh_->counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
-    FR_TRY(cudaStreamSynchronize(s));
-    int64_t n = which ? (int64_t)h[C_HITS] : (int64_t)h[C_PAIRS];
-    if (n > pcap_) n = pcap_;
-    if (count) *count = n;
-    if (!out || cap <= 0) return n > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
-    int64_t m = n < cap ? n : cap;
-    const int2 *src;
-    if (which) {
-        src = hits_.as<int2>();
-    } else {
+    const int2 *src = hits_.as<int2>();
+    if (!which) {
+        // compact the broad pairs past their holes into original ids first
         FR_TRY(outbuf_.reserve(sizeof(int2) * (size_t)(pcap_ > 0 ? pcap_ : 1)));
+        FR_TRY(cudaMemsetAsync(bvh_->counters() + C_COMPACT, 0, sizeof(unsigned), s));
         k_pairs_to_orig<<<kFrontBlocks, kThreads, 0, s>>>(pairs_.as<int2>(), bvh_->tree().sface,
                                                           bvh_->counters(), (unsigned)pcap_, outbuf_.as<int2>()); note_launch();
         FR_TRY(cudaGetLastError());
         src = outbuf_.as<int2>();
     }
+    unsigned h[C_NUM];
+    FR_TRY(cudaMemcpyAsync(h, bvh_->counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaStreamSynchronize(s));
+    int64_t n = which ? (int64_t)h[C_HITS] : (int64_t)h[C_COMPACT];
+    if (n > pcap_) n = pcap_;
+    if (count) *count = n;
+    if (!out || cap <= 0) return n > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
+    int64_t m = n < cap ? n : cap;
     if (m > 0)
         FR_TRY(cudaMemcpyAsync(out, src, sizeof(int2) * (size_t)m,
                                out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));

@@ -152,7 +152,7 @@ class Front {
     bvhcd_status keep(cudaStream_t s);
     bvhcd_status balance(cudaStream_t s);
     bvhcd_status reorder(cudaStream_t s);
-    bvhcd_status narrow(cudaStream_t s);
+    bvhcd_status narrow(cudaStream_t s, bool test);
     bvhcd_status check_quality(cudaStream_t s);
     bvhcd_status snapshot(cudaStream_t s);
     bvhcd_status grow_and_check(cudaStream_t s, bool *overflowed);
@@ -163,7 +163,7 @@ class Front {
     int capT_ = 0;
     int cur_ = 0;  // which buffer set holds the current front
     int last_op_ = -1;
-    int unroll_ = 2;  // entries per thread step in the batched front scans (1, 2 or 4)
+    int unroll_ = 1;  // entries per thread step in the batched front scans (1, 2 or 4)
     bool has_front_ = false;
     DBuf front_[2][2];  // [set][0 int, 1 ext] int2 entries
     int64_t fcap_[2] = {0, 0};
