@@ -235,18 +235,22 @@ struct Batch {
     float4 plo[kU], phi[kU], nlo[kU], nhi[kU];
 };
 
-// loads entries q0 + k*stride (internal ones first in the index space,
-// then external ones) and their primitive and node records
+// entries q0 + k*stride (internal ones first in the index space, then
+// external ones)
 template <int kU>
-__device__ __forceinline__ void load_batch(const FArgs &a, unsigned q0, unsigned stride, unsigned ni,
-                                           unsigned total, Batch<kU> &b) {
+__device__ __forceinline__ void load_ents(const FArgs &a, unsigned q0, unsigned stride, unsigned ni,
+                                          unsigned total, Batch<kU> &b) {
 #pragma unroll
     for (int k = 0; k < kU; k++) {
         const unsigned q = q0 + k * stride;
         b.v[k] = q < total;
         b.in_int[k] = q < ni;
-        b.e[k] = b.v[k] ? (b.in_int[k] ? a.in_int[q] : a.in_ext[q - ni]) : make_int2(0, 0);
+        b.e[k] = b.v[k] ? (b.in_int[k] ? __ldcs(&a.in_int[q]) : __ldcs(&a.in_ext[q - ni])) : make_int2(0, 0);
     }
+}
+// the primitive and node records of the batch's entries
+template <int kU>
+__device__ __forceinline__ void load_recs(const FArgs &a, Batch<kU> &b) {
 #pragma unroll
     for (int k = 0; k < kU; k++) {
         if (!b.v[k]) continue;
@@ -257,6 +261,18 @@ __device__ __forceinline__ void load_batch(const FArgs &a, unsigned q0, unsigned
         b.nhi[k] = ldg4(nb + 2 * b.e[k].y + 1);
     }
 }
+template <int kU>
+__device__ __forceinline__ void take_ents(Batch<kU> &dst, const Batch<kU> &src) {
+#pragma unroll
+    for (int k = 0; k < kU; k++) {
+        dst.e[k] = src.e[k];
+        dst.v[k] = src.v[k];
+        dst.in_int[k] = src.in_int[k];
+    }
+}
+// The scans walk the entry stream software-pipelined: the next batch's
+// entries are requested before the current batch's records, so a step waits
+// for one round trip (the records) instead of two (entries, then records).
 
 
 // Traversal below overlapping internal front nodes (the sprout half of
@@ -286,9 +302,12 @@ __global__ void __launch_bounds__(kThreads) k_maintain_int_scan(FArgs a) {
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned stride = gridDim.x * blockDim.x;
-    for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < ni; q0 += kU * stride) {
-        Batch<kU> b;
-        load_batch(a, q0, stride, ni, ni, b);
+    const unsigned q_start = blockIdx.x * blockDim.x + threadIdx.x;
+    Batch<kU> b, nb;
+    load_ents(a, q_start, stride, ni, ni, b);
+    for (unsigned q0 = q_start; q0 < ni; q0 += kU * stride, take_ents(b, nb)) {
+        load_ents(a, q0 + kU * stride, stride, ni, ni, nb);
+        load_recs(a, b);
 #pragma unroll
         for (int k = 0; k < kU; k++) {
             if (!b.v[k]) continue;
@@ -310,9 +329,12 @@ __global__ void __launch_bounds__(kThreads) k_maintain_ext(FArgs a) {
     Em em;
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     const unsigned stride = gridDim.x * blockDim.x;
-    for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < ne; q0 += kU * stride) {
-        Batch<kU> b;
-        load_batch(a, q0, stride, 0, ne, b);
+    const unsigned q_start = blockIdx.x * blockDim.x + threadIdx.x;
+    Batch<kU> b, nb;
+    load_ents(a, q_start, stride, 0, ne, b);
+    for (unsigned q0 = q_start; q0 < ne; q0 += kU * stride, take_ents(b, nb)) {
+        load_ents(a, q0 + kU * stride, stride, 0, ne, nb);
+        load_recs(a, b);
 #pragma unroll
         for (int k = 0; k < kU; k++) {
             if (!b.v[k]) continue;
@@ -345,9 +367,12 @@ __global__ void __launch_bounds__(kThreads) k_keep_scan(FArgs a) {
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     const unsigned stride = gridDim.x * blockDim.x;
-    for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < ni + ne; q0 += kU * stride) {
-        Batch<kU> b;
-        load_batch(a, q0, stride, ni, ni + ne, b);
+    const unsigned q_start = blockIdx.x * blockDim.x + threadIdx.x;
+    Batch<kU> b, nb;
+    load_ents(a, q_start, stride, ni, ni + ne, b);
+    for (unsigned q0 = q_start; q0 < ni + ne; q0 += kU * stride, take_ents(b, nb)) {
+        load_ents(a, q0 + kU * stride, stride, ni, ni + ne, nb);
+        load_recs(a, b);
 #pragma unroll
         for (int k = 0; k < kU; k++) {
             if (!b.v[k] || !overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k])) continue;
@@ -369,9 +394,12 @@ __global__ void __launch_bounds__(kThreads) k_balance_scan(FArgs a) {
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     const unsigned stride = gridDim.x * blockDim.x;
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[a.out_int_slot] = a.ctr[a.in_int_slot];
-    for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < ni + ne; q0 += kU * stride) {
-        Batch<kU> b;
-        load_batch(a, q0, stride, ni, ni + ne, b);
+    const unsigned q_start = blockIdx.x * blockDim.x + threadIdx.x;
+    Batch<kU> b, nb;
+    load_ents(a, q_start, stride, ni, ni + ne, b);
+    for (unsigned q0 = q_start; q0 < ni + ne; q0 += kU * stride, take_ents(b, nb)) {
+        load_ents(a, q0 + kU * stride, stride, ni, ni + ne, nb);
+        load_recs(a, b);
 #pragma unroll
         for (int k = 0; k < kU; k++) {
             if (!b.v[k]) continue;
@@ -401,9 +429,14 @@ __global__ void __launch_bounds__(kThreads) k_reorder(FArgs a) {
         a.ctr[a.out_int_slot] = a.log.intbeg[a.T];
         a.ctr[a.out_ext_slot] = a.log.extbeg[a.T];
     }
-    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < ni + ne; q += gridDim.x * blockDim.x) {
+    const unsigned stride = gridDim.x * blockDim.x, total = ni + ne;
+    unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+    int2 nxt = q < total ? (q < ni ? __ldcs(&a.in_int[q]) : __ldcs(&a.in_ext[q - ni])) : make_int2(-1, -1);
+    for (; q < total; q += stride) {
         const bool is_int = q < ni;
-        const int2 e = is_int ? a.in_int[q] : a.in_ext[q - ni];
+        const int2 e = nxt;  // prefetched one step ahead
+        const unsigned qn = q + stride;
+        if (qn < total) nxt = qn < ni ? __ldcs(&a.in_int[qn]) : __ldcs(&a.in_ext[qn - ni]);
         if (e.x < 0) continue;  // hole
         const unsigned key = ((unsigned)e.y << 1) | (is_int ? 0u : 1u);
         if (is_int) {
