@@ -17,7 +17,12 @@
  *  - restructure permutes the restructured primitives by the sort
  *    permutation (the reference's updatePrimMap, LBvhRestructureKernels.cu:68-77,
  *    applies its inverse and reads the slot->triangle map while other threads
- *    write it); the broad-phase pair set does not depend on this;
+ *    write it, so that map can stop being a permutation: triangles vanish
+ *    from the leaves and others appear twice).  orc_pipe_set_reference_
+ *    permutation() switches to the reference's update run in thread order,
+ *    which reproduces the reference bit for bit on a restructure that starts
+ *    from a consistent tree; it exists to pin the rest of the restructure
+ *    against the reference and is not what the product computes;
  *  - the narrow phase runs on every frame (the reference skips it on frames
  *    whose BVH was restructured, BvttFrontLooseIntra.cu:84-109).
  */
@@ -222,6 +227,7 @@ static inline int split_metric(unsigned a, unsigned b) {
 /* pipeline state                                                      */
 struct orc_pipe {
     int restr_enabled, cull, narrow_enabled;
+    int ref_perm;             /* restructure permutes as the reference does (test pinning) */
     int T, V, cap;            /* T prims, capacity of per-node arrays */
     const int *faces;         /* borrowed for the frame */
     const float *verts;
@@ -513,22 +519,50 @@ static void orc_restructure(orc_pipe *p) {
         }
     }
     radix_sort_u64(nr, keys, sorted);
-    /* 8: permutation inside each subtree: slot task[k] receives the triangle
-     * that sorts k-th (the reference's updatePrimMap :68-77 applies the
-     * inverse permutation; see the file header). */
-    for (k = 0; k < nr; k++) oldidx[k] = p->lidx[sorted[k]];
-    for (k = 0; k < nr; k++) {
-        int slot = task[k], t = oldidx[k];
-        p->lidx[slot] = t;
-        p->primmap[t] = slot;
-        for (int j = 0; j < 3; j++) p->lvid[3 * slot + j] = p->faces[3 * (size_t)t + j];
-        p->code[slot] = (unsigned)(keys[k] & 0xffffffffu);
+    if (p->ref_perm) {
+        /* 8-9 as the reference runs them under one sequential schedule
+         * (thread index order): updatePrimMap (:68-77) moves the triangle of
+         * slot task[k] to slot sorted[k] -- the inverse of the sort
+         * permutation -- reading the slot->triangle map while it writes it,
+         * so a slot written by an earlier thread is read back already
+         * overwritten and the map stops being a permutation;
+         * updatePrimAndExtNode (:79-120) then writes each triangle's box, and
+         * for restructured slots its vertex ids and Morton code, to
+         * primmap[t] (last writer wins, unwritten slots keep their old
+         * values), and refitIntNode refits the old topology. */
+        for (k = 0; k < nr; k++) {
+            int val = p->lidx[task[k]];
+            p->primmap[val] = sorted[k];
+            p->lidx[sorted[k]] = val;
+        }
+        for (int t = 0; t < T; t++) {
+            int pid = p->primmap[t];
+            tri_box(&p->lbox[pid], p->faces, p->verts, t);
+            if (p->extmark[pid]) {
+                for (int j = 0; j < 3; j++) p->lvid[3 * pid + j] = p->faces[3 * (size_t)t + j];
+                p->code[pid] = morton_of_box(&p->lbox[pid], &p->scene);
+            }
+        }
+        free(keys); free(sorted); free(oldidx);
+        orc_refit_internal(p);
+    } else {
+        /* 8: permutation inside each subtree: slot task[k] receives the
+         * triangle that sorts k-th (the reference's updatePrimMap :68-77
+         * applies the inverse permutation; see the file header). */
+        for (k = 0; k < nr; k++) oldidx[k] = p->lidx[sorted[k]];
+        for (k = 0; k < nr; k++) {
+            int slot = task[k], t = oldidx[k];
+            p->lidx[slot] = t;
+            p->primmap[t] = slot;
+            for (int j = 0; j < 3; j++) p->lvid[3 * slot + j] = p->faces[3 * (size_t)t + j];
+            p->code[slot] = (unsigned)(keys[k] & 0xffffffffu);
+        }
+        free(keys); free(sorted); free(oldidx);
+        /* 9: boxes of every primitive, then refit with the old topology
+         * (updatePrimAndExtNode :79-120, refitIntNode) */
+        orc_refit_leaves(p);
+        orc_refit_internal(p);
     }
-    free(keys); free(sorted); free(oldidx);
-    /* 9: boxes of every primitive, then refit with the old topology
-     * (updatePrimAndExtNode :79-120, refitIntNode) */
-    orc_refit_leaves(p);
-    orc_refit_internal(p);
     /* 10: split metrics and confined rebuild (restrIntNodes :122-166) */
     for (int i = 0; i < T; i++) p->metric[i] = (i != T - 1) ? split_metric(p->code[i], p->code[i + 1]) : 33;
     memset(p->depth, 0, sizeof(unsigned) * (size_t)(T + 1));
@@ -986,6 +1020,8 @@ int orc_pipe_frame(orc_pipe *p, int T, const int *faces, int V, const float *ver
 
 /* Marks subtrees (DFS roots) as degraded exactly as checkFrontQuality does
  * (BvttFrontGenerateKernels.cu:45-47); the next BVH maintain restructures. */
+void orc_pipe_set_reference_permutation(orc_pipe *p, int on) { p->ref_perm = on; }
+
 void orc_pipe_mark_restructure(orc_pipe *p, const int *roots, int n) {
     const int T = p->T;
     if (T < 2) return;

@@ -58,6 +58,9 @@ int orc_pipe_tree(const orc_pipe *p, int *inode, float *ibox, int *leaf,
 int orc_pipe_log(const orc_pipe *p, unsigned *intcnt, unsigned *extcnt,
                  unsigned *intbeg, unsigned *extbeg);
 void orc_set_threads(int n);
+/* Test pinning only: restructure with the reference's own primitive-map
+ * update (LBvhRestructureKernels.cu:68-120) run in thread order. */
+void orc_pipe_set_reference_permutation(orc_pipe *p, int on);
 void orc_pipe_mark_restructure(orc_pipe *p, const int *roots, int n);
 
 /* Standalone stages. */

@@ -54,6 +54,7 @@ def lib():
         L.orc_pipe_log.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_pipe_mark_restructure.argtypes = [ctypes.c_void_p, _i32p, ctypes.c_int]
+        L.orc_pipe_set_reference_permutation.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_scene_box.argtypes = [ctypes.c_int, _i32p, _f32p, _f32p]
         L.orc_morton_codes.argtypes = [ctypes.c_int, _i32p, _f32p, _f32p, _u32p]
         L.orc_brute_pairs.restype = ctypes.c_int64
@@ -141,9 +142,15 @@ def ref_narrow(pairs, faces, pos):
 class Pipeline:
     """CPU restatement of LBvhFixedDeformable + BvttFrontLooseIntra."""
 
-    def __init__(self, restructure=True, cull_adjacent=True, narrow=True):
+    def __init__(self, restructure=True, cull_adjacent=True, narrow=True,
+                 reference_permutation=False):
+        """reference_permutation: restructure with the reference's own
+        primitive-map update run in thread order (test pinning only; see
+        orc_pipe_set_reference_permutation)."""
         self._p = ctypes.c_void_p(lib().orc_pipe_create(int(restructure), int(cull_adjacent),
                                                         int(narrow)))
+        if reference_permutation:
+            lib().orc_pipe_set_reference_permutation(self._p, 1)
 
     def close(self):
         if self._p:

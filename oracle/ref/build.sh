@@ -1,7 +1,10 @@
 #!/bin/sh
-# Builds oracle/_ref/libref_tritri.so from the reference's gProximity header
-# where it lies in the reference tree (default /root/reference; override with
-# REF_ROOT).  Output goes to oracle/_ref/ only.  Skips quietly when the
+# Builds, from the reference's own sources where they lie in the reference
+# tree (default /root/reference; override with REF_ROOT):
+#   oracle/_ref/libref_tritri.so -- the gProximity triangle-pair predicate;
+#   oracle/_ref/ref_emu_driver   -- the reference's collision pipeline as host
+#                                   C++ (Makefile.refemu).
+# Output goes to oracle/_ref/ only.  Skips quietly when the
 # reference tree is absent (the GPU box has only the prebuilt files).
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -17,3 +20,5 @@ CUDA_INC=${CUDA_HOME:-/usr/local/cuda}/include
 g++ -O2 -std=c++17 -fPIC -shared -ffp-contract=off -w \
     -I"$GP" -I"$CUDA_INC" "$HERE/gproximity_tritri.cpp" -o "$OUT/libref_tritri.so"
 echo "built $OUT/libref_tritri.so"
+make -s -j8 -f "$HERE/Makefile.refemu" REF_ROOT="$REF_ROOT"
+echo "built $OUT/ref_emu_driver"

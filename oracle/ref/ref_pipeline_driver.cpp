@@ -1,6 +1,7 @@
-// ref_gpu_driver.cu -- runs the reference's own CUDA pipeline
+// ref_pipeline_driver.cpp -- runs the reference's own pipeline
 // (LBvhFixedDeformable + BvttFrontLooseIntra, compiled unmodified from the
-// reference tree by oracle/ref/Makefile.refgpu) on frames read from a file,
+// reference tree as host C++ with every kernel run one thread at a time by
+// oracle/ref/Makefile.refemu) on frames read from a file,
 // with the reference's STATIC_MANDATORY / divergent-marks schedule
 // (Mine/system/Logic/BenchmarkLogic.hpp:102-117), and writes per frame the
 // broad-phase pair list (applyCpResults) and the tree arrays.  It replaces
@@ -8,9 +9,11 @@
 // (Mine/Frameworks/CudaProject/CudaProjectApp.cpp:26-59, Mine/world/Scene.cpp).
 //
 // TEST INFRASTRUCTURE ONLY: it produces the golden fixtures under
-// tests/golden/ (oracle/ref/make_golden.py) and is never part of the product.
+// tests/golden/ (tests/golden/make_golden.py) and is never part of the product.
 //
 // Input file:  int32 magic 'BVHI', T, V, F; int32 faces[T*3]; float frames[F*V*3]
+// Marks file (optional): per frame int32 n, int32 roots[n] -- subtrees marked
+//   for restructuring just before that frame's BVH maintenance.
 // Output file: per frame: int32 magic 'FRAM', frame, bvh op, front op,
 //   opt tag, npairs, T; int32 pairs[npairs*2] (orig ids as emitted);
 //   int32 leaf_lca[T+1], leaf_par[T], prim_idx[T], prim_map[T];
@@ -30,6 +33,45 @@
 #include "world/Scene.h"
 
 using namespace mn;
+
+// The reference's constructor leaves its restructure scratch vectors empty
+// (Mine/collision/lbvh/LBvhFixedDeformable.cu:44-51 are commented out, "only
+// used in the restructuring scheme") while restructuring is switched on
+// (Mine/setting/CDBenchmarkSettings.h:54), so its first restructure writes
+// through null pointers (calibrateRestrRoots,
+// Mine/collision/lbvh/LBvhRestructureKernels.cu:32).  The driver sizes them
+// as those commented lines state.  They are private members; an explicit
+// instantiation names them, which the language exempts from access checks.
+template <typename Tag, typename Tag::type M>
+struct Expose {
+    friend typename Tag::type member(Tag) { return M; }
+};
+#define EXPOSE(NAME, ELEM)                                                     \
+    struct Tag_##NAME {                                                        \
+        using type = thrust::device_vector<ELEM> LBvhFixedDeformable::*;       \
+        friend type member(Tag_##NAME);                                        \
+    };                                                                         \
+    template struct Expose<Tag_##NAME, &LBvhFixedDeformable::NAME>;
+EXPOSE(d_prevLbds, int)
+EXPOSE(d_prevRbds, int)
+EXPOSE(d_gatherMap, int)
+EXPOSE(d_taskSequence, int)
+EXPOSE(d_sequence, int)
+EXPOSE(d_rtSubtrees, int)
+EXPOSE(d_sizePerSubtree, uint)
+EXPOSE(d_begPerSubtree, int)
+
+static void size_restructure_scratch(LBvhFixedDeformable &b) {
+    const int P = BvhSettings::prim_size(), I = BvhSettings::int_node_size();
+    (b.*member(Tag_d_prevLbds{})).resize(I);
+    (b.*member(Tag_d_prevRbds{})).resize(I);
+    (b.*member(Tag_d_gatherMap{})).resize(P);
+    (b.*member(Tag_d_taskSequence{})).resize(P);
+    (b.*member(Tag_d_sequence{})).resize(P);
+    (b.*member(Tag_d_rtSubtrees{})).resize((size_t)I << 1);
+    (b.*member(Tag_d_sizePerSubtree{})).resize((size_t)I << 1);
+    (b.*member(Tag_d_begPerSubtree{})).resize((size_t)I << 1);
+}
 
 static void schedule(int f, int *b, int *fr) {
     int bb = (f % 12) ? 1 : 0;  // REFIT : BUILD
@@ -55,9 +97,38 @@ static void put(FILE *o, const std::vector<T> &v) {
     if (!v.empty()) fwrite(v.data(), sizeof(T), v.size(), o);
 }
 
+// Marks the subtrees rooted at `roots` (DFS internal-node ids of the current
+// tree) for restructuring through the reference's public BvhRestrLog
+// interface, with the same three updates its quality check makes per
+// flagged node (checkFrontQuality, Mine/collision/bvtt_front/
+// BvttFrontGenerateKernels.cu:44-46) and the same clear-then-tag protocol
+// (BvttFrontLooseIntra::checkQuality, Mine/collision/bvtt_front/
+// BvttFrontLooseIntra.cu:219-228), so that the next maintain() takes the
+// restructure branch (LBvhFixedDeformable::maintain, Mine/collision/lbvh/
+// LBvhFixedDeformable.cu:69-80).
+static void mark_restructure(LBvhFixedDeformable &b, const std::vector<int> &roots) {
+    const int t = (int)b.getPrimNodeSize();
+    if (t < 2 || roots.empty()) return;
+    BvhRestrLog &log = b.restrLog();
+    if (!log.getUpdateTag()) log.clear(t);
+    std::vector<int> ir = dev_copy(log.getIntRange(), (size_t)t);
+    std::vector<int> rr = dev_copy(log.getRestrBvhRoot(), (size_t)t);
+    std::vector<int> lb = dev_copy(b.ctks().getLbds(), (size_t)t - 1);
+    std::vector<int> rb = dev_copy(b.ctks().getRbds(), (size_t)t - 1);
+    for (int i : roots) {
+        if (i < 0 || i >= t - 1) continue;
+        ir[i] += 1;
+        ir[i + rb[i] - lb[i]] -= 1;
+        if (i < rr[lb[i]]) rr[lb[i]] = i;
+    }
+    cudaMemcpy(log.getIntRange(), ir.data(), sizeof(int) * ir.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(log.getRestrBvhRoot(), rr.data(), sizeof(int) * rr.size(), cudaMemcpyHostToDevice);
+    log.setUpdateTag(true);
+}
+
 int main(int argc, char **argv) {
     if (argc < 3) {
-        fprintf(stderr, "usage: %s frames.bin out.bin\n", argv[0]);
+        fprintf(stderr, "usage: %s frames.bin out.bin [marks.bin]\n", argv[0]);
         return 2;
     }
     FILE *in = fopen(argv[1], "rb");
@@ -74,6 +145,19 @@ int main(int argc, char **argv) {
     if (fread(faces.data(), sizeof(int3), T, in) != (size_t)T) return 2;
     if (fread(frames.data(), sizeof(float3), frames.size(), in) != frames.size()) return 2;
     fclose(in);
+    // optional marks file: per frame int32 n, then n int32 subtree roots
+    std::vector<std::vector<int>> marks(F);
+    if (argc > 3) {
+        FILE *mk = fopen(argv[3], "rb");
+        if (!mk) return 2;
+        for (int f = 0; f < F; f++) {
+            int n = 0;
+            if (fread(&n, sizeof(int), 1, mk) != 1 || n < 0) return 2;
+            marks[f].resize(n);
+            if (n && fread(marks[f].data(), sizeof(int), n, mk) != (size_t)n) return 2;
+        }
+        fclose(mk);
+    }
 
     CudaDevice::startup();
     Logger::startup();
@@ -81,6 +165,7 @@ int main(int argc, char **argv) {
         LBvhKernelRegister lbvh_kernels;
         BvttFrontKernelRegister front_kernels;
         auto bvh = std::make_unique<LBvh<ModelType::FixedDeformableType>>(LBvhBuildConfig{});
+        size_restructure_scratch(*bvh);
         auto fl = std::make_unique<BvttFront<BvttFrontType::LooseIntraType>>(
             BvttFrontIntraBuildConfig<LBvh<ModelType::FixedDeformableType>>(
                 bvh.get(), BvttFrontType::LooseIntraType, BvttFrontSettings::ext_front_size(),
@@ -97,6 +182,7 @@ int main(int argc, char **argv) {
             sd.pos.assign(frames.begin() + (size_t)f * V, frames.begin() + (size_t)(f + 1) * V);
             int b, fr;
             schedule(f, &b, &fr);
+            mark_restructure(*bvh, marks[f]);
             bvh->maintain((LBvhFixedDeformableMaintenance)b, sd);
             fl->maintain((BvttFrontLooseIntraMaintenance)fr);
             fl->applyCpResults(d_cnt, d_pairs);
