@@ -33,8 +33,11 @@ EXPORTED = [
     "bvhcd_front_create", "bvhcd_front_destroy", "bvhcd_front_maintain", "bvhcd_front_stats_get",
     "bvhcd_front_pairs", "bvhcd_front_device_results", "bvhcd_front_export",
     "bvhcd_schedule_heuristic", "bvhcd_frame", "bvhcd_profile_enable", "bvhcd_profile_read",
-    "bvhcd_launch_count", "bvhcd_morton_order_noalloc",
+    "bvhcd_launch_count", "bvhcd_morton_order_noalloc", "bvhcd_bvh_set_scenes", "bvhcd_frame_graph",
+    "bvhcd_front_get_shapes", "bvhcd_front_set_shapes", "bvhcd_front_autotune",
 ]
+
+SHAPE_STAGES = ["keep", "prune_int", "prune_ext", "balance", "sprout", "narrow"]
 
 STAGES = ["bvh_build", "bvh_refit", "bvh_restructure", "front_generate", "front_update",
           "front_keep", "front_balance", "front_reorder", "narrow", "quality", "pure_bvh_cd"]
@@ -62,6 +65,13 @@ class Scene(ctypes.Structure):
     _fields_ = [("pos", ctypes.c_void_p), ("faces", ctypes.c_void_p),
                 ("num_vertices", ctypes.c_int32), ("num_faces", ctypes.c_int32),
                 ("on_device", ctypes.c_int32), ("faces_static", ctypes.c_int32)]
+
+
+class LaunchShapes(ctypes.Structure):
+    _fields_ = [("unroll", ctypes.c_int32 * 6), ("block", ctypes.c_int32 * 6)]
+
+    def as_dict(self):
+        return {k: (int(self.unroll[i]), int(self.block[i])) for i, k in enumerate(SHAPE_STAGES)}
 
 
 class FrontStats(ctypes.Structure):
@@ -118,6 +128,11 @@ def lib():
             "bvhcd_profile_read": (ctypes.c_int, [vp, vp, vp, i32]),
             "bvhcd_launch_count": (ctypes.c_int, [ctypes.POINTER(i64)]),
             "bvhcd_morton_order_noalloc": (ctypes.c_int, [vp, vp, i32, vp, vp, vp]),
+            "bvhcd_bvh_set_scenes": (ctypes.c_int, [vp, i32, vp]),
+            "bvhcd_frame_graph": (ctypes.c_int, [vp, vp, ctypes.POINTER(Scene), i32, i32, vp]),
+            "bvhcd_front_get_shapes": (ctypes.c_int, [vp, ctypes.POINTER(LaunchShapes)]),
+            "bvhcd_front_set_shapes": (ctypes.c_int, [vp, ctypes.POINTER(LaunchShapes)]),
+            "bvhcd_front_autotune": (ctypes.c_int, [vp, i32, ctypes.POINTER(LaunchShapes), vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -241,6 +256,14 @@ class LBvh:
         _check(lib().bvhcd_bvh_opt_tag(self._h, ctypes.byref(t)), "opt tag")
         return t.value
 
+    def set_scenes(self, tri_offsets):
+        """Batched scenes: scene s owns triangles [tri_offsets[s], tri_offsets[s+1])
+        of every scene passed to maintain; each gets its own tree and no pair
+        crosses scenes (bvhcd_bvh_set_scenes)."""
+        off = np.ascontiguousarray(tri_offsets, dtype=np.int32)
+        _check(lib().bvhcd_bvh_set_scenes(self._h, off.size - 1, off.ctypes.data), "set scenes")
+        self._offsets = off
+
     def request_restructure(self, roots, stream=None):
         """Mark subtrees (DFS ids) as degraded; the next maintain restructures."""
         r = np.ascontiguousarray(roots, dtype=np.int32)
@@ -248,10 +271,9 @@ class LBvh:
                "request restructure")
 
     def export(self, stream=None):
-        T = self.sizes()[0]
-        I = max(T - 1, 0)
-        inode = np.zeros((max(I, 1), 6), np.int32)
-        ibox = np.zeros((max(I, 1), 6), np.float32)
+        T, _, I = self.sizes()
+        inode = np.zeros((max(T - 1, 1), 6), np.int32)
+        ibox = np.zeros((max(T - 1, 1), 6), np.float32)
         leaf = np.zeros((max(T, 1), 4), np.int32)
         lbox = np.zeros((max(T, 1), 6), np.float32)
         lca = np.zeros(T + 1, np.int32)
@@ -322,6 +344,30 @@ class BvttFront:
                                         _stream_ptr(stream)), "front export")
         return out[:n.value]
 
+    def shapes(self) -> dict:
+        """Launch shape per front stage: {stage: (entries per thread step, threads per block)}."""
+        sh = LaunchShapes()
+        _check(lib().bvhcd_front_get_shapes(self._h, ctypes.byref(sh)), "get shapes")
+        return sh.as_dict()
+
+    def set_shapes(self, shapes: dict):
+        sh = LaunchShapes()
+        cur = self.shapes()
+        cur.update(shapes)
+        for i, k in enumerate(SHAPE_STAGES):
+            sh.unroll[i], sh.block[i] = cur[k]
+        _check(lib().bvhcd_front_set_shapes(self._h, ctypes.byref(sh)), "set shapes")
+
+    def autotune(self, repeats: int = 3, stream=None):
+        """Times every candidate launch shape of every front stage on the
+        current front and keeps the fastest (bvhcd_front_autotune).  Returns
+        ({stage: shape}, {stage: best mean ms per run})."""
+        sh = LaunchShapes()
+        best = np.zeros(6, np.float64)
+        _check(lib().bvhcd_front_autotune(self._h, int(repeats), ctypes.byref(sh), best.ctypes.data,
+                                          _stream_ptr(stream)), "autotune")
+        return sh.as_dict(), {k: float(best[i]) for i, k in enumerate(SHAPE_STAGES)}
+
     def device_results(self):
         hits, counts = ctypes.c_void_p(), ctypes.c_void_p()
         _check(lib().bvhcd_front_device_results(self._h, ctypes.byref(hits), ctypes.byref(counts)),
@@ -334,4 +380,15 @@ def frame(bvh: LBvh, front: BvttFront, f: int, start: int, pos, faces, stream=No
     sc, keep = _scene(pos, faces, faces_static)
     _check(lib().bvhcd_frame(bvh.handle, front.handle, int(f), int(start), ctypes.byref(sc),
                              _stream_ptr(stream)), "frame")
+    bvh._keep = keep
+
+
+def frame_graph(bvh: LBvh, front: BvttFront, pos, faces, bvh_op: int, front_op: int, stream=None):
+    """One frame through bvhcd_frame_graph: captured as a CUDA graph on first
+    use of its key, replayed afterwards.  pos / faces are CUDA tensors whose
+    storage stays the same from call to call (write each frame's positions
+    into `pos` in place)."""
+    sc, keep = _scene(pos, faces, True)
+    _check(lib().bvhcd_frame_graph(bvh.handle, front.handle, ctypes.byref(sc), int(bvh_op), int(front_op),
+                                   _stream_ptr(stream)), "frame graph")
     bvh._keep = keep

@@ -1,19 +1,54 @@
 // capi.cu -- extern "C" entry points declared in include/bvhcd.h.
 #include <new>
 
+#include <vector>
+
 #include "pipeline.h"
+#include "prims.cuh"
 
 struct bvhcd_bvh {
     bvhcd::LBvh impl;
     explicit bvhcd_bvh(const bvhcd_bvh_config &c) : impl(c) {}
 };
+// A frame (BVH op + front op) captured as a CUDA graph, keyed by the ops and
+// by the host state the frame starts from; `after` is the host state its
+// capture ended with, restored after every replay.
+struct FrameGraph {
+    int bvh_op, front_op;
+    bvhcd::LBvh::HostState bvh_before, bvh_after;
+    bvhcd::Front::HostState front_before, front_after;
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;
+};
+
 struct bvhcd_front {
     bvhcd::Front impl;
+    // graph-launched frames (bvhcd_frame_graph)
+    std::vector<FrameGraph> graphs;
+    const float *g_pos = nullptr;
+    const int32_t *g_faces = nullptr;
+    int g_T = -1, g_V = -1, g_scenes = -1, g_shapes = -1;  // layout / launch-shape epochs
+    bool g_warm = false;
     bvhcd_front(bvhcd::LBvh *b, const bvhcd_front_config &c) : impl(b, c) {}
+    ~bvhcd_front() { drop_graphs(); }
+    void drop_graphs() {
+        for (FrameGraph &g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+        g_warm = false;
+    }
 };
 
 namespace {
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+bool same_state(const bvhcd::LBvh::HostState &a, const bvhcd::LBvh::HostState &b) {
+    return a.T == b.T && a.V == b.V && a.opt_tag == b.opt_tag && a.built == b.built && a.updated == b.updated &&
+           a.vptr == b.vptr && a.fptr == b.fptr;
+}
+bool same_state(const bvhcd::Front::HostState &a, const bvhcd::Front::HostState &b) {
+    return a.cur == b.cur && a.last_op == b.last_op && a.has_front == b.has_front && a.int_swapped == b.int_swapped;
+}
 }  // namespace
 
 extern "C" {
@@ -70,10 +105,16 @@ bvhcd_status bvhcd_bvh_maintain(bvhcd_bvh *bvh, bvhcd_bvh_op op, const bvhcd_sce
 bvhcd_status bvhcd_bvh_sizes(const bvhcd_bvh *bvh, int32_t *prims, int32_t *ext_nodes, int32_t *int_nodes) {
     if (!bvh) return BVHCD_INVALID_ARG;
     int T = bvh->impl.T();
+    int S = bvh->impl.num_scenes();
     if (prims) *prims = T;
     if (ext_nodes) *ext_nodes = T;
-    if (int_nodes) *int_nodes = T > 0 ? T - 1 : 0;
+    if (int_nodes) *int_nodes = T >= S ? T - S : 0;
     return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_bvh_set_scenes(bvhcd_bvh *bvh, int32_t num_scenes, const int32_t *tri_offsets) {
+    if (!bvh) return BVHCD_INVALID_ARG;
+    return bvh->impl.set_scenes(num_scenes, tri_offsets);
 }
 
 bvhcd_status bvhcd_bvh_opt_tag(const bvhcd_bvh *bvh, int32_t *tag) {
@@ -182,6 +223,106 @@ bvhcd_status bvhcd_frame(bvhcd_bvh *bvh, bvhcd_front *front, int32_t frame, int3
     st = bvhcd_bvh_maintain(bvh, (bvhcd_bvh_op)b, scene, stream);
     if (st != BVHCD_OK) return st;
     return bvhcd_front_maintain(front, (bvhcd_front_op)f, stream);
+}
+
+bvhcd_status bvhcd_front_get_shapes(const bvhcd_front *front, bvhcd_launch_shapes *shapes) {
+    if (!front || !shapes) return BVHCD_INVALID_ARG;
+    front->impl.get_shapes(shapes);
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_front_set_shapes(bvhcd_front *front, const bvhcd_launch_shapes *shapes) {
+    if (!front || !shapes) return BVHCD_INVALID_ARG;
+    return front->impl.set_shapes(*shapes);
+}
+
+bvhcd_status bvhcd_front_autotune(bvhcd_front *front, int32_t repeats, bvhcd_launch_shapes *chosen,
+                                  double *best_ms, void *stream) {
+    if (!front) return BVHCD_INVALID_ARG;
+    return front->impl.autotune(repeats, chosen, best_ms, as_stream(stream));
+}
+
+bvhcd_status bvhcd_frame_graph(bvhcd_bvh *bvh, bvhcd_front *front, const bvhcd_scene *scene, int32_t bvh_op,
+                               int32_t front_op, void *stream) {
+    if (!bvh || !front || !scene || !stream) return BVHCD_INVALID_ARG;
+    if (&bvh->impl != front->impl.bvh()) return BVHCD_INVALID_ARG;
+    if (!scene->on_device || bvh->impl.restr_enabled() || front->impl.auto_grow()) return BVHCD_INVALID_ARG;
+    if (bvh_op < BVHCD_BVH_BUILD || bvh_op > BVHCD_BVH_UPDATE) return BVHCD_INVALID_ARG;
+    if (front_op < BVHCD_FRONT_PURE_BVH_CD || front_op > BVHCD_FRONT_RESTRUCTURE) return BVHCD_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    if (scene->pos != front->g_pos || scene->faces != front->g_faces || scene->num_faces != front->g_T ||
+        scene->num_vertices != front->g_V || bvh->impl.layout_epoch() != front->g_scenes ||
+        front->impl.shape_epoch() != front->g_shapes) {
+        front->drop_graphs();
+        front->g_pos = scene->pos;
+        front->g_faces = scene->faces;
+        front->g_T = scene->num_faces;
+        front->g_V = scene->num_vertices;
+        front->g_scenes = bvh->impl.layout_epoch();
+        front->g_shapes = front->impl.shape_epoch();
+    }
+    bvhcd_status st;
+    if (!front->g_warm) {
+        // the first frame runs as ordinary launches: it sizes every buffer,
+        // so no capture ever allocates
+        st = bvh->impl.maintain((bvhcd_bvh_op)bvh_op, *scene, s);
+        if (st == BVHCD_OK) st = front->impl.maintain((bvhcd_front_op)front_op, s);
+        if (st == BVHCD_OK) front->g_warm = true;
+        return st;
+    }
+    const bvhcd::LBvh::HostState hb = bvh->impl.host_state();
+    const bvhcd::Front::HostState hf = front->impl.host_state();
+    for (FrameGraph &g : front->graphs) {
+        if (g.bvh_op != bvh_op || g.front_op != front_op || !same_state(g.bvh_before, hb) ||
+            !same_state(g.front_before, hf))
+            continue;
+        cudaError_t e = cudaGraphLaunch(g.exec, s);
+        if (e != cudaSuccess) return bvhcd::cuda_status(e);
+        bvh->impl.set_host_state(g.bvh_after);
+        front->impl.set_host_state(g.front_after);
+        for (long long k = 0; k < g.launches; k++) bvhcd::note_launch();
+        return BVHCD_OK;
+    }
+    // capture this frame, then launch it (capturing runs only the host side)
+    bvhcd::Profiler *prof = bvh->impl.profiler();
+    const bool prof_on = prof->on;
+    prof->on = false;
+    const long long n0 = bvhcd::launch_count();
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        prof->on = prof_on;
+        return bvhcd::cuda_status(e);
+    }
+    st = bvh->impl.maintain((bvhcd_bvh_op)bvh_op, *scene, s);
+    if (st == BVHCD_OK) st = front->impl.maintain((bvhcd_front_op)front_op, s);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(s, &graph);
+    prof->on = prof_on;
+    if (st != BVHCD_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        bvh->impl.set_host_state(hb);
+        front->impl.set_host_state(hf);
+        return st != BVHCD_OK ? st : bvhcd::cuda_status(e);
+    }
+    FrameGraph g;
+    g.bvh_op = bvh_op;
+    g.front_op = front_op;
+    g.bvh_before = hb;
+    g.front_before = hf;
+    g.bvh_after = bvh->impl.host_state();
+    g.front_after = front->impl.host_state();
+    g.launches = bvhcd::launch_count() - n0;
+    e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e == cudaSuccess) e = cudaGraphLaunch(g.exec, s);
+    if (e != cudaSuccess) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        bvh->impl.set_host_state(hb);
+        front->impl.set_host_state(hf);
+        return bvhcd::cuda_status(e);
+    }
+    front->graphs.push_back(g);
+    return BVHCD_OK;
 }
 
 }  // extern "C"

@@ -214,9 +214,13 @@ __device__ __forceinline__ int prune_up(const FArgs &a, int n, int top, const fl
         if (overlap(lo, hi, plo, phi)) break;
     }
     if (n < top && n + 1 > 0) {
+        // the chain top's parent decides, unless the top is a root (node 0,
+        // or the root of one scene of a forest)
         int p = __ldg(&a.topo[n + 1]).z;
-        float4 lo = ldg4(a.nrec + 2 * p), hi = ldg4(a.nrec + 2 * p + 1);
-        if (!overlap(lo, hi, plo, phi)) return -1;
+        if (p >= 0) {
+            float4 lo = ldg4(a.nrec + 2 * p), hi = ldg4(a.nrec + 2 * p + 1);
+            if (!overlap(lo, hi, plo, phi)) return -1;
+        }
     }
     return n + 1;
 }
@@ -280,8 +284,8 @@ __device__ __forceinline__ void take_ents(Batch<kU> &dst, const Batch<kU> &src) 
 // with kFront; keepIntLooseIntraFronts, BvttFrontKeepKernels.cu:21-42, and the
 // overlap half of reorderIntLooseIntraFrontsWithLog,
 // BvttFrontReorderKernels.cu:43-62, without).
-template <bool kFront>
-__global__ void __launch_bounds__(kThreads) k_sprout(FArgs a) {
+template <bool kFront, int kB>
+__global__ void __launch_bounds__(kB) k_sprout(FArgs a) {
     Em em;
     const unsigned n = min(a.ctr[C_WORK], a.cap_work);
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -297,8 +301,8 @@ __global__ void __launch_bounds__(kThreads) k_sprout(FArgs a) {
 
 // maintainIntLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:12-57):
 // non-overlapping entries are pruned here, overlapping ones go to k_sprout<true>.
-template <int kU>
-__global__ void __launch_bounds__(kThreads) k_maintain_int_scan(FArgs a) {
+template <int kU, int kB>
+__global__ void __launch_bounds__(kB) k_maintain_int_scan(FArgs a) {
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned stride = gridDim.x * blockDim.x;
@@ -324,8 +328,8 @@ __global__ void __launch_bounds__(kThreads) k_maintain_int_scan(FArgs a) {
 }
 
 // maintainExtLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:60-93)
-template <int kU>
-__global__ void __launch_bounds__(kThreads) k_maintain_ext(FArgs a) {
+template <int kU, int kB>
+__global__ void __launch_bounds__(kB) k_maintain_ext(FArgs a) {
     Em em;
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     const unsigned stride = gridDim.x * blockDim.x;
@@ -361,8 +365,8 @@ __global__ void __launch_bounds__(kThreads) k_maintain_ext(FArgs a) {
 
 // keepIntLooseIntraFronts / keepExtLooseIntraFronts (BvttFrontKeepKernels.cu:11-58)
 // in one index space: [0, F_int) internal entries, then external ones.
-template <int kU>
-__global__ void __launch_bounds__(kThreads) k_keep_scan(FArgs a) {
+template <int kU, int kB>
+__global__ void __launch_bounds__(kB) k_keep_scan(FArgs a) {
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
@@ -387,8 +391,8 @@ __global__ void __launch_bounds__(kThreads) k_keep_scan(FArgs a) {
 // + keepExtLooseIntraFronts for the external front.  Non-overlapping entries
 // fill their node's bucket from the front, overlapping ones from the back
 // and are traversed by k_sprout<false>.
-template <int kU>
-__global__ void __launch_bounds__(kThreads) k_balance_scan(FArgs a) {
+template <int kU, int kB>
+__global__ void __launch_bounds__(kB) k_balance_scan(FArgs a) {
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
@@ -545,8 +549,8 @@ __device__ __forceinline__ v3 vload(const float *v, int i) {
 // keeps the pairs whose triangles intersect, as original triangle ids, and
 // counts the valid broad-phase pairs (the pair list has holes).  Without
 // kTest it only counts.
-template <bool kTest>
-__global__ void __launch_bounds__(kThreads) k_narrow(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
+template <bool kTest, int kB>
+__global__ void __launch_bounds__(kB) k_narrow(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
                                                      const float *__restrict__ verts, unsigned *ctr,
                                                      unsigned cap_pairs, int2 *hits, unsigned cap_hits) {
     const unsigned n = min(ctr[C_PAIRS], cap_pairs);
@@ -587,11 +591,11 @@ __global__ void k_counts64(const unsigned *__restrict__ ctr, unsigned cap_pairs,
     }
 }
 
-unsigned resident_blocks(const void *kernel) {
+unsigned resident_blocks(const void *kernel, int block = kThreads) {
     int nb = 0, dev = 0, sms = kSms;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, 0);
     return (unsigned)((nb > 0 ? nb : 1) * sms);
 }
 
@@ -600,13 +604,32 @@ unsigned resident_blocks(const void *kernel) {
 // One resident wave of blocks (blocks per SM at this kernel's occupancy x SM
 // count): the grid-stride kernels then run without a tail wave.
 #define RESIDENT(K) ([]() { static unsigned g_ = 0; if (!g_) g_ = resident_blocks((const void *)(K)); return g_; }())
-// Batched scans come in entry batches of 1, 2 or 4 per thread step.
-#define LAUNCH_U(KERNEL, U, S, ARG)                                                  \
-    do {                                                                             \
-        if ((U) == 1) KERNEL<1><<<RESIDENT(KERNEL<1>), kThreads, 0, S>>>(ARG);       \
-        else if ((U) == 4) KERNEL<4><<<RESIDENT(KERNEL<4>), kThreads, 0, S>>>(ARG);  \
-        else KERNEL<2><<<RESIDENT(KERNEL<2>), kThreads, 0, S>>>(ARG);                \
-        note_launch();                                                               \
+#define RESIDENT_B(K, B) \
+    ([]() { static unsigned g_ = 0; if (!g_) g_ = resident_blocks((const void *)(K), B); return g_; }())
+// Front scans in a launch shape: entries per thread step (1, 2, 4) x threads
+// per block (128, 256, 512).
+#define SCAN_AT(KERNEL, U, B, S, ARG) KERNEL<U, B><<<RESIDENT_B((KERNEL<U, B>), B), B, 0, S>>>(ARG)
+#define SCAN_U(KERNEL, U, B, S, ARG)                 \
+    do {                                             \
+        if ((U) == 1) SCAN_AT(KERNEL, 1, B, S, ARG); \
+        else if ((U) == 4) SCAN_AT(KERNEL, 4, B, S, ARG); \
+        else SCAN_AT(KERNEL, 2, B, S, ARG);          \
+    } while (0)
+#define LAUNCH_SCAN(KERNEL, SH, S, ARG)                            \
+    do {                                                           \
+        if ((SH).b == 128) SCAN_U(KERNEL, (SH).u, 128, S, ARG);      \
+        else if ((SH).b == 512) SCAN_U(KERNEL, (SH).u, 512, S, ARG); \
+        else SCAN_U(KERNEL, (SH).u, 256, S, ARG);                    \
+        note_launch();                                             \
+    } while (0)
+// Per-item kernels (sprout, narrow phase) in a block size.
+#define ITEM_AT(KERNEL, F, B, S, ...) KERNEL<F, B><<<RESIDENT_B((KERNEL<F, B>), B), B, 0, S>>>(__VA_ARGS__)
+#define LAUNCH_ITEM(KERNEL, F, SH, S, ...)                                \
+    do {                                                                  \
+        if ((SH).b == 128) ITEM_AT(KERNEL, F, 128, S, __VA_ARGS__);         \
+        else if ((SH).b == 512) ITEM_AT(KERNEL, F, 512, S, __VA_ARGS__);    \
+        else ITEM_AT(KERNEL, F, 256, S, __VA_ARGS__);                       \
+        note_launch();                                                    \
     } while (0)
 
 // ====================================================================== host
@@ -619,7 +642,11 @@ Front::~Front() {
 }
 
 bvhcd_status Front::init() {
-    if (const char *u = getenv("BVHCD_FRONT_UNROLL")) unroll_ = atoi(u);
+    if (const char *u = getenv("BVHCD_FRONT_UNROLL")) {
+        const int v = atoi(u);
+        for (int k = 0; k < BVHCD_SHAPE_COUNT; k++)
+            if (v == 1 || v == 2 || v == 4) shape_[k].u = v;
+    }
     if (cfg_.int_front_capacity <= 0 || cfg_.ext_front_capacity <= 0 || cfg_.pair_capacity <= 0)
         return BVHCD_INVALID_ARG;
     if (cfg_.int_front_capacity > 0x7fffffffLL || cfg_.ext_front_capacity > 0x7fffffffLL ||
@@ -670,7 +697,10 @@ FrontLog Front::log() const {
     return l;
 }
 
-static FArgs make_args(const LBvh *bvh, const FrontLog &log, int cull, const DBuf &work, int64_t cap_work) {
+// The work list's capacity is what its buffer holds, never a front capacity
+// that may have grown past it.
+static FArgs make_args(const LBvh *bvh, const FrontLog &log, int cull, const DBuf &work) {
+    const int64_t cap_work = (int64_t)(work.bytes / sizeof(int2));
     Tree t = bvh->tree();
     FArgs a;
     a.nrec = t.nrec; a.lrec = t.lrec; a.topo = t.topo; a.lca = t.lca; a.sface = t.sface;
@@ -683,7 +713,7 @@ static FArgs make_args(const LBvh *bvh, const FrontLog &log, int cull, const DBu
     a.pairs = nullptr;
     a.cap_pairs = 0;
     a.work = work.as<int2>();
-    a.cap_work = (unsigned)cap_work;
+    a.cap_work = (unsigned)(cap_work < 0xffffffffLL ? cap_work : 0xffffffffLL);
     a.cull = cull;
     a.T = t.T;
     return a;
@@ -712,7 +742,7 @@ bvhcd_status Front::reorder(cudaStream_t s) {
     FrontLog l = log();
     FR_TRY(log_prepare(l, T, scratch_.p, s));
     FR_TRY(log_clear(l, T, s));
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_, fcap_[0]);
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_);
     const int nx = 1 - cur_;
     a.in_int = front_[nx][0].as<int2>(); a.in_ext = front_[nx][1].as<int2>();
     a.out_int = front_[cur_][0].as<int2>(); a.out_ext = front_[cur_][1].as<int2>();
@@ -728,7 +758,7 @@ bvhcd_status Front::generate(cudaStream_t s, bool pure) {
     const int T = bvh_->T();
     unsigned *ctr = bvh_->counters();
     FrontLog l = log();
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_, fcap_[0]);
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_);
     a.pairs = pairs_.as<int2>();
     a.cap_pairs = (unsigned)pcap_;
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
@@ -777,13 +807,15 @@ bvhcd_status Front::check_quality(cudaStream_t s) {
     return BVHCD_OK;
 }
 
-// pruneSprout (BvttFrontLooseIntra.cu:254-283)
-bvhcd_status Front::prune_sprout(cudaStream_t s) {
+// pruneSprout (BvttFrontLooseIntra.cu:254-283): the update kernels write the
+// new front into the other buffer set, then the quality check and the
+// reorder back.
+bvhcd_status Front::update_kernels(cudaStream_t s) {
     const int T = bvh_->T();
     unsigned *ctr = bvh_->counters();
     FrontLog l = log();
     FR_TRY(log_clear(l, T, s));
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_, fcap_[0]);
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_);
     const int nx = 1 - cur_;
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
     a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
@@ -797,13 +829,18 @@ bvhcd_status Front::prune_sprout(cudaStream_t s) {
     FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
     {
         StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_UPDATE, s);
-        LAUNCH_U(k_maintain_int_scan, unroll_, s, a);
-        LAUNCH_U(k_maintain_ext, unroll_, s, a);
-        k_sprout<true><<<RESIDENT(k_sprout<true>), kThreads, 0, s>>>(a); note_launch();
+        LAUNCH_SCAN(k_maintain_int_scan, shape_[BVHCD_SHAPE_PRUNE_INT], s, a);
+        LAUNCH_SCAN(k_maintain_ext, shape_[BVHCD_SHAPE_PRUNE_EXT], s, a);
+        LAUNCH_ITEM(k_sprout, true, shape_[BVHCD_SHAPE_SPROUT], s, a);
     }
-    FR_TRY(cudaGetLastError());
+    return cuda_status(cudaGetLastError());
+}
+
+bvhcd_status Front::prune_sprout(cudaStream_t s) {
+    bvhcd_status st = update_kernels(s);
+    if (st != BVHCD_OK) return st;
     if (bvh_->restr_enabled()) {
-        bvhcd_status st = check_quality(s);
+        st = check_quality(s);
         if (st != BVHCD_OK) return st;
     }
     return reorder(s);
@@ -812,7 +849,7 @@ bvhcd_status Front::prune_sprout(cudaStream_t s) {
 bvhcd_status Front::keep(cudaStream_t s) {
     StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_KEEP, s);
     unsigned *ctr = bvh_->counters();
-    FArgs a = make_args(bvh_, log(), cfg_.cull_adjacent, work_, fcap_[0]);
+    FArgs a = make_args(bvh_, log(), cfg_.cull_adjacent, work_);
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
     a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
     a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
@@ -820,21 +857,20 @@ bvhcd_status Front::keep(cudaStream_t s) {
     a.cap_pairs = (unsigned)pcap_;
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
     FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
-    LAUNCH_U(k_keep_scan, unroll_, s, a);
-    k_sprout<false><<<RESIDENT(k_sprout<false>), kThreads, 0, s>>>(a); note_launch();
+    LAUNCH_SCAN(k_keep_scan, shape_[BVHCD_SHAPE_KEEP], s, a);
+    LAUNCH_ITEM(k_sprout, false, shape_[BVHCD_SHAPE_SPROUT], s, a);
     return cuda_status(cudaGetLastError());
 }
 
 // balance (BvttFrontLooseIntra.cu:285-312).  The external front stays where
 // it is; only the internal front moves to the other buffer.
-bvhcd_status Front::balance(cudaStream_t s) {
-    StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_BALANCE, s);
+bvhcd_status Front::balance_kernels(cudaStream_t s) {
     const int T = bvh_->T();
     unsigned *ctr = bvh_->counters();
     FrontLog l = log();
     FR_TRY(log_prepare(l, T, scratch_.p, s));
     FR_TRY(log_clear(l, T, s));
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_, fcap_[0]);
+    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_);
     const int nx = 1 - cur_;
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
     a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
@@ -845,11 +881,20 @@ bvhcd_status Front::balance(cudaStream_t s) {
     a.cap_pairs = (unsigned)pcap_;
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
     FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
-    LAUNCH_U(k_balance_scan, unroll_, s, a);
-    k_sprout<false><<<RESIDENT(k_sprout<false>), kThreads, 0, s>>>(a); note_launch();
-    FR_TRY(cudaGetLastError());
+    LAUNCH_SCAN(k_balance_scan, shape_[BVHCD_SHAPE_BALANCE], s, a);
+    LAUNCH_ITEM(k_sprout, false, shape_[BVHCD_SHAPE_SPROUT], s, a);
+    return cuda_status(cudaGetLastError());
+}
+
+bvhcd_status Front::balance(cudaStream_t s) {
+    StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_BALANCE, s);
+    bvhcd_status st = balance_kernels(s);
+    if (st != BVHCD_OK) return st;
+    unsigned *ctr = bvh_->counters();
+    const int nx = 1 - cur_;
     // swap the internal front buffers of the two sets, keep the external one
     std::swap(front_[0][0], front_[1][0]);
+    int_swapped_ = !int_swapped_;
     FR_TRY(cudaMemcpyAsync(ctr + 2 * cur_, ctr + 2 * nx, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
     return BVHCD_OK;
 }
@@ -859,15 +904,13 @@ bvhcd_status Front::narrow(cudaStream_t s, bool test) {
     unsigned *ctr = bvh_->counters();
     FR_TRY(cudaMemsetAsync(ctr + C_HITS, 0, sizeof(unsigned), s));
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));
+    const Shape sh = shape_[BVHCD_SHAPE_NARROW];
     if (test)
-        k_narrow<true><<<RESIDENT(k_narrow<true>), kThreads, 0, s>>>(
-            pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr, (unsigned)pcap_, hits_.as<int2>(),
-            (unsigned)pcap_);
+        LAUNCH_ITEM(k_narrow, true, sh, s, pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
+                    (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_);
     else
-        k_narrow<false><<<RESIDENT(k_narrow<false>), kThreads, 0, s>>>(
-            pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr, (unsigned)pcap_, hits_.as<int2>(),
-            (unsigned)pcap_);
-    note_launch();
+        LAUNCH_ITEM(k_narrow, false, sh, s, pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
+                    (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_);
     return cuda_status(cudaGetLastError());
 }
 
@@ -911,6 +954,11 @@ bvhcd_status Front::grow_and_check(cudaStream_t s, bool *overflowed) {
             front_[set][k] = nb;
         }
         fcap_[k] = nc;
+        if (k == 0) {
+            // every work item comes from one internal entry of the input front
+            work_.release();
+            FR_TRY(work_.reserve(sizeof(int2) * (size_t)nc));
+        }
     }
     if (npc != pcap_) {
         pairs_.release();
@@ -968,6 +1016,99 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     last_op_ = run_op;
     k_counts64<<<1, 32, 0, s>>>(ctr, (unsigned)pcap_, (unsigned)pcap_, counts64_.as<int64_t>()); note_launch();
     return cuda_status(cudaGetLastError());
+}
+
+void Front::get_shapes(bvhcd_launch_shapes *sh) const {
+    for (int k = 0; k < BVHCD_SHAPE_COUNT; k++) {
+        sh->unroll[k] = shape_[k].u;
+        sh->block[k] = shape_[k].b;
+    }
+}
+
+bvhcd_status Front::set_shapes(const bvhcd_launch_shapes &sh) {
+    for (int k = 0; k < BVHCD_SHAPE_COUNT; k++) {
+        const int u = sh.unroll[k], b = sh.block[k];
+        if ((u != 1 && u != 2 && u != 4) || (b != 128 && b != 256 && b != 512)) return BVHCD_INVALID_ARG;
+    }
+    for (int k = 0; k < BVHCD_SHAPE_COUNT; k++) shape_[k] = Shape{sh.unroll[k], sh.block[k]};
+    shape_epoch_++;
+    return BVHCD_OK;
+}
+
+// Mean device time of `repeats` runs of fn on stream s, after one untimed run.
+template <typename Fn>
+static bvhcd_status time_runs(Fn fn, int repeats, cudaStream_t s, double *ms) {
+    bvhcd_status st = fn();
+    if (st != BVHCD_OK) return st;
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    if (e == cudaSuccess) e = cudaEventRecord(a, s);
+    for (int r = 0; r < repeats && e == cudaSuccess && st == BVHCD_OK; r++) st = fn();
+    if (e == cudaSuccess) e = cudaEventRecord(b, s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    float f = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&f, a, b);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (st != BVHCD_OK) return st;
+    if (e != cudaSuccess) return cuda_status(e);
+    *ms = (double)f / repeats;
+    return BVHCD_OK;
+}
+
+// Autotuner over the launch shapes (see bvhcd_front_autotune).  Each stage's
+// kernels run on the real front and tree; none commits its output (keep and
+// the narrow phase only rewrite pairs and hits, the update and balance
+// kernels write the other buffer set), and a final GENERATE leaves the front
+// consistent.
+bvhcd_status Front::autotune(int repeats, bvhcd_launch_shapes *chosen, double *best_ms, cudaStream_t s) {
+    if (repeats < 1 || repeats > 1000) return BVHCD_INVALID_ARG;
+    if (!bvh_->built() || !has_front_) return BVHCD_NOT_READY;
+    if (best_ms)
+        for (int k = 0; k < BVHCD_SHAPE_COUNT; k++) best_ms[k] = 0.0;
+    if (bvh_->T() >= 2) {
+        Profiler *prof = bvh_->profiler();
+        const bool prof_on = prof->on;
+        prof->on = false;
+        static const int kUs[3] = {1, 2, 4}, kBs[3] = {128, 256, 512};
+        bvhcd_status st = BVHCD_OK;
+        auto tune = [&](int stage, bool scan, auto fn) {
+            Shape best = shape_[stage];
+            double bt = 1e300;
+            for (int ui = 0; ui < (scan ? 3 : 1) && st == BVHCD_OK; ui++)
+                for (int bi = 0; bi < 3 && st == BVHCD_OK; bi++) {
+                    shape_[stage] = Shape{scan ? kUs[ui] : shape_[stage].u, kBs[bi]};
+                    double ms = 0.0;
+                    st = time_runs(fn, repeats, s, &ms);
+                    if (st == BVHCD_OK && ms < bt) {
+                        bt = ms;
+                        best = shape_[stage];
+                    }
+                }
+            shape_[stage] = best;
+            if (best_ms) best_ms[stage] = bt;
+        };
+        const bool test = cfg_.narrow_phase != 0;
+        tune(BVHCD_SHAPE_KEEP, true, [&] { return keep(s); });
+        tune(BVHCD_SHAPE_SPROUT, false, [&] { return keep(s); });
+        tune(BVHCD_SHAPE_NARROW, false, [&] { return narrow(s, test); });
+        tune(BVHCD_SHAPE_PRUNE_INT, true, [&] { return update_kernels(s); });
+        tune(BVHCD_SHAPE_PRUNE_EXT, true, [&] { return update_kernels(s); });
+        tune(BVHCD_SHAPE_BALANCE, true, [&] { return balance_kernels(s); });
+        if (st == BVHCD_OK) st = generate(s, false);
+        if (st == BVHCD_OK) st = narrow(s, test);
+        prof->on = prof_on;
+        if (st != BVHCD_OK) return st;
+        last_op_ = BVHCD_FRONT_GENERATE;
+        k_counts64<<<1, 32, 0, s>>>(bvh_->counters(), (unsigned)pcap_, (unsigned)pcap_, counts64_.as<int64_t>());
+        note_launch();
+        FR_TRY(cudaGetLastError());
+        FR_TRY(cudaStreamSynchronize(s));
+    }
+    shape_epoch_++;
+    if (chosen) get_shapes(chosen);
+    return BVHCD_OK;
 }
 
 bvhcd_status Front::stats(bvhcd_front_stats *st, cudaStream_t s) {

@@ -34,6 +34,7 @@ bvhcd_status cuda_status(cudaError_t e) {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kBoxTile = 4096;  // triangles per block of the per-scene box reduction
 inline unsigned grid_for(int64_t n, int per = kThreads) {
     int64_t g = (n + per - 1) / per;
     if (g < 1) g = 1;
@@ -46,20 +47,9 @@ __device__ __forceinline__ int split_metric(unsigned a, unsigned b) {
 }
 
 // ---------------------------------------------------------------- scene box
-__global__ void __launch_bounds__(kThreads) k_box_partial(int T, const int *__restrict__ faces,
-                                                          const float *__restrict__ verts,
-                                                          float *partial) {
-    float mn[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
-    float mx[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
-        float3 a = load_vert(verts, __ldg(faces + 3 * (size_t)t));
-        float3 b = load_vert(verts, __ldg(faces + 3 * (size_t)t + 1));
-        float3 c = load_vert(verts, __ldg(faces + 3 * (size_t)t + 2));
-        float4 lo, hi;
-        tri_box(a, b, c, lo, hi);
-        mn[0] = fminf(mn[0], lo.x); mn[1] = fminf(mn[1], lo.y); mn[2] = fminf(mn[2], lo.z);
-        mx[0] = fmaxf(mx[0], hi.x); mx[1] = fmaxf(mx[1], hi.y); mx[2] = fmaxf(mx[2], hi.z);
-    }
+// Block-wide min/max of three coordinates; the result lands in out[0..5]
+// (shared) for threads 0..5 after the call.
+__device__ __forceinline__ void block_box(float (&mn)[3], float (&mx)[3], float *out) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
@@ -76,8 +66,33 @@ __global__ void __launch_bounds__(kThreads) k_box_partial(int T, const int *__re
         float v = s[0][threadIdx.x];
         for (int q = 1; q < kThreads / 32; q++)
             v = threadIdx.x < 3 ? fminf(v, s[q][threadIdx.x]) : fmaxf(v, s[q][threadIdx.x]);
-        partial[6 * blockIdx.x + threadIdx.x] = v;
+        out[threadIdx.x] = v;
     }
+}
+
+__device__ __forceinline__ void box_of_range(int first, int end, int step, const int *__restrict__ faces,
+                                             const float *__restrict__ verts, float (&mn)[3],
+                                             float (&mx)[3]) {
+    for (int t = first; t < end; t += step) {
+        float3 a = load_vert(verts, __ldg(faces + 3 * (size_t)t));
+        float3 b = load_vert(verts, __ldg(faces + 3 * (size_t)t + 1));
+        float3 c = load_vert(verts, __ldg(faces + 3 * (size_t)t + 2));
+        float4 lo, hi;
+        tri_box(a, b, c, lo, hi);
+        mn[0] = fminf(mn[0], lo.x); mn[1] = fminf(mn[1], lo.y); mn[2] = fminf(mn[2], lo.z);
+        mx[0] = fmaxf(mx[0], hi.x); mx[1] = fmaxf(mx[1], hi.y); mx[2] = fmaxf(mx[2], hi.z);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_box_partial(int T, const int *__restrict__ faces,
+                                                          const float *__restrict__ verts,
+                                                          float *partial) {
+    float mn[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+    float mx[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+    box_of_range(blockIdx.x * blockDim.x + threadIdx.x, T, gridDim.x * blockDim.x, faces, verts, mn, mx);
+    __shared__ float out[6];
+    block_box(mn, mx, out);
+    if (threadIdx.x < 6) partial[6 * blockIdx.x + threadIdx.x] = out[threadIdx.x];
 }
 
 __global__ void __launch_bounds__(kThreads) k_box_final(int n, const float *partial, float *scene) {
@@ -88,23 +103,70 @@ __global__ void __launch_bounds__(kThreads) k_box_final(int n, const float *part
             mn[k] = fminf(mn[k], partial[6 * q + k]);
             mx[k] = fmaxf(mx[k], partial[6 * q + 3 + k]);
         }
+    __shared__ float out[6];
+    block_box(mn, mx, out);
+    if (threadIdx.x < 6) scene[threadIdx.x] = out[threadIdx.x];
+}
+
+// ---------------------------------------------------------------- batched scenes
+// A batch of independent scenes is built as one forest.  Scene s owns the
+// input triangles [off[s], off[s+1]) and, in the tree, the leaves
+// [off[s], off[s+1]) sorted by (scene, Morton code) and the internal nodes
+// with DFS ids [off[s] - s, off[s+1] - s - 1).  Each scene's subtree is the
+// tree the scene would get on its own, shifted by those offsets: its own box
+// normalises its codes, a scene boundary is a split no climb crosses (the
+// confined rebuild of a restructure, with scenes as the subtrees), and the
+// escape after a scene's last leaf ends the traversal.
+
+// Exact float min/max through integer atomics on the bit pattern: non-negative
+// floats order like their bits as signed ints, negative ones in reverse of
+// their bits as unsigned ints.
+__device__ __forceinline__ void atomic_min_f32(float *a, float v) {
+    if (v >= 0.f) atomicMin(reinterpret_cast<int *>(a), __float_as_int(v));
+    else atomicMax(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_f32(float *a, float v) {
+    if (v >= 0.f) atomicMax(reinterpret_cast<int *>(a), __float_as_int(v));
+    else atomicMin(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
+}
+
+__global__ void k_sbox_init(int S, float *sbox) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * S; i += gridDim.x * blockDim.x)
+        sbox[i] = (i % 6) < 3 ? 3.402823466e+38f : -3.402823466e+38f;
+}
+
+// Per-scene boxes: one block per tile {scene, first, end} of one scene's
+// triangles; the tile's box is merged into its scene's with the atomics above
+// (min/max are exact, so the box equals the scene's own reduction).
+__global__ void __launch_bounds__(kThreads) k_sbox_tiles(const int4 *__restrict__ tiles,
+                                                         const int *__restrict__ faces,
+                                                         const float *__restrict__ verts, float *sbox) {
+    const int4 tl = tiles[blockIdx.x];
+    float mn[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+    float mx[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+    box_of_range(tl.y + threadIdx.x, tl.z, blockDim.x, faces, verts, mn, mx);
+    __shared__ float out[6];
+    block_box(mn, mx, out);
+    if (threadIdx.x < 3) atomic_min_f32(sbox + 6 * tl.x + threadIdx.x, out[threadIdx.x]);
+    else if (threadIdx.x < 6) atomic_max_f32(sbox + 6 * tl.x + threadIdx.x, out[threadIdx.x]);
+}
+
+// 64-bit keys (scene << 30 | 30-bit code of the triangle in its scene's box).
+__global__ void k_morton_seg(int T, const int *__restrict__ faces, const float *__restrict__ verts,
+                             const int *__restrict__ scene_of, const float *__restrict__ sbox,
+                             unsigned long long *keys, int *vals) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+        const int sc = __ldg(scene_of + t);
+        float3 a = load_vert(verts, __ldg(faces + 3 * (size_t)t));
+        float3 b = load_vert(verts, __ldg(faces + 3 * (size_t)t + 1));
+        float3 c = load_vert(verts, __ldg(faces + 3 * (size_t)t + 2));
+        float4 lo, hi;
+        tri_box(a, b, c, lo, hi);
+        float box[6];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
-            mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
-        }
-    __shared__ float s[kThreads / 32][6];
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0)
-        for (int k = 0; k < 3; k++) { s[w][k] = mn[k]; s[w][3 + k] = mx[k]; }
-    __syncthreads();
-    if (threadIdx.x < 6) {
-        float v = s[0][threadIdx.x];
-        for (int q = 1; q < kThreads / 32; q++)
-            v = threadIdx.x < 3 ? fminf(v, s[q][threadIdx.x]) : fmaxf(v, s[q][threadIdx.x]);
-        scene[threadIdx.x] = v;
+        for (int k = 0; k < 6; k++) box[k] = __ldg(sbox + 6 * sc + k);
+        keys[t] = ((unsigned long long)sc << 30) | morton_box(lo, hi, box);
+        vals[t] = t;
     }
 }
 
@@ -129,22 +191,44 @@ __global__ void k_morton(int T, const int *__restrict__ faces, const float *__re
 // Mine/utility/CudaKernelUtils.cu:28-32; buildPrimitives,
 // LBvhBuildKernels.cu:114-133, here storing the vertex ids too;
 // calcExtNodeSplitMetrics, Mine/collision/lbvh/BvhExtNode.cu:128-134).
+__device__ __forceinline__ void write_leaf(int i, int t, unsigned k, int metric_i,
+                                           const int *__restrict__ faces, const float *__restrict__ verts,
+                                           int4 *sface, int *primmap, unsigned *code, int *metric,
+                                           float4 *lrec) {
+    int4 f = make_int4(__ldg(faces + 3 * (size_t)t), __ldg(faces + 3 * (size_t)t + 1),
+                       __ldg(faces + 3 * (size_t)t + 2), t);
+    sface[i] = f;
+    primmap[t] = i;
+    code[i] = k;
+    metric[i] = metric_i;
+    float4 lo, hi;
+    tri_box(load_vert(verts, f.x), load_vert(verts, f.y), load_vert(verts, f.z), lo, hi);
+    lrec[2 * i] = lo;
+    lrec[2 * i + 1] = hi;
+}
+
 __global__ void k_leaves(int T, const unsigned *__restrict__ keys, const int *__restrict__ vals,
                          const int *__restrict__ faces, const float *__restrict__ verts,
                          int4 *sface, int *primmap, unsigned *code, int *metric, float4 *lrec) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) {
-        int t = vals[i];
-        int4 f = make_int4(__ldg(faces + 3 * (size_t)t), __ldg(faces + 3 * (size_t)t + 1),
-                           __ldg(faces + 3 * (size_t)t + 2), t);
-        sface[i] = f;
-        primmap[t] = i;
-        unsigned k = keys[i];
-        code[i] = k;
-        metric[i] = (i != T - 1) ? split_metric(k, keys[i + 1]) : 33;
-        float4 lo, hi;
-        tri_box(load_vert(verts, f.x), load_vert(verts, f.y), load_vert(verts, f.z), lo, hi);
-        lrec[2 * i] = lo;
-        lrec[2 * i + 1] = hi;
+        const unsigned k = keys[i];
+        write_leaf(i, vals[i], k, (i != T - 1) ? split_metric(k, keys[i + 1]) : 33, faces, verts, sface,
+                   primmap, code, metric, lrec);
+    }
+}
+
+// Leaves of a forest: the scene id of every slot goes to leafscene (the
+// metric across a scene boundary is never read: the boundary decides).
+__global__ void k_leaves_seg(int T, const unsigned long long *__restrict__ keys, const int *__restrict__ vals,
+                             const int *__restrict__ faces, const float *__restrict__ verts,
+                             int4 *sface, int *primmap, unsigned *code, int *metric, float4 *lrec,
+                             int *leafscene) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) {
+        const unsigned long long k = keys[i];
+        const unsigned c = (unsigned)(k & 0x3fffffffu);
+        leafscene[i] = (int)(k >> 30);
+        const int m = (i != T - 1) ? split_metric(c, (unsigned)(keys[i + 1] & 0x3fffffffu)) : 33;
+        write_leaf(i, vals[i], c, m, faces, verts, sface, primmap, code, metric, lrec);
     }
 }
 
@@ -172,7 +256,9 @@ struct Climb {
 
 // Bottom-up construction (buildIntNodes, LBvhBuildKernels.cu:135-172; with
 // kSeg the confined rebuild of restrIntNodes,
-// Mine/collision/lbvh/LBvhRestructureKernels.cu:122-166).  Internal nodes are
+// Mine/collision/lbvh/LBvhRestructureKernels.cu:122-166, over the listed
+// leaves, or over all leaves of a forest when `leaves` is null, with
+// `prev_topo` null: a scene root has no father).  Internal nodes are
 // indexed by split.  The second thread to reach a node merges the child
 // boxes, records posb = distance from the bottom of its left chain and, at a
 // chain top, the chain length of the chain's leftmost leaf.
@@ -183,7 +269,7 @@ __global__ void __launch_bounds__(kThreads) k_climb(int T, int n, const int *__r
                                                     const float4 *__restrict__ lrec,
                                                     const int4 *__restrict__ prev_topo, Climb c) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int idx = kSeg ? leaves[k] : k;
+        const int idx = (kSeg && leaves) ? leaves[k] : k;
         const int sub = kSeg ? seg[idx] : 0;
         int l = idx - 1, r = idx, bd = 0;
         bool mark;
@@ -225,7 +311,7 @@ __global__ void __launch_bounds__(kThreads) k_climb(int T, int n, const int *__r
             const bool is_root = kSeg ? (bd == 3) : (l + 1 == 0 && r == T - 1);
             if (is_root) {
                 c.upar[cur] = -1;
-                const bool right = kSeg ? ((prev_topo[sub].w & 4) != 0) : false;
+                const bool right = (kSeg && prev_topo) ? ((prev_topo[sub].w & 4) != 0) : false;
                 c.umark[cur] = m | (right ? 4u : 0u);
                 c.clen[rx] = pb + 1;
                 break;
@@ -256,9 +342,17 @@ __global__ void __launch_bounds__(kThreads) k_climb(int T, int n, const int *__r
 
 // DFS id of every internal node: chain offset of its leftmost leaf plus its
 // position from the chain top (calcIntNodeOrders, LBvhBuildKernels.cu:174-185).
+// In a forest the split after a scene's last leaf is no node (`leafscene`
+// non-null marks those splits).
+__device__ __forceinline__ bool scene_end(const int *leafscene, int s, int T) {
+    return leafscene && s + 1 < T && __ldg(leafscene + s + 1) != __ldg(leafscene + s);
+}
+
 __global__ void k_dfs_ids(int nint, const int *__restrict__ urx, const int *__restrict__ posb,
-                          const unsigned *__restrict__ coff, const int *__restrict__ clen, int *dfs) {
+                          const unsigned *__restrict__ coff, const int *__restrict__ clen,
+                          const int *__restrict__ leafscene, int *dfs) {
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nint; u += gridDim.x * blockDim.x) {
+        if (scene_end(leafscene, u, nint + 1)) continue;
         int rx = urx[u];
         dfs[u] = (int)coff[rx] + clen[rx] - 1 - posb[u];
     }
@@ -271,21 +365,23 @@ __device__ __forceinline__ int lca_of(int s, int T, const unsigned *coff, const 
 
 // Escape links and leaf parents (updateBvhExtNodeLinks, LBvhBuildKernels.cu:187-200).
 __global__ void k_leaf_links(int T, const unsigned *__restrict__ coff, const int *__restrict__ clen,
-                             const int *__restrict__ ulpar, const int *__restrict__ dfs, int *lca,
-                             float4 *lrec) {
+                             const int *__restrict__ ulpar, const int *__restrict__ dfs,
+                             const int *__restrict__ leafscene, int *lca, float4 *lrec) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x) {
         lca[s] = lca_of(s, T, coff, clen);
         if (s == 0) lca[T] = -1;
         reinterpret_cast<float *>(lrec)[8 * (size_t)s + 3] = __int_as_float(dfs[ulpar[s]]);
-        reinterpret_cast<float *>(lrec)[8 * (size_t)s + 7] = __int_as_float(lca_of(s + 1, T, coff, clen));
+        const int esc = scene_end(leafscene, s, T) ? -1 : lca_of(s + 1, T, coff, clen);
+        reinterpret_cast<float *>(lrec)[8 * (size_t)s + 7] = __int_as_float(esc);
     }
 }
 
 // Internal nodes in DFS order (reorderIntNode, LBvhBuildKernels.cu:202-217).
 __global__ void k_write_nodes(int nint, int T, Climb c, const int *__restrict__ dfs,
                               const unsigned *__restrict__ coff, const int *__restrict__ clen,
-                              float4 *nrec, int4 *topo, int2 *nrange) {
+                              const int *__restrict__ leafscene, float4 *nrec, int4 *topo, int2 *nrange) {
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nint; u += gridDim.x * blockDim.x) {
+        if (scene_end(leafscene, u, T)) continue;
         int d = dfs[u];
         unsigned m = c.umark[u];
         int lc = c.ulc[u], rc = c.urc[u], p = c.upar[u];
@@ -294,7 +390,7 @@ __global__ void k_write_nodes(int nint, int T, Climb c, const int *__restrict__ 
         nrange[d] = make_int2(rx, ry);
         float4 lo = c.ubox[2 * u], hi = c.ubox[2 * u + 1];
         lo.w = __int_as_float(rx);
-        hi.w = __int_as_float(lca_of(ry + 1, T, coff, clen));
+        hi.w = __int_as_float(scene_end(leafscene, ry, T) ? -1 : lca_of(ry + 1, T, coff, clen));
         nrec[2 * d] = lo;
         nrec[2 * d + 1] = hi;
     }
@@ -574,7 +670,7 @@ LBvh::~LBvh() {
                     &ulc_, &urc_, &upar_, &urx_, &ury_, &umark_, &ubox_, &uflag_, &posb_, &clen_,
                     &coff_, &dfs_, &ulpar_, &scene_, &partial_, &scratch_, &task_, &tmpface_,
                     &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &flagbuf_,
-                    &ctr_};
+                    &ctr_, &scene_of_, &leafscene_, &sbox_, &tiles_};
     for (DBuf *b : bufs) b->release();
     if (h_ctr_) cudaFreeHost(h_ctr_);
 }
@@ -707,38 +803,95 @@ bvhcd_status LBvh::build(cudaStream_t s) {
     const int T = T_;
     built_ = false;
     if (T == 0) { built_ = true; return BVHCD_OK; }
-    bvhcd_status st = scene_box(s);
-    if (st != BVHCD_OK) return st;
-    k_morton<<<grid_for(T), kThreads, 0, s>>>(T, fptr_, vptr_, scene_.as<float>(), keys_.as<unsigned>(),
-                                              vals_.as<int>()); note_launch();
-    BV_TRY(radix_sort_u32(keys_.as<unsigned>(), vals_.as<int>(), keys2_.as<unsigned>(), vals2_.as<int>(),
-                          T, 30, scratch_.p, s));
-    k_leaves<<<grid_for(T), kThreads, 0, s>>>(T, keys_.as<unsigned>(), vals_.as<int>(), fptr_, vptr_,
-                                              sface_.as<int4>(), primmap_.as<int>(), code_.as<unsigned>(),
-                                              metric_.as<int>(), lrec_.as<float4>()); note_launch();
-    if (T == 1) {
-        // a single leaf: no internal node, lca = {leaf 0, end}, no parent
-        k_single_leaf<<<1, 32, 0, s>>>(lca_.as<int>(), lrec_.as<float4>()); note_launch();
-        BV_TRY(cudaGetLastError());
-        built_ = true;
-        return BVHCD_OK;
+    int *leafscene = nullptr;
+    if (S_ > 1) {
+        // a forest of S_ scenes: per-scene boxes, (scene, code) keys
+        if (T != h_off_[S_]) return BVHCD_INVALID_ARG;
+        k_sbox_init<<<1, kThreads, 0, s>>>(S_, sbox_.as<float>()); note_launch();
+        k_sbox_tiles<<<ntiles_, kThreads, 0, s>>>(tiles_.as<int4>(), fptr_, vptr_, sbox_.as<float>()); note_launch();
+        k_morton_seg<<<grid_for(T), kThreads, 0, s>>>(T, fptr_, vptr_, scene_of_.as<int>(), sbox_.as<float>(),
+                                                      k64_.as<unsigned long long>(), vals_.as<int>()); note_launch();
+        int sbits = 0;
+        while ((1 << sbits) < S_) sbits++;
+        BV_TRY(radix_sort_u64(k64_.as<unsigned long long>(), vals_.as<int>(), k64b_.as<unsigned long long>(),
+                              vals2_.as<int>(), T, 30 + sbits, scratch_.p, s));
+        leafscene = leafscene_.as<int>();
+        k_leaves_seg<<<grid_for(T), kThreads, 0, s>>>(T, k64_.as<unsigned long long>(), vals_.as<int>(), fptr_,
+                                                      vptr_, sface_.as<int4>(), primmap_.as<int>(),
+                                                      code_.as<unsigned>(), metric_.as<int>(),
+                                                      lrec_.as<float4>(), leafscene); note_launch();
+    } else {
+        bvhcd_status st = scene_box(s);
+        if (st != BVHCD_OK) return st;
+        k_morton<<<grid_for(T), kThreads, 0, s>>>(T, fptr_, vptr_, scene_.as<float>(), keys_.as<unsigned>(),
+                                                  vals_.as<int>()); note_launch();
+        BV_TRY(radix_sort_u32(keys_.as<unsigned>(), vals_.as<int>(), keys2_.as<unsigned>(), vals2_.as<int>(),
+                              T, 30, scratch_.p, s));
+        k_leaves<<<grid_for(T), kThreads, 0, s>>>(T, keys_.as<unsigned>(), vals_.as<int>(), fptr_, vptr_,
+                                                  sface_.as<int4>(), primmap_.as<int>(), code_.as<unsigned>(),
+                                                  metric_.as<int>(), lrec_.as<float4>()); note_launch();
+        if (T == 1) {
+            // a single leaf: no internal node, lca = {leaf 0, end}, no parent
+            k_single_leaf<<<1, 32, 0, s>>>(lca_.as<int>(), lrec_.as<float4>()); note_launch();
+            BV_TRY(cudaGetLastError());
+            built_ = true;
+            return BVHCD_OK;
+        }
     }
     Climb c = make_climb(ulc_, urc_, upar_, urx_, ury_, umark_, ubox_, uflag_, posb_, clen_, ulpar_);
     BV_TRY(cudaMemsetAsync(uflag_.p, 0, sizeof(unsigned) * (size_t)T, s));
     BV_TRY(cudaMemsetAsync(clen_.as<int>() + T, 0, sizeof(int), s));
-    k_climb<false><<<grid_for(T), kThreads, 0, s>>>(T, T, nullptr, nullptr, metric_.as<int>(),
-                                                    lrec_.as<float4>(), nullptr, c); note_launch();
+    if (leafscene)
+        k_climb<true><<<grid_for(T), kThreads, 0, s>>>(T, T, nullptr, leafscene, metric_.as<int>(),
+                                                       lrec_.as<float4>(), nullptr, c);
+    else
+        k_climb<false><<<grid_for(T), kThreads, 0, s>>>(T, T, nullptr, nullptr, metric_.as<int>(),
+                                                        lrec_.as<float4>(), nullptr, c);
+    note_launch();
     BV_TRY(scan_u32(clen_.as<unsigned>(), coff_.as<unsigned>(), T + 1, false, nullptr, scratch_.p, s));
     k_dfs_ids<<<grid_for(T - 1), kThreads, 0, s>>>(T - 1, urx_.as<int>(), posb_.as<int>(),
-                                                   coff_.as<unsigned>(), clen_.as<int>(), dfs_.as<int>()); note_launch();
+                                                   coff_.as<unsigned>(), clen_.as<int>(), leafscene,
+                                                   dfs_.as<int>()); note_launch();
     k_leaf_links<<<grid_for(T), kThreads, 0, s>>>(T, coff_.as<unsigned>(), clen_.as<int>(), ulpar_.as<int>(),
-                                                  dfs_.as<int>(), lca_.as<int>(), lrec_.as<float4>()); note_launch();
+                                                  dfs_.as<int>(), leafscene, lca_.as<int>(),
+                                                  lrec_.as<float4>()); note_launch();
     k_write_nodes<<<grid_for(T - 1), kThreads, 0, s>>>(T - 1, T, c, dfs_.as<int>(), coff_.as<unsigned>(),
-                                                       clen_.as<int>(), nrec_.as<float4>(), topo_.as<int4>(),
-                                                       nrange_.as<int2>()); note_launch();
+                                                       clen_.as<int>(), leafscene, nrec_.as<float4>(),
+                                                       topo_.as<int4>(), nrange_.as<int2>()); note_launch();
     BV_TRY(cudaMemsetAsync(refit_flag_.p, 0, sizeof(unsigned) * (size_t)T, s));
     BV_TRY(cudaGetLastError());
     built_ = true;
+    return BVHCD_OK;
+}
+
+// Batched scenes (see the forest kernels above).  The layout is static: the
+// per-triangle scene ids and the box tiles are uploaded once here.
+bvhcd_status LBvh::set_scenes(int S, const int32_t *off) {
+    if (S < 1 || !off || off[0] != 0) return BVHCD_INVALID_ARG;
+    if (S > 1 && restr_enabled()) return BVHCD_INVALID_ARG;
+    if (S > (1 << 22)) return BVHCD_INVALID_ARG;
+    for (int k = 0; k < S; k++)
+        if (off[k + 1] - off[k] < (S > 1 ? 2 : 0)) return BVHCD_INVALID_ARG;
+    const int T = off[S];
+    std::vector<int> scene_of((size_t)T);
+    std::vector<int4> tiles;
+    for (int k = 0; k < S; k++) {
+        for (int t = off[k]; t < off[k + 1]; t++) scene_of[(size_t)t] = k;
+        for (int t = off[k]; t < off[k + 1]; t += kBoxTile)
+            tiles.push_back(make_int4(k, t, t + kBoxTile < off[k + 1] ? t + kBoxTile : off[k + 1], 0));
+    }
+    h_off_.assign(off, off + S + 1);
+    S_ = S;
+    epoch_++;
+    built_ = false;
+    if (S == 1) return BVHCD_OK;
+    BV_TRY(scene_of_.reserve(sizeof(int) * (size_t)(T > 0 ? T : 1)));
+    BV_TRY(leafscene_.reserve(sizeof(int) * (size_t)(T > 0 ? T : 1)));
+    BV_TRY(sbox_.reserve(sizeof(float) * 6 * (size_t)S));
+    BV_TRY(tiles_.reserve(sizeof(int4) * tiles.size()));
+    BV_TRY(cudaMemcpy(scene_of_.p, scene_of.data(), sizeof(int) * (size_t)T, cudaMemcpyHostToDevice));
+    BV_TRY(cudaMemcpy(tiles_.p, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice));
+    ntiles_ = (int)tiles.size();
     return BVHCD_OK;
 }
 
@@ -831,6 +984,7 @@ bvhcd_status LBvh::restructure(cudaStream_t s) {
 // LBvhFixedDeformable::maintain (LBvhFixedDeformable.cu:68-87)
 bvhcd_status LBvh::maintain(bvhcd_bvh_op op, const bvhcd_scene &scene, cudaStream_t s) {
     if (op < BVHCD_BVH_BUILD || op > BVHCD_BVH_UPDATE) return BVHCD_INVALID_ARG;
+    if (S_ > 1 && scene.num_faces != h_off_[S_]) return BVHCD_INVALID_ARG;
     int prevT = T_;
     bool was_built = built_;
     bvhcd_status st = upload(scene, s);

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
 #include <vector>
 
 #include "../../include/bvhcd.h"
@@ -83,6 +84,25 @@ class LBvh {
     bvhcd_status export_tree(int32_t *inode, float *ibox, int32_t *leaf, float *lbox, int32_t *lca,
                              uint32_t *codes, int32_t *primmap, cudaStream_t s) const;
     bvhcd_status request_restructure(const int32_t *roots, int32_t n, cudaStream_t s);
+    bvhcd_status set_scenes(int S, const int32_t *tri_offsets);
+    int num_scenes() const { return S_; }
+    int layout_epoch() const { return epoch_; }  // bumped by every set_scenes
+
+    // Host-side state a maintain() call advances; a captured frame graph
+    // restores the state its capture ended with after every replay.
+    struct HostState {
+        int T, V, opt_tag, rt_subtrees, rt_intnodes;
+        bool built, updated;
+        const float *vptr;
+        const int *fptr;
+    };
+    HostState host_state() const {
+        return HostState{T_, V_, opt_tag_, rt_subtrees_, rt_intnodes_, built_, updated_, vptr_, fptr_};
+    }
+    void set_host_state(const HostState &h) {
+        T_ = h.T; V_ = h.V; opt_tag_ = h.opt_tag; rt_subtrees_ = h.rt_subtrees; rt_intnodes_ = h.rt_intnodes;
+        built_ = h.built; updated_ = h.updated; vptr_ = h.vptr; fptr_ = h.fptr;
+    }
 
     Tree tree() const;
     int T() const { return T_; }
@@ -127,6 +147,11 @@ class LBvh {
         ubox_, uflag_, posb_, clen_, coff_, dfs_, ulpar_, scene_, partial_, scratch_, task_, tmpface_;
     // restructure log
     DBuf intrange_, rtroot_, intmark_, extrange_, extmark_, leafroot_, flagbuf_;
+    // batched scenes: S_ scenes, triangle offsets, per-triangle scene id,
+    // per-slot scene id, per-scene boxes, box-reduction tiles
+    int S_ = 1, ntiles_ = 0, epoch_ = 0;
+    std::vector<int> h_off_;
+    DBuf scene_of_, leafscene_, sbox_, tiles_;
     DBuf ctr_;
     unsigned *h_ctr_ = nullptr;  // pinned
     Profiler prof_;
@@ -144,13 +169,39 @@ class Front {
     bvhcd_status export_front(int which, int32_t *out, int64_t cap, int64_t *count, cudaStream_t s);
     bvhcd_status device_results(const int32_t **hits, const int64_t **counts);
 
+    // Host-side state a maintain() call advances (see LBvh::HostState);
+    // int_swapped: balance() exchanged the internal-front buffers of the two
+    // sets an odd number of times.
+    struct HostState {
+        int cur, last_op;
+        bool has_front, int_swapped;
+    };
+    HostState host_state() const { return HostState{cur_, last_op_, has_front_, int_swapped_}; }
+    void set_host_state(const HostState &h) {
+        cur_ = h.cur;
+        last_op_ = h.last_op;
+        has_front_ = h.has_front;
+        if (h.int_swapped != int_swapped_) {
+            std::swap(front_[0][0], front_[1][0]);
+            int_swapped_ = h.int_swapped;
+        }
+    }
+    bool auto_grow() const { return cfg_.auto_grow != 0; }
+    LBvh *bvh() const { return bvh_; }
+    void get_shapes(bvhcd_launch_shapes *sh) const;
+    bvhcd_status set_shapes(const bvhcd_launch_shapes &sh);
+    bvhcd_status autotune(int repeats, bvhcd_launch_shapes *chosen, double *best_ms, cudaStream_t s);
+    int shape_epoch() const { return shape_epoch_; }
+
   private:
     bvhcd_status ensure_node_capacity(int T);
     bvhcd_status run(bvhcd_front_op op, cudaStream_t s);
     bvhcd_status generate(cudaStream_t s, bool pure);
     bvhcd_status prune_sprout(cudaStream_t s);
+    bvhcd_status update_kernels(cudaStream_t s);
     bvhcd_status keep(cudaStream_t s);
     bvhcd_status balance(cudaStream_t s);
+    bvhcd_status balance_kernels(cudaStream_t s);
     bvhcd_status reorder(cudaStream_t s);
     bvhcd_status narrow(cudaStream_t s, bool test);
     bvhcd_status check_quality(cudaStream_t s);
@@ -163,8 +214,15 @@ class Front {
     int capT_ = 0;
     int cur_ = 0;  // which buffer set holds the current front
     int last_op_ = -1;
-    int unroll_ = 1;  // entries per thread step in the batched front scans (1, 2 or 4)
+    // launch shape per front stage (BVHCD_SHAPE_*): entries per thread step
+    // in the scans, threads per block
+    struct Shape {
+        int u, b;
+    };
+    Shape shape_[BVHCD_SHAPE_COUNT] = {{2, 256}, {2, 256}, {2, 256}, {2, 256}, {1, 256}, {1, 256}};
+    int shape_epoch_ = 0;
     bool has_front_ = false;
+    bool int_swapped_ = false;
     DBuf front_[2][2];  // [set][0 int, 1 ext] int2 entries
     int64_t fcap_[2] = {0, 0};
     DBuf pairs_, hits_, outbuf_, work_;

@@ -15,6 +15,10 @@ a fixed seed with the shapes, sizes and motion the workload names:
                       40,500 triangles, radius 0.25); per-frame vertex motion
                       at most 2% of an edge length.
 * ``stacked_layers``  four cloth layers 1e-3 apart with seeded in-plane shear.
+* ``batched_cloth_sphere`` 256 independent cloth-over-sphere scenes whose
+                      triangle counts are drawn log-uniform in [1k, 200k]
+                      (about 90% cloth, 10% icosphere), each with its own
+                      seeded damped wave; concatenated with triangle offsets.
 
 All arrays are float32 positions (V, 3) and int32 faces (T, 3).
 """
@@ -154,3 +158,97 @@ def stacked_layers_frames(n: int = 512, layers: int = 4, frames: int = 50, seed:
             pts.append(np.stack([sx, sy, np.full_like(x, l * gap)], axis=1))
         out.append(np.concatenate(pts).astype(np.float32))
     return faces, out
+
+
+_ICO_CACHE: dict = {}
+
+
+def _unit_icosphere(freq: int):
+    if freq not in _ICO_CACHE:
+        _ICO_CACHE[freq] = icosphere(freq)
+    return _ICO_CACHE[freq]
+
+
+class BatchedScenes:
+    """Independent cloth-over-sphere scenes concatenated into one triangle
+    and vertex list.  Scene s owns triangles [tri_offsets[s],
+    tri_offsets[s+1]) and vertices [vert_offsets[s], vert_offsets[s+1]);
+    its faces hold global vertex ids.  positions(f) gives frame f of every
+    scene at once.  Every scene lives in its own unit frame (cloth on
+    [0,1]^2 at height 0.2 over a sphere of radius 0.25 centred at (0.5, 0.5,
+    0)), so the scenes overlap in space: only the batching keeps them apart."""
+
+    def __init__(self, num_scenes: int = 256, t_min: int = 1000, t_max: int = 200_000, seed: int = 4242,
+                 amplitude: float = 0.2, height: float = 0.2, radius: float = 0.25):
+        rng = np.random.default_rng(seed)
+        target = np.exp(rng.uniform(math.log(t_min), math.log(t_max), size=num_scenes))
+        faces, tri_off, vert_off = [], [0], [0]
+        xs, ys, rs, par = [], [], [], []
+        static = []
+        lam, omega = 0.5, 2 * np.pi
+        self.cloth_verts = []
+        for sc in range(num_scenes):
+            n = max(3, int(round(math.sqrt(0.45 * target[sc]))) + 1)
+            nu = max(1, int(round(math.sqrt(0.005 * target[sc]))))
+            x, y, cf = cloth_grid(n)
+            sv, sf = _unit_icosphere(nu)
+            sv = sv * radius + np.array([0.5, 0.5, 0.0])
+            v0 = vert_off[-1]
+            faces.append(cf + v0)
+            faces.append(sf + v0 + x.size)
+            tri_off.append(tri_off[-1] + cf.shape[0] + sf.shape[0])
+            vert_off.append(v0 + x.size + sv.shape[0])
+            cx, cy = rng.uniform(0.3, 0.7, size=2)
+            phi = rng.uniform(0.0, 2 * np.pi)
+            k = 2 * np.pi * rng.uniform(2.0, 4.0)
+            edge = 1.0 / (n - 1)
+            dt = 0.02 * edge / (amplitude * (omega + lam)) * 0.999
+            xs.append(x)
+            ys.append(y)
+            rs.append(np.hypot(x - cx, y - cy))
+            par.append(np.repeat(np.array([[k, phi, dt]]), x.size, axis=0))
+            static.append((v0 + x.size, sv))
+            self.cloth_verts.append((v0, x.size))
+        self.num_scenes = num_scenes
+        self.faces = np.concatenate(faces).astype(np.int32)
+        self.tri_offsets = np.asarray(tri_off, dtype=np.int32)
+        self.vert_offsets = np.asarray(vert_off, dtype=np.int64)
+        self.num_faces = int(self.tri_offsets[-1])
+        self.num_vertices = int(self.vert_offsets[-1])
+        self._cloth_idx = np.concatenate([np.arange(v0, v0 + nv) for v0, nv in self.cloth_verts])
+        self._x = np.concatenate(xs)
+        self._y = np.concatenate(ys)
+        self._r = np.concatenate(rs)
+        p = np.concatenate(par)
+        self._k, self._phi, self._dt = p[:, 0], p[:, 1], p[:, 2]
+        self._amp, self._h, self._lam, self._omega = amplitude, height, lam, omega
+        self._base = np.zeros((self.num_vertices, 3), dtype=np.float32)
+        for v0, sv in static:
+            self._base[v0:v0 + sv.shape[0]] = sv
+        self._base[self._cloth_idx, 0] = self._x
+        self._base[self._cloth_idx, 1] = self._y
+
+    def positions(self, f: int) -> np.ndarray:
+        t = f * self._dt
+        z = self._h + self._amp * np.exp(-self._lam * t) * np.sin(self._k * self._r - self._omega * t + self._phi)
+        out = self._base.copy()
+        out[self._cloth_idx, 2] = z
+        return out
+
+    def scene(self, s: int, f: int):
+        """(faces, positions) of scene s alone at frame f, local vertex ids."""
+        v0, v1 = int(self.vert_offsets[s]), int(self.vert_offsets[s + 1])
+        t0, t1 = int(self.tri_offsets[s]), int(self.tri_offsets[s + 1])
+        return self.faces[t0:t1] - v0, self.positions(f)[v0:v1]
+
+    def subset(self, ids):
+        """The scenes `ids` (sorted) as their own batch: (faces with batch-local
+        vertex ids, triangle offsets, global vertex index of every batch
+        vertex)."""
+        ids = np.asarray(sorted(ids), dtype=np.int64)
+        vidx = np.concatenate([np.arange(self.vert_offsets[s], self.vert_offsets[s + 1]) for s in ids])
+        remap = np.full(self.num_vertices, -1, dtype=np.int64)
+        remap[vidx] = np.arange(vidx.size)
+        faces = np.concatenate([self.faces[self.tri_offsets[s]:self.tri_offsets[s + 1]] for s in ids])
+        off = np.concatenate([[0], np.cumsum([self.tri_offsets[s + 1] - self.tri_offsets[s] for s in ids])])
+        return remap[faces].astype(np.int32), off.astype(np.int32), vidx

@@ -215,6 +215,71 @@ bvhcd_status bvhcd_launch_count(int64_t *n);
 bvhcd_status bvhcd_morton_order_noalloc(const float *pos, const int32_t *faces, int32_t num_faces,
                                         uint32_t *codes, int32_t *order, void *stream);
 
+/* ---- Batched scenes.  No counterpart in the reference, which builds one
+ * tree over all meshes of a SceneData (Mine/world/Scene.cpp:31-40).  The
+ * num_faces triangles of every bvhcd_scene given to this BVH are num_scenes
+ * independent scenes: scene s owns triangles [tri_offsets[s],
+ * tri_offsets[s+1]) (a host array of num_scenes + 1 ints, tri_offsets[0] = 0,
+ * at least 2 triangles per scene when num_scenes > 1; faces keep global
+ * vertex ids).  Each scene gets its own tree -- the tree it would get on its
+ * own, with its Morton slots shifted by tri_offsets[s] and its internal-node
+ * ids by tri_offsets[s] - s -- no pair crosses scenes, and every stage runs
+ * over all scenes in one launch.  Pairs carry global triangle ids;
+ * bvhcd_bvh_sizes reports num_faces - num_scenes internal nodes.  Requires
+ * enable_restr = 0.  num_scenes = 1 returns to a single scene; the next
+ * maintain rebuilds either way. */
+bvhcd_status bvhcd_bvh_set_scenes(bvhcd_bvh *bvh, int32_t num_scenes, const int32_t *tri_offsets);
+
+/* ---- Launch shapes of the front stages.  No counterpart in the reference,
+ * whose launcher derives one block size per kernel from occupancy
+ * (Mine/system/CudaDevice/CudaDevice.cu:86-95).  unroll: front entries one
+ * thread tests per step (1, 2 or 4; read by the four front scans); block:
+ * threads per block (128, 256 or 512).  Results never depend on the shapes. */
+enum {
+    BVHCD_SHAPE_KEEP = 0,       /* keep scan */
+    BVHCD_SHAPE_PRUNE_INT = 1,  /* prune/sprout update, internal entries */
+    BVHCD_SHAPE_PRUNE_EXT = 2,  /* prune/sprout update, external entries */
+    BVHCD_SHAPE_BALANCE = 3,    /* balance scan */
+    BVHCD_SHAPE_SPROUT = 4,     /* traversal below overlapping front nodes */
+    BVHCD_SHAPE_NARROW = 5,     /* narrow phase */
+    BVHCD_SHAPE_COUNT = 6
+};
+typedef struct {
+    int32_t unroll[BVHCD_SHAPE_COUNT];
+    int32_t block[BVHCD_SHAPE_COUNT];
+} bvhcd_launch_shapes;
+bvhcd_status bvhcd_front_get_shapes(const bvhcd_front *front, bvhcd_launch_shapes *shapes);
+/* Values outside the sets above return BVHCD_INVALID_ARG. */
+bvhcd_status bvhcd_front_set_shapes(bvhcd_front *front, const bvhcd_launch_shapes *shapes);
+/* Autotuner: on the front's current tree and front (it needs a generated
+ * front: BVHCD_NOT_READY otherwise), times each stage in every candidate
+ * shape -- 9 for the scans, 3 block sizes for sprout and the narrow phase --
+ * `repeats` times after one untimed run, and keeps the fastest.  The stages
+ * run on the real front without committing it; at the end the front is
+ * regenerated from the current tree (a GENERATE, pairs and hits included), so
+ * the next frame continues from a consistent state.  `chosen` (may be NULL)
+ * receives the shapes, `best_ms` (may be NULL, BVHCD_SHAPE_COUNT doubles)
+ * the mean time per run of each stage in its chosen shape.  Synchronises
+ * `stream`. */
+bvhcd_status bvhcd_front_autotune(bvhcd_front *front, int32_t repeats, bvhcd_launch_shapes *chosen,
+                                  double *best_ms, void *stream);
+
+/* ---- Graph-launched frame.  No counterpart in the reference.  Runs
+ * bvhcd_bvh_maintain(bvh_op) then bvhcd_front_maintain(front_op) on
+ * `stream` (not the legacy default stream).  The first call runs ordinary
+ * launches (it sizes every buffer); afterwards each distinct (bvh_op,
+ * front_op, host-side state of both handles) is captured once as a CUDA
+ * graph, launched, and replayed by later calls with the same key.  The scene
+ * must be device-resident (on_device = 1) and use the same pointers and sizes
+ * on every call: the graphs read it in place, so the caller writes each
+ * frame's positions into that buffer before the call.  Requires
+ * enable_restr = 0 on the BVH and auto_grow = 0 on the front (capacities are
+ * fixed inside a graph; an overflow still shows in bvhcd_front_stats).
+ * Another scene pointer or size, bvhcd_bvh_set_scenes, or a change of
+ * launch shapes drops the captured graphs.  The stage profiler does not time graph-launched frames. */
+bvhcd_status bvhcd_frame_graph(bvhcd_bvh *bvh, bvhcd_front *front, const bvhcd_scene *scene,
+                               int32_t bvh_op, int32_t front_op, void *stream);
+
 /* ---- Scheduler: BenchmarkLogic::maintainScheme, STATIC_MANDATORY with
  * divergent marks (Mine/system/Logic/BenchmarkLogic.hpp:90-156). */
 bvhcd_status bvhcd_schedule_heuristic(int32_t frame, int32_t start_frame, int32_t *bvh_op,
