@@ -35,7 +35,13 @@ EXPORTED = [
     "bvhcd_schedule_heuristic", "bvhcd_frame", "bvhcd_profile_enable", "bvhcd_profile_read",
     "bvhcd_launch_count", "bvhcd_morton_order_noalloc", "bvhcd_bvh_set_scenes", "bvhcd_frame_graph",
     "bvhcd_front_get_shapes", "bvhcd_front_set_shapes", "bvhcd_front_autotune",
+    "bvhcd_bvh_copy_state", "bvhcd_front_copy_state",
+    "bvhcd_learner_create", "bvhcd_learner_destroy", "bvhcd_learner_set_params", "bvhcd_learner_get_params",
+    "bvhcd_learner_frame", "bvhcd_learner_observe", "bvhcd_learner_cut", "bvhcd_learner_features",
+    "bvhcd_learner_work", "bvhcd_mlp_gradient", "bvhcd_mlp_train", "bvhcd_mlp_predict",
 ]
+
+MLP_PARAMS = 5443
 
 SHAPE_STAGES = ["keep", "prune_int", "prune_ext", "balance", "sprout", "narrow"]
 
@@ -133,6 +139,22 @@ def lib():
             "bvhcd_front_get_shapes": (ctypes.c_int, [vp, ctypes.POINTER(LaunchShapes)]),
             "bvhcd_front_set_shapes": (ctypes.c_int, [vp, ctypes.POINTER(LaunchShapes)]),
             "bvhcd_front_autotune": (ctypes.c_int, [vp, i32, ctypes.POINTER(LaunchShapes), vp, vp]),
+            "bvhcd_bvh_copy_state": (ctypes.c_int, [vp, vp, vp]),
+            "bvhcd_front_copy_state": (ctypes.c_int, [vp, vp, vp]),
+            "bvhcd_learner_create": (ctypes.c_int, [vp, vp, i32, ctypes.POINTER(vp)]),
+            "bvhcd_learner_destroy": (ctypes.c_int, [vp]),
+            "bvhcd_learner_set_params": (ctypes.c_int, [vp, vp]),
+            "bvhcd_learner_get_params": (ctypes.c_int, [vp, vp]),
+            "bvhcd_learner_frame": (ctypes.c_int, [vp, ctypes.POINTER(Scene), i32, ctypes.POINTER(i32),
+                                                   ctypes.POINTER(i32), vp]),
+            "bvhcd_learner_observe": (ctypes.c_int, [vp, i32, i32, vp]),
+            "bvhcd_learner_cut": (ctypes.c_int, [vp, vp, i32, ctypes.POINTER(i32), vp]),
+            "bvhcd_learner_features": (ctypes.c_int, [vp, vp, i32, ctypes.POINTER(i32), vp]),
+            "bvhcd_learner_work": (ctypes.c_int, [vp, vp, vp, i32, vp]),
+            "bvhcd_mlp_gradient": (ctypes.c_int, [vp, vp, vp, i32, vp, vp, vp, vp]),
+            "bvhcd_mlp_train": (ctypes.c_int, [vp, vp, vp, i32, vp, i32, i32, ctypes.c_float, ctypes.c_uint32,
+                                               vp, vp]),
+            "bvhcd_mlp_predict": (ctypes.c_int, [vp, vp, i32, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -392,3 +414,112 @@ def frame_graph(bvh: LBvh, front: BvttFront, pos, faces, bvh_op: int, front_op: 
     _check(lib().bvhcd_frame_graph(bvh.handle, front.handle, ctypes.byref(sc), int(bvh_op), int(front_op),
                                    _stream_ptr(stream)), "frame graph")
     bvh._keep = keep
+
+
+def copy_state(dst_bvh: LBvh, src_bvh: LBvh, dst_front: "BvttFront" = None, src_front: "BvttFront" = None,
+               stream=None):
+    """dst becomes a copy of src (bvhcd_bvh_copy_state / bvhcd_front_copy_state)."""
+    _check(lib().bvhcd_bvh_copy_state(dst_bvh.handle, src_bvh.handle, _stream_ptr(stream)), "bvh copy")
+    if dst_front is not None:
+        _check(lib().bvhcd_front_copy_state(dst_front.handle, src_front.handle, _stream_ptr(stream)), "front copy")
+    dst_bvh._keep = src_bvh._keep
+
+
+def _dev_ptr(t):
+    import torch
+    assert isinstance(t, torch.Tensor) and t.is_cuda and t.is_contiguous()
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Learner:
+    """The learned scheduler over a BVH (enable_restr) and its front
+    (bvhcd_learner_*, bvhcd_mlp_*)."""
+
+    def __init__(self, bvh: LBvh, front: BvttFront, max_subtree_leaves: int = 512):
+        h = ctypes.c_void_p()
+        _check(lib().bvhcd_learner_create(bvh.handle, front.handle, int(max_subtree_leaves), ctypes.byref(h)),
+               "learner create")
+        self._h = h
+        self._bvh, self._front = bvh, front
+
+    def close(self):
+        if self._h:
+            lib().bvhcd_learner_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == MLP_PARAMS
+        _check(lib().bvhcd_learner_set_params(self._h, p.ctypes.data), "set params")
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(MLP_PARAMS, np.float32)
+        _check(lib().bvhcd_learner_get_params(self._h, p.ctypes.data), "get params")
+        return p
+
+    def frame(self, pos, faces, frame: int, stream=None):
+        sc, keep = _scene(pos, faces, True)
+        tag, fop = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().bvhcd_learner_frame(self._h, ctypes.byref(sc), int(frame), ctypes.byref(tag),
+                                         ctypes.byref(fop), _stream_ptr(stream)), "learner frame")
+        self._bvh._keep = keep
+        return tag.value, fop.value
+
+    def observe(self, tree_changed: bool, generated: bool, stream=None):
+        _check(lib().bvhcd_learner_observe(self._h, int(tree_changed), int(generated), _stream_ptr(stream)),
+               "observe")
+
+    def cut(self, stream=None) -> np.ndarray:
+        n = ctypes.c_int32()
+        _check(lib().bvhcd_learner_cut(self._h, None, 0, ctypes.byref(n), _stream_ptr(stream)), "cut")
+        out = np.zeros(max(n.value, 1), np.int32)
+        _check(lib().bvhcd_learner_cut(self._h, out.ctypes.data, out.size, ctypes.byref(n), _stream_ptr(stream)),
+               "cut")
+        return out[:n.value]
+
+    def features(self, stream=None) -> np.ndarray:
+        n = ctypes.c_int32()
+        _check(lib().bvhcd_learner_features(self._h, None, 0, ctypes.byref(n), _stream_ptr(stream)), "features")
+        X = np.zeros((max(n.value, 1), 16), np.float32)
+        _check(lib().bvhcd_learner_features(self._h, X.ctypes.data, X.shape[0], ctypes.byref(n),
+                                            _stream_ptr(stream)), "features")
+        return X[:n.value]
+
+    def work(self, front: BvttFront, n: int, stream=None) -> np.ndarray:
+        out = np.zeros(max(n, 1), np.int64)
+        _check(lib().bvhcd_learner_work(self._h, front.handle, out.ctypes.data, out.size, _stream_ptr(stream)),
+               "work")
+        return out[:n]
+
+    def gradient(self, X, y, class_weight=(1.0, 1.0, 1.0), stream=None):
+        """X: (n, 16) float32 CUDA tensor, y: (n,) int32 CUDA tensor."""
+        cw = np.ascontiguousarray(class_weight, dtype=np.float32)
+        g = np.zeros(MLP_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        _check(lib().bvhcd_mlp_gradient(self._h, _dev_ptr(X), _dev_ptr(y), int(X.shape[0]), cw.ctypes.data,
+                                        g.ctypes.data, loss.ctypes.data, _stream_ptr(stream)), "mlp gradient")
+        return g, float(loss[0])
+
+    def train(self, X, y, class_weight=(1.0, 1.0, 1.0), epochs=10, batch=4096, lr=1e-3, seed=0, stream=None):
+        cw = np.ascontiguousarray(class_weight, dtype=np.float32)
+        loss = np.zeros(1, np.float32)
+        _check(lib().bvhcd_mlp_train(self._h, _dev_ptr(X), _dev_ptr(y), int(X.shape[0]), cw.ctypes.data,
+                                     int(epochs), int(batch), float(lr), int(seed), loss.ctypes.data,
+                                     _stream_ptr(stream)), "mlp train")
+        return float(loss[0])
+
+    def predict(self, X, stream=None):
+        import torch
+        n = int(X.shape[0])
+        logits = torch.empty((max(n, 1), 3), dtype=torch.float32, device=X.device)
+        vote = torch.empty(max(n, 1), dtype=torch.int32, device=X.device)
+        _check(lib().bvhcd_mlp_predict(self._h, _dev_ptr(X), n, _dev_ptr(logits), _dev_ptr(vote),
+                                       _stream_ptr(stream)), "mlp predict")
+        torch.cuda.synchronize()
+        return logits[:n].cpu().numpy(), vote[:n].cpu().numpy()

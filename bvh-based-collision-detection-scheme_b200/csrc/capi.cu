@@ -3,6 +3,7 @@
 
 #include <vector>
 
+#include "learn.h"
 #include "pipeline.h"
 #include "prims.cuh"
 
@@ -37,6 +38,11 @@ struct bvhcd_front {
         graphs.clear();
         g_warm = false;
     }
+};
+
+struct bvhcd_learner {
+    bvhcd::Learner impl;
+    bvhcd_learner(bvhcd::LBvh *b, bvhcd::Front *f, int smax) : impl(b, f, smax) {}
 };
 
 namespace {
@@ -223,6 +229,110 @@ bvhcd_status bvhcd_frame(bvhcd_bvh *bvh, bvhcd_front *front, int32_t frame, int3
     st = bvhcd_bvh_maintain(bvh, (bvhcd_bvh_op)b, scene, stream);
     if (st != BVHCD_OK) return st;
     return bvhcd_front_maintain(front, (bvhcd_front_op)f, stream);
+}
+
+bvhcd_status bvhcd_bvh_copy_state(bvhcd_bvh *dst, const bvhcd_bvh *src, void *stream) {
+    if (!dst || !src) return BVHCD_INVALID_ARG;
+    return dst->impl.copy_state_from(src->impl, as_stream(stream));
+}
+
+bvhcd_status bvhcd_front_copy_state(bvhcd_front *dst, const bvhcd_front *src, void *stream) {
+    if (!dst || !src) return BVHCD_INVALID_ARG;
+    if (dst->impl.bvh() == src->impl.bvh()) return BVHCD_INVALID_ARG;  // two fronts on one BVH share counters
+    dst->drop_graphs();
+    return dst->impl.copy_state_from(src->impl, as_stream(stream));
+}
+
+bvhcd_status bvhcd_learner_create(bvhcd_bvh *bvh, bvhcd_front *front, int32_t max_subtree_leaves,
+                                  bvhcd_learner **out) {
+    if (!bvh || !front || !out || &bvh->impl != front->impl.bvh()) return BVHCD_INVALID_ARG;
+    bvhcd_learner *l = new (std::nothrow) bvhcd_learner(&bvh->impl, &front->impl, max_subtree_leaves);
+    if (!l) return BVHCD_OUT_OF_MEMORY;
+    bvhcd_status st = l->impl.init();
+    if (st != BVHCD_OK) {
+        delete l;
+        return st;
+    }
+    *out = l;
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_learner_destroy(bvhcd_learner *l) {
+    delete l;
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_learner_set_params(bvhcd_learner *l, const float *params) {
+    if (!l || !params) return BVHCD_INVALID_ARG;
+    return l->impl.set_params(params);
+}
+
+bvhcd_status bvhcd_learner_get_params(const bvhcd_learner *l, float *params) {
+    if (!l || !params) return BVHCD_INVALID_ARG;
+    return l->impl.get_params(params);
+}
+
+bvhcd_status bvhcd_learner_frame(bvhcd_learner *l, const bvhcd_scene *scene, int32_t frame, int32_t *bvh_tag,
+                                 int32_t *front_op, void *stream) {
+    if (!l || !scene) return BVHCD_INVALID_ARG;
+    return l->impl.frame(*scene, frame, as_stream(stream), bvh_tag, front_op);
+}
+
+bvhcd_status bvhcd_learner_observe(bvhcd_learner *l, int32_t tree_changed, int32_t front_generated, void *stream) {
+    if (!l) return BVHCD_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    l->impl.tick(tree_changed != 0, front_generated != 0);
+    bvhcd_status st = BVHCD_OK;
+    if (tree_changed) st = l->impl.on_tree_changed(s);
+    if (st == BVHCD_OK && front_generated) st = l->impl.on_front_generated(s);
+    return st;
+}
+
+bvhcd_status bvhcd_learner_cut(const bvhcd_learner *l, int32_t *roots, int32_t cap, int32_t *n, void *stream) {
+    if (!l || !n || cap < 0) return BVHCD_INVALID_ARG;
+    *n = l->impl.ncut();
+    if (!roots) return BVHCD_OK;
+    if (cap < *n) return BVHCD_CAPACITY_EXCEEDED;
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e = cudaMemcpyAsync(roots, l->impl.roots(), sizeof(int32_t) * (size_t)*n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return bvhcd::cuda_status(e);
+}
+
+bvhcd_status bvhcd_learner_features(bvhcd_learner *l, float *X, int32_t cap_rows, int32_t *n, void *stream) {
+    if (!l || !n || cap_rows < 0) return BVHCD_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    bvhcd_status st = l->impl.features(s);
+    if (st != BVHCD_OK) return st;
+    *n = l->impl.ncut();
+    if (!X) return BVHCD_OK;
+    if (cap_rows < *n) return BVHCD_CAPACITY_EXCEEDED;
+    cudaError_t e = cudaMemcpyAsync(X, l->impl.X(), sizeof(float) * 16 * (size_t)*n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return bvhcd::cuda_status(e);
+}
+
+bvhcd_status bvhcd_learner_work(bvhcd_learner *l, const bvhcd_front *front, int64_t *out, int32_t cap, void *stream) {
+    if (!l || !front || !out || cap < l->impl.ncut()) return BVHCD_INVALID_ARG;
+    return l->impl.work(front->impl, out, as_stream(stream));
+}
+
+bvhcd_status bvhcd_mlp_gradient(bvhcd_learner *l, const float *X, const int32_t *y, int32_t n,
+                                const float *class_weight, float *grad, float *loss, void *stream) {
+    if (!l || !X || !y || !class_weight || n <= 0) return BVHCD_INVALID_ARG;
+    return l->impl.gradient(X, y, class_weight, n, grad, loss, as_stream(stream));
+}
+
+bvhcd_status bvhcd_mlp_train(bvhcd_learner *l, const float *X, const int32_t *y, int32_t n, const float *class_weight,
+                             int32_t epochs, int32_t batch, float lr, uint32_t seed, float *last_loss, void *stream) {
+    if (!l || !X || !y || !class_weight) return BVHCD_INVALID_ARG;
+    return l->impl.train(X, y, n, class_weight, epochs, batch, lr, seed, last_loss, as_stream(stream));
+}
+
+bvhcd_status bvhcd_mlp_predict(bvhcd_learner *l, const float *X, int32_t n, float *logits, int32_t *vote,
+                               void *stream) {
+    if (!l || !X || n < 0) return BVHCD_INVALID_ARG;
+    return l->impl.predict(X, n, logits, vote, as_stream(stream));
 }
 
 bvhcd_status bvhcd_front_get_shapes(const bvhcd_front *front, bvhcd_launch_shapes *shapes) {

@@ -839,7 +839,7 @@ bvhcd_status Front::update_kernels(cudaStream_t s) {
 bvhcd_status Front::prune_sprout(cudaStream_t s) {
     bvhcd_status st = update_kernels(s);
     if (st != BVHCD_OK) return st;
-    if (bvh_->restr_enabled()) {
+    if (bvh_->restr_enabled() && quality_check_) {
         st = check_quality(s);
         if (st != BVHCD_OK) return st;
     }
@@ -1015,6 +1015,28 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     }
     last_op_ = run_op;
     k_counts64<<<1, 32, 0, s>>>(ctr, (unsigned)pcap_, (unsigned)pcap_, counts64_.as<int64_t>()); note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+bvhcd_status Front::copy_state_from(const Front &src, cudaStream_t s) {
+    if (&src == this) return BVHCD_OK;
+    bvhcd_status st = ensure_node_capacity(src.capT_);
+    if (st != BVHCD_OK) return st;
+    const DBuf *from[] = {&src.front_[0][0], &src.front_[0][1], &src.front_[1][0], &src.front_[1][1], &src.pairs_,
+                          &src.hits_, &src.work_, &src.intcnt_, &src.extcnt_, &src.intbeg_, &src.extbeg_,
+                          &src.intback_, &src.extback_, &src.snapshot_, &src.counts64_};
+    DBuf *to[] = {&front_[0][0], &front_[0][1], &front_[1][0], &front_[1][1], &pairs_, &hits_, &work_, &intcnt_,
+                  &extcnt_, &intbeg_, &extbeg_, &intback_, &extback_, &snapshot_, &counts64_};
+    for (size_t k = 0; k < sizeof(to) / sizeof(to[0]); k++) FR_TRY(to[k]->copy_from(*from[k], s));
+    fcap_[0] = src.fcap_[0];
+    fcap_[1] = src.fcap_[1];
+    pcap_ = src.pcap_;
+    cur_ = src.cur_;
+    last_op_ = src.last_op_;
+    has_front_ = src.has_front_;
+    int_swapped_ = src.int_swapped_;
+    for (int k = 0; k < BVHCD_SHAPE_COUNT; k++) shape_[k] = src.shape_[k];
+    shape_epoch_++;
     return cuda_status(cudaGetLastError());
 }
 

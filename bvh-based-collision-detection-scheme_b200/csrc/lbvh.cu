@@ -864,6 +864,30 @@ bvhcd_status LBvh::build(cudaStream_t s) {
     return BVHCD_OK;
 }
 
+bvhcd_status LBvh::copy_state_from(const LBvh &src, cudaStream_t s) {
+    if (&src == this) return BVHCD_OK;
+    if (src.cfg_.enable_restr != cfg_.enable_restr) return BVHCD_INVALID_ARG;
+    const DBuf *from[] = {&src.verts_, &src.faces_, &src.nrec_, &src.lrec_, &src.topo_, &src.nrange_, &src.lca_,
+                          &src.sface_, &src.primmap_, &src.code_, &src.refit_flag_, &src.intrange_, &src.rtroot_,
+                          &src.intmark_, &src.extrange_, &src.extmark_, &src.leafroot_, &src.ctr_,
+                          &src.scene_of_, &src.leafscene_, &src.sbox_, &src.tiles_, &src.scene_};
+    DBuf *to[] = {&verts_, &faces_, &nrec_, &lrec_, &topo_, &nrange_, &lca_, &sface_, &primmap_, &code_,
+                  &refit_flag_, &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &ctr_,
+                  &scene_of_, &leafscene_, &sbox_, &tiles_, &scene_};
+    bvhcd_status st = ensure_capacity(src.capT_, src.capV_);
+    if (st != BVHCD_OK) return st;
+    for (size_t k = 0; k < sizeof(to) / sizeof(to[0]); k++) BV_TRY(to[k]->copy_from(*from[k], s));
+    T_ = src.T_; V_ = src.V_;
+    built_ = src.built_; updated_ = src.updated_;
+    opt_tag_ = src.opt_tag_; rt_subtrees_ = src.rt_subtrees_; rt_intnodes_ = src.rt_intnodes_;
+    // input read in place stays where it is; an owned copy maps to this handle's copy
+    vptr_ = src.vptr_ == src.verts_.as<float>() ? verts_.as<float>() : src.vptr_;
+    fptr_ = src.fptr_ == src.faces_.as<int>() ? faces_.as<int>() : src.fptr_;
+    S_ = src.S_; ntiles_ = src.ntiles_; h_off_ = src.h_off_;
+    epoch_++;
+    return cuda_status(cudaGetLastError());
+}
+
 // Batched scenes (see the forest kernels above).  The layout is static: the
 // per-triangle scene ids and the box tiles are uploaded once here.
 bvhcd_status LBvh::set_scenes(int S, const int32_t *off) {
@@ -1014,6 +1038,22 @@ bvhcd_status LBvh::request_restructure(const int32_t *roots, int32_t n, cudaStre
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     tmp.release();
     BV_TRY(e);
+    updated_ = true;
+    return BVHCD_OK;
+}
+
+bvhcd_status LBvh::request_restructure_device(const int32_t *roots, int32_t n, cudaStream_t s) {
+    if (n < 0 || (n > 0 && !roots)) return BVHCD_INVALID_ARG;
+    if (!built_) return BVHCD_NOT_READY;
+    if (!cfg_.enable_restr || T_ < 2 || n == 0) return BVHCD_OK;
+    const int T = T_;
+    if (!updated_) {
+        k_fill<<<grid_for(T), kThreads, 0, s>>>(T, rtroot_.as<int>(), INT_MAX); note_launch();
+        BV_TRY(cudaMemsetAsync(intrange_.p, 0, sizeof(int) * (size_t)T, s));
+    }
+    k_mark_roots<<<grid_for(n), kThreads, 0, s>>>(n, T - 1, roots, nrange_.as<int2>(), intrange_.as<int>(),
+                                                  rtroot_.as<int>()); note_launch();
+    BV_TRY(cudaGetLastError());
     updated_ = true;
     return BVHCD_OK;
 }

@@ -1,0 +1,681 @@
+// learn.cu -- the learned scheduler.  No counterpart in the reference, whose
+// scheduler is the static cycle of BenchmarkLogic::maintainScheme
+// (Mine/system/Logic/BenchmarkLogic.hpp:90-156) plus the front-quality check
+// (checkFrontQuality, Mine/collision/bvtt_front/BvttFrontGenerateKernels.cu:34-49).
+//
+// The tree is cut into disjoint subtrees (every internal node with at most
+// smax leaves whose parent has more); per subtree 16 features are computed on
+// the GPU every frame, a 16-64-64-3 MLP (BF16 weights, FP32 accumulation)
+// votes refit / restructure / regenerate-the-front, and the votes become the
+// reference's own maintenance operations: restructure marks on the voted
+// subtrees (the BvhRestrLog marks checkFrontQuality would write), and a front
+// GENERATE when subtrees holding most leaves vote for it.  None of this
+// changes a result: every operation keeps the pair set exact.
+//
+// Training runs on the GPU as well: one kernel computes the loss gradient of
+// a minibatch (forward and backward for 128 rows per block, outer-product
+// sums in shared memory), one applies Adam to the FP32 master weights and
+// writes the BF16 copy the forward passes read.
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "learn.h"
+#include "prims.cuh"
+
+namespace bvhcd {
+
+#define LN_TRY(x)                                        \
+    do {                                                 \
+        cudaError_t e__ = (x);                           \
+        if (e__ != cudaSuccess) return cuda_status(e__); \
+    } while (0)
+
+namespace {
+
+constexpr int kThreads = 256;
+inline unsigned blocks_for(int64_t n, int per = kThreads) {
+    int64_t g = (n + per - 1) / per;
+    if (g < 1) g = 1;
+    if (g > 65535LL * 16) g = 65535LL * 16;
+    return (unsigned)g;
+}
+
+// ---------------------------------------------------------------- tree cut
+// cut roots: internal nodes with <= smax leaves whose parent has more (or
+// that are the root)
+__global__ void k_cut_flags(int nint, const int2 *__restrict__ nrange, const int4 *__restrict__ topo, int smax,
+                            unsigned *flag) {
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nint; d += gridDim.x * blockDim.x) {
+        const int2 r = nrange[d];
+        const int size = r.y - r.x + 1;
+        bool cut = size <= smax;
+        if (cut) {
+            const int p = topo[d].z;
+            if (p >= 0) {
+                const int2 q = nrange[p];
+                cut = (q.y - q.x + 1) > smax;
+            }
+        }
+        flag[d] = cut ? 1u : 0u;
+    }
+}
+
+__global__ void k_cut_compact(int nint, const unsigned *__restrict__ flag, const unsigned *__restrict__ pos,
+                              int *roots) {
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nint; d += gridDim.x * blockDim.x)
+        if (flag[d]) roots[pos[d]] = d;
+}
+
+// ---------------------------------------------------------------- snapshots
+__device__ __forceinline__ float box_area(const float4 &lo, const float4 &hi) {
+    const float x = fmaxf(hi.x - lo.x, 0.f), y = fmaxf(hi.y - lo.y, 0.f), z = fmaxf(hi.z - lo.z, 0.f);
+    return 2.f * (x * y + y * z + z * x);
+}
+__device__ __forceinline__ float box_volume(const float4 &lo, const float4 &hi) {
+    return fmaxf(hi.x - lo.x, 0.f) * fmaxf(hi.y - lo.y, 0.f) * fmaxf(hi.z - lo.z, 0.f);
+}
+
+// per node {area, volume} and per leaf box centre, at the last build
+__global__ void k_build_snapshot(int T, const float4 *__restrict__ nrec, const float4 *__restrict__ lrec,
+                                 float2 *av, float4 *cen) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) {
+        if (i < T - 1) {
+            const float4 lo = nrec[2 * i], hi = nrec[2 * i + 1];
+            av[i] = make_float2(box_area(lo, hi), box_volume(lo, hi));
+        }
+        const float4 lo = lrec[2 * i], hi = lrec[2 * i + 1];
+        cen[i] = make_float4(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z),
+                             sqrtf((hi.x - lo.x) * (hi.x - lo.x) + (hi.y - lo.y) * (hi.y - lo.y) +
+                                   (hi.z - lo.z) * (hi.z - lo.z)));
+    }
+}
+
+// mean leaf-box diagonal at the build: a fixed-order two-level sum, so the
+// features (and the votes) do not depend on the schedule
+constexpr int kDiagBlocks = 256;
+__global__ void __launch_bounds__(kThreads) k_diag_partial(int T, const float4 *__restrict__ cen, double *part) {
+    const int per = (T + kDiagBlocks - 1) / kDiagBlocks;
+    const int a = blockIdx.x * per, b = min(T, a + per);
+    double v = 0.0;
+    for (int i = a + threadIdx.x; i < b; i += blockDim.x) v += cen[i].w;
+    __shared__ double s[kThreads];
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = kThreads / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+}
+__global__ void k_diag_final(int T, const double *__restrict__ part, float *diag) {
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int k = 0; k < kDiagBlocks; k++) v += part[k];
+        const double m = T > 0 ? v / T : 1.0;
+        diag[0] = (float)(m > 1e-30 ? m : 1e-30);
+    }
+}
+
+// ---------------------------------------------------------------- features
+// One warp per cut subtree.  The subtree of DFS node r with leaves [x, y]
+// holds the internal nodes [r, r + y - x) and the leaves [x, y]; front
+// entries per node are differences of the front log's begins.
+__global__ void __launch_bounds__(kThreads) k_features(int ncut, const int *__restrict__ roots, Tree t,
+                                                       const unsigned *__restrict__ intbeg,
+                                                       const unsigned *__restrict__ extbeg,
+                                                       const unsigned *__restrict__ gen_intbeg,
+                                                       const unsigned *__restrict__ gen_extbeg,
+                                                       const float2 *__restrict__ av_b,
+                                                       const float4 *__restrict__ cen_b,
+                                                       const float *__restrict__ diag, float since_build,
+                                                       float since_gen, float *X) {
+    const int lane = threadIdx.x & 31;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const float inv_diag = 1.f / __ldg(diag);
+    for (int c = w; c < ncut; c += nw) {
+        const int r = roots[c];
+        const int2 rg = t.nrange[r];
+        const int size = rg.y - rg.x + 1;
+        float sah_now = 0.f, sah_b = 0.f;
+        for (int d = r + lane; d < r + size - 1; d += 32) {
+            sah_now += box_area(t.nrec[2 * d], t.nrec[2 * d + 1]);
+            sah_b += av_b[d].x;
+        }
+        float dsum = 0.f, dmax = 0.f, dbig = 0.f;
+        for (int s = rg.x + lane; s <= rg.y; s += 32) {
+            const float4 lo = t.lrec[2 * s], hi = t.lrec[2 * s + 1];
+            const float4 cb = cen_b[s];
+            const float dx = 0.5f * (lo.x + hi.x) - cb.x, dy = 0.5f * (lo.y + hi.y) - cb.y,
+                        dz = 0.5f * (lo.z + hi.z) - cb.z;
+            const float dd = sqrtf(dx * dx + dy * dy + dz * dz) * inv_diag;
+            dsum += dd;
+            dmax = fmaxf(dmax, dd);
+            dbig += dd > 0.5f ? 1.f : 0.f;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sah_now += __shfl_xor_sync(0xffffffffu, sah_now, o);
+            sah_b += __shfl_xor_sync(0xffffffffu, sah_b, o);
+            dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+            dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+            dbig += __shfl_xor_sync(0xffffffffu, dbig, o);
+        }
+        if (lane == 0) {
+            const float a_now = box_area(t.nrec[2 * r], t.nrec[2 * r + 1]);
+            const float v_now = box_volume(t.nrec[2 * r], t.nrec[2 * r + 1]);
+            const float2 ab = av_b[r];
+            int depth = 0;
+            for (int p = t.topo[r].z; p >= 0 && depth < 64; p = t.topo[p].z) depth++;
+            const float ie = (float)(intbeg[r + size - 1] - intbeg[r]);
+            const float ee = (float)(extbeg[rg.y + 1] - extbeg[rg.x]);
+            const float ie0 = (float)(gen_intbeg[r + size - 1] - gen_intbeg[r]);
+            const float ee0 = (float)(gen_extbeg[rg.y + 1] - gen_extbeg[rg.x]);
+            const float inv = 1.f / (float)size;
+            float *x = X + 16 * (size_t)c;
+            x[0] = log2f((float)size) * (1.f / 16.f);
+            x[1] = depth * (1.f / 32.f);
+            x[2] = fminf((sah_now / fmaxf(a_now, 1e-30f)) / fmaxf(sah_b / fmaxf(ab.x, 1e-30f), 1e-30f), 16.f);
+            x[3] = fminf(fmaxf(logf(fmaxf(v_now, 1e-30f) / fmaxf(ab.y, 1e-30f)), -8.f), 8.f);
+            x[4] = fminf(a_now / fmaxf(ab.x, 1e-30f), 16.f);
+            x[5] = fminf(dsum * inv, 16.f);
+            x[6] = fminf(dmax, 16.f);
+            x[7] = fminf((ie + ee) / fmaxf(ie0 + ee0, 1.f), 16.f);
+            x[8] = fminf(fmaxf(ie / fmaxf(ee, 1.f) - ie0 / fmaxf(ee0, 1.f), -16.f), 16.f);
+            x[9] = fminf(ee * inv, 64.f) * (1.f / 16.f);
+            x[10] = fminf(ie * inv, 64.f) * (1.f / 16.f);
+            x[11] = since_build * (1.f / 12.f);
+            x[12] = since_gen * (1.f / 6.f);
+            x[13] = dbig * inv;
+            x[14] = log2f((float)t.T) * (1.f / 24.f);
+            x[15] = 1.f;
+        }
+    }
+}
+
+// front entries per cut subtree, for counterfactual labelling
+__global__ void k_work(int ncut, const int *__restrict__ roots, const int2 *__restrict__ nrange,
+                       const unsigned *__restrict__ intbeg, const unsigned *__restrict__ extbeg, int64_t *out) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncut; c += gridDim.x * blockDim.x) {
+        const int r = roots[c];
+        const int2 rg = nrange[r];
+        const int size = rg.y - rg.x + 1;
+        out[c] = (int64_t)(intbeg[r + size - 1] - intbeg[r]) + (int64_t)(extbeg[rg.y + 1] - extbeg[rg.x]);
+    }
+}
+
+// ---------------------------------------------------------------- MLP
+// params (FP32 master, kMlpParams): W1[16][64], b1[64], W2[64][64], b2[64],
+// W3[64][3], b3[3]; the forward reads the BF16 copy of the weight matrices
+// and the FP32 biases.
+constexpr int kIn = 16, kH = 64, kOut = 3;
+constexpr int oW1 = 0, oB1 = oW1 + kIn * kH, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH,
+              oB3 = oW3 + kH * kOut;
+static_assert(oB3 + kOut == kMlpParams, "parameter layout");
+
+__device__ __forceinline__ float bf(const __nv_bfloat16 *w, int i) { return __bfloat162float(w[i]); }
+
+// one thread per row: logits and the argmax vote
+__global__ void __launch_bounds__(kThreads) k_mlp_infer(int n, const float *__restrict__ X,
+                                                        const __nv_bfloat16 *__restrict__ wq,
+                                                        const float *__restrict__ p, float *logits, int *vote) {
+    __shared__ float w[kMlpParams];
+    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
+        const bool bias = (i >= oB1 && i < oW2) || (i >= oB2 && i < oW3) || i >= oB3;
+        w[i] = bias ? p[i] : bf(wq, i);
+    }
+    __syncthreads();
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        float x[kIn], h1[kH];
+#pragma unroll
+        for (int k = 0; k < kIn; k++) x[k] = X[kIn * (size_t)r + k];
+        for (int j = 0; j < kH; j++) {
+            float a = w[oB1 + j];
+#pragma unroll
+            for (int k = 0; k < kIn; k++) a = fmaf(x[k], w[oW1 + k * kH + j], a);
+            h1[j] = fmaxf(a, 0.f);
+        }
+        float o[kOut] = {w[oB3], w[oB3 + 1], w[oB3 + 2]};
+        for (int j = 0; j < kH; j++) {
+            float a = w[oB2 + j];
+            for (int k = 0; k < kH; k++) a = fmaf(h1[k], w[oW2 + k * kH + j], a);
+            a = fmaxf(a, 0.f);
+#pragma unroll
+            for (int c = 0; c < kOut; c++) o[c] = fmaf(a, w[oW3 + j * kOut + c], o[c]);
+        }
+        int best = 0;
+#pragma unroll
+        for (int c = 0; c < kOut; c++) {
+            if (logits) logits[kOut * (size_t)r + c] = o[c];
+            if (o[c] > o[best]) best = c;
+        }
+        if (vote) vote[r] = best;
+    }
+}
+
+// Minibatch gradient of the class-weighted cross-entropy
+// L = (1/N) sum_r cw[y_r] CE(softmax(logits_r), y_r), accumulated into grad
+// (FP32) and loss.  128 rows per block: thread r (of 128) runs its row's
+// forward and backward into shared memory, then all 256 threads sum the
+// outer products over the block's rows and add them to the global gradient.
+constexpr int kRows = 128;
+struct GradSmem {  // rows padded by one word: row-per-thread access is conflict-free
+    float w[kMlpParams];
+    float x[kRows][kIn + 1];
+    float h1[kRows][kH + 1];
+    float h2[kRows][kH + 1];
+    float d1[kRows][kH + 1];
+    float d2[kRows][kH + 1];
+    float dl[kRows][kOut];
+};
+
+__global__ void __launch_bounds__(kThreads) k_mlp_grad(int n, const float *__restrict__ X, const int *__restrict__ y,
+                                                       const float *__restrict__ cw, float inv_n,
+                                                       const __nv_bfloat16 *__restrict__ wq,
+                                                       const float *__restrict__ p, float *grad, float *loss) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GradSmem &sm = *reinterpret_cast<GradSmem *>(smem_raw);
+    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
+        const bool bias = (i >= oB1 && i < oW2) || (i >= oB2 && i < oW3) || i >= oB3;
+        sm.w[i] = bias ? p[i] : bf(wq, i);
+    }
+    const int r0 = blockIdx.x * kRows;
+    const int rows = min(kRows, n - r0);
+    for (int i = threadIdx.x; i < kRows * kIn; i += blockDim.x) {
+        const int r = i / kIn, k = i % kIn;
+        sm.x[r][k] = r < rows ? X[kIn * (size_t)(r0 + r) + k] : 0.f;
+    }
+    __syncthreads();
+    float my_loss = 0.f;
+    if (threadIdx.x < kRows) {
+        const int r = threadIdx.x;
+        if (r < rows) {
+            for (int j = 0; j < kH; j++) {
+                float a = sm.w[oB1 + j];
+                for (int k = 0; k < kIn; k++) a = fmaf(sm.x[r][k], sm.w[oW1 + k * kH + j], a);
+                sm.h1[r][j] = fmaxf(a, 0.f);
+            }
+            float o[kOut] = {sm.w[oB3], sm.w[oB3 + 1], sm.w[oB3 + 2]};
+            for (int j = 0; j < kH; j++) {
+                float a = sm.w[oB2 + j];
+                for (int k = 0; k < kH; k++) a = fmaf(sm.h1[r][k], sm.w[oW2 + k * kH + j], a);
+                a = fmaxf(a, 0.f);
+                sm.h2[r][j] = a;
+                for (int c = 0; c < kOut; c++) o[c] = fmaf(a, sm.w[oW3 + j * kOut + c], o[c]);
+            }
+            const float m = fmaxf(o[0], fmaxf(o[1], o[2]));
+            float e[kOut], z = 0.f;
+            for (int c = 0; c < kOut; c++) {
+                e[c] = expf(o[c] - m);
+                z += e[c];
+            }
+            const int lab = y[r0 + r];
+            const float wt = cw[lab] * inv_n;
+            my_loss = wt * (logf(z) + m - o[lab]);
+            for (int c = 0; c < kOut; c++) sm.dl[r][c] = wt * (e[c] / z - (c == lab ? 1.f : 0.f));
+            for (int j = 0; j < kH; j++) {
+                float g = 0.f;
+                for (int c = 0; c < kOut; c++) g = fmaf(sm.dl[r][c], sm.w[oW3 + j * kOut + c], g);
+                sm.d2[r][j] = sm.h2[r][j] > 0.f ? g : 0.f;
+            }
+            for (int k = 0; k < kH; k++) {
+                float g = 0.f;
+                for (int j = 0; j < kH; j++) g = fmaf(sm.d2[r][j], sm.w[oW2 + k * kH + j], g);
+                sm.d1[r][k] = sm.h1[r][k] > 0.f ? g : 0.f;
+            }
+        } else {
+            for (int j = 0; j < kH; j++) sm.h1[r][j] = sm.h2[r][j] = sm.d1[r][j] = sm.d2[r][j] = 0.f;
+            for (int c = 0; c < kOut; c++) sm.dl[r][c] = 0.f;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
+        float g = 0.f;
+        if (i < oB1) {
+            const int k = i / kH, j = i % kH;
+            for (int r = 0; r < kRows; r++) g = fmaf(sm.x[r][k], sm.d1[r][j], g);
+        } else if (i < oW2) {
+            const int j = i - oB1;
+            for (int r = 0; r < kRows; r++) g += sm.d1[r][j];
+        } else if (i < oB2) {
+            const int k = (i - oW2) / kH, j = (i - oW2) % kH;
+            for (int r = 0; r < kRows; r++) g = fmaf(sm.h1[r][k], sm.d2[r][j], g);
+        } else if (i < oW3) {
+            const int j = i - oB2;
+            for (int r = 0; r < kRows; r++) g += sm.d2[r][j];
+        } else if (i < oB3) {
+            const int j = (i - oW3) / kOut, c = (i - oW3) % kOut;
+            for (int r = 0; r < kRows; r++) g = fmaf(sm.h2[r][j], sm.dl[r][c], g);
+        } else {
+            const int c = i - oB3;
+            for (int r = 0; r < kRows; r++) g += sm.dl[r][c];
+        }
+        atomicAdd(grad + i, g);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) my_loss += __shfl_xor_sync(0xffffffffu, my_loss, o);
+    if ((threadIdx.x & 31) == 0 && my_loss != 0.f) atomicAdd(loss, my_loss);
+}
+
+// Adam on the FP32 master weights (Kingma & Ba), then the BF16 copy.
+__global__ void k_adam(int n, float *p, float *g, float *m, float *v, __nv_bfloat16 *wq, float lr, float b1,
+                       float b2, float eps, float c1, float c2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        p[i] = pi;
+        wq[i] = __float2bfloat16_rn(pi);
+        g[i] = 0.f;
+    }
+}
+
+__global__ void k_to_bf16(int n, const float *__restrict__ p, __nv_bfloat16 *wq) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        wq[i] = __float2bfloat16_rn(p[i]);
+}
+
+// gather rows `idx` of X / y into a contiguous minibatch
+__global__ void k_gather_rows(int n, const int *__restrict__ idx, const float *__restrict__ X,
+                              const int *__restrict__ y, float *Xb, int *yb) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * kIn; i += gridDim.x * blockDim.x) {
+        const int r = i / kIn, k = i % kIn;
+        Xb[i] = X[kIn * (size_t)idx[r] + k];
+        if (k == 0) yb[r] = y[idx[r]];
+    }
+}
+
+// votes -> restructure root list and the leaf-weighted share of front
+// regeneration votes: out[0] = restructure roots, out[1] = leaves voting
+// regenerate, out[2] = leaves covered by the cut
+__global__ void k_actions(int ncut, const int *__restrict__ roots, const int *__restrict__ vote,
+                          const int2 *__restrict__ nrange, int *rt_roots, unsigned long long *out) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncut; c += gridDim.x * blockDim.x) {
+        const int r = roots[c];
+        const int2 rg = nrange[r];
+        const unsigned long long size = (unsigned long long)(rg.y - rg.x + 1);
+        atomicAdd(out + 2, size);
+        if (vote[c] == 1) rt_roots[atomicAdd(out, 1ull)] = r;
+        else if (vote[c] == 2) atomicAdd(out + 1, size);
+    }
+}
+
+}  // namespace
+
+// ====================================================================== host
+Learner::~Learner() {
+    DBuf *bufs[] = {&roots_, &flag_, &pos_, &scratch_, &av_b_, &cen_b_, &diag_, &dpart_, &gen_intbeg_,
+                    &gen_extbeg_, &X_, &logits_, &vote_, &rt_roots_, &act_, &work_, &p_, &wq_, &g_, &m_, &v_,
+                    &loss_, &bx_, &by_, &bidx_, &cw_};
+    for (DBuf *b : bufs) b->release();
+    if (h_act_) cudaFreeHost(h_act_);
+}
+
+bvhcd_status Learner::init() {
+    // restructure marks need a BVH that restructures; a forest has no restructure
+    if (smax_ < 2 || !bvh_->restr_enabled() || bvh_->num_scenes() != 1) return BVHCD_INVALID_ARG;
+    front_->set_quality_check(false);
+    LN_TRY(p_.reserve(sizeof(float) * kMlpParams));
+    LN_TRY(wq_.reserve(sizeof(__nv_bfloat16) * kMlpParams));
+    LN_TRY(g_.reserve(sizeof(float) * kMlpParams));
+    LN_TRY(m_.reserve(sizeof(float) * kMlpParams));
+    LN_TRY(v_.reserve(sizeof(float) * kMlpParams));
+    LN_TRY(loss_.reserve(sizeof(float)));
+    LN_TRY(act_.reserve(sizeof(unsigned long long) * 4));
+    LN_TRY(diag_.reserve(sizeof(float)));
+    LN_TRY(dpart_.reserve(sizeof(double) * kDiagBlocks));
+    LN_TRY(cw_.reserve(sizeof(float) * 3));
+    LN_TRY(cudaMallocHost(&h_act_, sizeof(unsigned long long) * 4));
+    // He-style initialisation from a fixed LCG, so an untrained network is reproducible
+    std::vector<float> p(kMlpParams, 0.f);
+    unsigned long long st = 0x9E3779B97F4A7C15ull;
+    auto rnd = [&]() {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        return ((st >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0;
+    };
+    for (int i = oW1; i < oB1; i++) p[i] = (float)(rnd() * std::sqrt(6.0 / kIn));
+    for (int i = oW2; i < oB2; i++) p[i] = (float)(rnd() * std::sqrt(6.0 / kH));
+    for (int i = oW3; i < oB3; i++) p[i] = (float)(rnd() * std::sqrt(6.0 / kH));
+    return set_params(p.data());
+}
+
+bvhcd_status Learner::set_params(const float *host) {
+    LN_TRY(cudaMemcpy(p_.p, host, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice));
+    k_to_bf16<<<blocks_for(kMlpParams), kThreads>>>(kMlpParams, p_.as<float>(), wq_.as<__nv_bfloat16>());
+    note_launch();
+    LN_TRY(cudaMemset(g_.p, 0, sizeof(float) * kMlpParams));
+    LN_TRY(cudaMemset(m_.p, 0, sizeof(float) * kMlpParams));
+    LN_TRY(cudaMemset(v_.p, 0, sizeof(float) * kMlpParams));
+    adam_t_ = 0;
+    LN_TRY(cudaDeviceSynchronize());
+    return BVHCD_OK;
+}
+
+bvhcd_status Learner::get_params(float *host) const {
+    LN_TRY(cudaMemcpy(host, p_.p, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost));
+    return BVHCD_OK;
+}
+
+// After a build or a restructure: the cut and the build-time references.
+bvhcd_status Learner::on_tree_changed(cudaStream_t s) {
+    const int T = bvh_->T();
+    ncut_ = 0;
+    since_build_ = 0;
+    if (T < 2) return BVHCD_OK;
+    Tree t = bvh_->tree();
+    LN_TRY(flag_.reserve(sizeof(unsigned) * (size_t)(T + 1)));
+    LN_TRY(pos_.reserve(sizeof(unsigned) * (size_t)(T + 1)));
+    LN_TRY(roots_.reserve(sizeof(int) * (size_t)(T + 1)));
+    LN_TRY(scratch_.reserve(scan_scratch_bytes((int64_t)T + 1)));
+    LN_TRY(av_b_.reserve(sizeof(float2) * (size_t)T));
+    LN_TRY(cen_b_.reserve(sizeof(float4) * (size_t)T));
+    LN_TRY(cudaMemsetAsync(flag_.p, 0, sizeof(unsigned) * (size_t)(T + 1), s));
+    k_cut_flags<<<blocks_for(T - 1), kThreads, 0, s>>>(T - 1, t.nrange, t.topo, smax_, flag_.as<unsigned>());
+    note_launch();
+    LN_TRY(scan_u32(flag_.as<unsigned>(), pos_.as<unsigned>(), T, false, nullptr, scratch_.p, s));
+    k_cut_compact<<<blocks_for(T - 1), kThreads, 0, s>>>(T - 1, flag_.as<unsigned>(), pos_.as<unsigned>(),
+                                                         roots_.as<int>());
+    note_launch();
+    k_build_snapshot<<<blocks_for(T), kThreads, 0, s>>>(T, t.nrec, t.lrec, av_b_.as<float2>(), cen_b_.as<float4>());
+    note_launch();
+    k_diag_partial<<<kDiagBlocks, kThreads, 0, s>>>(T, cen_b_.as<float4>(), dpart_.as<double>());
+    note_launch();
+    k_diag_final<<<1, 32, 0, s>>>(T, dpart_.as<double>(), diag_.as<float>());
+    note_launch();
+    unsigned n = 0;  // exclusive scan over T flags (flag[T-1] = 0): pos[T-1] counts every cut root
+    LN_TRY(cudaMemcpyAsync(&n, pos_.as<unsigned>() + (T - 1), sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    LN_TRY(cudaStreamSynchronize(s));
+    ncut_ = (int)n;
+    LN_TRY(X_.reserve(sizeof(float) * 16 * (size_t)(ncut_ > 0 ? ncut_ : 1)));
+    LN_TRY(logits_.reserve(sizeof(float) * 3 * (size_t)(ncut_ > 0 ? ncut_ : 1)));
+    LN_TRY(vote_.reserve(sizeof(int) * (size_t)(ncut_ > 0 ? ncut_ : 1)));
+    LN_TRY(rt_roots_.reserve(sizeof(int) * (size_t)(ncut_ > 0 ? ncut_ : 1)));
+    LN_TRY(work_.reserve(sizeof(int64_t) * (size_t)(ncut_ > 0 ? ncut_ : 1)));
+    return BVHCD_OK;
+}
+
+// After a front GENERATE: the per-node entry counts of the fresh front.
+bvhcd_status Learner::on_front_generated(cudaStream_t s) {
+    const int T = bvh_->T();
+    since_gen_ = 0;
+    if (T < 2) return BVHCD_OK;
+    FrontLog l = front_->front_log();
+    LN_TRY(gen_intbeg_.reserve(sizeof(unsigned) * (size_t)(T + 1)));
+    LN_TRY(gen_extbeg_.reserve(sizeof(unsigned) * (size_t)(T + 1)));
+    LN_TRY(cudaMemcpyAsync(gen_intbeg_.p, l.intbeg, sizeof(unsigned) * (size_t)(T + 1), cudaMemcpyDeviceToDevice, s));
+    LN_TRY(cudaMemcpyAsync(gen_extbeg_.p, l.extbeg, sizeof(unsigned) * (size_t)(T + 1), cudaMemcpyDeviceToDevice, s));
+    return BVHCD_OK;
+}
+
+bvhcd_status Learner::features(cudaStream_t s) {
+    if (ncut_ == 0) return BVHCD_OK;
+    if (!gen_intbeg_.p) return BVHCD_NOT_READY;
+    FrontLog l = front_->front_log();
+    k_features<<<blocks_for((int64_t)ncut_ * 32), kThreads, 0, s>>>(
+        ncut_, roots_.as<int>(), bvh_->tree(), l.intbeg, l.extbeg, gen_intbeg_.as<unsigned>(),
+        gen_extbeg_.as<unsigned>(), av_b_.as<float2>(), cen_b_.as<float4>(), diag_.as<float>(), (float)since_build_,
+        (float)since_gen_, X_.as<float>());
+    note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+bvhcd_status Learner::work(const Front &f, int64_t *host, cudaStream_t s) {
+    if (ncut_ == 0) return BVHCD_OK;
+    FrontLog l = f.front_log();
+    k_work<<<blocks_for(ncut_), kThreads, 0, s>>>(ncut_, roots_.as<int>(), bvh_->tree().nrange, l.intbeg, l.extbeg,
+                                                 work_.as<int64_t>());
+    note_launch();
+    LN_TRY(cudaMemcpyAsync(host, work_.p, sizeof(int64_t) * (size_t)ncut_, cudaMemcpyDeviceToHost, s));
+    LN_TRY(cudaStreamSynchronize(s));
+    return BVHCD_OK;
+}
+
+bvhcd_status Learner::predict(const float *X, int n, float *logits, int *vote, cudaStream_t s) {
+    if (n <= 0) return BVHCD_OK;
+    k_mlp_infer<<<blocks_for(n), kThreads, 0, s>>>(n, X, wq_.as<__nv_bfloat16>(), p_.as<float>(), logits, vote);
+    note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+bvhcd_status Learner::gradient(const float *X, const int *y, const float *cw, int n, float *grad_host,
+                               float *loss_host, cudaStream_t s) {
+    if (n <= 0) return BVHCD_INVALID_ARG;
+    LN_TRY(cudaMemsetAsync(g_.p, 0, sizeof(float) * kMlpParams, s));
+    LN_TRY(cudaMemsetAsync(loss_.p, 0, sizeof(float), s));
+    LN_TRY(cudaMemcpyAsync(cw_.p, cw, sizeof(float) * 3, cudaMemcpyHostToDevice, s));
+    LN_TRY(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GradSmem)));
+    k_mlp_grad<<<(n + kRows - 1) / kRows, kThreads, sizeof(GradSmem), s>>>(
+        n, X, y, cw_.as<float>(), 1.f / n, wq_.as<__nv_bfloat16>(), p_.as<float>(), g_.as<float>(), loss_.as<float>());
+    note_launch();
+    LN_TRY(cudaGetLastError());
+    if (grad_host) LN_TRY(cudaMemcpyAsync(grad_host, g_.p, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, s));
+    if (loss_host) LN_TRY(cudaMemcpyAsync(loss_host, loss_.p, sizeof(float), cudaMemcpyDeviceToHost, s));
+    LN_TRY(cudaStreamSynchronize(s));
+    LN_TRY(cudaMemsetAsync(g_.p, 0, sizeof(float) * kMlpParams, s));
+    return BVHCD_OK;
+}
+
+// Minibatch Adam over (X, y) resident on the device; minibatches follow a
+// fixed-seed shuffle per epoch.  Returns the mean loss of the last epoch.
+bvhcd_status Learner::train(const float *X, const int *y, int n, const float *cw, int epochs, int batch, float lr,
+                            unsigned seed, float *last_loss, cudaStream_t s) {
+    if (n <= 0 || epochs <= 0 || batch <= 0 || batch > (1 << 20)) return BVHCD_INVALID_ARG;
+    LN_TRY(bx_.reserve(sizeof(float) * 16 * (size_t)batch));
+    LN_TRY(by_.reserve(sizeof(int) * (size_t)batch));
+    LN_TRY(bidx_.reserve(sizeof(int) * (size_t)n));
+    LN_TRY(cudaMemcpyAsync(cw_.p, cw, sizeof(float) * 3, cudaMemcpyHostToDevice, s));
+    LN_TRY(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GradSmem)));
+    std::vector<int> order((size_t)n);
+    unsigned long long st = 0x2545F4914F6CDD1Dull ^ seed;
+    double epoch_loss = 0.0;
+    for (int ep = 0; ep < epochs; ep++) {
+        for (int i = 0; i < n; i++) order[(size_t)i] = i;
+        for (int i = n - 1; i > 0; i--) {  // Fisher-Yates with an LCG
+            st = st * 6364136223846793005ull + 1442695040888963407ull;
+            const int j = (int)((st >> 33) % (unsigned long long)(i + 1));
+            std::swap(order[(size_t)i], order[(size_t)j]);
+        }
+        LN_TRY(cudaMemcpyAsync(bidx_.p, order.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+        LN_TRY(cudaMemsetAsync(loss_.p, 0, sizeof(float), s));
+        int nb = 0;
+        for (int b0 = 0; b0 < n; b0 += batch, nb++) {
+            const int m = n - b0 < batch ? n - b0 : batch;
+            k_gather_rows<<<blocks_for((int64_t)m * 16), kThreads, 0, s>>>(m, bidx_.as<int>() + b0, X, y,
+                                                                             bx_.as<float>(), by_.as<int>());
+            note_launch();
+            k_mlp_grad<<<(m + kRows - 1) / kRows, kThreads, sizeof(GradSmem), s>>>(
+                m, bx_.as<float>(), by_.as<int>(), cw_.as<float>(), 1.f / m, wq_.as<__nv_bfloat16>(), p_.as<float>(),
+                g_.as<float>(), loss_.as<float>());
+            note_launch();
+            adam_t_++;
+            const float b1 = 0.9f, b2 = 0.999f;
+            k_adam<<<blocks_for(kMlpParams), kThreads, 0, s>>>(kMlpParams, p_.as<float>(), g_.as<float>(), m_.as<float>(),
+                                                             v_.as<float>(), wq_.as<__nv_bfloat16>(), lr, b1, b2, 1e-8f,
+                                                             1.f - std::pow(b1, (float)adam_t_),
+                                                             1.f - std::pow(b2, (float)adam_t_));
+            note_launch();
+        }
+        float l = 0.f;
+        LN_TRY(cudaMemcpyAsync(&l, loss_.p, sizeof(float), cudaMemcpyDeviceToHost, s));
+        LN_TRY(cudaStreamSynchronize(s));
+        epoch_loss = nb ? l / nb : 0.0;
+    }
+    if (last_loss) *last_loss = (float)epoch_loss;
+    return cuda_status(cudaGetLastError());
+}
+
+// One decision: features -> votes -> restructure marks for the next BVH
+// maintain and the regenerate flag for the next front op.
+bvhcd_status Learner::decide(cudaStream_t s, int *n_restructure, double *regen_share) {
+    *n_restructure = 0;
+    *regen_share = 0.0;
+    if (ncut_ == 0) return BVHCD_OK;
+    bvhcd_status st = features(s);
+    if (st != BVHCD_OK) return st;
+    st = predict(X_.as<float>(), ncut_, nullptr, vote_.as<int>(), s);
+    if (st != BVHCD_OK) return st;
+    LN_TRY(cudaMemsetAsync(act_.p, 0, sizeof(unsigned long long) * 4, s));
+    k_actions<<<blocks_for(ncut_), kThreads, 0, s>>>(ncut_, roots_.as<int>(), vote_.as<int>(), bvh_->tree().nrange,
+                                                    rt_roots_.as<int>(), act_.as<unsigned long long>());
+    note_launch();
+    LN_TRY(cudaMemcpyAsync(h_act_, act_.p, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, s));
+    LN_TRY(cudaStreamSynchronize(s));
+    *n_restructure = (int)h_act_[0];
+    *regen_share = h_act_[2] ? (double)h_act_[1] / (double)h_act_[2] : 0.0;
+    if (*n_restructure > 0) {
+        st = bvh_->request_restructure_device(rt_roots_.as<int>(), *n_restructure, s);
+        if (st != BVHCD_OK) return st;
+    }
+    return BVHCD_OK;
+}
+
+// The learned frame: BVH refit (a restructure when the previous decision
+// marked subtrees; a build on the first frame), the front op of the
+// reference's cycle -- or GENERATE after a build or restructure, or when the
+// previous decision voted it -- then the next decision.
+bvhcd_status Learner::frame(const bvhcd_scene &scene, int32_t frame_no, cudaStream_t s, int32_t *bvh_op_run,
+                            int32_t *front_op_run) {
+    if (frame_no < 0) return BVHCD_INVALID_ARG;
+    const bool first = !bvh_->built() || frame_no == 0;
+    bvhcd_status st = bvh_->maintain(first ? BVHCD_BVH_BUILD : BVHCD_BVH_REFIT, scene, s);
+    if (st != BVHCD_OK) return st;
+    const int tag = bvh_->opt_tag();
+    const bool rebuilt = first || tag == 1 || tag == 2;
+    if (rebuilt) {
+        st = on_tree_changed(s);
+        if (st != BVHCD_OK) return st;
+    } else {
+        since_build_++;
+    }
+    bvhcd_front_op fop;
+    const int k = frame_no % 6;
+    if (rebuilt || regen_pending_ || !front_->has_front()) fop = BVHCD_FRONT_GENERATE;
+    else if (k == 0) fop = BVHCD_FRONT_UPDATE;
+    else if (k == 5) fop = BVHCD_FRONT_REORDER;
+    else fop = BVHCD_FRONT_KEEP;
+    st = front_->maintain(fop, s);
+    if (st != BVHCD_OK) return st;
+    if (fop == BVHCD_FRONT_GENERATE) {
+        st = on_front_generated(s);
+        if (st != BVHCD_OK) return st;
+    } else {
+        since_gen_++;
+    }
+    if (bvh_op_run) *bvh_op_run = first ? 2 : tag;  // the reference's opt tag: 0 refit, 1 restructure, 2 build
+    if (front_op_run) *front_op_run = (int32_t)fop;
+    int nr = 0;
+    double share = 0.0;
+    st = decide(s, &nr, &share);
+    if (st != BVHCD_OK) return st;
+    regen_pending_ = share > regen_threshold_;
+    last_restructure_ = nr;
+    last_regen_share_ = share;
+    return BVHCD_OK;
+}
+
+}  // namespace bvhcd

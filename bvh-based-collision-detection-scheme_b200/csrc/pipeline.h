@@ -36,6 +36,13 @@ struct DBuf {
     }
     template <typename T>
     T *as() const { return reinterpret_cast<T *>(p); }
+    // this buffer becomes a device copy of `src` (grown to its size)
+    cudaError_t copy_from(const DBuf &src, cudaStream_t s) {
+        if (!src.p) return cudaSuccess;
+        cudaError_t e = reserve(src.bytes);
+        if (e != cudaSuccess) return e;
+        return cudaMemcpyAsync(p, src.p, src.bytes, cudaMemcpyDeviceToDevice, s);
+    }
 };
 
 bvhcd_status cuda_status(cudaError_t e);
@@ -84,7 +91,12 @@ class LBvh {
     bvhcd_status export_tree(int32_t *inode, float *ibox, int32_t *leaf, float *lbox, int32_t *lca,
                              uint32_t *codes, int32_t *primmap, cudaStream_t s) const;
     bvhcd_status request_restructure(const int32_t *roots, int32_t n, cudaStream_t s);
+    // the same with the roots already on the device; enqueued only
+    bvhcd_status request_restructure_device(const int32_t *roots, int32_t n, cudaStream_t s);
     bvhcd_status set_scenes(int S, const int32_t *tri_offsets);
+    // Device and host state of `src` (same configuration) copied into this
+    // handle: a fork point for counterfactual runs.
+    bvhcd_status copy_state_from(const LBvh &src, cudaStream_t s);
     int num_scenes() const { return S_; }
     int layout_epoch() const { return epoch_; }  // bumped by every set_scenes
 
@@ -188,6 +200,12 @@ class Front {
     }
     bool auto_grow() const { return cfg_.auto_grow != 0; }
     LBvh *bvh() const { return bvh_; }
+    bvhcd_status copy_state_from(const Front &src, cudaStream_t s);
+    const FrontLog front_log() const { return log(); }
+    // the front-quality check of an UPDATE (checkFrontQuality) marks
+    // subtrees for restructuring; a scheduler that marks them itself turns it off
+    void set_quality_check(bool on) { quality_check_ = on; }
+    bool has_front() const { return has_front_; }
     void get_shapes(bvhcd_launch_shapes *sh) const;
     bvhcd_status set_shapes(const bvhcd_launch_shapes &sh);
     bvhcd_status autotune(int repeats, bvhcd_launch_shapes *chosen, double *best_ms, cudaStream_t s);
@@ -223,6 +241,7 @@ class Front {
     int shape_epoch_ = 0;
     bool has_front_ = false;
     bool int_swapped_ = false;
+    bool quality_check_ = true;
     DBuf front_[2][2];  // [set][0 int, 1 ext] int2 entries
     int64_t fcap_[2] = {0, 0};
     DBuf pairs_, hits_, outbuf_, work_;

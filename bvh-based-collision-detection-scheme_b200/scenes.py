@@ -107,11 +107,13 @@ def icosphere(freq: int, radius: float = 1.0, center=(0.0, 0.0, 0.0)):
 def cloth_over_sphere_frames(n: int = 512, frames: int = 100, seed: int = 2024,
                              sphere_freq: int = 45, amplitude: float = 0.2,
                              height: float = 0.2, radius: float = 0.25,
-                             first_frame: int = 0):
+                             first_frame: int = 0, wave_freq: float | None = None):
     """Cloth (n x n on [0,1]^2) folded by a seeded damped radial wave,
     z = height + A e^{-lambda t} sin(k r - omega t + phi), over a static
     icosphere centred under the cloth.  The step in t is chosen so that no
     vertex moves more than 2% of an edge length (1/(n-1)) per frame.
+    wave_freq, when given, fixes the wave number k = 2 pi wave_freq (else k is
+    drawn from the seed in 2 pi [2, 4]).
     Returns (faces, [pos per frame]) with the sphere appended after the cloth
     (vertex ids offset by the cloth's vertex count)."""
     x, y, cfaces = cloth_grid(n)
@@ -119,6 +121,8 @@ def cloth_over_sphere_frames(n: int = 512, frames: int = 100, seed: int = 2024,
     cx, cy = rng.uniform(0.3, 0.7, size=2)
     phi = rng.uniform(0.0, 2 * np.pi)
     k = 2 * np.pi * rng.uniform(2.0, 4.0)
+    if wave_freq is not None:      # the learned scheduler's training variants set it
+        k = 2 * np.pi * float(wave_freq)
     lam, omega = 0.5, 2 * np.pi
     edge = 1.0 / (n - 1)
     dt = 0.02 * edge / (amplitude * (omega + lam)) * 0.999

@@ -230,6 +230,86 @@ bvhcd_status bvhcd_morton_order_noalloc(const float *pos, const int32_t *faces, 
  * maintain rebuilds either way. */
 bvhcd_status bvhcd_bvh_set_scenes(bvhcd_bvh *bvh, int32_t num_scenes, const int32_t *tri_offsets);
 
+/* ---- State copies.  No counterpart in the reference.  dst becomes a copy of
+ * src -- tree, restructure log, counters, fronts, pairs and their host-side
+ * state -- so the two continue independently from the same frame (the
+ * learned scheduler's counterfactual runs fork this way).  dst must have the
+ * configuration src has (the same enable_restr; a front bound to another BVH
+ * handle, itself a copy of src's BVH).  Device input that src reads in place
+ * is read in place by dst too.  Asynchronous on `stream`. */
+bvhcd_status bvhcd_bvh_copy_state(bvhcd_bvh *dst, const bvhcd_bvh *src, void *stream);
+bvhcd_status bvhcd_front_copy_state(bvhcd_front *dst, const bvhcd_front *src, void *stream);
+
+/* ---- Learned scheduler.  No counterpart in the reference, whose schedule is
+ * the static cycle of BenchmarkLogic::maintainScheme plus the front-quality
+ * check (Mine/system/Logic/BenchmarkLogic.hpp:90-156,
+ * Mine/collision/bvtt_front/BvttFrontGenerateKernels.cu:34-49).
+ *
+ * The tree is cut into disjoint subtrees (internal nodes with at most
+ * max_subtree_leaves leaves whose parent has more).  Every frame the GPU
+ * computes 16 features per subtree (subtree size and depth, SAH ratio, box
+ * volume and area growth since the last build, mean / max / large leaf
+ * displacement since the last build in mean leaf diagonals, front entries and
+ * their int/ext balance against the last front generation, front density,
+ * frames since build and since generation, tree size, a constant) and a
+ * 16-64-64-3 MLP (BF16 weight matrices, FP32 biases and accumulation) votes
+ * per subtree: 0 refit, 1 restructure, 2 regenerate the front.  The votes
+ * become the reference's own operations: restructure marks on the voted
+ * subtrees (applied by the next BVH maintain with the reference's restructure
+ * decision), and a front GENERATE in the next frame when subtrees holding more
+ * than half of the cut's leaves vote for it.  Pair sets never depend on it.
+ * The BVH must have enable_restr = 1 and one scene; the learner turns the
+ * front's own quality check off.  The weights live on the device: set them
+ * (BVHCD_MLP_PARAMS floats: W1[16][64], b1[64], W2[64][64], b2[64],
+ * W3[64][3], b3[3], row-major, input index first) or train them with
+ * bvhcd_mlp_train. */
+#define BVHCD_MLP_PARAMS 5443
+typedef struct bvhcd_learner bvhcd_learner;
+bvhcd_status bvhcd_learner_create(bvhcd_bvh *bvh, bvhcd_front *front, int32_t max_subtree_leaves,
+                                  bvhcd_learner **out);
+bvhcd_status bvhcd_learner_destroy(bvhcd_learner *learner);
+bvhcd_status bvhcd_learner_set_params(bvhcd_learner *learner, const float *params);
+bvhcd_status bvhcd_learner_get_params(const bvhcd_learner *learner, float *params);
+/* One learned frame: BVH refit (build on frame 0; a restructure when the
+ * previous decision marked subtrees), the front op of the reference's cycle
+ * (UPDATE at frame % 6 == 0, REORDER at 5, KEEP otherwise) or GENERATE after a
+ * rebuild or a regenerate vote, then the next decision.  bvh_tag receives the
+ * reference's opt tag (0 refit, 1 restructure, 2 build), front_op the op run;
+ * either may be NULL.  Synchronises `stream` once (the decision's counts). */
+bvhcd_status bvhcd_learner_frame(bvhcd_learner *learner, const bvhcd_scene *scene, int32_t frame,
+                                 int32_t *bvh_tag, int32_t *front_op, void *stream);
+/* Trace recording under another schedule: after each frame's maintains, tell
+ * the learner whether the tree was rebuilt or restructured and whether the
+ * front was generated (it recomputes the cut and its references). */
+bvhcd_status bvhcd_learner_observe(bvhcd_learner *learner, int32_t tree_changed, int32_t front_generated,
+                                   void *stream);
+/* The cut's subtree roots (DFS ids) to host memory; roots may be NULL to ask
+ * for the count. */
+bvhcd_status bvhcd_learner_cut(const bvhcd_learner *learner, int32_t *roots, int32_t cap, int32_t *n, void *stream);
+/* The features of the current frame (n rows of 16 floats) to host memory; X
+ * may be NULL to compute them on the device only. */
+bvhcd_status bvhcd_learner_features(bvhcd_learner *learner, float *X, int32_t cap_rows, int32_t *n, void *stream);
+/* Front entries per cut subtree in `front` (any front over a tree that shares
+ * this learner's cut ranges: a copy, or one restructured inside them). */
+bvhcd_status bvhcd_learner_work(bvhcd_learner *learner, const bvhcd_front *front, int64_t *out, int32_t cap,
+                                void *stream);
+/* Training on the GPU.  X (n x 16 floats) and y (n labels in {0,1,2}) are
+ * device arrays, class_weight 3 host floats; the loss is the class-weighted
+ * mean cross-entropy (1/n) sum_r w[y_r] CE_r.  gradient: the loss gradient of
+ * all n rows at the current weights, to host memory (BVHCD_MLP_PARAMS floats,
+ * d loss / d master weight, the BF16 rounding passed straight through).
+ * train: `epochs` passes of Adam (beta 0.9 / 0.999, eps 1e-8) over minibatches
+ * of `batch` rows in a seeded shuffle; last_loss receives the mean minibatch
+ * loss of the last epoch.  predict: logits (n x 3) and votes of device rows;
+ * either output may be NULL. */
+bvhcd_status bvhcd_mlp_gradient(bvhcd_learner *learner, const float *X, const int32_t *y, int32_t n,
+                                const float *class_weight, float *grad, float *loss, void *stream);
+bvhcd_status bvhcd_mlp_train(bvhcd_learner *learner, const float *X, const int32_t *y, int32_t n,
+                             const float *class_weight, int32_t epochs, int32_t batch, float lr, uint32_t seed,
+                             float *last_loss, void *stream);
+bvhcd_status bvhcd_mlp_predict(bvhcd_learner *learner, const float *X, int32_t n, float *logits, int32_t *vote,
+                               void *stream);
+
 /* ---- Launch shapes of the front stages.  No counterpart in the reference,
  * whose launcher derives one block size per kernel from occupancy
  * (Mine/system/CudaDevice/CudaDevice.cu:86-95).  unroll: front entries one
