@@ -405,6 +405,28 @@ __global__ void k_actions(int ncut, const int *__restrict__ roots, const int *__
     }
 }
 
+// restructure marks (the BvhRestrLog marks checkFrontQuality writes,
+// BvttFrontGenerateKernels.cu:44-46) for the voted roots, count on the device;
+// the log is reset first (no other marker runs beside the learner)
+__global__ void k_mark_voted(int T, const unsigned long long *__restrict__ act, const int *__restrict__ roots,
+                             const int2 *__restrict__ nrange, int *intrange, int *rtroot) {
+    const int n = (int)act[0];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int i = roots[k];
+        const int2 r = nrange[i];
+        atomicAdd(intrange + i, 1);
+        atomicAdd(intrange + i + r.y - r.x, -1);
+        atomicMin(rtroot + r.x, i);
+    }
+}
+
+__global__ void k_reset_marks(int T, int *intrange, int *rtroot) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) {
+        intrange[i] = 0;
+        rtroot[i] = INT_MAX;
+    }
+}
+
 }  // namespace
 
 // ====================================================================== host
@@ -414,6 +436,7 @@ Learner::~Learner() {
                     &loss_, &bx_, &by_, &bidx_, &cw_};
     for (DBuf *b : bufs) b->release();
     if (h_act_) cudaFreeHost(h_act_);
+    if (ev_) cudaEventDestroy(ev_);
 }
 
 bvhcd_status Learner::init() {
@@ -431,6 +454,7 @@ bvhcd_status Learner::init() {
     LN_TRY(dpart_.reserve(sizeof(double) * kDiagBlocks));
     LN_TRY(cw_.reserve(sizeof(float) * 3));
     LN_TRY(cudaMallocHost(&h_act_, sizeof(unsigned long long) * 4));
+    LN_TRY(cudaEventCreateWithFlags(&ev_, cudaEventDisableTiming));
     // He-style initialisation from a fixed LCG, so an untrained network is reproducible
     std::vector<float> p(kMlpParams, 0.f);
     unsigned long long st = 0x9E3779B97F4A7C15ull;
@@ -466,6 +490,7 @@ bvhcd_status Learner::on_tree_changed(cudaStream_t s) {
     const int T = bvh_->T();
     ncut_ = 0;
     since_build_ = 0;
+    tree_epoch_++;
     if (T < 2) return BVHCD_OK;
     Tree t = bvh_->tree();
     LN_TRY(flag_.reserve(sizeof(unsigned) * (size_t)(T + 1)));
@@ -634,14 +659,56 @@ bvhcd_status Learner::decide(cudaStream_t s, int *n_restructure, double *regen_s
     return BVHCD_OK;
 }
 
-// The learned frame: BVH refit (a restructure when the previous decision
-// marked subtrees; a build on the first frame), the front op of the
-// reference's cycle -- or GENERATE after a build or restructure, or when the
-// previous decision voted it -- then the next decision.
+// Decision without a host wait: the votes are turned into restructure marks
+// and counts on the device, the counts copied to pinned memory and an event
+// recorded; a later frame applies them once the event has completed, unless
+// the tree changed in between (the marks name subtrees of the tree they were
+// voted on).
+bvhcd_status Learner::decide_async(cudaStream_t s) {
+    if (pending_ || ncut_ == 0 || bvh_->updated()) return BVHCD_OK;
+    bvhcd_status st = features(s);
+    if (st != BVHCD_OK) return st;
+    st = predict(X_.as<float>(), ncut_, nullptr, vote_.as<int>(), s);
+    if (st != BVHCD_OK) return st;
+    const int T = bvh_->T();
+    LN_TRY(cudaMemsetAsync(act_.p, 0, sizeof(unsigned long long) * 4, s));
+    k_actions<<<blocks_for(ncut_), kThreads, 0, s>>>(ncut_, roots_.as<int>(), vote_.as<int>(), bvh_->tree().nrange,
+                                                    rt_roots_.as<int>(), act_.as<unsigned long long>());
+    note_launch();
+    k_reset_marks<<<blocks_for(T), kThreads, 0, s>>>(T, bvh_->intrange(), bvh_->rtroot());
+    note_launch();
+    k_mark_voted<<<blocks_for(ncut_), kThreads, 0, s>>>(T, act_.as<unsigned long long>(), rt_roots_.as<int>(),
+                                                       bvh_->tree().nrange, bvh_->intrange(), bvh_->rtroot());
+    note_launch();
+    LN_TRY(cudaMemcpyAsync(h_act_, act_.p, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, s));
+    LN_TRY(cudaEventRecord(ev_, s));
+    pending_ = true;
+    pending_epoch_ = tree_epoch_;
+    return BVHCD_OK;
+}
+
+void Learner::poll() {
+    if (!pending_ || cudaEventQuery(ev_) != cudaSuccess) return;
+    pending_ = false;
+    if (pending_epoch_ != tree_epoch_) return;
+    last_restructure_ = (int)h_act_[0];
+    last_regen_share_ = h_act_[2] ? (double)h_act_[1] / (double)h_act_[2] : 0.0;
+    if (last_restructure_ > 0) bvh_->set_updated(true);
+    regen_pending_ = last_regen_share_ > regen_threshold_;
+    decisions_applied_++;
+}
+
+// The learned frame: apply a completed decision, BVH refit (a restructure
+// when a decision marked subtrees; a build on the first frame), the front op
+// of the reference's cycle -- or GENERATE after a build or restructure, or
+// when a decision voted it -- then, every decide_every frames, the next
+// decision (queued, applied in a later frame).
 bvhcd_status Learner::frame(const bvhcd_scene &scene, int32_t frame_no, cudaStream_t s, int32_t *bvh_op_run,
                             int32_t *front_op_run) {
     if (frame_no < 0) return BVHCD_INVALID_ARG;
+    poll();
     const bool first = !bvh_->built() || frame_no == 0;
+    if (first) pending_ = false;
     bvhcd_status st = bvh_->maintain(first ? BVHCD_BVH_BUILD : BVHCD_BVH_REFIT, scene, s);
     if (st != BVHCD_OK) return st;
     const int tag = bvh_->opt_tag();
@@ -668,13 +735,8 @@ bvhcd_status Learner::frame(const bvhcd_scene &scene, int32_t frame_no, cudaStre
     }
     if (bvh_op_run) *bvh_op_run = first ? 2 : tag;  // the reference's opt tag: 0 refit, 1 restructure, 2 build
     if (front_op_run) *front_op_run = (int32_t)fop;
-    int nr = 0;
-    double share = 0.0;
-    st = decide(s, &nr, &share);
-    if (st != BVHCD_OK) return st;
-    regen_pending_ = share > regen_threshold_;
-    last_restructure_ = nr;
-    last_regen_share_ = share;
+    if (fop == BVHCD_FRONT_GENERATE) regen_pending_ = false;
+    if (frame_no % decide_every_ == 0) return decide_async(s);
     return BVHCD_OK;
 }
 

@@ -34,6 +34,10 @@ class Learner {
     bvhcd_status train(const float *X, const int *y, int n, const float *cw, int epochs, int batch, float lr,
                        unsigned seed, float *last_loss, cudaStream_t s);
     bvhcd_status decide(cudaStream_t s, int *n_restructure, double *regen_share);
+    bvhcd_status decide_async(cudaStream_t s);
+    void poll();
+    void set_decide_every(int k) { decide_every_ = k > 0 ? k : 1; }
+    long long decisions_applied() const { return decisions_applied_; }
     bvhcd_status frame(const bvhcd_scene &scene, int32_t frame_no, cudaStream_t s, int32_t *bvh_tag,
                        int32_t *front_op_run);
 
@@ -51,6 +55,10 @@ class Learner {
     bool regen_pending_ = false;
     double regen_threshold_ = 0.5, last_regen_share_ = 0.0;
     int last_restructure_ = 0;
+    int decide_every_ = 3, tree_epoch_ = 0, pending_epoch_ = -1;
+    bool pending_ = false;
+    long long decisions_applied_ = 0;
+    cudaEvent_t ev_ = nullptr;
     unsigned long long *h_act_ = nullptr;
     DBuf roots_, flag_, pos_, scratch_, av_b_, cen_b_, diag_, dpart_, gen_intbeg_, gen_extbeg_, X_, logits_, vote_,
         rt_roots_, act_, work_, p_, wq_, g_, m_, v_, loss_, bx_, by_, bidx_, cw_;

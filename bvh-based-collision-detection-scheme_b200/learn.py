@@ -244,9 +244,11 @@ def _digest(p):
     return hashlib.sha256(p.tobytes()).hexdigest()
 
 
-def evaluate(torch, weights, n, frames, seed, check_every=1):
+def evaluate(torch, weights, n, frames, seed, check_every=1, decide_every=3):
     """Heuristic vs learned on one held-out sequence: device ms per frame and
-    equal pair sets."""
+    equal pair sets.  A third run, "cycle", is the learned mode's cycle with
+    no network (refit every frame, the front cycle, never a rebuild): what
+    the network adds beyond dropping the mandatory rebuilds."""
     w = np.load(weights)
     smax = int(w["smax"])
     faces, pos = scenes.cloth_over_sphere_frames(n, frames, seed=seed, amplitude=0.2)
@@ -257,23 +259,27 @@ def evaluate(torch, weights, n, frames, seed, check_every=1):
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * frames)]
     out = {}
     digests = {}
-    for mode in ("heuristic", "learned"):
-        bvh = bvhcd.LBvh(T, V, enable_restr=True)
+    for mode in ("heuristic", "learned", "cycle"):
+        bvh = bvhcd.LBvh(T, V, enable_restr=mode != "cycle")
         front = bvhcd.BvttFront(bvh, *caps, cull_adjacent=True, narrow_phase=True)
         lrn = None
         if mode == "learned":
             lrn = bvhcd.Learner(bvh, front, smax)
             lrn.set_params(w["params"])
+            lrn.set_decide_every(decide_every)
         tags, ops, dig = [], [], []
         for f in range(frames):
             ev[2 * f].record()
-            if lrn is None:
+            if mode == "heuristic":
                 bvhcd.frame(bvh, front, f, 0, dpos[f], dfaces)
+            elif mode == "cycle":
+                bvh.maintain(bvhcd.BVH_BUILD if f == 0 else bvhcd.BVH_REFIT, dpos[f], dfaces)
+                front.maintain(bvhcd.FRONT_GENERATE if f == 0 else cycle_front_op(f))
             else:
                 tag, op = lrn.frame(dpos[f], dfaces, f)
             ev[2 * f + 1].record()
             if lrn is None:      # read after the frame's end event: no sync inside the timed region
-                tag = bvh.opt_tag()
+                tag = bvh.opt_tag() if f else 2
                 op = front.stats()["front_op_run"]
             tags.append(tag)
             ops.append(op)
@@ -285,7 +291,8 @@ def evaluate(torch, weights, n, frames, seed, check_every=1):
         assert st["overflow"] == 0, st
         out[mode] = {"total_ms": round(float(sum(ms)), 3), "mean_ms": round(float(np.mean(ms)), 4),
                      "p50_ms": round(float(np.median(ms)), 4), "p99_ms": round(float(np.percentile(ms, 99)), 4),
-                     "builds": int(sum(1 for f, t in enumerate(tags) if t == 2 or (lrn is None and f % 12 == 0))),
+                     "builds": int(sum(1 for f, t in enumerate(tags)
+                                       if t == 2 or (mode == "heuristic" and f % 12 == 0))),
                      "restructures": int(sum(1 for t in tags if t == 1)),
                      "generates": int(sum(1 for o in ops if o == bvhcd.FRONT_GENERATE))}
         digests[mode] = dig
@@ -293,9 +300,11 @@ def evaluate(torch, weights, n, frames, seed, check_every=1):
             lrn.close()
         front.close()
         bvh.close()
-    out["pairs_equal"] = digests["heuristic"] == digests["learned"]
+    out["pairs_equal"] = digests["heuristic"] == digests["learned"] == digests["cycle"]
     out["frames_checked"] = len(digests["heuristic"])
     out["speedup"] = round(out["heuristic"]["total_ms"] / out["learned"]["total_ms"], 4)
+    out["speedup_cycle"] = round(out["heuristic"]["total_ms"] / out["cycle"]["total_ms"], 4)
+    out["decide_every"] = decide_every
     out["workload"] = f"cloth {n}x{n} over icosphere, {T} triangles, {frames} frames, seed {seed}"
     return out
 
@@ -303,7 +312,8 @@ def evaluate(torch, weights, n, frames, seed, check_every=1):
 def cmd_eval(args):
     import torch
     torch.cuda.set_device(0)
-    res = [evaluate(torch, args.weights, args.n, args.frames, s, args.check_every) for s in args.seeds]
+    res = [evaluate(torch, args.weights, args.n, args.frames, s, args.check_every, args.decide_every)
+           for s in args.seeds]
     print(json.dumps(res), flush=True)
 
 
@@ -332,6 +342,7 @@ def main():
     e.add_argument("--frames", type=int, default=200)
     e.add_argument("--seeds", type=int, nargs="+", default=[90001, 90002])
     e.add_argument("--check-every", type=int, default=1)
+    e.add_argument("--decide-every", type=int, default=3)
     a = ap.parse_args()
     cmd_train(a) if a.cmd == "train" else cmd_eval(a)
 
