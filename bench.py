@@ -11,7 +11,9 @@ flushed (256 MB write) between timed frames, outside the frame's events.
 The JSON line also carries "batched": 256 independent scenes (about 9.7M
 triangles) as one forest with graph-launched frames, against the same scenes
 run one by one through their own handles (scene-frames/s, p50/p99 frame
-times, and a per-scene pair-set check of the two forms).
+times, and a per-scene pair-set check of the two forms), and "learned": the
+learned scheduler against the reference's heuristic on a held-out 1M-triangle
+cloth (learn.py).
 
 --impl reference times the CPU restatement of the reference pipeline
 (oracle/, OpenMP on all host cores) on the same workload: the reference
@@ -176,15 +178,20 @@ def run_ours(args):
         dist.barrier()
     value = dev_ms / (K * world)
 
-    e2e = roof = batched = None
+    e2e = roof = batched = fp16 = None
     if not args.only_value:
         e2e = e2e_pass(bvhcd, torch, pipeline, host, faces, flush, hits_host, stream, W, K, V, world)
         # roofline of the dominant stage, from a stage-timed replay
         roof = roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
+        fp16 = fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
+    learned = None
     if not args.only_value and not args.no_batched:
         del dev, host, flush
         torch.cuda.empty_cache()
         batched = batched_pass(bvhcd, torch, args, world, rank)
+    if not args.only_value and not args.no_learned:
+        torch.cuda.empty_cache()
+        learned = learned_pass(torch, args)
 
     out = None
     if rank == 0:
@@ -208,7 +215,9 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "roofline": roof,
             "clocks": clk.summary(),
+            "fp16_node_boxes": fp16,
             "batched": batched,
+            "learned": learned,
         }
         if cpu:
             out["cpu_baseline"] = cpu
@@ -323,13 +332,7 @@ def batched_pass(bvhcd, torch, args, world, rank):
     F = args.batched_frames
     B = scenes.BatchedScenes()
     sizes = np.diff(B.tri_offsets)
-    owner = np.empty(B.num_scenes, dtype=np.int64)
-    load = np.zeros(world)
-    for sc in np.argsort(-sizes, kind="stable"):
-        r = int(np.argmin(load))
-        owner[sc] = r
-        load[r] += sizes[sc]
-    mine = np.flatnonzero(owner == rank)
+    mine = scenes.shard_scenes(sizes, world, rank)
     faces, off, vidx = B.subset(mine)
     T, V, S = int(off[-1]), int(vidx.size), len(mine)
     stream = torch.cuda.Stream()      # graphs are captured on a stream of their own
@@ -456,6 +459,49 @@ def _batched_on(bvhcd, torch, args, world, B, sizes, off, faces, vidx, T, V, S, 
     }
 
 
+def fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
+    """The same frames with FP16 node boxes (precision mode): device ms per
+    frame, timed as `value`, and the last frame's front sizes."""
+    bvh = bvhcd.LBvh(T, dev.shape[1], enable_restr=True, node_box_fp16=True)
+    front = bvhcd.BvttFront(bvh, cull_adjacent=True, narrow_phase=True, auto_grow=False, **CAPS)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for f in range(W):
+        bvhcd.frame(bvh, front, f, 0, dev[f], dfaces, stream=stream, faces_static=f > 0)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    torch.cuda.synchronize()
+    for i in range(K):
+        flush.zero_()
+        starts[i].record(stream)
+        bvhcd.frame(bvh, front, W + i, 0, dev[W + i], dfaces, stream=stream, faces_static=True)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    st = front.stats()
+    if st["overflow"]:
+        raise RuntimeError(f"fp16 leg overflow: {st}")
+    ms = float(sum(a.elapsed_time(b) for a, b in zip(starts, ends))) / K
+    front.close()
+    bvh.close()
+    return {"value": round(ms, 4), "unit": "ms/frame", "node_records": "16 B (FP16, outward-rounded)",
+            "front_sizes_last_frame": [st["int_front"], st["ext_front"]],
+            "pairs_last_frame": [st["broad_pairs"], st["narrow_hits"]]}
+
+
+def learned_pass(torch, args):
+    """The learned scheduler (weights trained on the GPU by learn.py, shipped
+    in learned_scheduler.npz) against the reference's heuristic schedule on a
+    held-out 708x708 cloth over the sphere (1,040,198 triangles, 200 frames,
+    seed 90001), with the no-network refit cycle as the ablation; broad and
+    narrow pair sets compared every 10 frames."""
+    import learn
+    r = learn.evaluate(torch, learn.WEIGHTS, 708, args.learned_frames, 90001, check_every=10, decide_every=3)
+    import numpy as np  # noqa: F401
+    w = np.load(learn.WEIGHTS)
+    rep = json.loads(str(w["report"]))
+    r["training"] = {k: rep[k] for k in ("rows", "sequences", "label_counts", "val_acc", "seconds")}
+    return r
+
+
 def cpu_baseline(faces, frames, args, budget_s=20.0):
     """Oracle pipeline (CPU restatement, OpenMP) on a bounded sample: the
     first frames of the same schedule, stopped after ~budget_s."""
@@ -527,6 +573,8 @@ def main():
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-scene batched leg")
     ap.add_argument("--batched-frames", type=int, default=30)
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-scheduler leg")
+    ap.add_argument("--learned-frames", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

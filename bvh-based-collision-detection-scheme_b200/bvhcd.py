@@ -39,6 +39,7 @@ EXPORTED = [
     "bvhcd_learner_create", "bvhcd_learner_destroy", "bvhcd_learner_set_params", "bvhcd_learner_get_params",
     "bvhcd_learner_frame", "bvhcd_learner_observe", "bvhcd_learner_cut", "bvhcd_learner_features",
     "bvhcd_learner_work", "bvhcd_mlp_gradient", "bvhcd_mlp_train", "bvhcd_mlp_predict",
+    "bvhcd_learner_set_decide_every", "bvhcd_front_contacts",
 ]
 
 MLP_PARAMS = 5443
@@ -57,14 +58,15 @@ class BvhcdError(RuntimeError):
 
 class BvhConfig(ctypes.Structure):
     _fields_ = [("prim_capacity", ctypes.c_int32), ("vert_capacity", ctypes.c_int32),
-                ("enable_restr", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
+                ("enable_restr", ctypes.c_int32), ("node_box_fp16", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 4)]
 
 
 class FrontConfig(ctypes.Structure):
     _fields_ = [("int_front_capacity", ctypes.c_int64), ("ext_front_capacity", ctypes.c_int64),
                 ("pair_capacity", ctypes.c_int64), ("cull_adjacent", ctypes.c_int32),
                 ("narrow_phase", ctypes.c_int32), ("auto_grow", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 5)]
+                ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4)]
 
 
 class Scene(ctypes.Structure):
@@ -86,7 +88,7 @@ class FrontStats(ctypes.Structure):
                 ("overflow", ctypes.c_int32), ("bvh_opt_tag", ctypes.c_int32),
                 ("front_op_run", ctypes.c_int32), ("restr_pending", ctypes.c_int32),
                 ("num_rt_subtrees", ctypes.c_int32), ("num_rt_int_nodes", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 6)]
+                ("flagged", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -141,6 +143,8 @@ def lib():
             "bvhcd_front_autotune": (ctypes.c_int, [vp, i32, ctypes.POINTER(LaunchShapes), vp, vp]),
             "bvhcd_bvh_copy_state": (ctypes.c_int, [vp, vp, vp]),
             "bvhcd_front_copy_state": (ctypes.c_int, [vp, vp, vp]),
+            "bvhcd_front_contacts": (ctypes.c_int, [vp, i32, vp, i64, ctypes.POINTER(i64), ctypes.POINTER(i64),
+                                                    i32, vp]),
             "bvhcd_learner_create": (ctypes.c_int, [vp, vp, i32, ctypes.POINTER(vp)]),
             "bvhcd_learner_destroy": (ctypes.c_int, [vp]),
             "bvhcd_learner_set_params": (ctypes.c_int, [vp, vp]),
@@ -148,6 +152,7 @@ def lib():
             "bvhcd_learner_frame": (ctypes.c_int, [vp, ctypes.POINTER(Scene), i32, ctypes.POINTER(i32),
                                                    ctypes.POINTER(i32), vp]),
             "bvhcd_learner_observe": (ctypes.c_int, [vp, i32, i32, vp]),
+            "bvhcd_learner_set_decide_every": (ctypes.c_int, [vp, i32]),
             "bvhcd_learner_cut": (ctypes.c_int, [vp, vp, i32, ctypes.POINTER(i32), vp]),
             "bvhcd_learner_features": (ctypes.c_int, [vp, vp, i32, ctypes.POINTER(i32), vp]),
             "bvhcd_learner_work": (ctypes.c_int, [vp, vp, vp, i32, vp]),
@@ -229,8 +234,9 @@ def _scene(pos, faces, faces_static=False):
 class LBvh:
     """LBvhFixedDeformable: maintain(BUILD | REFIT | UPDATE, scene) per frame."""
 
-    def __init__(self, prim_capacity: int, vert_capacity: int = 0, enable_restr: bool = True):
-        cfg = BvhConfig(int(prim_capacity), int(vert_capacity), int(enable_restr))
+    def __init__(self, prim_capacity: int, vert_capacity: int = 0, enable_restr: bool = True,
+                 node_box_fp16: bool = False):
+        cfg = BvhConfig(int(prim_capacity), int(vert_capacity), int(enable_restr), int(node_box_fp16))
         h = ctypes.c_void_p()
         _check(lib().bvhcd_bvh_create(ctypes.byref(cfg), ctypes.byref(h)), "bvh create")
         self._h = h
@@ -313,9 +319,10 @@ class BvttFront:
 
     def __init__(self, bvh: LBvh, int_front_capacity: int = 2_300_000,
                  ext_front_capacity: int = 2_300_000, pair_capacity: int = 1_600_000,
-                 cull_adjacent: bool = True, narrow_phase: bool = True, auto_grow: bool = False):
+                 cull_adjacent: bool = True, narrow_phase: bool = True, auto_grow: bool = False,
+                 precision: int = 0):
         cfg = FrontConfig(int(int_front_capacity), int(ext_front_capacity), int(pair_capacity),
-                          int(cull_adjacent), int(narrow_phase), int(auto_grow))
+                          int(cull_adjacent), int(narrow_phase), int(auto_grow), int(precision))
         h = ctypes.c_void_p()
         _check(lib().bvhcd_front_create(bvh.handle, ctypes.byref(cfg), ctypes.byref(h)), "front create")
         self._h = h
@@ -365,6 +372,20 @@ class BvttFront:
         _check(lib().bvhcd_front_export(self._h, int(which), out.ctypes.data, n.value, ctypes.byref(n),
                                         _stream_ptr(stream)), "front export")
         return out[:n.value]
+
+    def contacts(self, which: int = 0, stream=None):
+        """which 0: (n, 4) contact midpoint xyz + segment length per hit (order
+        of pairs(narrow=True)); 1: (n, 4) with the distance in column 3 per
+        broad pair (order of pairs()).  Returns (array, items computed in FP64)."""
+        n, fl = ctypes.c_int64(), ctypes.c_int64()
+        st = lib().bvhcd_front_contacts(self._h, int(which), None, 0, ctypes.byref(n), ctypes.byref(fl), 0,
+                                        _stream_ptr(stream))
+        if st not in (0, 3):
+            _check(st, "contacts")
+        out = np.zeros((max(n.value, 1), 4), np.float32)
+        _check(lib().bvhcd_front_contacts(self._h, int(which), out.ctypes.data, n.value, ctypes.byref(n),
+                                          ctypes.byref(fl), 0, _stream_ptr(stream)), "contacts")
+        return out[:n.value], int(fl.value)
 
     def shapes(self) -> dict:
         """Launch shape per front stage: {stage: (entries per thread step, threads per block)}."""
@@ -452,6 +473,9 @@ class Learner:
             self.close()
         except Exception:
             pass
+
+    def set_decide_every(self, frames: int):
+        _check(lib().bvhcd_learner_set_decide_every(self._h, int(frames)), "decide every")
 
     def set_params(self, params):
         p = np.ascontiguousarray(params, dtype=np.float32)

@@ -231,6 +231,12 @@ bvhcd_status bvhcd_frame(bvhcd_bvh *bvh, bvhcd_front *front, int32_t frame, int3
     return bvhcd_front_maintain(front, (bvhcd_front_op)f, stream);
 }
 
+bvhcd_status bvhcd_front_contacts(bvhcd_front *front, int32_t which, float *out, int64_t cap, int64_t *count,
+                                  int64_t *flagged, int32_t out_on_device, void *stream) {
+    if (!front) return BVHCD_INVALID_ARG;
+    return front->impl.contacts(which, out, cap, count, flagged, out_on_device != 0, as_stream(stream));
+}
+
 bvhcd_status bvhcd_bvh_copy_state(bvhcd_bvh *dst, const bvhcd_bvh *src, void *stream) {
     if (!dst || !src) return BVHCD_INVALID_ARG;
     return dst->impl.copy_state_from(src->impl, as_stream(stream));
@@ -276,6 +282,12 @@ bvhcd_status bvhcd_learner_frame(bvhcd_learner *l, const bvhcd_scene *scene, int
                                  int32_t *front_op, void *stream) {
     if (!l || !scene) return BVHCD_INVALID_ARG;
     return l->impl.frame(*scene, frame, as_stream(stream), bvh_tag, front_op);
+}
+
+bvhcd_status bvhcd_learner_set_decide_every(bvhcd_learner *l, int32_t frames) {
+    if (!l || frames < 1) return BVHCD_INVALID_ARG;
+    l->impl.set_decide_every(frames);
+    return BVHCD_OK;
 }
 
 bvhcd_status bvhcd_learner_observe(bvhcd_learner *l, int32_t tree_changed, int32_t front_generated, void *stream) {

@@ -42,6 +42,7 @@ struct Tree {
     int4 *sface;       // T
     int *primmap;      // T (orig -> slot)
     unsigned *code;    // T
+    uint4 *nrec16;     // T-1 FP16 node records {6 outward-rounded halves, escape}, or null
     int T;
 };
 
@@ -65,6 +66,7 @@ enum CounterSlot {
     C_WORK = 10,              // overlapping internal entries queued for traversal
     C_PAIRS_VALID = 11,       // broad-phase pairs (C_PAIRS counts reserved slots, holes included)
     C_COMPACT = 12,           // compaction cursor of the pair export
+    C_FLAGGED = 13,           // precision mode: pairs re-decided in FP64
     C_NUM = 16
 };
 

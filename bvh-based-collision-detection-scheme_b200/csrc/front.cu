@@ -9,7 +9,10 @@
 #include <climits>
 #include <cstdlib>
 
+#include <cuda_fp16.h>
+
 #include "pipeline.h"
+#include "tritri.cuh"
 #include "prims.cuh"
 
 namespace bvhcd {
@@ -35,6 +38,8 @@ inline unsigned grid_for(int64_t n) {
 
 struct FArgs {
     const float4 *nrec, *lrec;
+    const uint4 *nrec16;   // FP16 node records, or null for the FP32 ones
+    const int2 *nrange;
     const int4 *topo;
     const int *lca;
     const int4 *sface;
@@ -51,6 +56,28 @@ struct FArgs {
     int cull;
     int T;
 };
+
+// A node's box and escape link: from the FP32 record ({lo.xyz, rangex},
+// {hi.xyz, escape}), or, with FP16 node boxes, from the 16-byte record {min.xyz,
+// max.xyz as halves rounded outward, escape}.  The FP16 box contains the FP32
+// one, so a traversal on it visits a superset of the nodes and still tests
+// every overlapping leaf in FP32: the pair set does not change.
+__device__ __forceinline__ float half_lo(unsigned w) { return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu))); }
+__device__ __forceinline__ float half_hi(unsigned w) { return __half2float(__ushort_as_half((unsigned short)(w >> 16))); }
+__device__ __forceinline__ void node_rec(const FArgs &a, int n, float4 &lo, float4 &hi) {
+    if (a.nrec16) {
+        const uint4 r = __ldg(a.nrec16 + n);
+        lo = make_float4(half_lo(r.x), half_hi(r.x), half_lo(r.y), __int_as_float(-1));
+        hi = make_float4(half_hi(r.y), half_lo(r.z), half_hi(r.z), __int_as_float((int)r.w));
+    } else {
+        lo = ldg4(a.nrec + 2 * n);
+        hi = ldg4(a.nrec + 2 * n + 1);
+    }
+}
+// the node's leftmost leaf (its lo.w in the FP32 record)
+__device__ __forceinline__ int node_rangex(const FArgs &a, int n, const float4 &lo) {
+    return a.nrec16 ? __ldg(&a.nrange[n]).x : __float_as_int(lo.w);
+}
 
 // Per-node counter increment aggregated over the converged lanes of a warp
 // that hit the same node: one atomic per distinct node instead of one per
@@ -156,8 +183,9 @@ __device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const
             lhi = ldg4(a.lrec + 2 * leaf + 1);
         } else {
             int n = st >> 1;
-            float4 nlo = ldg4(a.nrec + 2 * n), nhi = ldg4(a.nrec + 2 * n + 1);
-            leaf = __float_as_int(nlo.w);
+            float4 nlo, nhi;
+            node_rec(a, n, nlo, nhi);
+            leaf = node_rangex(a, n, nlo);
             llo = ldg4(a.lrec + 2 * leaf);
             lhi = ldg4(a.lrec + 2 * leaf + 1);
             const int last = __float_as_int(llo.w);  // parent of the leftmost leaf
@@ -166,8 +194,7 @@ __device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const
                 if (!overlap(nlo, nhi, plo, phi)) { stopped = true; break; }
                 if (n >= last) break;
                 ++n;
-                nlo = ldg4(a.nrec + 2 * n);
-                nhi = ldg4(a.nrec + 2 * n + 1);
+                node_rec(a, n, nlo, nhi);
             }
             if (stopped) {
                 if (kFront) emit_int(a, em, prim, n);
@@ -182,8 +209,7 @@ __device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const
 }
 
 // left child of internal node d, tagged, and its escape
-__device__ __forceinline__ int left_child_tagged(const FArgs &a, int d, const float4 &nlo) {
-    const int rx = __float_as_int(nlo.w);
+__device__ __forceinline__ int left_child_tagged(const FArgs &a, int d, int rx) {
     const int last = __float_as_int(__ldg(reinterpret_cast<const float *>(a.lrec) + 8 * (size_t)rx + 3));
     return last == d ? ((rx << 1) | 1) : ((d + 1) << 1);
 }
@@ -210,7 +236,8 @@ __global__ void __launch_bounds__(kThreads) k_generate(FArgs a) {
 __device__ __forceinline__ int prune_up(const FArgs &a, int n, int top, const float4 &plo,
                                         const float4 &phi) {
     for (; n >= top; --n) {
-        float4 lo = ldg4(a.nrec + 2 * n), hi = ldg4(a.nrec + 2 * n + 1);
+        float4 lo, hi;
+        node_rec(a, n, lo, hi);
         if (overlap(lo, hi, plo, phi)) break;
     }
     if (n < top && n + 1 > 0) {
@@ -218,7 +245,8 @@ __device__ __forceinline__ int prune_up(const FArgs &a, int n, int top, const fl
         // or the root of one scene of a forest)
         int p = __ldg(&a.topo[n + 1]).z;
         if (p >= 0) {
-            float4 lo = ldg4(a.nrec + 2 * p), hi = ldg4(a.nrec + 2 * p + 1);
+            float4 lo, hi;
+            node_rec(a, p, lo, hi);
             if (!overlap(lo, hi, plo, phi)) return -1;
         }
     }
@@ -260,9 +288,12 @@ __device__ __forceinline__ void load_recs(const FArgs &a, Batch<kU> &b) {
         if (!b.v[k]) continue;
         b.plo[k] = ldg4(a.lrec + 2 * b.e[k].x);
         b.phi[k] = ldg4(a.lrec + 2 * b.e[k].x + 1);
-        const float4 *nb = b.in_int[k] ? a.nrec : a.lrec;
-        b.nlo[k] = ldg4(nb + 2 * b.e[k].y);
-        b.nhi[k] = ldg4(nb + 2 * b.e[k].y + 1);
+        if (b.in_int[k]) {
+            node_rec(a, b.e[k].y, b.nlo[k], b.nhi[k]);
+        } else {
+            b.nlo[k] = ldg4(a.lrec + 2 * b.e[k].y);
+            b.nhi[k] = ldg4(a.lrec + 2 * b.e[k].y + 1);
+        }
     }
 }
 template <int kU>
@@ -292,8 +323,9 @@ __global__ void __launch_bounds__(kB) k_sprout(FArgs a) {
         const int2 e = a.work[q];
         if (e.x < 0) continue;  // hole
         const float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
-        const float4 nlo = ldg4(a.nrec + 2 * e.y), nhi = ldg4(a.nrec + 2 * e.y + 1);
-        traverse<kFront>(a, em, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, nlo),
+        float4 nlo, nhi;
+        node_rec(a, e.y, nlo, nhi);
+        traverse<kFront>(a, em, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, node_rangex(a, e.y, nlo)),
                          __float_as_int(nhi.w));
     }
     em_close(a, em);
@@ -319,7 +351,7 @@ __global__ void __launch_bounds__(kB) k_maintain_int_scan(FArgs a) {
                 emit_work(a, em, b.e[k]);
                 continue;
             }
-            const int top = __ldg(&a.lca[__float_as_int(b.nlo[k].w)]) >> 1;
+            const int top = __ldg(&a.lca[node_rangex(a, b.e[k].y, b.nlo[k])]) >> 1;
             const int m = prune_up(a, b.e[k].y - 1, top, b.plo[k], b.phi[k]);
             if (m >= 0) emit_int(a, em, b.e[k].x, m);
         }
@@ -349,7 +381,8 @@ __global__ void __launch_bounds__(kB) k_maintain_ext(FArgs a) {
                 continue;
             }
             const int gfa = __float_as_int(b.nlo[k].w);
-            const float4 glo = ldg4(a.nrec + 2 * gfa), ghi = ldg4(a.nrec + 2 * gfa + 1);
+            float4 glo, ghi;
+            node_rec(a, gfa, glo, ghi);
             if (overlap(glo, ghi, b.plo[k], b.phi[k])) {
                 emit_ext(a, em, prim, st);
                 continue;
@@ -570,17 +603,144 @@ __global__ void __launch_bounds__(kB) k_narrow(const int2 *__restrict__ pairs, c
     if ((threadIdx.x & 31) == 0 && valid) atomicAdd(ctr + C_PAIRS_VALID, valid);
 }
 
-// applyCpResults (BvttFrontLooseIntra.cu:63-67): broad pairs as original ids,
-// compacted past the holes
-__global__ void k_pairs_to_orig(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
-                                unsigned *ctr, unsigned cap_pairs, int2 *out) {
+// The precision mode's narrow phase: the FP32 test decides where it is
+// certain, the FP64 test where it is not (the flagged pairs, counted), so the
+// hits are those of an FP64 evaluation of every pair (tritri.cuh).
+template <bool kUnused, int kB>
+__global__ void __launch_bounds__(kB) k_narrow_prec(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
+                                                     const float *__restrict__ verts, unsigned *ctr,
+                                                     unsigned cap_pairs, int2 *hits, unsigned cap_hits) {
     const unsigned n = min(ctr[C_PAIRS], cap_pairs);
+    unsigned valid = 0, flagged = 0;
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         int2 p = pairs[q];
-        if (p.x < 0) continue;
-        emit(out, ctr + C_COMPACT, cap_pairs, make_int2(__ldg(&sface[p.x]).w, __ldg(&sface[p.y]).w),
-             ctr + C_OVERFLOW, 4u);
+        if (p.x < 0) continue;  // hole
+        ++valid;
+        int4 a = __ldg(&sface[p.x]), b = __ldg(&sface[p.y]);
+        const v3 A0 = vload(verts, a.x), A1 = vload(verts, a.y), A2 = vload(verts, a.z);
+        const v3 B0 = vload(verts, b.x), B1 = vload(verts, b.y), B2 = vload(verts, b.z);
+        int hit = prec::tritri_sat32_certain(prec::fk(A0.x, A0.y, A0.z), prec::fk(A1.x, A1.y, A1.z),
+                                             prec::fk(A2.x, A2.y, A2.z), prec::fk(B0.x, B0.y, B0.z),
+                                             prec::fk(B1.x, B1.y, B1.z), prec::fk(B2.x, B2.y, B2.z));
+        if (hit < 0) {
+            ++flagged;
+            hit = prec::tritri_sat64(prec::mk(A0.x, A0.y, A0.z), prec::mk(A1.x, A1.y, A1.z),
+                                     prec::mk(A2.x, A2.y, A2.z), prec::mk(B0.x, B0.y, B0.z),
+                                     prec::mk(B1.x, B1.y, B1.z), prec::mk(B2.x, B2.y, B2.z))
+                      ? 1
+                      : 0;
+        }
+        if (hit) emit(hits, ctr + C_HITS, cap_hits, make_int2(a.w, b.w), ctr + C_OVERFLOW, 8u);
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        valid += __shfl_xor_sync(0xffffffffu, valid, o);
+        flagged += __shfl_xor_sync(0xffffffffu, flagged, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (valid) atomicAdd(ctr + C_PAIRS_VALID, valid);
+        if (flagged) atomicAdd(ctr + C_FLAGGED, flagged);
+    }
+}
+
+// Contact points of hits (kDist false: midpoint xyz and length of the
+// intersection segment; NaN for coplanar pairs) or distances of broad pairs
+// (kDist true: w = distance), over pairs of original triangle ids.  With
+// kPrec, ill-conditioned cases are evaluated in FP64: nearly parallel planes
+// (sin^2 of their angle below 1e-6) for contact points, distances below a
+// thousandth of the pair's size for distances.
+template <bool kDist, bool kPrec>
+__global__ void k_contacts(const int2 *__restrict__ list, const unsigned *__restrict__ count, unsigned cap,
+                           const int *__restrict__ faces, const float *__restrict__ verts, float4 *out,
+                           unsigned *nflag) {
+    const unsigned n = min(*count, cap);
+    unsigned fl = 0;
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int2 pr = list[q];
+        prec::V<float> P[3], Q[3];
+        for (int k = 0; k < 3; k++) {
+            const v3 a = vload(verts, __ldg(faces + 3 * (size_t)pr.x + k));
+            const v3 b = vload(verts, __ldg(faces + 3 * (size_t)pr.y + k));
+            P[k] = prec::V<float>{a.x, a.y, a.z};
+            Q[k] = prec::V<float>{b.x, b.y, b.z};
+        }
+        float4 r;
+        if (!kDist) {
+            float o[4], cond = 0.f;
+            int st = prec::contact_point(P, Q, o, &cond);
+            if (kPrec && (st != 1 || cond < 1e-6f)) {
+                prec::V<double> Pd[3], Qd[3];
+                for (int k = 0; k < 3; k++) {
+                    Pd[k] = prec::V<double>{P[k].x, P[k].y, P[k].z};
+                    Qd[k] = prec::V<double>{Q[k].x, Q[k].y, Q[k].z};
+                }
+                double od[4], cd = 0.0;
+                st = prec::contact_point(Pd, Qd, od, &cd);
+                for (int k = 0; k < 4; k++) o[k] = (float)od[k];
+                ++fl;
+            }
+            r = st == 1 ? make_float4(o[0], o[1], o[2], o[3]) : make_float4(__int_as_float(0x7fc00000),
+                                                                          __int_as_float(0x7fc00000),
+                                                                          __int_as_float(0x7fc00000), 0.f);
+        } else {
+            // intersecting pairs are at distance 0 (decided as the narrow phase decides)
+            int hit;
+            if (kPrec) {
+                hit = prec::tritri_sat32_certain(prec::fk(P[0].x, P[0].y, P[0].z), prec::fk(P[1].x, P[1].y, P[1].z),
+                                                 prec::fk(P[2].x, P[2].y, P[2].z), prec::fk(Q[0].x, Q[0].y, Q[0].z),
+                                                 prec::fk(Q[1].x, Q[1].y, Q[1].z), prec::fk(Q[2].x, Q[2].y, Q[2].z));
+                if (hit < 0)
+                    hit = prec::tritri_sat64(prec::mk(P[0].x, P[0].y, P[0].z), prec::mk(P[1].x, P[1].y, P[1].z),
+                                             prec::mk(P[2].x, P[2].y, P[2].z), prec::mk(Q[0].x, Q[0].y, Q[0].z),
+                                             prec::mk(Q[1].x, Q[1].y, Q[1].z), prec::mk(Q[2].x, Q[2].y, Q[2].z));
+            } else {
+                hit = tritri_sat32(v3{P[0].x, P[0].y, P[0].z}, v3{P[1].x, P[1].y, P[1].z}, v3{P[2].x, P[2].y, P[2].z},
+                                   v3{Q[0].x, Q[0].y, Q[0].z}, v3{Q[1].x, Q[1].y, Q[1].z}, v3{Q[2].x, Q[2].y, Q[2].z});
+            }
+            float d = hit ? 0.f : prec::tri_distance(P, Q, 1.17549435e-38f);
+            if (kPrec && !hit) {
+                float size = 0.f;
+                for (int k = 0; k < 3; k++) {
+                    const prec::V<float> e = P[k] - Q[k];
+                    size = fmaxf(size, fabsf(e.x) + fabsf(e.y) + fabsf(e.z));
+                }
+                if (d < 1e-3f * size) {
+                    prec::V<double> Pd[3], Qd[3];
+                    for (int k = 0; k < 3; k++) {
+                        Pd[k] = prec::V<double>{P[k].x, P[k].y, P[k].z};
+                        Qd[k] = prec::V<double>{Q[k].x, Q[k].y, Q[k].z};
+                    }
+                    d = (float)prec::tri_distance(Pd, Qd, 2.2250738585072014e-308);
+                    ++fl;
+                }
+            }
+            r = make_float4(0.f, 0.f, 0.f, d);
+        }
+        out[q] = r;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) fl += __shfl_xor_sync(0xffffffffu, fl, o);
+    if ((threadIdx.x & 31) == 0 && fl) atomicAdd(nflag, fl);
+}
+
+// Order-preserving compaction of the broad pairs past their holes, into
+// original ids: flags, an exclusive scan, a scatter.  Every export of the same
+// frame lists the pairs in the same order (their slot order).
+__global__ void k_pair_flags(const int2 *__restrict__ pairs, const unsigned *__restrict__ ctr, unsigned cap,
+                             unsigned n_all, unsigned *flags) {
+    const unsigned n = min(ctr[C_PAIRS], cap);
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n_all; q += gridDim.x * blockDim.x)
+        flags[q] = (q < n && pairs[q].x >= 0) ? 1u : 0u;
+}
+__global__ void k_pair_scatter(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
+                               const unsigned *__restrict__ ctr, unsigned cap, const unsigned *__restrict__ flags,
+                               const unsigned *__restrict__ pos, int2 *out) {
+    const unsigned n = min(ctr[C_PAIRS], cap);
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        if (flags[q]) {
+            const int2 p = pairs[q];
+            out[pos[q]] = make_int2(__ldg(&sface[p.x]).w, __ldg(&sface[p.y]).w);
+        }
 }
 
 __global__ void k_counts64(const unsigned *__restrict__ ctr, unsigned cap_pairs, unsigned cap_hits,
@@ -637,7 +797,7 @@ Front::~Front() {
     for (auto &set : front_)
         for (auto &b : set) b.release();
     DBuf *bufs[] = {&pairs_, &hits_, &outbuf_, &work_, &intcnt_, &extcnt_, &intbeg_, &extbeg_, &intback_,
-                    &extback_, &snapshot_, &scratch_, &counts64_};
+                    &extback_, &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_};
     for (DBuf *b : bufs) b->release();
 }
 
@@ -704,6 +864,7 @@ static FArgs make_args(const LBvh *bvh, const FrontLog &log, int cull, const DBu
     Tree t = bvh->tree();
     FArgs a;
     a.nrec = t.nrec; a.lrec = t.lrec; a.topo = t.topo; a.lca = t.lca; a.sface = t.sface;
+    a.nrec16 = t.nrec16; a.nrange = t.nrange;
     a.log = log;
     a.ctr = bvh->counters();
     a.in_int = a.in_ext = nullptr;
@@ -905,7 +1066,11 @@ bvhcd_status Front::narrow(cudaStream_t s, bool test) {
     FR_TRY(cudaMemsetAsync(ctr + C_HITS, 0, sizeof(unsigned), s));
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));
     const Shape sh = shape_[BVHCD_SHAPE_NARROW];
-    if (test)
+    FR_TRY(cudaMemsetAsync(ctr + C_FLAGGED, 0, sizeof(unsigned), s));
+    if (test && cfg_.precision)
+        LAUNCH_ITEM(k_narrow_prec, true, sh, s, pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
+                    (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_);
+    else if (test)
         LAUNCH_ITEM(k_narrow, true, sh, s, pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
                     (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_);
     else
@@ -1148,7 +1313,24 @@ bvhcd_status Front::stats(bvhcd_front_stats *st, cudaStream_t s) {
     st->restr_pending = bvh_->updated() ? 1 : 0;
     st->num_rt_subtrees = bvh_->last_rt_subtrees();
     st->num_rt_int_nodes = bvh_->last_rt_intnodes();
+    st->flagged = (int32_t)h[C_FLAGGED];
     return BVHCD_OK;
+}
+
+bvhcd_status Front::compact_pairs(cudaStream_t s) {
+    const size_t n = (size_t)(pcap_ > 0 ? pcap_ : 1);
+    FR_TRY(outbuf_.reserve(sizeof(int2) * n));
+    FR_TRY(cflag_.reserve(sizeof(unsigned) * 2 * n));
+    FR_TRY(cscratch_.reserve(scan_scratch_bytes((int64_t)n)));
+    unsigned *flags = cflag_.as<unsigned>(), *pos = flags + n;
+    unsigned *ctr = bvh_->counters();
+    k_pair_flags<<<grid_for((int64_t)n), kThreads, 0, s>>>(pairs_.as<int2>(), ctr, (unsigned)pcap_, (unsigned)n, flags);
+    note_launch();
+    FR_TRY(scan_u32(flags, pos, (int64_t)n, false, ctr + C_COMPACT, cscratch_.p, s));
+    k_pair_scatter<<<kFrontBlocks, kThreads, 0, s>>>(pairs_.as<int2>(), bvh_->tree().sface, ctr, (unsigned)pcap_,
+                                                     flags, pos, outbuf_.as<int2>());
+    note_launch();
+    return cuda_status(cudaGetLastError());
 }
 
 bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, bool out_dev,
@@ -1156,11 +1338,8 @@ bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, 
     const int2 *src = hits_.as<int2>();
     if (!which) {
         // compact the broad pairs past their holes into original ids first
-        FR_TRY(outbuf_.reserve(sizeof(int2) * (size_t)(pcap_ > 0 ? pcap_ : 1)));
-        FR_TRY(cudaMemsetAsync(bvh_->counters() + C_COMPACT, 0, sizeof(unsigned), s));
-        k_pairs_to_orig<<<kFrontBlocks, kThreads, 0, s>>>(pairs_.as<int2>(), bvh_->tree().sface,
-                                                          bvh_->counters(), (unsigned)pcap_, outbuf_.as<int2>()); note_launch();
-        FR_TRY(cudaGetLastError());
+        bvhcd_status st = compact_pairs(s);
+        if (st != BVHCD_OK) return st;
         src = outbuf_.as<int2>();
     }
     unsigned h[C_NUM];
@@ -1176,6 +1355,50 @@ bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, 
                                out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
     FR_TRY(cudaStreamSynchronize(s));
     if (h[C_OVERFLOW] & (which ? 8u : 4u)) return BVHCD_CAPACITY_EXCEEDED;
+    return n > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
+}
+
+// Contact points of the hits (which = 0) or distances of the broad pairs
+// (which = 1), in the order bvhcd_front_pairs returns them.
+bvhcd_status Front::contacts(int which, float *out, int64_t cap, int64_t *count, int64_t *flagged, bool out_dev,
+                             cudaStream_t s) {
+    if (which < 0 || which > 1 || cap < 0) return BVHCD_INVALID_ARG;
+    const int2 *list = hits_.as<int2>();
+    unsigned *ctr = bvh_->counters();
+    const unsigned *cnt = ctr + C_HITS;
+    if (which == 1) {
+        bvhcd_status st = compact_pairs(s);
+        if (st != BVHCD_OK) return st;
+        list = outbuf_.as<int2>();
+        cnt = ctr + C_COMPACT;
+    }
+    FR_TRY(cbuf_.reserve(sizeof(float4) * (size_t)(pcap_ > 0 ? pcap_ : 1) + 16));
+    float4 *res = cbuf_.as<float4>();
+    unsigned *nflag = reinterpret_cast<unsigned *>(res + (pcap_ > 0 ? pcap_ : 1));
+    FR_TRY(cudaMemsetAsync(nflag, 0, sizeof(unsigned), s));
+    const int *faces = bvh_->faces();
+    const float *verts = bvh_->verts();
+    const unsigned g = RESIDENT((k_contacts<false, false>));
+    if (which == 0 && cfg_.precision) k_contacts<false, true><<<g, kThreads, 0, s>>>(list, cnt, (unsigned)pcap_, faces, verts, res, nflag);
+    else if (which == 0) k_contacts<false, false><<<g, kThreads, 0, s>>>(list, cnt, (unsigned)pcap_, faces, verts, res, nflag);
+    else if (cfg_.precision) k_contacts<true, true><<<g, kThreads, 0, s>>>(list, cnt, (unsigned)pcap_, faces, verts, res, nflag);
+    else k_contacts<true, false><<<g, kThreads, 0, s>>>(list, cnt, (unsigned)pcap_, faces, verts, res, nflag);
+    note_launch();
+    FR_TRY(cudaGetLastError());
+    unsigned h[C_NUM], hf = 0;
+    FR_TRY(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaMemcpyAsync(&hf, nflag, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaStreamSynchronize(s));
+    int64_t n = which ? (int64_t)h[C_COMPACT] : (int64_t)h[C_HITS];
+    if (n > pcap_) n = pcap_;
+    if (count) *count = n;
+    if (flagged) *flagged = hf;
+    int64_t m = n < cap ? n : cap;
+    if (out && m > 0) {
+        FR_TRY(cudaMemcpyAsync(out, res, sizeof(float4) * (size_t)m,
+                               out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+        FR_TRY(cudaStreamSynchronize(s));
+    }
     return n > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
 }
 

@@ -14,6 +14,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <cuda_fp16.h>
+
 #include "pipeline.h"
 #include "prims.cuh"
 
@@ -440,6 +442,22 @@ __global__ void __launch_bounds__(kThreads) k_refit(int T, const int4 *__restric
     }
 }
 
+// ---------------------------------------------------------------- FP16 node records
+// {min.xyz rounded down, max.xyz rounded up to FP16, escape}: 16 bytes per
+// internal node for the front traversals (the FP32 records stay the master).
+__global__ void k_node_fp16(int nint, const float4 *__restrict__ nrec, uint4 *nrec16) {
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nint; d += gridDim.x * blockDim.x) {
+        const float4 lo = nrec[2 * d], hi = nrec[2 * d + 1];
+        auto h = [](__half x) { return (unsigned)__half_as_ushort(x); };
+        uint4 r;
+        r.x = h(__float2half_rd(lo.x)) | (h(__float2half_rd(lo.y)) << 16);
+        r.y = h(__float2half_rd(lo.z)) | (h(__float2half_ru(hi.x)) << 16);
+        r.z = h(__float2half_ru(hi.y)) | (h(__float2half_ru(hi.z)) << 16);
+        r.w = (unsigned)__float_as_int(hi.w);
+        nrec16[d] = r;
+    }
+}
+
 // ---------------------------------------------------------------- restructure
 // calibrateLeafRangeMarks (LBvhRestructureKernels.cu:9-17)
 __global__ void k_rs_leaf_marks(int T, const int *__restrict__ rtroot, const int *__restrict__ intmark,
@@ -670,7 +688,7 @@ LBvh::~LBvh() {
                     &ulc_, &urc_, &upar_, &urx_, &ury_, &umark_, &ubox_, &uflag_, &posb_, &clen_,
                     &coff_, &dfs_, &ulpar_, &scene_, &partial_, &scratch_, &task_, &tmpface_,
                     &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &flagbuf_,
-                    &ctr_, &scene_of_, &leafscene_, &sbox_, &tiles_};
+                    &ctr_, &scene_of_, &leafscene_, &sbox_, &tiles_, &nrec16_};
     for (DBuf *b : bufs) b->release();
     if (h_ctr_) cudaFreeHost(h_ctr_);
 }
@@ -750,6 +768,7 @@ Tree LBvh::tree() const {
     t.sface = sface_.as<int4>();
     t.primmap = primmap_.as<int>();
     t.code = code_.as<unsigned>();
+    t.nrec16 = cfg_.node_box_fp16 ? nrec16_.as<uint4>() : nullptr;
     t.T = T_;
     return t;
 }
@@ -866,14 +885,15 @@ bvhcd_status LBvh::build(cudaStream_t s) {
 
 bvhcd_status LBvh::copy_state_from(const LBvh &src, cudaStream_t s) {
     if (&src == this) return BVHCD_OK;
-    if (src.cfg_.enable_restr != cfg_.enable_restr) return BVHCD_INVALID_ARG;
+    if (src.cfg_.enable_restr != cfg_.enable_restr || src.cfg_.node_box_fp16 != cfg_.node_box_fp16)
+        return BVHCD_INVALID_ARG;
     const DBuf *from[] = {&src.verts_, &src.faces_, &src.nrec_, &src.lrec_, &src.topo_, &src.nrange_, &src.lca_,
                           &src.sface_, &src.primmap_, &src.code_, &src.refit_flag_, &src.intrange_, &src.rtroot_,
                           &src.intmark_, &src.extrange_, &src.extmark_, &src.leafroot_, &src.ctr_,
-                          &src.scene_of_, &src.leafscene_, &src.sbox_, &src.tiles_, &src.scene_};
+                          &src.scene_of_, &src.leafscene_, &src.sbox_, &src.tiles_, &src.scene_, &src.nrec16_};
     DBuf *to[] = {&verts_, &faces_, &nrec_, &lrec_, &topo_, &nrange_, &lca_, &sface_, &primmap_, &code_,
                   &refit_flag_, &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &ctr_,
-                  &scene_of_, &leafscene_, &sbox_, &tiles_, &scene_};
+                  &scene_of_, &leafscene_, &sbox_, &tiles_, &scene_, &nrec16_};
     bvhcd_status st = ensure_capacity(src.capT_, src.capV_);
     if (st != BVHCD_OK) return st;
     for (size_t k = 0; k < sizeof(to) / sizeof(to[0]); k++) BV_TRY(to[k]->copy_from(*from[k], s));
@@ -1005,8 +1025,21 @@ bvhcd_status LBvh::restructure(cudaStream_t s) {
     return BVHCD_OK;
 }
 
+bvhcd_status LBvh::node_fp16(cudaStream_t s) {
+    if (!cfg_.node_box_fp16 || T_ < 2 || !built_) return BVHCD_OK;
+    BV_TRY(nrec16_.reserve(sizeof(uint4) * (size_t)(capT_ + 2)));
+    k_node_fp16<<<grid_for(T_ - 1), kThreads, 0, s>>>(T_ - 1, nrec_.as<float4>(), nrec16_.as<uint4>()); note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
 // LBvhFixedDeformable::maintain (LBvhFixedDeformable.cu:68-87)
 bvhcd_status LBvh::maintain(bvhcd_bvh_op op, const bvhcd_scene &scene, cudaStream_t s) {
+    bvhcd_status st = maintain_tree(op, scene, s);
+    if (st != BVHCD_OK) return st;
+    return node_fp16(s);
+}
+
+bvhcd_status LBvh::maintain_tree(bvhcd_bvh_op op, const bvhcd_scene &scene, cudaStream_t s) {
     if (op < BVHCD_BVH_BUILD || op > BVHCD_BVH_UPDATE) return BVHCD_INVALID_ARG;
     if (S_ > 1 && scene.num_faces != h_off_[S_]) return BVHCD_INVALID_ARG;
     int prevT = T_;

@@ -88,6 +88,7 @@ class LBvh {
     ~LBvh();
     bvhcd_status init();
     bvhcd_status maintain(bvhcd_bvh_op op, const bvhcd_scene &scene, cudaStream_t s);
+    bvhcd_status maintain_tree(bvhcd_bvh_op op, const bvhcd_scene &scene, cudaStream_t s);
     bvhcd_status export_tree(int32_t *inode, float *ibox, int32_t *leaf, float *lbox, int32_t *lca,
                              uint32_t *codes, int32_t *primmap, cudaStream_t s) const;
     bvhcd_status request_restructure(const int32_t *roots, int32_t n, cudaStream_t s);
@@ -122,6 +123,7 @@ class LBvh {
     bool built() const { return built_; }
     int opt_tag() const { return opt_tag_; }
     const float *verts() const { return vptr_; }
+    const int *faces() const { return fptr_; }
     bool restr_enabled() const { return cfg_.enable_restr != 0; }
 
     // BvhRestrLog (Mine/collision/auxiliary/BvhRestrLog.h:57-80): written by
@@ -143,6 +145,7 @@ class LBvh {
     bvhcd_status restructure(cudaStream_t s);
     bvhcd_status scene_box(cudaStream_t s);
     bvhcd_status climb_and_order(cudaStream_t s);
+    bvhcd_status node_fp16(cudaStream_t s);
 
     bvhcd_bvh_config cfg_;
     int T_ = 0, V_ = 0, capT_ = 0, capV_ = 0;
@@ -153,7 +156,7 @@ class LBvh {
     // owned copies of host input
     DBuf verts_, faces_;
     // tree
-    DBuf nrec_, lrec_, topo_, nrange_, lca_, sface_, primmap_, code_, refit_flag_;
+    DBuf nrec_, lrec_, topo_, nrange_, lca_, sface_, primmap_, code_, refit_flag_, nrec16_;
     // build scratch
     DBuf keys_, vals_, keys2_, vals2_, k64_, k64b_, metric_, ulc_, urc_, upar_, urx_, ury_, umark_,
         ubox_, uflag_, posb_, clen_, coff_, dfs_, ulpar_, scene_, partial_, scratch_, task_, tmpface_;
@@ -179,6 +182,8 @@ class Front {
     bvhcd_status pairs(int which, int32_t *out, int64_t cap, int64_t *count, bool out_dev,
                        cudaStream_t s);
     bvhcd_status export_front(int which, int32_t *out, int64_t cap, int64_t *count, cudaStream_t s);
+    bvhcd_status contacts(int which, float *out, int64_t cap, int64_t *count, int64_t *flagged, bool out_dev,
+                          cudaStream_t s);
     bvhcd_status device_results(const int32_t **hits, const int64_t **counts);
 
     // Host-side state a maintain() call advances (see LBvh::HostState);
@@ -225,6 +230,7 @@ class Front {
     bvhcd_status check_quality(cudaStream_t s);
     bvhcd_status snapshot(cudaStream_t s);
     bvhcd_status grow_and_check(cudaStream_t s, bool *overflowed);
+    bvhcd_status compact_pairs(cudaStream_t s);
     FrontLog log() const;
 
     LBvh *bvh_;
@@ -244,7 +250,7 @@ class Front {
     bool quality_check_ = true;
     DBuf front_[2][2];  // [set][0 int, 1 ext] int2 entries
     int64_t fcap_[2] = {0, 0};
-    DBuf pairs_, hits_, outbuf_, work_;
+    DBuf pairs_, hits_, outbuf_, work_, cbuf_, cflag_, cscratch_;
     int64_t pcap_ = 0;
     DBuf intcnt_, extcnt_, intbeg_, extbeg_, intback_, extback_, snapshot_, scratch_, counts64_;
 };

@@ -143,15 +143,19 @@ def cloth_over_sphere_frames(n: int = 512, frames: int = 100, seed: int = 2024,
 
 
 def stacked_layers_frames(n: int = 512, layers: int = 4, frames: int = 50, seed: int = 77,
-                          gap: float = 1e-3, max_shear: float = 0.5):
+                          gap: float = 1e-3, max_shear: float = 0.5, z_noise: float = 0.0):
     """`layers` cloths at z = 0, gap, 2 gap, ... with a seeded in-plane shear
-    of up to +-max_shear edge lengths per frame per layer."""
+    of up to +-max_shear edge lengths per frame per layer.  z_noise > 0 adds a
+    seeded, frame-constant vertical jitter of up to +-z_noise gaps, so that
+    neighbouring layers cut through each other at grazing angles."""
     x, y, cf = cloth_grid(n)
     rng = np.random.default_rng(seed)
     edge = 1.0 / (n - 1)
     V = x.size
     faces = np.concatenate([cf + l * V for l in range(layers)]).astype(np.int32)
     shear = np.zeros((layers, 2))
+    jit = (rng.uniform(-z_noise, z_noise, size=(layers, x.size)) * gap if z_noise > 0
+           else np.zeros((layers, x.size)))
     out = []
     for f in range(frames):
         shear += rng.uniform(-max_shear, max_shear, size=(layers, 2)) * edge
@@ -159,7 +163,7 @@ def stacked_layers_frames(n: int = 512, layers: int = 4, frames: int = 50, seed:
         for l in range(layers):
             sx = x + shear[l, 0] * y
             sy = y + shear[l, 1] * x
-            pts.append(np.stack([sx, sy, np.full_like(x, l * gap)], axis=1))
+            pts.append(np.stack([sx, sy, l * gap + jit[l]], axis=1))
         out.append(np.concatenate(pts).astype(np.float32))
     return faces, out
 
@@ -256,3 +260,17 @@ class BatchedScenes:
         faces = np.concatenate([self.faces[self.tri_offsets[s]:self.tri_offsets[s + 1]] for s in ids])
         off = np.concatenate([[0], np.cumsum([self.tri_offsets[s + 1] - self.tri_offsets[s] for s in ids])])
         return remap[faces].astype(np.int32), off.astype(np.int32), vidx
+
+
+def shard_scenes(sizes, world: int, rank: int):
+    """Scenes of rank `rank` when `world` ranks share a batch: scenes dealt
+    largest first to the rank with the fewest triangles so far (ties to the
+    lowest rank).  Returns the sorted scene ids."""
+    sizes = np.asarray(sizes)
+    load = np.zeros(world)
+    owner = np.empty(sizes.size, dtype=np.int64)
+    for sc in np.argsort(-sizes, kind="stable"):
+        r = int(np.argmin(load))
+        owner[sc] = r
+        load[r] += sizes[sc]
+    return np.flatnonzero(owner == rank)

@@ -54,7 +54,11 @@ typedef struct {
     int32_t prim_capacity;   /* max triangles (reference default 150000) */
     int32_t vert_capacity;   /* max vertices */
     int32_t enable_restr;    /* quality-triggered restructuring (reference: on) */
-    int32_t reserved[5];
+    int32_t node_box_fp16;   /* precision mode: the front traversals read internal-node
+                                boxes stored as FP16 rounded outward (16-byte records
+                                instead of 32-byte ones); leaf tests stay FP32, so the
+                                pair set is the same.  Fronts may differ (looser boxes). */
+    int32_t reserved[4];
 } bvhcd_bvh_config;
 
 /* BvttFrontIntraBuildConfig{intFrontSize, extFrontSize, cpNum}
@@ -66,7 +70,11 @@ typedef struct {
     int32_t cull_adjacent;       /* drop pairs sharing a vertex id (covertex) */
     int32_t narrow_phase;        /* run the tri-tri test after the broad phase */
     int32_t auto_grow;           /* on overflow: grow buffers and replay (syncs) */
-    int32_t reserved[5];
+    int32_t precision;           /* 0: the reference's FP32 narrow phase; 1: FP32 where
+                                    certain, FP64 for the pairs it flags (hits equal an
+                                    FP64 evaluation of every pair), FP64 contact points /
+                                    distances where FP32 is ill-conditioned */
+    int32_t reserved[4];
 } bvhcd_front_config;
 
 /* SceneData{pos, fids} (Mine/world/Scene.h:16-20). */
@@ -92,7 +100,8 @@ typedef struct {
     int32_t restr_pending;   /* quality check marked the BVH for restructuring */
     int32_t num_rt_subtrees; /* restructure decision inputs (LBvhFixedDeformable.cu:240-241) */
     int32_t num_rt_int_nodes;
-    int32_t reserved[6];
+    int32_t flagged;         /* precision mode: pairs the narrow phase re-decided in FP64 */
+    int32_t reserved[5];
 } bvhcd_front_stats;
 
 typedef struct bvhcd_bvh bvhcd_bvh;
@@ -230,6 +239,20 @@ bvhcd_status bvhcd_morton_order_noalloc(const float *pos, const int32_t *faces, 
  * maintain rebuilds either way. */
 bvhcd_status bvhcd_bvh_set_scenes(bvhcd_bvh *bvh, int32_t num_scenes, const int32_t *tri_offsets);
 
+/* ---- Contact points and distances (precision mode extension; the
+ * reference's narrow phase returns a hit flag only, narrow_phase.cu:8-24).
+ * which = 0: for every hit, in the order bvhcd_front_pairs(which = 1) returns
+ * them, the midpoint (x, y, z) and length (w) of the two triangles'
+ * intersection segment (NaN point for coplanar pairs); which = 1: for every
+ * broad-phase pair, in the order of bvhcd_front_pairs(which = 0), the distance
+ * between the two triangles (w; 0 for intersecting pairs).  FP32; with
+ * precision = 1, FP64 for nearly parallel planes (contacts) and for distances
+ * below a thousandth of the pair's size.  out: 4 floats per item (host, or
+ * device with out_on_device); flagged (may be NULL) receives how many items
+ * were computed in FP64.  Synchronises `stream`. */
+bvhcd_status bvhcd_front_contacts(bvhcd_front *front, int32_t which, float *out, int64_t cap, int64_t *count,
+                                  int64_t *flagged, int32_t out_on_device, void *stream);
+
 /* ---- State copies.  No counterpart in the reference.  dst becomes a copy of
  * src -- tree, restructure log, counters, fronts, pairs and their host-side
  * state -- so the two continue independently from the same frame (the
@@ -270,12 +293,16 @@ bvhcd_status bvhcd_learner_create(bvhcd_bvh *bvh, bvhcd_front *front, int32_t ma
 bvhcd_status bvhcd_learner_destroy(bvhcd_learner *learner);
 bvhcd_status bvhcd_learner_set_params(bvhcd_learner *learner, const float *params);
 bvhcd_status bvhcd_learner_get_params(const bvhcd_learner *learner, float *params);
-/* One learned frame: BVH refit (build on frame 0; a restructure when the
- * previous decision marked subtrees), the front op of the reference's cycle
- * (UPDATE at frame % 6 == 0, REORDER at 5, KEEP otherwise) or GENERATE after a
- * rebuild or a regenerate vote, then the next decision.  bvh_tag receives the
- * reference's opt tag (0 refit, 1 restructure, 2 build), front_op the op run;
- * either may be NULL.  Synchronises `stream` once (the decision's counts). */
+/* One learned frame: BVH refit (build on frame 0; a restructure when a
+ * decision marked subtrees), the front op of the reference's cycle (UPDATE at
+ * frame % 6 == 0, REORDER at 5, KEEP otherwise) or GENERATE after a rebuild or
+ * a regenerate vote.  Every `decide_every` frames (default 3) it queues a
+ * decision -- features, votes, marks and counts on the device, an event --
+ * and the first frame that finds the event complete applies it; the host never
+ * waits for it.  A decision voted on a tree that has changed since is dropped.
+ * bvh_tag receives the reference's opt tag (0 refit, 1 restructure, 2 build),
+ * front_op the op run; either may be NULL. */
+bvhcd_status bvhcd_learner_set_decide_every(bvhcd_learner *learner, int32_t frames);
 bvhcd_status bvhcd_learner_frame(bvhcd_learner *learner, const bvhcd_scene *scene, int32_t frame,
                                  int32_t *bvh_tag, int32_t *front_op, void *stream);
 /* Trace recording under another schedule: after each frame's maintains, tell

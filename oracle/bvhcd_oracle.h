@@ -80,6 +80,15 @@ void orc_narrow_exact(int64_t n, const int *pairs, const int *faces, const float
                       unsigned char *hit);
 void orc_schedule(int frame, int start, int *bvh_op, int *front_op);
 
+/* Precision mode references (precision_oracle.c): FP64 SAT, intersection
+ * segment (midpoint xyz, length; returns 1, 0 = none, 2 = coplanar), triangle
+ * distance, and all three over a pair list (any output may be NULL). */
+int orc_tritri_sat64(const float *p9, const float *q9);
+int orc_contact64(const float *p9, const float *q9, double *out4);
+double orc_tri_distance64(const float *p9, const float *q9);
+void orc_precision_pairs(int64_t n, const int *pairs, const int *faces, const float *verts,
+                         unsigned char *hit64, double *contact4, double *dist);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,14 @@ def lib():
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_pipe_mark_restructure.argtypes = [ctypes.c_void_p, _i32p, ctypes.c_int]
         L.orc_pipe_set_reference_permutation.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_precision_pairs.argtypes = [ctypes.c_int64, _i32p, _i32p, _f32p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_tritri_sat64.restype = ctypes.c_int
+        L.orc_tritri_sat64.argtypes = [_f32p, _f32p]
+        L.orc_contact64.restype = ctypes.c_int
+        L.orc_contact64.argtypes = [_f32p, _f32p, ctypes.c_void_p]
+        L.orc_tri_distance64.restype = ctypes.c_double
+        L.orc_tri_distance64.argtypes = [_f32p, _f32p]
         L.orc_scene_box.argtypes = [ctypes.c_int, _i32p, _f32p, _f32p]
         L.orc_morton_codes.argtypes = [ctypes.c_int, _i32p, _f32p, _f32p, _u32p]
         L.orc_brute_pairs.restype = ctypes.c_int64
@@ -216,3 +224,33 @@ class Pipeline:
         arrs = [np.zeros(T + 1, dtype=np.uint32) for _ in range(4)]
         lib().orc_pipe_log(self._p, *[a.ctypes.data for a in arrs])
         return dict(zip(["intcnt", "extcnt", "intbeg", "extbeg"], arrs))
+
+
+def precision_pairs(pairs, faces, verts):
+    """FP64 references of the precision mode over a pair list of original
+    triangle ids: (FP64 SAT hit mask, contact midpoint + segment length per
+    pair -- NaN where not a hit or coplanar, distance per pair -- 0 for hits)."""
+    pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+    faces = np.ascontiguousarray(faces, dtype=np.int32)
+    verts = np.ascontiguousarray(verts, dtype=np.float32)
+    n = pairs.shape[0]
+    hit = np.zeros(max(n, 1), np.uint8)
+    con = np.zeros((max(n, 1), 4), np.float64)
+    dist = np.zeros(max(n, 1), np.float64)
+    lib().orc_precision_pairs(n, pairs, faces, verts, hit.ctypes.data, con.ctypes.data, dist.ctypes.data)
+    return hit[:n].astype(bool), con[:n], dist[:n]
+
+
+def tritri_sat64(p9, q9):
+    return bool(lib().orc_tritri_sat64(np.ascontiguousarray(p9, np.float32), np.ascontiguousarray(q9, np.float32)))
+
+
+def contact64(p9, q9):
+    out = np.zeros(4, np.float64)
+    st = lib().orc_contact64(np.ascontiguousarray(p9, np.float32), np.ascontiguousarray(q9, np.float32),
+                             out.ctypes.data)
+    return st, out
+
+
+def tri_distance64(p9, q9):
+    return float(lib().orc_tri_distance64(np.ascontiguousarray(p9, np.float32), np.ascontiguousarray(q9, np.float32)))

@@ -61,6 +61,7 @@ def test_learned_frames_keep_exact_pairs(cuda, lib_built, oracle, cloth_c1, bias
     faces, frames = cloth_c1
     T, V = faces.shape[0], frames[0].shape[0]
     bvh, front, lrn = _learner(lib_built, T, V)
+    lrn.set_decide_every(2)
     rng = np.random.default_rng(11)
     if bias is None:
         p = rng.normal(0, 0.3, m.N_PARAMS).astype(np.float32)
@@ -80,7 +81,8 @@ def test_learned_frames_keep_exact_pairs(cuda, lib_built, oracle, cloth_c1, bias
         assert np.array_equal(oracle.canon_pairs(front.pairs(narrow=True)),
                               oracle.canon_pairs(ref.pairs(narrow=True))), f
     if bias == (0.0, 0.0, 8.0):
-        assert all(fop == lib_built.FRONT_GENERATE for _, fop in tags[1:])
+        # decisions are applied a frame or more after they are queued
+        assert sum(fop == lib_built.FRONT_GENERATE for _, fop in tags[1:]) >= 4
     if bias == (0.0, 8.0, 0.0):
         assert any(tag in (1, 2) for tag, _ in tags[1:])    # the marks reached the BVH
     if bias == (8.0, 0.0, 0.0):
