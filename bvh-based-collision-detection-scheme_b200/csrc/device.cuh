@@ -67,11 +67,27 @@ enum CounterSlot {
     C_PAIRS_VALID = 11,       // broad-phase pairs (C_PAIRS counts reserved slots, holes included)
     C_COMPACT = 12,           // compaction cursor of the pair export
     C_FLAGGED = 13,           // precision mode: pairs re-decided in FP64
+    C_TOPK = 14,              // refit plan: nodes whose leaf range crosses a refit block
     C_NUM = 16
 };
 
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
 __device__ __forceinline__ float4 ldcg4(const float4 *p) { return __ldcg(p); }
+// A 32-byte record {lo, hi} (32-byte aligned, read-only for the kernel's
+// lifetime) in one 256-bit load: a gather of records then costs one request
+// per warp instead of two.
+__device__ __forceinline__ void ldg8(const float4 *p, float4 &lo, float4 &hi) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(lo.x), "=f"(lo.y), "=f"(lo.z), "=f"(lo.w), "=f"(hi.x), "=f"(hi.y), "=f"(hi.z), "=f"(hi.w)
+        : "l"(p));
+}
+// the same record stored whole in one 256-bit store (a whole 32-byte sector:
+// no partial-sector write for the memory to merge)
+__device__ __forceinline__ void stg8(float4 *p, const float4 &lo, const float4 &hi) {
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(lo.x), "f"(lo.y),
+                 "f"(lo.z), "f"(lo.w), "f"(hi.x), "f"(hi.y), "f"(hi.z), "f"(hi.w)
+                 : "memory");
+}
 
 // AABB overlap, touching counts (BvhBvCompletePort::overlaps,
 // Mine/collision/lbvh/BvhBV.h:54-65).  n = node box, b = query box.

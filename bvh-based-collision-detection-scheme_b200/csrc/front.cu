@@ -70,8 +70,7 @@ __device__ __forceinline__ void node_rec(const FArgs &a, int n, float4 &lo, floa
         lo = make_float4(half_lo(r.x), half_hi(r.x), half_lo(r.y), __int_as_float(-1));
         hi = make_float4(half_hi(r.y), half_lo(r.z), half_hi(r.z), __int_as_float((int)r.w));
     } else {
-        lo = ldg4(a.nrec + 2 * n);
-        hi = ldg4(a.nrec + 2 * n + 1);
+        ldg8(a.nrec + 2 * n, lo, hi);
     }
 }
 // the node's leftmost leaf (its lo.w in the FP32 record)
@@ -179,15 +178,13 @@ __device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const
         float4 llo, lhi;
         if (st & 1) {
             leaf = st >> 1;
-            llo = ldg4(a.lrec + 2 * leaf);
-            lhi = ldg4(a.lrec + 2 * leaf + 1);
+            ldg8(a.lrec + 2 * leaf, llo, lhi);
         } else {
             int n = st >> 1;
             float4 nlo, nhi;
             node_rec(a, n, nlo, nhi);
             leaf = node_rangex(a, n, nlo);
-            llo = ldg4(a.lrec + 2 * leaf);
-            lhi = ldg4(a.lrec + 2 * leaf + 1);
+            ldg8(a.lrec + 2 * leaf, llo, lhi);
             const int last = __float_as_int(llo.w);  // parent of the leftmost leaf
             bool stopped = false;
             while (true) {
@@ -224,7 +221,8 @@ template <bool kFront>
 __global__ void __launch_bounds__(kThreads) k_generate(FArgs a) {
     Em em;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.T - 1; i += gridDim.x * blockDim.x) {
-        float4 plo = ldg4(a.lrec + 2 * i), phi = ldg4(a.lrec + 2 * i + 1);
+        float4 plo, phi;
+        ldg8(a.lrec + 2 * i, plo, phi);
         traverse<kFront>(a, em, i, plo, phi, prim_face(a, i), __float_as_int(phi.w), -1);
     }
     em_close(a, em);
@@ -286,13 +284,11 @@ __device__ __forceinline__ void load_recs(const FArgs &a, Batch<kU> &b) {
 #pragma unroll
     for (int k = 0; k < kU; k++) {
         if (!b.v[k]) continue;
-        b.plo[k] = ldg4(a.lrec + 2 * b.e[k].x);
-        b.phi[k] = ldg4(a.lrec + 2 * b.e[k].x + 1);
+        ldg8(a.lrec + 2 * b.e[k].x, b.plo[k], b.phi[k]);
         if (b.in_int[k]) {
             node_rec(a, b.e[k].y, b.nlo[k], b.nhi[k]);
         } else {
-            b.nlo[k] = ldg4(a.lrec + 2 * b.e[k].y);
-            b.nhi[k] = ldg4(a.lrec + 2 * b.e[k].y + 1);
+            ldg8(a.lrec + 2 * b.e[k].y, b.nlo[k], b.nhi[k]);
         }
     }
 }
@@ -322,7 +318,8 @@ __global__ void __launch_bounds__(kB) k_sprout(FArgs a) {
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const int2 e = a.work[q];
         if (e.x < 0) continue;  // hole
-        const float4 plo = ldg4(a.lrec + 2 * e.x), phi = ldg4(a.lrec + 2 * e.x + 1);
+        float4 plo, phi;
+        ldg8(a.lrec + 2 * e.x, plo, phi);
         float4 nlo, nhi;
         node_rec(a, e.y, nlo, nhi);
         traverse<kFront>(a, em, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, node_rangex(a, e.y, nlo)),

@@ -399,46 +399,441 @@ __global__ void k_write_nodes(int nint, int T, Climb c, const int *__restrict__ 
 }
 
 // ---------------------------------------------------------------- refit
-// refitExtNode + refitIntNode (Mine/collision/lbvh/LBvhUpdateKernels.cu:35-74)
-// fused: each slot's thread computes its leaf box from the three vertices,
-// then climbs.  A node receives two arrivals per refit, so the parity of its
-// flag tells the second arrival without clearing flags between refits.  The
-// climbing thread keeps its own child's box in registers and loads only the
-// sibling's; the parent's topology (static) is requested before the atomic so
-// one level costs one atomic round trip plus one sibling load.
-__global__ void __launch_bounds__(kThreads) k_refit(int T, const int4 *__restrict__ sface,
-                                                    const float *__restrict__ verts, float4 *lrec,
-                                                    float4 *nrec, const int4 *__restrict__ topo,
-                                                    unsigned *flag) {
+// refitExtNode + refitIntNode (Mine/collision/lbvh/LBvhUpdateKernels.cu:35-74):
+// leaf boxes from the three vertices, then every internal box as the union of
+// its children's, bottom-up.
+//
+// A climb over the whole tree with one arrival counter per node pays a fence
+// around every arrival on its longest leaf-to-root chain (about 0.7 us each
+// on B200, at any scope), and the chains set the refit's time.  This refit
+// runs level by level instead, in node height order (a parent is higher than
+// its children), with a CTA barrier between levels and no fences:
+//  - the leaves are cut into blocks of kRefitW; a node whose leaf range lies
+//    in one block is local to it, the others (the top of the tree and the
+//    spines above each block boundary) cross;
+//  - k_refit_local: one CTA per leaf block computes the leaf boxes, then the
+//    local node boxes level by level in shared memory;
+//  - k_refit_top: one CTA computes the crossing node boxes level by level,
+//    from the final boxes of their local children.
+// Min and max are exact, so the boxes equal those of any other bottom-up
+// order.  The plan (splits, heights, which node is where) depends on the
+// topology only; refit_plan rebuilds it after every build and restructure.
+constexpr int kRefitW = 2048;        // leaves per local block
+constexpr int kRefitThreads = 1024;  // threads per refit CTA
+constexpr int kRefitSlots = kRefitW / kRefitThreads;
+constexpr int kMaxLevels = 64;       // levels a level-sorted list holds (deeper: one pass per level over all)
+constexpr int kLevelHdr = kMaxLevels + 3;  // per list: level count (or -1), then level offsets
+constexpr int kTopCap = 6144;        // crossing nodes the top pass keeps in shared memory
+constexpr int kTopPer = kTopCap / kRefitThreads;
+// boxes of the block's leaves and splits, then its level-sorted work list
+constexpr size_t kLocalSmem = (size_t)2 * kRefitW * 6 * sizeof(float) + (size_t)kRefitW * sizeof(int2);
+// boxes of the crossing nodes, then their level-sorted work list
+constexpr size_t kTopSmem = (size_t)kTopCap * (6 * sizeof(float) + sizeof(int2));
+
+// Node heights (leaves 0, a node one above its higher child), bottom-up with
+// arrival counters: run once per topology, so its fences do not matter.
+__global__ void __launch_bounds__(kThreads) k_heights(int T, const float4 *__restrict__ lrec,
+                                                      const int4 *__restrict__ topo, unsigned *flag, int *height) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x) {
-        const int4 f = __ldg(&sface[s]);
-        int p = __float_as_int(reinterpret_cast<const float *>(lrec)[8 * (size_t)s + 3]);
-        float4 lo, hi;
-        tri_box(load_vert(verts, f.x), load_vert(verts, f.y), load_vert(verts, f.z), lo, hi);
-        float *w = reinterpret_cast<float *>(lrec + 2 * (size_t)s);
-        w[0] = lo.x; w[1] = lo.y; w[2] = lo.z;
-        w[4] = hi.x; w[5] = hi.y; w[6] = hi.z;
-        int child = s;
-        bool child_leaf = true;
-        // at most T - 1 ancestors; the bound keeps a corrupted tree from looping
+        int p = __float_as_int(__ldg(reinterpret_cast<const float *>(lrec) + 8 * (size_t)s + 3));
+        int h = 0;
         for (int guard = T; p >= 0 && guard > 0; --guard) {
-            const int4 t = __ldg(&topo[p]);
-            cuda::atomic_ref<unsigned, cuda::thread_scope_device> fl(flag[p]);
-            if ((fl.fetch_add(1u, cuda::memory_order_acq_rel) & 1u) == 0u) break;
-            const bool from_left = (child == t.x) && (((t.w & 1) != 0) == child_leaf);
-            const int sib = from_left ? t.y : t.x;
-            const bool sib_leaf = from_left ? (t.w & 2) != 0 : (t.w & 1) != 0;
-            const float4 *src = sib_leaf ? lrec : nrec;
-            const float4 slo = __ldcg(src + 2 * (size_t)sib), shi = __ldcg(src + 2 * (size_t)sib + 1);
-            lo.x = fminf(lo.x, slo.x); lo.y = fminf(lo.y, slo.y); lo.z = fminf(lo.z, slo.z);
-            hi.x = fmaxf(hi.x, shi.x); hi.y = fmaxf(hi.y, shi.y); hi.z = fmaxf(hi.z, shi.z);
-            float *q = reinterpret_cast<float *>(nrec + 2 * (size_t)p);
-            q[0] = lo.x; q[1] = lo.y; q[2] = lo.z;
-            q[4] = hi.x; q[5] = hi.y; q[6] = hi.z;
-            child = p;
-            child_leaf = false;
-            p = t.z;
+            atomicMax(&height[p], h + 1);
+            __threadfence();
+            if (atomicAdd(&flag[p], 1u) == 0u) break;
+            __threadfence();
+            h = __ldcg(&height[p]);
+            p = __ldg(&topo[p]).z;
         }
+    }
+}
+
+// split of each internal node (the last leaf of its left subtree: every
+// internal node has its own) and whether its leaf range crosses a block
+__global__ void k_plan_split(int nint, const int4 *__restrict__ topo, const int2 *__restrict__ nrange, int *split,
+                             unsigned *cross) {
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nint; d += gridDim.x * blockDim.x) {
+        const int4 t = topo[d];
+        split[d] = (t.w & 1) ? t.x : nrange[t.x].y;
+        const int2 r = nrange[d];
+        cross[d] = (r.x / kRefitW) != (r.y / kRefitW) ? 1u : 0u;
+    }
+}
+
+// plan[split(d)] = {d, or -1 if d crosses; left ref; right ref; height},
+// refs (leaf << 1 | 1) or (split << 1).  top[k] for the k-th crossing node
+// = {d; left ref; right ref; height}, refs (leaf << 2 | 1), (local node << 2)
+// or (crossing k << 2 | 2).
+__global__ void k_plan_write(int nint, const int4 *__restrict__ topo, const int *__restrict__ split,
+                             const unsigned *__restrict__ cross, const unsigned *__restrict__ topk,
+                             const int *__restrict__ height, int4 *plan, int4 *top) {
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nint; d += gridDim.x * blockDim.x) {
+        const int4 t = topo[d];
+        const bool lleaf = (t.w & 1) != 0, rleaf = (t.w & 2) != 0;
+        const bool c = cross[d] != 0;
+        const int h = height[d];
+        plan[split[d]] = make_int4(c ? -1 : d, lleaf ? (t.x << 1) | 1 : split[t.x] << 1,
+                                   rleaf ? (t.y << 1) | 1 : split[t.y] << 1, h);
+        if (c) {
+            auto ref = [&](int ch, bool leaf) {
+                return leaf ? (ch << 2) | 1 : cross[ch] ? (int)(topk[ch] << 2) | 2 : ch << 2;
+            };
+            top[topk[d]] = make_int4(d, ref(t.x, lleaf), ref(t.y, rleaf), h);
+        }
+    }
+}
+
+// boxes as 6 floats (24 bytes, 8-byte aligned): three 64-bit accesses
+__device__ __forceinline__ void box_store6(float *b, const float4 &lo, const float4 &hi) {
+    float2 *q = reinterpret_cast<float2 *>(b);
+    q[0] = make_float2(lo.x, lo.y);
+    q[1] = make_float2(lo.z, hi.x);
+    q[2] = make_float2(hi.y, hi.z);
+}
+__device__ __forceinline__ void box_load6(const float *b, float4 &lo, float4 &hi) {
+    const float2 *q = reinterpret_cast<const float2 *>(b);
+    const float2 u = q[0], v = q[1], w = q[2];
+    lo = make_float4(u.x, u.y, v.x, 0.f);
+    hi = make_float4(v.y, w.x, w.y, 0.f);
+}
+__device__ __forceinline__ void box_union6(const float *b, float4 &lo, float4 &hi) {
+    float4 clo, chi;
+    box_load6(b, clo, chi);
+    lo.x = fminf(lo.x, clo.x); lo.y = fminf(lo.y, clo.y); lo.z = fminf(lo.z, clo.z);
+    hi.x = fmaxf(hi.x, chi.x); hi.y = fmaxf(hi.y, chi.y); hi.z = fmaxf(hi.z, chi.z);
+}
+// the box fields of a 32-byte record ({lo.xyz, link}, {hi.xyz, link}); the
+// links stay
+__device__ __forceinline__ void rec_store_box(float4 *rec, const float4 &lo, const float4 &hi) {
+    float *w = reinterpret_cast<float *>(rec);
+    w[0] = lo.x; w[1] = lo.y; w[2] = lo.z;
+    w[4] = hi.x; w[5] = hi.y; w[6] = hi.z;
+}
+
+// Level-sorted work lists, built once per topology by one CTA per list:
+// count per level, offsets, scatter.  hdr[0] = number of levels L (or -1
+// when the heights span more than kMaxLevels), hdr[1 + h] = offset of level
+// h, h = 0..L.
+__device__ void level_sort_begin(int *cnt) {
+    if (threadIdx.x <= kMaxLevels) cnt[threadIdx.x] = 0;
+}
+__device__ void level_sort_offsets(const int *cnt, int *cur, int L, int *hdr) {
+    if (threadIdx.x != 0) return;
+    int acc = 0;
+    hdr[0] = L;
+    for (int h = 0; h <= L; h++) {
+        hdr[1 + h] = acc;
+        cur[h] = acc;
+        acc += cnt[h];
+    }
+    hdr[2 + L] = acc;
+}
+
+// Local lists: for leaf block b, its local nodes by height (level h - 1 holds
+// height h) as {node, split slot, left child slot, right child slot}; slots
+// index the block's boxes (leaves 0..kRefitW-1, splits kRefitW + split - L0).
+__global__ void __launch_bounds__(kRefitThreads) k_plan_local(int T, const int4 *__restrict__ plan, int4 *llist,
+                                                              int *lhdr) {
+    __shared__ int cnt[kMaxLevels + 1], cur[kMaxLevels + 1], hmax;
+    const int L0 = blockIdx.x * kRefitW, nl = min(kRefitW, T - L0);
+    int *hdr = lhdr + (size_t)blockIdx.x * kLevelHdr;
+    level_sort_begin(cnt);
+    if (threadIdx.x == 0) hmax = 0;
+    __syncthreads();
+    int4 e[kRefitSlots];
+    int hm = 0;
+#pragma unroll
+    for (int i = 0; i < kRefitSlots; i++) {
+        const int j = threadIdx.x + i * kRefitThreads;
+        e[i] = (j < nl && L0 + j < T - 1) ? __ldg(&plan[L0 + j]) : make_int4(-1, -1, -1, 0);
+        if (e[i].x >= 0) hm = max(hm, e[i].w);
+    }
+    atomicMax(&hmax, hm);
+    __syncthreads();
+    const int H = hmax;
+    if (H > kMaxLevels) {
+        if (threadIdx.x == 0) hdr[0] = -1;
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < kRefitSlots; i++)
+        if (e[i].x >= 0) atomicAdd(&cnt[e[i].w - 1], 1);
+    __syncthreads();
+    level_sort_offsets(cnt, cur, max(H - 1, 0), hdr);
+    __syncthreads();
+    auto slot = [&](int ref) { return (ref & 1) ? (ref >> 1) - L0 : kRefitW + (ref >> 1) - L0; };
+#pragma unroll
+    for (int i = 0; i < kRefitSlots; i++) {
+        if (e[i].x < 0) continue;
+        const int pos = atomicAdd(&cur[e[i].w - 1], 1);
+        llist[L0 + pos] = make_int4(e[i].x, threadIdx.x + i * kRefitThreads, slot(e[i].y), slot(e[i].z));
+    }
+}
+
+// Top list: the crossing nodes that have a crossing child, by height (level
+// h - H0, H0 the lowest crossing height), as {k, crossing child k or -1, the
+// other or -1, 0}.
+__global__ void __launch_bounds__(kRefitThreads) k_plan_top(const unsigned *__restrict__ ctr,
+                                                            const int4 *__restrict__ top, int4 *tlist, int *thdr) {
+    __shared__ int cnt[kMaxLevels + 1], cur[kMaxLevels + 1], hlo, hhi;
+    const int K = (int)ctr[C_TOPK];
+    level_sort_begin(cnt);
+    if (threadIdx.x == 0) { hlo = INT_MAX; hhi = 0; }
+    __syncthreads();
+    int h0 = INT_MAX, h1 = 0;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const int w = __ldg(&top[k]).w;
+        h0 = min(h0, w);
+        h1 = max(h1, w);
+    }
+    atomicMin(&hlo, h0);
+    atomicMax(&hhi, h1);
+    __syncthreads();
+    const int H0 = hlo, H1 = hhi;
+    if (K > kTopCap || H1 - H0 > kMaxLevels) {
+        if (threadIdx.x == 0) thdr[0] = -1;
+        return;
+    }
+    auto pending = [](const int4 &e) { return (e.y & 3) == 2 || (e.z & 3) == 2; };
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const int4 e = __ldg(&top[k]);
+        if (pending(e)) atomicAdd(&cnt[e.w - H0], 1);
+    }
+    __syncthreads();
+    level_sort_offsets(cnt, cur, H1 - H0, thdr);
+    __syncthreads();
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const int4 e = __ldg(&top[k]);
+        if (!pending(e)) continue;
+        const int pos = atomicAdd(&cur[e.w - H0], 1);
+        tlist[pos] = make_int4(k, (e.y & 3) == 2 ? e.y >> 2 : -1, (e.z & 3) == 2 ? e.z >> 2 : -1, 0);
+    }
+}
+
+// One CTA per block of kRefitW leaves: leaf boxes, then the block's local
+// nodes level by level from its level-sorted list, all in shared memory.
+__global__ void __launch_bounds__(kRefitThreads, 2) k_refit_local(int T, const int4 *__restrict__ sface,
+                                                                  const float *__restrict__ verts,
+                                                                  const int4 *__restrict__ plan,
+                                                                  const int4 *__restrict__ llist,
+                                                                  const int *__restrict__ lhdr, float4 *lrec,
+                                                                  float4 *nrec) {
+    extern __shared__ __align__(16) float sb[];  // boxes: the block's leaves, then its splits
+    int2 *slist = reinterpret_cast<int2 *>(sb + 12 * kRefitW);
+    __shared__ int sofs[kLevelHdr], hmax;
+    const int L0 = blockIdx.x * kRefitW;
+    const int nl = min(kRefitW, T - L0);
+    const int *hdr = lhdr + (size_t)blockIdx.x * kLevelHdr;
+    if (threadIdx.x == 0) hmax = 0;
+    const int L = __ldg(&hdr[0]);
+    const int nloc = L >= 0 ? __ldg(&hdr[2 + L]) : 0;
+    if (L >= 0 && threadIdx.x <= L + 1) sofs[threadIdx.x] = __ldg(&hdr[1 + threadIdx.x]);
+    int4 w[kRefitSlots];
+    int3 f[kRefitSlots];
+    float2 leaf_links[kRefitSlots];
+#pragma unroll
+    for (int i = 0; i < kRefitSlots; i++) {
+        const int t = threadIdx.x + i * kRefitThreads;
+        w[i] = t < nloc ? __ldg(&llist[L0 + t]) : make_int4(-1, 0, 0, 0);
+        int4 fc = make_int4(0, 0, 0, 0);
+        float4 rlo = make_float4(0.f, 0.f, 0.f, 0.f), rhi = rlo;
+        if (t < nl) {
+            fc = __ldg(&sface[L0 + t]);
+            ldg8(lrec + 2 * (size_t)(L0 + t), rlo, rhi);  // its links
+        }
+        f[i] = make_int3(fc.x, fc.y, fc.z);
+        leaf_links[i] = make_float2(rlo.w, rhi.w);
+    }
+#pragma unroll
+    for (int i = 0; i < kRefitSlots; i++) {
+        const int t = threadIdx.x + i * kRefitThreads;
+        if (w[i].x >= 0) slist[t] = make_int2(w[i].y, (w[i].z << 16) | w[i].w);
+        if (t >= nl) continue;
+        float4 lo, hi;
+        tri_box(load_vert(verts, f[i].x), load_vert(verts, f[i].y), load_vert(verts, f[i].z), lo, hi);
+        box_store6(sb + 6 * t, lo, hi);
+        lo.w = leaf_links[i].x;
+        hi.w = leaf_links[i].y;
+        stg8(lrec + 2 * (size_t)(L0 + t), lo, hi);
+    }
+    // the links of this thread's list nodes, for their whole-record stores
+    float2 node_links[kRefitSlots];
+#pragma unroll
+    for (int i = 0; i < kRefitSlots; i++) {
+        float4 rlo = make_float4(0.f, 0.f, 0.f, 0.f), rhi = rlo;
+        if (w[i].x >= 0) ldg8(nrec + 2 * (size_t)w[i].x, rlo, rhi);
+        node_links[i] = make_float2(rlo.w, rhi.w);
+    }
+    __syncthreads();
+    if (L >= 0) {
+        for (int h = 0; h <= L; h++) {
+            for (int t = sofs[h] + threadIdx.x; t < sofs[h + 1]; t += blockDim.x) {
+                const int2 q = slist[t];
+                float4 lo, hi;
+                box_load6(sb + 6 * (q.y >> 16), lo, hi);
+                box_union6(sb + 6 * (q.y & 0xffff), lo, hi);
+                box_store6(sb + 6 * (kRefitW + q.x), lo, hi);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int i = 0; i < kRefitSlots; i++) {
+            if (w[i].x < 0) continue;
+            float4 lo, hi;
+            box_load6(sb + 6 * (kRefitW + w[i].y), lo, hi);
+            lo.w = node_links[i].x;
+            hi.w = node_links[i].y;
+            stg8(nrec + 2 * (size_t)w[i].x, lo, hi);
+        }
+    } else {
+        // a block with a chain of more than kMaxLevels local nodes: one pass
+        // per height over the block's splits
+        int4 e[kRefitSlots];
+        int hm = 0;
+#pragma unroll
+        for (int i = 0; i < kRefitSlots; i++) {
+            const int j = threadIdx.x + i * kRefitThreads;
+            e[i] = (j < nl && L0 + j < T - 1) ? __ldg(&plan[L0 + j]) : make_int4(-1, -1, -1, 0);
+            if (e[i].x >= 0) hm = max(hm, e[i].w);
+        }
+        atomicMax(&hmax, hm);
+        __syncthreads();
+        const int Hm = hmax;
+        auto slot = [&](int ref) { return (ref & 1) ? (ref >> 1) - L0 : kRefitW + (ref >> 1) - L0; };
+        for (int h = 1; h <= Hm; h++) {
+#pragma unroll
+            for (int i = 0; i < kRefitSlots; i++) {
+                if (e[i].x < 0 || e[i].w != h) continue;
+                float4 lo, hi;
+                box_load6(sb + 6 * slot(e[i].y), lo, hi);
+                box_union6(sb + 6 * slot(e[i].z), lo, hi);
+                box_store6(sb + 6 * (kRefitW + threadIdx.x + i * kRefitThreads), lo, hi);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int i = 0; i < kRefitSlots; i++) {
+            if (e[i].x < 0) continue;
+            float4 lo, hi;
+            box_load6(sb + 6 * (kRefitW + threadIdx.x + i * kRefitThreads), lo, hi);
+            rec_store_box(nrec + 2 * (size_t)e[i].x, lo, hi);
+        }
+    }
+}
+
+// The crossing nodes in one CTA: a node's slot starts as the union of its
+// non-crossing children's (final) boxes, then the nodes with crossing
+// children take those in level by level from the top list.  With more than
+// kTopCap crossing nodes (or too many levels), the slots are global scratch
+// and every level passes over all nodes (the CTA barrier orders both).
+__device__ __forceinline__ void top_init_box(const int4 &e, const float4 *__restrict__ lrec,
+                                             const float4 *__restrict__ nrec, float *b) {
+    float4 lo = make_float4(3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f, 0.f);
+    float4 hi = make_float4(-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f, 0.f);
+    const int r[2] = {e.y, e.z};
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        if ((r[c] & 3) == 2) continue;
+        float4 clo, chi;
+        ldg8(((r[c] & 3) == 1 ? lrec : nrec) + 2 * (size_t)(r[c] >> 2), clo, chi);
+        lo.x = fminf(lo.x, clo.x); lo.y = fminf(lo.y, clo.y); lo.z = fminf(lo.z, clo.z);
+        hi.x = fmaxf(hi.x, chi.x); hi.y = fmaxf(hi.y, chi.y); hi.z = fmaxf(hi.z, chi.z);
+    }
+    box_store6(b, lo, hi);
+}
+
+__global__ void __launch_bounds__(kRefitThreads) k_refit_top(const unsigned *__restrict__ ctr,
+                                                             const int4 *__restrict__ top,
+                                                             const int4 *__restrict__ tlist,
+                                                             const int *__restrict__ thdr,
+                                                             const float4 *__restrict__ lrec, float4 *nrec,
+                                                             float *gbox, int cap) {
+    extern __shared__ __align__(16) float sbox[];
+    __shared__ int sofs[kLevelHdr];
+    const int K = min((int)ctr[C_TOPK], cap);
+    const int L = __ldg(&thdr[0]);
+    if (L >= 0 && K <= kTopCap) {
+        int2 *slist = reinterpret_cast<int2 *>(sbox + 6 * kTopCap);
+        const int npend = __ldg(&thdr[2 + L]);
+        if (threadIdx.x <= L + 1) sofs[threadIdx.x] = __ldg(&thdr[1 + threadIdx.x]);
+        // this thread's crossing nodes k = threadIdx.x + i * kRefitThreads:
+        // their ids and links (for the whole-record stores), and their slots
+        int d[kTopPer];
+        float2 links[kTopPer];
+#pragma unroll
+        for (int i = 0; i < kTopPer; i++) {
+            const int t = threadIdx.x + i * kRefitThreads;
+            if (t < npend) {
+                const int4 q = __ldg(&tlist[t]);
+                slist[t] = make_int2(q.x, ((q.y & 0xffff) << 16) | (q.z & 0xffff));
+            }
+            d[i] = -1;
+            links[i] = make_float2(0.f, 0.f);
+            if (t >= K) continue;
+            const int4 e = __ldg(&top[t]);
+            float4 rlo, rhi;
+            ldg8(nrec + 2 * (size_t)e.x, rlo, rhi);
+            top_init_box(e, lrec, nrec, sbox + 6 * t);
+            d[i] = e.x;
+            links[i] = make_float2(rlo.w, rhi.w);
+        }
+        __syncthreads();
+        for (int h = 0; h <= L; h++) {
+            for (int t = sofs[h] + threadIdx.x; t < sofs[h + 1]; t += blockDim.x) {
+                const int2 q = slist[t];
+                const int c1 = (q.y >> 16) & 0xffff, c2 = q.y & 0xffff;
+                float *b = sbox + 6 * q.x;
+                float4 lo, hi;
+                box_load6(b, lo, hi);
+                if (c1 != 0xffff) box_union6(sbox + 6 * c1, lo, hi);
+                if (c2 != 0xffff) box_union6(sbox + 6 * c2, lo, hi);
+                box_store6(b, lo, hi);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int i = 0; i < kTopPer; i++) {
+            if (d[i] < 0) continue;
+            float4 lo, hi;
+            box_load6(sbox + 6 * (threadIdx.x + i * kRefitThreads), lo, hi);
+            lo.w = links[i].x;
+            hi.w = links[i].y;
+            stg8(nrec + 2 * (size_t)d[i], lo, hi);
+        }
+        return;
+    }
+    // the general form: slots in global scratch, one pass per height
+    __shared__ int hlo, hhi;
+    if (threadIdx.x == 0) { hlo = INT_MAX; hhi = 0; }
+    __syncthreads();
+    int h0 = INT_MAX, h1 = 0;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const int4 e = __ldg(&top[k]);
+        top_init_box(e, lrec, nrec, gbox + 6 * (size_t)k);
+        h0 = min(h0, e.w);
+        h1 = max(h1, e.w);
+    }
+    atomicMin(&hlo, h0);
+    atomicMax(&hhi, h1);
+    __syncthreads();
+    const int H0 = hlo, H1 = hhi;
+    for (int h = H0; h <= H1; h++) {
+        for (int k = threadIdx.x; k < K; k += blockDim.x) {
+            const int4 e = __ldg(&top[k]);
+            if (e.w != h || ((e.y & 3) != 2 && (e.z & 3) != 2)) continue;
+            float *b = gbox + 6 * (size_t)k;
+            float4 lo, hi;
+            box_load6(b, lo, hi);
+            if ((e.y & 3) == 2) box_union6(gbox + 6 * (size_t)(e.y >> 2), lo, hi);
+            if ((e.z & 3) == 2) box_union6(gbox + 6 * (size_t)(e.z >> 2), lo, hi);
+            box_store6(b, lo, hi);
+        }
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        float4 lo, hi;
+        box_load6(gbox + 6 * (size_t)k, lo, hi);
+        rec_store_box(nrec + 2 * (size_t)__ldg(&top[k]).x, lo, hi);
     }
 }
 
@@ -688,7 +1083,9 @@ LBvh::~LBvh() {
                     &ulc_, &urc_, &upar_, &urx_, &ury_, &umark_, &ubox_, &uflag_, &posb_, &clen_,
                     &coff_, &dfs_, &ulpar_, &scene_, &partial_, &scratch_, &task_, &tmpface_,
                     &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &flagbuf_,
-                    &ctr_, &scene_of_, &leafscene_, &sbox_, &tiles_, &nrec16_};
+                    &ctr_, &scene_of_, &leafscene_, &sbox_, &tiles_, &nrec16_, &split_, &cross_, &topk_,
+                    &plan_, &top_, &gbox_, &height_, &llist_, &lhdr_, &tlist_,
+                    &thdr_};
     for (DBuf *b : bufs) b->release();
     if (h_ctr_) cudaFreeHost(h_ctr_);
 }
@@ -721,6 +1118,17 @@ bvhcd_status LBvh::ensure_capacity(int T, int V) {
     BV_TRY(primmap_.reserve(sizeof(int) * n));
     BV_TRY(code_.reserve(sizeof(unsigned) * n));
     BV_TRY(refit_flag_.reserve(sizeof(unsigned) * n));
+    BV_TRY(split_.reserve(sizeof(int) * n));
+    BV_TRY(cross_.reserve(sizeof(unsigned) * n));
+    BV_TRY(topk_.reserve(sizeof(unsigned) * n));
+    BV_TRY(plan_.reserve(sizeof(int4) * n));
+    BV_TRY(top_.reserve(sizeof(int4) * n));
+    BV_TRY(gbox_.reserve(sizeof(float) * 6 * n));
+    BV_TRY(height_.reserve(sizeof(int) * n));
+    BV_TRY(llist_.reserve(sizeof(int4) * (n + kRefitW)));
+    BV_TRY(lhdr_.reserve(sizeof(int) * kLevelHdr * (n / kRefitW + 2)));
+    BV_TRY(tlist_.reserve(sizeof(int4) * n));
+    BV_TRY(thdr_.reserve(sizeof(int) * kLevelHdr));
     BV_TRY(keys_.reserve(sizeof(unsigned) * n));
     BV_TRY(vals_.reserve(sizeof(int) * n));
     BV_TRY(keys2_.reserve(sizeof(unsigned) * n));
@@ -877,10 +1285,9 @@ bvhcd_status LBvh::build(cudaStream_t s) {
     k_write_nodes<<<grid_for(T - 1), kThreads, 0, s>>>(T - 1, T, c, dfs_.as<int>(), coff_.as<unsigned>(),
                                                        clen_.as<int>(), leafscene, nrec_.as<float4>(),
                                                        topo_.as<int4>(), nrange_.as<int2>()); note_launch();
-    BV_TRY(cudaMemsetAsync(refit_flag_.p, 0, sizeof(unsigned) * (size_t)T, s));
     BV_TRY(cudaGetLastError());
     built_ = true;
-    return BVHCD_OK;
+    return refit_plan(s);
 }
 
 bvhcd_status LBvh::copy_state_from(const LBvh &src, cudaStream_t s) {
@@ -890,10 +1297,13 @@ bvhcd_status LBvh::copy_state_from(const LBvh &src, cudaStream_t s) {
     const DBuf *from[] = {&src.verts_, &src.faces_, &src.nrec_, &src.lrec_, &src.topo_, &src.nrange_, &src.lca_,
                           &src.sface_, &src.primmap_, &src.code_, &src.refit_flag_, &src.intrange_, &src.rtroot_,
                           &src.intmark_, &src.extrange_, &src.extmark_, &src.leafroot_, &src.ctr_,
-                          &src.scene_of_, &src.leafscene_, &src.sbox_, &src.tiles_, &src.scene_, &src.nrec16_};
+                          &src.scene_of_, &src.leafscene_, &src.sbox_, &src.tiles_, &src.scene_, &src.nrec16_,
+                          &src.split_, &src.cross_, &src.topk_, &src.plan_, &src.top_,
+                          &src.height_, &src.llist_, &src.lhdr_, &src.tlist_, &src.thdr_};
     DBuf *to[] = {&verts_, &faces_, &nrec_, &lrec_, &topo_, &nrange_, &lca_, &sface_, &primmap_, &code_,
                   &refit_flag_, &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &ctr_,
-                  &scene_of_, &leafscene_, &sbox_, &tiles_, &scene_, &nrec16_};
+                  &scene_of_, &leafscene_, &sbox_, &tiles_, &scene_, &nrec16_, &split_, &cross_, &topk_,
+                  &plan_, &top_, &height_, &llist_, &lhdr_, &tlist_, &thdr_};
     bvhcd_status st = ensure_capacity(src.capT_, src.capV_);
     if (st != BVHCD_OK) return st;
     for (size_t k = 0; k < sizeof(to) / sizeof(to[0]); k++) BV_TRY(to[k]->copy_from(*from[k], s));
@@ -939,12 +1349,52 @@ bvhcd_status LBvh::set_scenes(int S, const int32_t *off) {
     return BVHCD_OK;
 }
 
+// The refit plan of the current topology (see k_heights / k_plan_split /
+// k_plan_write).
+bvhcd_status LBvh::refit_plan(cudaStream_t s) {
+    const int nint = T_ - S_;  // internal nodes: one tree of n - 1 per scene of n leaves
+    if (nint <= 0) return BVHCD_OK;
+    BV_TRY(cudaMemsetAsync(plan_.p, 0xFF, sizeof(int4) * (size_t)T_, s));
+    BV_TRY(cudaMemsetAsync(height_.p, 0, sizeof(int) * (size_t)nint, s));
+    BV_TRY(cudaMemsetAsync(refit_flag_.p, 0, sizeof(unsigned) * (size_t)nint, s));
+    k_heights<<<grid_for(T_), kThreads, 0, s>>>(T_, lrec_.as<float4>(), topo_.as<int4>(), refit_flag_.as<unsigned>(),
+                                                height_.as<int>()); note_launch();
+    k_plan_split<<<grid_for(nint), kThreads, 0, s>>>(nint, topo_.as<int4>(), nrange_.as<int2>(), split_.as<int>(),
+                                                     cross_.as<unsigned>()); note_launch();
+    BV_TRY(scan_u32(cross_.as<unsigned>(), topk_.as<unsigned>(), nint, false, ctr_.as<unsigned>() + C_TOPK,
+                    scratch_.p, s));
+    k_plan_write<<<grid_for(nint), kThreads, 0, s>>>(nint, topo_.as<int4>(), split_.as<int>(), cross_.as<unsigned>(),
+                                                     topk_.as<unsigned>(), height_.as<int>(), plan_.as<int4>(),
+                                                     top_.as<int4>()); note_launch();
+    const int nb = (T_ + kRefitW - 1) / kRefitW;
+    k_plan_local<<<nb, kRefitThreads, 0, s>>>(T_, plan_.as<int4>(), llist_.as<int4>(), lhdr_.as<int>()); note_launch();
+    if (nb > 1) {
+        k_plan_top<<<1, kRefitThreads, 0, s>>>(ctr_.as<unsigned>(), top_.as<int4>(), tlist_.as<int4>(),
+                                                thdr_.as<int>()); note_launch();
+    }
+    return cuda_status(cudaGetLastError());
+}
+
 bvhcd_status LBvh::refit(cudaStream_t s) {
     StageScope prof_scope(&prof_, BVHCD_STAGE_BVH_REFIT, s);
     const int T = T_;
     if (T == 0) return BVHCD_OK;
-    k_refit<<<grid_for(T), kThreads, 0, s>>>(T, sface_.as<int4>(), vptr_, lrec_.as<float4>(), nrec_.as<float4>(),
-                                             topo_.as<int4>(), refit_flag_.as<unsigned>()); note_launch();
+    static const bool attrs = [] {
+        cudaFuncSetAttribute(k_refit_local, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLocalSmem);
+        cudaFuncSetAttribute(k_refit_top, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTopSmem);
+        return true;
+    }();
+    (void)attrs;
+    const int nb = (T + kRefitW - 1) / kRefitW;
+    k_refit_local<<<nb, kRefitThreads, kLocalSmem, s>>>(T, sface_.as<int4>(), vptr_, plan_.as<int4>(),
+                                                        llist_.as<int4>(), lhdr_.as<int>(), lrec_.as<float4>(),
+                                                        nrec_.as<float4>()); note_launch();
+    if (nb > 1) {
+        // nodes cross blocks only when there are several
+        k_refit_top<<<1, kRefitThreads, kTopSmem, s>>>(ctr_.as<unsigned>(), top_.as<int4>(), tlist_.as<int4>(),
+                                                       thdr_.as<int>(), lrec_.as<float4>(), nrec_.as<float4>(),
+                                                       gbox_.as<float>(), capT_ + 2); note_launch();
+    }
     return cuda_status(cudaGetLastError());
 }
 
@@ -1022,7 +1472,7 @@ bvhcd_status LBvh::restructure(cudaStream_t s) {
                                                  nrange_.as<int2>(), lrec_.as<float4>()); note_launch();
     BV_TRY(cudaGetLastError());
     opt_tag_ = 1;
-    return BVHCD_OK;
+    return refit_plan(s);
 }
 
 bvhcd_status LBvh::node_fp16(cudaStream_t s) {

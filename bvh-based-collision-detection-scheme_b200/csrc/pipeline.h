@@ -142,6 +142,7 @@ class LBvh {
     bvhcd_status upload(const bvhcd_scene &scene, cudaStream_t s);
     bvhcd_status build(cudaStream_t s);
     bvhcd_status refit(cudaStream_t s);
+    bvhcd_status refit_plan(cudaStream_t s);
     bvhcd_status restructure(cudaStream_t s);
     bvhcd_status scene_box(cudaStream_t s);
     bvhcd_status climb_and_order(cudaStream_t s);
@@ -157,6 +158,12 @@ class LBvh {
     DBuf verts_, faces_;
     // tree
     DBuf nrec_, lrec_, topo_, nrange_, lca_, sface_, primmap_, code_, refit_flag_, nrec16_;
+    // refit plan (a function of the topology): split of each internal node,
+    // crossing flags and ranks, per-split local entries, crossing-node
+    // entries, node heights, level-sorted lists (per leaf block and for the
+    // crossing nodes) with their level offsets, and the top pass's global
+    // storage when the crossing nodes exceed its shared memory
+    DBuf split_, cross_, topk_, plan_, top_, gbox_, height_, llist_, lhdr_, tlist_, thdr_;
     // build scratch
     DBuf keys_, vals_, keys2_, vals2_, k64_, k64b_, metric_, ulc_, urc_, upar_, urx_, ury_, umark_,
         ubox_, uflag_, posb_, clen_, coff_, dfs_, ulpar_, scene_, partial_, scratch_, task_, tmpface_;
