@@ -68,6 +68,7 @@ enum CounterSlot {
     C_COMPACT = 12,           // compaction cursor of the pair export
     C_FLAGGED = 13,           // precision mode: pairs re-decided in FP64
     C_TOPK = 14,              // refit plan: nodes whose leaf range crosses a refit block
+    C_REFIT_DONE = 15,        // refit: leaf blocks finished (the last one runs the crossing nodes)
     C_NUM = 16
 };
 

@@ -403,32 +403,38 @@ __global__ void k_write_nodes(int nint, int T, Climb c, const int *__restrict__ 
 // leaf boxes from the three vertices, then every internal box as the union of
 // its children's, bottom-up.
 //
-// A climb over the whole tree with one arrival counter per node pays a fence
-// around every arrival on its longest leaf-to-root chain (about 0.7 us each
-// on B200, at any scope), and the chains set the refit's time.  This refit
-// runs level by level instead, in node height order (a parent is higher than
-// its children), with a CTA barrier between levels and no fences:
+// A climb over the whole tree with one arrival counter per node pays a
+// device-scope atomic and fence per level on its longest leaf-to-root chain,
+// and those chains set its time.  This refit runs level by level instead, in
+// node height order (a parent is higher than its children), in shared
+// memory, with CTA barriers between levels:
 //  - the leaves are cut into blocks of kRefitW; a node whose leaf range lies
 //    in one block is local to it, the others (the top of the tree and the
 //    spines above each block boundary) cross;
-//  - k_refit_local: one CTA per leaf block computes the leaf boxes, then the
-//    local node boxes level by level in shared memory;
-//  - k_refit_top: one CTA computes the crossing node boxes level by level,
-//    from the final boxes of their local children.
-// Min and max are exact, so the boxes equal those of any other bottom-up
-// order.  The plan (splits, heights, which node is where) depends on the
-// topology only; refit_plan rebuilds it after every build and restructure.
-constexpr int kRefitW = 2048;        // leaves per local block
+//  - one CTA per leaf block computes its leaf boxes, then its local nodes
+//    from a level-sorted list, and exports the boxes the crossing nodes need
+//    (those of its local subtree roots and boundary leaves) to a compact
+//    array;
+//  - the CTA that finishes last (a counter after a fence; nothing waits)
+//    computes the crossing nodes level by level from that array.
+// Every record is written whole (box and links) in one 256-bit store: the
+// links come from the plan, so no record is read.  Min and max are exact,
+// so the boxes equal those of any bottom-up order.  The plan (splits,
+// heights, lists, links, exports) depends on the topology only; refit_plan
+// rebuilds it after every build and restructure.
+constexpr int kRefitW = 4096;        // leaves per local block
 constexpr int kRefitThreads = 1024;  // threads per refit CTA
 constexpr int kRefitSlots = kRefitW / kRefitThreads;
-constexpr int kMaxLevels = 64;       // levels a level-sorted list holds (deeper: one pass per level over all)
-constexpr int kLevelHdr = kMaxLevels + 3;  // per list: level count (or -1), then level offsets
-constexpr int kTopCap = 6144;        // crossing nodes the top pass keeps in shared memory
-constexpr int kTopPer = kTopCap / kRefitThreads;
-// boxes of the block's leaves and splits, then its level-sorted work list
-constexpr size_t kLocalSmem = (size_t)2 * kRefitW * 6 * sizeof(float) + (size_t)kRefitW * sizeof(int2);
-// boxes of the crossing nodes, then their level-sorted work list
-constexpr size_t kTopSmem = (size_t)kTopCap * (6 * sizeof(float) + sizeof(int2));
+constexpr int kMaxLevels = 64;       // levels a level-sorted list holds (deeper: one pass per height)
+// per list: level count L (or -1), level offsets 0..L+1, then at fixed places
+// the node count (crossing list) or export count (block list), the list
+// length, and the first narrow level
+constexpr int kLevelHdr = kMaxLevels + 6;
+constexpr int kHdrCount = kLevelHdr - 3, kHdrLen = kLevelHdr - 2, kHdrNarrow = kLevelHdr - 1;
+constexpr int kLevelThreads = 256;  // threads that run the wide levels of a list
+// boxes of the block's leaves and nodes, then its level-sorted work list; the
+// last CTA reuses it for the crossing nodes' boxes and list
+constexpr size_t kLocalSmem = (size_t)2 * kRefitW * 6 * sizeof(float) + (size_t)kRefitW * sizeof(int);
 
 // Node heights (leaves 0, a node one above its higher child), bottom-up with
 // arrival counters: run once per topology, so its fences do not matter.
@@ -460,29 +466,10 @@ __global__ void k_plan_split(int nint, const int4 *__restrict__ topo, const int2
     }
 }
 
-// plan[split(d)] = {d, or -1 if d crosses; left ref; right ref; height},
-// refs (leaf << 1 | 1) or (split << 1).  top[k] for the k-th crossing node
-// = {d; left ref; right ref; height}, refs (leaf << 2 | 1), (local node << 2)
-// or (crossing k << 2 | 2).
-__global__ void k_plan_write(int nint, const int4 *__restrict__ topo, const int *__restrict__ split,
-                             const unsigned *__restrict__ cross, const unsigned *__restrict__ topk,
-                             const int *__restrict__ height, int4 *plan, int4 *top) {
-    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nint; d += gridDim.x * blockDim.x) {
-        const int4 t = topo[d];
-        const bool lleaf = (t.w & 1) != 0, rleaf = (t.w & 2) != 0;
-        const bool c = cross[d] != 0;
-        const int h = height[d];
-        plan[split[d]] = make_int4(c ? -1 : d, lleaf ? (t.x << 1) | 1 : split[t.x] << 1,
-                                   rleaf ? (t.y << 1) | 1 : split[t.y] << 1, h);
-        if (c) {
-            auto ref = [&](int ch, bool leaf) {
-                return leaf ? (ch << 2) | 1 : cross[ch] ? (int)(topk[ch] << 2) | 2 : ch << 2;
-            };
-            top[topk[d]] = make_int4(d, ref(t.x, lleaf), ref(t.y, rleaf), h);
-        }
-    }
+__device__ __forceinline__ void box_empty(float4 &lo, float4 &hi) {
+    lo = make_float4(3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f, 0.f);
+    hi = make_float4(-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f, 0.f);
 }
-
 // boxes as 6 floats (24 bytes, 8-byte aligned): three 64-bit accesses
 __device__ __forceinline__ void box_store6(float *b, const float4 &lo, const float4 &hi) {
     float2 *q = reinterpret_cast<float2 *>(b);
@@ -496,24 +483,68 @@ __device__ __forceinline__ void box_load6(const float *b, float4 &lo, float4 &hi
     lo = make_float4(u.x, u.y, v.x, 0.f);
     hi = make_float4(v.y, w.x, w.y, 0.f);
 }
-__device__ __forceinline__ void box_union6(const float *b, float4 &lo, float4 &hi) {
-    float4 clo, chi;
-    box_load6(b, clo, chi);
+__device__ __forceinline__ void box_union(float4 &lo, float4 &hi, const float4 &clo, const float4 &chi) {
     lo.x = fminf(lo.x, clo.x); lo.y = fminf(lo.y, clo.y); lo.z = fminf(lo.z, clo.z);
     hi.x = fmaxf(hi.x, chi.x); hi.y = fmaxf(hi.y, chi.y); hi.z = fmaxf(hi.z, chi.z);
 }
+__device__ __forceinline__ void box_union6(const float *b, float4 &lo, float4 &hi) {
+    float4 clo, chi;
+    box_load6(b, clo, chi);
+    box_union(lo, hi, clo, chi);
+}
 // the box fields of a 32-byte record ({lo.xyz, link}, {hi.xyz, link}); the
-// links stay
+// links stay (the deep-tree forms only)
 __device__ __forceinline__ void rec_store_box(float4 *rec, const float4 &lo, const float4 &hi) {
     float *w = reinterpret_cast<float *>(rec);
     w[0] = lo.x; w[1] = lo.y; w[2] = lo.z;
     w[4] = hi.x; w[5] = hi.y; w[6] = hi.z;
 }
 
+// plan[split(d)] = {d, or -1 if d crosses; left ref; right ref; height},
+// refs (leaf << 1 | 1) or (split << 1).  top[k] for the k-th crossing node
+// = {d; left ref; right ref; height}, refs (leaf << 2 | 1), (local node << 2)
+// or (crossing k << 2 | 2).  A non-crossing child of crossing node k on side
+// c is marked for export to slot 2k + c (lexp per leaf, nexp per node); a
+// crossing child's export slot holds the empty box.
+__global__ void k_plan_write(int nint, const int4 *__restrict__ topo, const int *__restrict__ split,
+                             const unsigned *__restrict__ cross, const unsigned *__restrict__ topk,
+                             const int *__restrict__ height, int4 *plan, int4 *top, int *lexp, int *nexp,
+                             float *gext) {
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nint; d += gridDim.x * blockDim.x) {
+        const int4 t = topo[d];
+        const bool lleaf = (t.w & 1) != 0, rleaf = (t.w & 2) != 0;
+        const bool c = cross[d] != 0;
+        const int h = height[d];
+        plan[split[d]] = make_int4(c ? -1 : d, lleaf ? (t.x << 1) | 1 : split[t.x] << 1,
+                                   rleaf ? (t.y << 1) | 1 : split[t.y] << 1, h);
+        if (!c) continue;
+        const int k = (int)topk[d];
+        auto ref = [&](int ch, bool leaf) {
+            return leaf ? (ch << 2) | 1 : cross[ch] ? (int)(topk[ch] << 2) | 2 : ch << 2;
+        };
+        top[k] = make_int4(d, ref(t.x, lleaf), ref(t.y, rleaf), h);
+        const int ch[2] = {t.x, t.y};
+        const bool leaf[2] = {lleaf, rleaf};
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            const int slot = 2 * k + side;
+            if (leaf[side]) lexp[ch[side]] = slot;
+            else if (!cross[ch[side]]) nexp[ch[side]] = slot;
+            else {
+                float4 lo, hi;
+                box_empty(lo, hi);
+                box_store6(gext + 6 * (size_t)slot, lo, hi);
+            }
+        }
+    }
+}
+
 // Level-sorted work lists, built once per topology by one CTA per list:
 // count per level, offsets, scatter.  hdr[0] = number of levels L (or -1
 // when the heights span more than kMaxLevels), hdr[1 + h] = offset of level
-// h, h = 0..L.
+// h, h = 0..L + 1, hdr[kHdrLen] = the list length, hdr[kHdrNarrow] = the
+// first level from which every level has at most 32 nodes (one warp runs
+// those, with warp barriers).
 __device__ void level_sort_begin(int *cnt) {
     if (threadIdx.x <= kMaxLevels) cnt[threadIdx.x] = 0;
 }
@@ -527,18 +558,30 @@ __device__ void level_sort_offsets(const int *cnt, int *cur, int L, int *hdr) {
         acc += cnt[h];
     }
     hdr[2 + L] = acc;
+    hdr[kHdrLen] = acc;
+    int lw = L + 1;
+    while (lw > 0 && cnt[lw - 1] <= 32) lw--;
+    hdr[kHdrNarrow] = lw;
 }
 
 // Local lists: for leaf block b, its local nodes by height (level h - 1 holds
-// height h) as {node, split slot, left child slot, right child slot}; slots
-// index the block's boxes (leaves 0..kRefitW-1, splits kRefitW + split - L0).
-__global__ void __launch_bounds__(kRefitThreads) k_plan_local(int T, const int4 *__restrict__ plan, int4 *llist,
-                                                              int *lhdr) {
-    __shared__ int cnt[kMaxLevels + 1], cur[kMaxLevels + 1], hmax;
+// height h).  A node's box slot is kRefitW + its list position; the entry is
+// {node, left child slot << 16 | right child slot, node links (rangex,
+// escape)}; a leaf's slot is its index in the block.  llink holds every
+// leaf's links (parent, escape).  lexport[b * kRefitW + x] = {export slot,
+// box slot with the list, box slot without it (kRefitW + split - L0)},
+// hdr[kHdrCount] their count.
+__global__ void __launch_bounds__(kRefitThreads) k_plan_local(int T, const int4 *__restrict__ plan,
+                                                              const float4 *__restrict__ lrec,
+                                                              const float4 *__restrict__ nrec,
+                                                              const int *__restrict__ lexp,
+                                                              const int *__restrict__ nexp, int4 *llist,
+                                                              int2 *llink, int4 *lexport, int *lhdr) {
+    __shared__ int cnt[kMaxLevels + 1], cur[kMaxLevels + 1], hmax, nex, pos_of[kRefitW];
     const int L0 = blockIdx.x * kRefitW, nl = min(kRefitW, T - L0);
     int *hdr = lhdr + (size_t)blockIdx.x * kLevelHdr;
     level_sort_begin(cnt);
-    if (threadIdx.x == 0) hmax = 0;
+    if (threadIdx.x == 0) { hmax = 0; nex = 0; }
     __syncthreads();
     int4 e[kRefitSlots];
     int hm = 0;
@@ -547,34 +590,62 @@ __global__ void __launch_bounds__(kRefitThreads) k_plan_local(int T, const int4 
         const int j = threadIdx.x + i * kRefitThreads;
         e[i] = (j < nl && L0 + j < T - 1) ? __ldg(&plan[L0 + j]) : make_int4(-1, -1, -1, 0);
         if (e[i].x >= 0) hm = max(hm, e[i].w);
+        if (j < nl) {
+            float4 lo, hi;
+            ldg8(lrec + 2 * (size_t)(L0 + j), lo, hi);
+            llink[L0 + j] = make_int2(__float_as_int(lo.w), __float_as_int(hi.w));
+        }
     }
     atomicMax(&hmax, hm);
     __syncthreads();
     const int H = hmax;
-    if (H > kMaxLevels) {
-        if (threadIdx.x == 0) hdr[0] = -1;
-        return;
-    }
+    const bool listed = H <= kMaxLevels;
+    if (listed) {
 #pragma unroll
-    for (int i = 0; i < kRefitSlots; i++)
-        if (e[i].x >= 0) atomicAdd(&cnt[e[i].w - 1], 1);
-    __syncthreads();
-    level_sort_offsets(cnt, cur, max(H - 1, 0), hdr);
-    __syncthreads();
-    auto slot = [&](int ref) { return (ref & 1) ? (ref >> 1) - L0 : kRefitW + (ref >> 1) - L0; };
+        for (int i = 0; i < kRefitSlots; i++)
+            if (e[i].x >= 0) atomicAdd(&cnt[e[i].w - 1], 1);
+        __syncthreads();
+        level_sort_offsets(cnt, cur, max(H - 1, 0), hdr);
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kRefitSlots; i++)
+            if (e[i].x >= 0) pos_of[threadIdx.x + i * kRefitThreads] = atomicAdd(&cur[e[i].w - 1], 1);
+        __syncthreads();
+        auto slot = [&](int ref) { return (ref & 1) ? (ref >> 1) - L0 : kRefitW + pos_of[(ref >> 1) - L0]; };
+#pragma unroll
+        for (int i = 0; i < kRefitSlots; i++) {
+            if (e[i].x < 0) continue;
+            float4 lo, hi;
+            ldg8(nrec + 2 * (size_t)e[i].x, lo, hi);
+            llist[L0 + pos_of[threadIdx.x + i * kRefitThreads]] = make_int4(
+                e[i].x, (slot(e[i].y) << 16) | slot(e[i].z), __float_as_int(lo.w), __float_as_int(hi.w));
+        }
+    } else if (threadIdx.x == 0) {
+        hdr[0] = -1;
+    }
 #pragma unroll
     for (int i = 0; i < kRefitSlots; i++) {
+        const int j = threadIdx.x + i * kRefitThreads;
+        if (j >= nl) continue;
+        const int le = __ldg(&lexp[L0 + j]);
+        if (le >= 0) lexport[(size_t)L0 + atomicAdd(&nex, 1)] = make_int4(le, j, j, 0);
         if (e[i].x < 0) continue;
-        const int pos = atomicAdd(&cur[e[i].w - 1], 1);
-        llist[L0 + pos] = make_int4(e[i].x, threadIdx.x + i * kRefitThreads, slot(e[i].y), slot(e[i].z));
+        const int ne = __ldg(&nexp[e[i].x]);
+        if (ne >= 0)
+            lexport[(size_t)L0 + atomicAdd(&nex, 1)] = make_int4(ne, listed ? kRefitW + pos_of[j] : -1, kRefitW + j, 0);
     }
+    __syncthreads();
+    if (threadIdx.x == 0) hdr[kHdrCount] = nex;
 }
 
 // Top list: the crossing nodes that have a crossing child, by height (level
 // h - H0, H0 the lowest crossing height), as {k, crossing child k or -1, the
-// other or -1, 0}.
+// other or -1, 0}; tlink[k] = node k's links (rangex, escape); thdr[kHdrCount]
+// = the number of crossing nodes.
 __global__ void __launch_bounds__(kRefitThreads) k_plan_top(const unsigned *__restrict__ ctr,
-                                                            const int4 *__restrict__ top, int4 *tlist, int *thdr) {
+                                                            const int4 *__restrict__ top,
+                                                            const float4 *__restrict__ nrec, int4 *tlist,
+                                                            int2 *tlink, int *thdr) {
     __shared__ int cnt[kMaxLevels + 1], cur[kMaxLevels + 1], hlo, hhi;
     const int K = (int)ctr[C_TOPK];
     level_sort_begin(cnt);
@@ -582,15 +653,19 @@ __global__ void __launch_bounds__(kRefitThreads) k_plan_top(const unsigned *__re
     __syncthreads();
     int h0 = INT_MAX, h1 = 0;
     for (int k = threadIdx.x; k < K; k += blockDim.x) {
-        const int w = __ldg(&top[k]).w;
-        h0 = min(h0, w);
-        h1 = max(h1, w);
+        const int4 e = __ldg(&top[k]);
+        h0 = min(h0, e.w);
+        h1 = max(h1, e.w);
+        float4 lo, hi;
+        ldg8(nrec + 2 * (size_t)e.x, lo, hi);
+        tlink[k] = make_int2(__float_as_int(lo.w), __float_as_int(hi.w));
     }
     atomicMin(&hlo, h0);
     atomicMax(&hhi, h1);
+    if (threadIdx.x == 0) { thdr[kHdrCount] = K; thdr[kHdrLen] = 0; }
     __syncthreads();
     const int H0 = hlo, H1 = hhi;
-    if (K > kTopCap || H1 - H0 > kMaxLevels) {
+    if (H1 - H0 > kMaxLevels) {
         if (threadIdx.x == 0) thdr[0] = -1;
         return;
     }
@@ -610,17 +685,136 @@ __global__ void __launch_bounds__(kRefitThreads) k_plan_top(const unsigned *__re
     }
 }
 
+// Levels 0..L of a level-sorted list: the wide ones by the first kN threads
+// with a named barrier among them (kN = the CTA: the CTA barrier), from level
+// lw on (each at most 32 nodes) by warp 0 with warp barriers.  work(t)
+// handles list position t.  Every thread of the CTA calls it.
+template <int kN, typename F>
+__device__ __forceinline__ void run_levels(const int *ofs, int L, int lw, F work) {
+    if (threadIdx.x < kN) {
+        for (int h = 0; h < lw && h <= L; h++) {
+            for (int t = ofs[h] + threadIdx.x; t < ofs[h + 1]; t += kN) work(t);
+            if (kN == kRefitThreads) __syncthreads();
+            else asm volatile("bar.sync 1, %0;" ::"n"(kN) : "memory");
+        }
+    }
+    if (threadIdx.x < 32) {
+        for (int h = lw; h <= L; h++) {
+            const int t = ofs[h] + threadIdx.x;
+            if (t < ofs[h + 1]) work(t);
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void top_level_work(const int4 &q, float *box) {
+    float *b = box + 6 * (size_t)q.x;
+    float4 lo, hi;
+    box_load6(b, lo, hi);
+    if (q.y >= 0) box_union6(box + 6 * (size_t)q.y, lo, hi);
+    if (q.z >= 0) box_union6(box + 6 * (size_t)q.z, lo, hi);
+    box_store6(b, lo, hi);
+}
+
+struct RefitTop {
+    const int4 *top, *tlist;
+    const int2 *tlink;
+    const int *thdr;
+    const float *gext;  // 2 export slots per crossing node
+    float *gbox;        // crossing-node slots when shared memory is too small
+    unsigned *done;     // leaf blocks finished
+};
+
+// The crossing nodes, run by the CTA that finished last: a node's slot
+// starts as the union of its two export slots (the final boxes of its
+// non-crossing children; empty for a crossing child), then the nodes with
+// crossing children take those in level by level.  Slots and list in
+// shared memory when they fit, else in global scratch (the CTA barrier
+// orders both); without a list (heights spanning more than kMaxLevels) one
+// pass per height.
+__device__ void refit_top(const RefitTop &g, float4 *nrec, float *smem, int *sofs) {
+    // the header at fixed places: one round trip
+    const int L = __ldg(&g.thdr[0]);
+    const int K = __ldg(&g.thdr[kHdrCount]);
+    const int npend = __ldg(&g.thdr[kHdrLen]);
+    const int lw = __ldg(&g.thdr[kHdrNarrow]);
+    const int ofs_t = threadIdx.x <= kMaxLevels + 1 ? __ldg(&g.thdr[1 + threadIdx.x]) : 0;
+    if (K <= 0) return;
+    const size_t box_floats = ((size_t)6 * K + 3) & ~(size_t)3;
+    const bool in_smem = box_floats * sizeof(float) + (size_t)npend * sizeof(int4) <= kLocalSmem;
+    float *box = in_smem ? smem : g.gbox;
+    int4 *slist = reinterpret_cast<int4 *>(smem + box_floats);
+    if (L >= 0 && threadIdx.x <= L + 1) sofs[threadIdx.x] = ofs_t;
+    for (int k0 = 0; k0 < K; k0 += 2 * kRefitThreads) {
+        // this round's loads first: two nodes' export slots and list entries
+        float2 x[2][6];
+        int4 q[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int k = k0 + u * kRefitThreads + threadIdx.x;
+            const float2 *src = reinterpret_cast<const float2 *>(g.gext + 12 * (size_t)min(k, K - 1));
+#pragma unroll
+            for (int c = 0; c < 6; c++) x[u][c] = __ldcg(src + c);
+            q[u] = (in_smem && k < npend) ? __ldg(&g.tlist[k]) : make_int4(0, 0, 0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int k = k0 + u * kRefitThreads + threadIdx.x;
+            if (k >= K) continue;
+            float4 lo = make_float4(fminf(x[u][0].x, x[u][3].x), fminf(x[u][0].y, x[u][3].y),
+                                    fminf(x[u][1].x, x[u][4].x), 0.f);
+            float4 hi = make_float4(fmaxf(x[u][1].y, x[u][4].y), fmaxf(x[u][2].x, x[u][5].x),
+                                    fmaxf(x[u][2].y, x[u][5].y), 0.f);
+            box_store6(box + 6 * (size_t)k, lo, hi);
+            if (in_smem && k < npend) slist[k] = q[u];
+        }
+    }
+    __syncthreads();
+    if (L >= 0) {
+        if (in_smem) run_levels<kLevelThreads>(sofs, L, lw, [&](int t) { top_level_work(slist[t], box); });
+        else run_levels<kLevelThreads>(sofs, L, lw, [&](int t) { top_level_work(__ldg(&g.tlist[t]), box); });
+    } else {
+        int hmin = INT_MAX, hmax = 0;
+        for (int k = 0; k < K; k++) {
+            const int h = __ldg(&g.top[k]).w;
+            hmin = min(hmin, h);
+            hmax = max(hmax, h);
+        }
+        for (int h = hmin; h <= hmax; h++) {
+            for (int k = threadIdx.x; k < K; k += blockDim.x) {
+                const int4 e = __ldg(&g.top[k]);
+                if (e.w != h || ((e.y & 3) != 2 && (e.z & 3) != 2)) continue;
+                top_level_work(make_int4(k, (e.y & 3) == 2 ? e.y >> 2 : -1, (e.z & 3) == 2 ? e.z >> 2 : -1, 0), box);
+            }
+            __syncthreads();
+        }
+    }
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const int d = __ldg(&g.top[k]).x;
+        const int2 lk = __ldg(&g.tlink[k]);
+        float4 lo, hi;
+        box_load6(box + 6 * (size_t)k, lo, hi);
+        lo.w = __int_as_float(lk.x);
+        hi.w = __int_as_float(lk.y);
+        stg8(nrec + 2 * (size_t)d, lo, hi);
+    }
+}
+
 // One CTA per block of kRefitW leaves: leaf boxes, then the block's local
-// nodes level by level from its level-sorted list, all in shared memory.
-__global__ void __launch_bounds__(kRefitThreads, 2) k_refit_local(int T, const int4 *__restrict__ sface,
-                                                                  const float *__restrict__ verts,
-                                                                  const int4 *__restrict__ plan,
-                                                                  const int4 *__restrict__ llist,
-                                                                  const int *__restrict__ lhdr, float4 *lrec,
-                                                                  float4 *nrec) {
-    extern __shared__ __align__(16) float sb[];  // boxes: the block's leaves, then its splits
-    int2 *slist = reinterpret_cast<int2 *>(sb + 12 * kRefitW);
-    __shared__ int sofs[kLevelHdr], hmax;
+// nodes level by level from its level-sorted list, all in shared memory,
+// then its exports; the last CTA to finish runs the crossing nodes.
+__global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *__restrict__ sface,
+                                                            const float *__restrict__ verts,
+                                                            const int4 *__restrict__ plan,
+                                                            const int4 *__restrict__ llist,
+                                                            const int2 *__restrict__ llink,
+                                                            const int4 *__restrict__ lexport,
+                                                            const int *__restrict__ lhdr, float4 *lrec,
+                                                            float4 *nrec, float *gext, RefitTop g) {
+    extern __shared__ __align__(16) float sb[];  // boxes: the block's leaves, then its nodes
+    int *slist = reinterpret_cast<int *>(sb + 12 * kRefitW);
+    __shared__ int sofs[kLevelHdr], hmax, last;
     const int L0 = blockIdx.x * kRefitW;
     const int nl = min(kRefitW, T - L0);
     const int *hdr = lhdr + (size_t)blockIdx.x * kLevelHdr;
@@ -629,65 +823,42 @@ __global__ void __launch_bounds__(kRefitThreads, 2) k_refit_local(int T, const i
     const int nloc = L >= 0 ? __ldg(&hdr[2 + L]) : 0;
     if (L >= 0 && threadIdx.x <= L + 1) sofs[threadIdx.x] = __ldg(&hdr[1 + threadIdx.x]);
     int4 w[kRefitSlots];
-    int3 f[kRefitSlots];
-    float2 leaf_links[kRefitSlots];
 #pragma unroll
     for (int i = 0; i < kRefitSlots; i++) {
         const int t = threadIdx.x + i * kRefitThreads;
         w[i] = t < nloc ? __ldg(&llist[L0 + t]) : make_int4(-1, 0, 0, 0);
-        int4 fc = make_int4(0, 0, 0, 0);
-        float4 rlo = make_float4(0.f, 0.f, 0.f, 0.f), rhi = rlo;
-        if (t < nl) {
-            fc = __ldg(&sface[L0 + t]);
-            ldg8(lrec + 2 * (size_t)(L0 + t), rlo, rhi);  // its links
-        }
-        f[i] = make_int3(fc.x, fc.y, fc.z);
-        leaf_links[i] = make_float2(rlo.w, rhi.w);
-    }
-#pragma unroll
-    for (int i = 0; i < kRefitSlots; i++) {
-        const int t = threadIdx.x + i * kRefitThreads;
-        if (w[i].x >= 0) slist[t] = make_int2(w[i].y, (w[i].z << 16) | w[i].w);
+        if (t < nloc) slist[t] = w[i].y;
         if (t >= nl) continue;
+        const int4 f = __ldg(&sface[L0 + t]);
+        const int2 lk = __ldg(&llink[L0 + t]);
         float4 lo, hi;
-        tri_box(load_vert(verts, f[i].x), load_vert(verts, f[i].y), load_vert(verts, f[i].z), lo, hi);
+        tri_box(load_vert(verts, f.x), load_vert(verts, f.y), load_vert(verts, f.z), lo, hi);
         box_store6(sb + 6 * t, lo, hi);
-        lo.w = leaf_links[i].x;
-        hi.w = leaf_links[i].y;
+        lo.w = __int_as_float(lk.x);
+        hi.w = __int_as_float(lk.y);
         stg8(lrec + 2 * (size_t)(L0 + t), lo, hi);
-    }
-    // the links of this thread's list nodes, for their whole-record stores
-    float2 node_links[kRefitSlots];
-#pragma unroll
-    for (int i = 0; i < kRefitSlots; i++) {
-        float4 rlo = make_float4(0.f, 0.f, 0.f, 0.f), rhi = rlo;
-        if (w[i].x >= 0) ldg8(nrec + 2 * (size_t)w[i].x, rlo, rhi);
-        node_links[i] = make_float2(rlo.w, rhi.w);
     }
     __syncthreads();
     if (L >= 0) {
-        for (int h = 0; h <= L; h++) {
-            for (int t = sofs[h] + threadIdx.x; t < sofs[h + 1]; t += blockDim.x) {
-                const int2 q = slist[t];
-                float4 lo, hi;
-                box_load6(sb + 6 * (q.y >> 16), lo, hi);
-                box_union6(sb + 6 * (q.y & 0xffff), lo, hi);
-                box_store6(sb + 6 * (kRefitW + q.x), lo, hi);
-            }
-            __syncthreads();
-        }
+        run_levels<kRefitThreads>(sofs, L, __ldg(&hdr[kHdrNarrow]), [&](int t) {
+            const int q = slist[t];
+            float4 lo, hi;
+            box_load6(sb + 6 * (q >> 16), lo, hi);
+            box_union6(sb + 6 * (q & 0xffff), lo, hi);
+            box_store6(sb + 6 * (kRefitW + t), lo, hi);
+        });
 #pragma unroll
         for (int i = 0; i < kRefitSlots; i++) {
             if (w[i].x < 0) continue;
             float4 lo, hi;
-            box_load6(sb + 6 * (kRefitW + w[i].y), lo, hi);
-            lo.w = node_links[i].x;
-            hi.w = node_links[i].y;
+            box_load6(sb + 6 * (kRefitW + threadIdx.x + i * kRefitThreads), lo, hi);
+            lo.w = __int_as_float(w[i].z);
+            hi.w = __int_as_float(w[i].w);
             stg8(nrec + 2 * (size_t)w[i].x, lo, hi);
         }
     } else {
         // a block with a chain of more than kMaxLevels local nodes: one pass
-        // per height over the block's splits
+        // per height over the block's splits (slot kRefitW + split - L0)
         int4 e[kRefitSlots];
         int hm = 0;
 #pragma unroll
@@ -719,122 +890,28 @@ __global__ void __launch_bounds__(kRefitThreads, 2) k_refit_local(int T, const i
             rec_store_box(nrec + 2 * (size_t)e[i].x, lo, hi);
         }
     }
-}
-
-// The crossing nodes in one CTA: a node's slot starts as the union of its
-// non-crossing children's (final) boxes, then the nodes with crossing
-// children take those in level by level from the top list.  With more than
-// kTopCap crossing nodes (or too many levels), the slots are global scratch
-// and every level passes over all nodes (the CTA barrier orders both).
-__device__ __forceinline__ void top_init_box(const int4 &e, const float4 *__restrict__ lrec,
-                                             const float4 *__restrict__ nrec, float *b) {
-    float4 lo = make_float4(3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f, 0.f);
-    float4 hi = make_float4(-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f, 0.f);
-    const int r[2] = {e.y, e.z};
-#pragma unroll
-    for (int c = 0; c < 2; c++) {
-        if ((r[c] & 3) == 2) continue;
-        float4 clo, chi;
-        ldg8(((r[c] & 3) == 1 ? lrec : nrec) + 2 * (size_t)(r[c] >> 2), clo, chi);
-        lo.x = fminf(lo.x, clo.x); lo.y = fminf(lo.y, clo.y); lo.z = fminf(lo.z, clo.z);
-        hi.x = fmaxf(hi.x, chi.x); hi.y = fmaxf(hi.y, chi.y); hi.z = fmaxf(hi.z, chi.z);
-    }
-    box_store6(b, lo, hi);
-}
-
-__global__ void __launch_bounds__(kRefitThreads) k_refit_top(const unsigned *__restrict__ ctr,
-                                                             const int4 *__restrict__ top,
-                                                             const int4 *__restrict__ tlist,
-                                                             const int *__restrict__ thdr,
-                                                             const float4 *__restrict__ lrec, float4 *nrec,
-                                                             float *gbox, int cap) {
-    extern __shared__ __align__(16) float sbox[];
-    __shared__ int sofs[kLevelHdr];
-    const int K = min((int)ctr[C_TOPK], cap);
-    const int L = __ldg(&thdr[0]);
-    if (L >= 0 && K <= kTopCap) {
-        int2 *slist = reinterpret_cast<int2 *>(sbox + 6 * kTopCap);
-        const int npend = __ldg(&thdr[2 + L]);
-        if (threadIdx.x <= L + 1) sofs[threadIdx.x] = __ldg(&thdr[1 + threadIdx.x]);
-        // this thread's crossing nodes k = threadIdx.x + i * kRefitThreads:
-        // their ids and links (for the whole-record stores), and their slots
-        int d[kTopPer];
-        float2 links[kTopPer];
-#pragma unroll
-        for (int i = 0; i < kTopPer; i++) {
-            const int t = threadIdx.x + i * kRefitThreads;
-            if (t < npend) {
-                const int4 q = __ldg(&tlist[t]);
-                slist[t] = make_int2(q.x, ((q.y & 0xffff) << 16) | (q.z & 0xffff));
-            }
-            d[i] = -1;
-            links[i] = make_float2(0.f, 0.f);
-            if (t >= K) continue;
-            const int4 e = __ldg(&top[t]);
-            float4 rlo, rhi;
-            ldg8(nrec + 2 * (size_t)e.x, rlo, rhi);
-            top_init_box(e, lrec, nrec, sbox + 6 * t);
-            d[i] = e.x;
-            links[i] = make_float2(rlo.w, rhi.w);
-        }
-        __syncthreads();
-        for (int h = 0; h <= L; h++) {
-            for (int t = sofs[h] + threadIdx.x; t < sofs[h + 1]; t += blockDim.x) {
-                const int2 q = slist[t];
-                const int c1 = (q.y >> 16) & 0xffff, c2 = q.y & 0xffff;
-                float *b = sbox + 6 * q.x;
-                float4 lo, hi;
-                box_load6(b, lo, hi);
-                if (c1 != 0xffff) box_union6(sbox + 6 * c1, lo, hi);
-                if (c2 != 0xffff) box_union6(sbox + 6 * c2, lo, hi);
-                box_store6(b, lo, hi);
-            }
-            __syncthreads();
-        }
-#pragma unroll
-        for (int i = 0; i < kTopPer; i++) {
-            if (d[i] < 0) continue;
-            float4 lo, hi;
-            box_load6(sbox + 6 * (threadIdx.x + i * kRefitThreads), lo, hi);
-            lo.w = links[i].x;
-            hi.w = links[i].y;
-            stg8(nrec + 2 * (size_t)d[i], lo, hi);
-        }
-        return;
-    }
-    // the general form: slots in global scratch, one pass per height
-    __shared__ int hlo, hhi;
-    if (threadIdx.x == 0) { hlo = INT_MAX; hhi = 0; }
-    __syncthreads();
-    int h0 = INT_MAX, h1 = 0;
-    for (int k = threadIdx.x; k < K; k += blockDim.x) {
-        const int4 e = __ldg(&top[k]);
-        top_init_box(e, lrec, nrec, gbox + 6 * (size_t)k);
-        h0 = min(h0, e.w);
-        h1 = max(h1, e.w);
-    }
-    atomicMin(&hlo, h0);
-    atomicMax(&hhi, h1);
-    __syncthreads();
-    const int H0 = hlo, H1 = hhi;
-    for (int h = H0; h <= H1; h++) {
-        for (int k = threadIdx.x; k < K; k += blockDim.x) {
-            const int4 e = __ldg(&top[k]);
-            if (e.w != h || ((e.y & 3) != 2 && (e.z & 3) != 2)) continue;
-            float *b = gbox + 6 * (size_t)k;
-            float4 lo, hi;
-            box_load6(b, lo, hi);
-            if ((e.y & 3) == 2) box_union6(gbox + 6 * (size_t)(e.y >> 2), lo, hi);
-            if ((e.z & 3) == 2) box_union6(gbox + 6 * (size_t)(e.z >> 2), lo, hi);
-            box_store6(b, lo, hi);
-        }
-        __syncthreads();
-    }
-    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    if (gridDim.x == 1) return;  // one block: no node crosses
+    const int nex = __ldg(&hdr[kHdrCount]);
+    for (int x = threadIdx.x; x < nex; x += blockDim.x) {
+        const int4 ex = __ldg(&lexport[(size_t)L0 + x]);
         float4 lo, hi;
-        box_load6(gbox + 6 * (size_t)k, lo, hi);
-        rec_store_box(nrec + 2 * (size_t)__ldg(&top[k]).x, lo, hi);
+        box_load6(sb + 6 * (L >= 0 ? ex.y : ex.z), lo, hi);
+        float2 *q = reinterpret_cast<float2 *>(gext + 6 * (size_t)ex.x);
+        __stcg(q, make_float2(lo.x, lo.y));
+        __stcg(q + 1, make_float2(lo.z, hi.x));
+        __stcg(q + 2, make_float2(hi.y, hi.z));
     }
+    // the last CTA to finish runs the crossing nodes
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(g.done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    refit_top(g, nrec, sb, sofs);
+    if (threadIdx.x == 0) *g.done = 0u;
 }
 
 // ---------------------------------------------------------------- FP16 node records
@@ -1085,7 +1162,7 @@ LBvh::~LBvh() {
                     &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &flagbuf_,
                     &ctr_, &scene_of_, &leafscene_, &sbox_, &tiles_, &nrec16_, &split_, &cross_, &topk_,
                     &plan_, &top_, &gbox_, &height_, &llist_, &lhdr_, &tlist_,
-                    &thdr_};
+                    &thdr_, &llink_, &tlink_, &lexp_, &nexp_, &lexport_, &gext_};
     for (DBuf *b : bufs) b->release();
     if (h_ctr_) cudaFreeHost(h_ctr_);
 }
@@ -1129,6 +1206,12 @@ bvhcd_status LBvh::ensure_capacity(int T, int V) {
     BV_TRY(lhdr_.reserve(sizeof(int) * kLevelHdr * (n / kRefitW + 2)));
     BV_TRY(tlist_.reserve(sizeof(int4) * n));
     BV_TRY(thdr_.reserve(sizeof(int) * kLevelHdr));
+    BV_TRY(llink_.reserve(sizeof(int2) * n));
+    BV_TRY(lexp_.reserve(sizeof(int) * n));
+    BV_TRY(nexp_.reserve(sizeof(int) * n));
+    BV_TRY(lexport_.reserve(sizeof(int4) * (n + kRefitW)));
+    BV_TRY(gext_.reserve(sizeof(float) * 12 * n));
+    BV_TRY(tlink_.reserve(sizeof(int2) * n));
     BV_TRY(keys_.reserve(sizeof(unsigned) * n));
     BV_TRY(vals_.reserve(sizeof(int) * n));
     BV_TRY(keys2_.reserve(sizeof(unsigned) * n));
@@ -1262,7 +1345,7 @@ bvhcd_status LBvh::build(cudaStream_t s) {
             k_single_leaf<<<1, 32, 0, s>>>(lca_.as<int>(), lrec_.as<float4>()); note_launch();
             BV_TRY(cudaGetLastError());
             built_ = true;
-            return BVHCD_OK;
+            return refit_plan(s);
         }
     }
     Climb c = make_climb(ulc_, urc_, upar_, urx_, ury_, umark_, ubox_, uflag_, posb_, clen_, ulpar_);
@@ -1299,11 +1382,13 @@ bvhcd_status LBvh::copy_state_from(const LBvh &src, cudaStream_t s) {
                           &src.intmark_, &src.extrange_, &src.extmark_, &src.leafroot_, &src.ctr_,
                           &src.scene_of_, &src.leafscene_, &src.sbox_, &src.tiles_, &src.scene_, &src.nrec16_,
                           &src.split_, &src.cross_, &src.topk_, &src.plan_, &src.top_,
-                          &src.height_, &src.llist_, &src.lhdr_, &src.tlist_, &src.thdr_};
+                          &src.height_, &src.llist_, &src.lhdr_, &src.tlist_, &src.thdr_,
+                          &src.llink_, &src.tlink_, &src.lexport_, &src.gext_};
     DBuf *to[] = {&verts_, &faces_, &nrec_, &lrec_, &topo_, &nrange_, &lca_, &sface_, &primmap_, &code_,
                   &refit_flag_, &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &ctr_,
                   &scene_of_, &leafscene_, &sbox_, &tiles_, &scene_, &nrec16_, &split_, &cross_, &topk_,
-                  &plan_, &top_, &height_, &llist_, &lhdr_, &tlist_, &thdr_};
+                  &plan_, &top_, &height_, &llist_, &lhdr_, &tlist_, &thdr_, &llink_, &tlink_,
+                  &lexport_, &gext_};
     bvhcd_status st = ensure_capacity(src.capT_, src.capV_);
     if (st != BVHCD_OK) return st;
     for (size_t k = 0; k < sizeof(to) / sizeof(to[0]); k++) BV_TRY(to[k]->copy_from(*from[k], s));
@@ -1349,28 +1434,36 @@ bvhcd_status LBvh::set_scenes(int S, const int32_t *off) {
     return BVHCD_OK;
 }
 
-// The refit plan of the current topology (see k_heights / k_plan_split /
-// k_plan_write).
+// The refit plan of the current topology (see k_heights, k_plan_split,
+// k_plan_write, k_plan_local, k_plan_top).
 bvhcd_status LBvh::refit_plan(cudaStream_t s) {
     const int nint = T_ - S_;  // internal nodes: one tree of n - 1 per scene of n leaves
-    if (nint <= 0) return BVHCD_OK;
-    BV_TRY(cudaMemsetAsync(plan_.p, 0xFF, sizeof(int4) * (size_t)T_, s));
-    BV_TRY(cudaMemsetAsync(height_.p, 0, sizeof(int) * (size_t)nint, s));
-    BV_TRY(cudaMemsetAsync(refit_flag_.p, 0, sizeof(unsigned) * (size_t)nint, s));
-    k_heights<<<grid_for(T_), kThreads, 0, s>>>(T_, lrec_.as<float4>(), topo_.as<int4>(), refit_flag_.as<unsigned>(),
-                                                height_.as<int>()); note_launch();
-    k_plan_split<<<grid_for(nint), kThreads, 0, s>>>(nint, topo_.as<int4>(), nrange_.as<int2>(), split_.as<int>(),
-                                                     cross_.as<unsigned>()); note_launch();
-    BV_TRY(scan_u32(cross_.as<unsigned>(), topk_.as<unsigned>(), nint, false, ctr_.as<unsigned>() + C_TOPK,
-                    scratch_.p, s));
-    k_plan_write<<<grid_for(nint), kThreads, 0, s>>>(nint, topo_.as<int4>(), split_.as<int>(), cross_.as<unsigned>(),
-                                                     topk_.as<unsigned>(), height_.as<int>(), plan_.as<int4>(),
-                                                     top_.as<int4>()); note_launch();
     const int nb = (T_ + kRefitW - 1) / kRefitW;
-    k_plan_local<<<nb, kRefitThreads, 0, s>>>(T_, plan_.as<int4>(), llist_.as<int4>(), lhdr_.as<int>()); note_launch();
+    if (T_ <= 0) return BVHCD_OK;
+    BV_TRY(cudaMemsetAsync(lexp_.p, 0xFF, sizeof(int) * (size_t)T_, s));
+    BV_TRY(cudaMemsetAsync(ctr_.as<unsigned>() + C_REFIT_DONE, 0, sizeof(unsigned), s));
+    if (nint > 0) {
+        BV_TRY(cudaMemsetAsync(nexp_.p, 0xFF, sizeof(int) * (size_t)nint, s));
+        BV_TRY(cudaMemsetAsync(plan_.p, 0xFF, sizeof(int4) * (size_t)T_, s));
+        BV_TRY(cudaMemsetAsync(height_.p, 0, sizeof(int) * (size_t)nint, s));
+        BV_TRY(cudaMemsetAsync(refit_flag_.p, 0, sizeof(unsigned) * (size_t)nint, s));
+        k_heights<<<grid_for(T_), kThreads, 0, s>>>(T_, lrec_.as<float4>(), topo_.as<int4>(),
+                                                    refit_flag_.as<unsigned>(), height_.as<int>()); note_launch();
+        k_plan_split<<<grid_for(nint), kThreads, 0, s>>>(nint, topo_.as<int4>(), nrange_.as<int2>(),
+                                                         split_.as<int>(), cross_.as<unsigned>()); note_launch();
+        BV_TRY(scan_u32(cross_.as<unsigned>(), topk_.as<unsigned>(), nint, false, ctr_.as<unsigned>() + C_TOPK,
+                        scratch_.p, s));
+        k_plan_write<<<grid_for(nint), kThreads, 0, s>>>(nint, topo_.as<int4>(), split_.as<int>(),
+                                                         cross_.as<unsigned>(), topk_.as<unsigned>(),
+                                                         height_.as<int>(), plan_.as<int4>(), top_.as<int4>(),
+                                                         lexp_.as<int>(), nexp_.as<int>(), gext_.as<float>()); note_launch();
+    }
+    k_plan_local<<<nb, kRefitThreads, 0, s>>>(T_, plan_.as<int4>(), lrec_.as<float4>(), nrec_.as<float4>(),
+                                               lexp_.as<int>(), nexp_.as<int>(), llist_.as<int4>(), llink_.as<int2>(),
+                                               lexport_.as<int4>(), lhdr_.as<int>()); note_launch();
     if (nb > 1) {
-        k_plan_top<<<1, kRefitThreads, 0, s>>>(ctr_.as<unsigned>(), top_.as<int4>(), tlist_.as<int4>(),
-                                                thdr_.as<int>()); note_launch();
+        k_plan_top<<<1, kRefitThreads, 0, s>>>(ctr_.as<unsigned>(), top_.as<int4>(), nrec_.as<float4>(),
+                                                tlist_.as<int4>(), tlink_.as<int2>(), thdr_.as<int>()); note_launch();
     }
     return cuda_status(cudaGetLastError());
 }
@@ -1380,21 +1473,22 @@ bvhcd_status LBvh::refit(cudaStream_t s) {
     const int T = T_;
     if (T == 0) return BVHCD_OK;
     static const bool attrs = [] {
-        cudaFuncSetAttribute(k_refit_local, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLocalSmem);
-        cudaFuncSetAttribute(k_refit_top, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTopSmem);
+        cudaFuncSetAttribute(k_refit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLocalSmem);
         return true;
     }();
     (void)attrs;
+    RefitTop g;
+    g.top = top_.as<int4>();
+    g.tlist = tlist_.as<int4>();
+    g.tlink = tlink_.as<int2>();
+    g.thdr = thdr_.as<int>();
+    g.gext = gext_.as<float>();
+    g.gbox = gbox_.as<float>();
+    g.done = ctr_.as<unsigned>() + C_REFIT_DONE;
     const int nb = (T + kRefitW - 1) / kRefitW;
-    k_refit_local<<<nb, kRefitThreads, kLocalSmem, s>>>(T, sface_.as<int4>(), vptr_, plan_.as<int4>(),
-                                                        llist_.as<int4>(), lhdr_.as<int>(), lrec_.as<float4>(),
-                                                        nrec_.as<float4>()); note_launch();
-    if (nb > 1) {
-        // nodes cross blocks only when there are several
-        k_refit_top<<<1, kRefitThreads, kTopSmem, s>>>(ctr_.as<unsigned>(), top_.as<int4>(), tlist_.as<int4>(),
-                                                       thdr_.as<int>(), lrec_.as<float4>(), nrec_.as<float4>(),
-                                                       gbox_.as<float>(), capT_ + 2); note_launch();
-    }
+    k_refit<<<nb, kRefitThreads, kLocalSmem, s>>>(T, sface_.as<int4>(), vptr_, plan_.as<int4>(), llist_.as<int4>(),
+                                                  llink_.as<int2>(), lexport_.as<int4>(), lhdr_.as<int>(),
+                                                  lrec_.as<float4>(), nrec_.as<float4>(), gext_.as<float>(), g); note_launch();
     return cuda_status(cudaGetLastError());
 }
 

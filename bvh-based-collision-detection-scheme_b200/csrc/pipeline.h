@@ -161,9 +161,11 @@ class LBvh {
     // refit plan (a function of the topology): split of each internal node,
     // crossing flags and ranks, per-split local entries, crossing-node
     // entries, node heights, level-sorted lists (per leaf block and for the
-    // crossing nodes) with their level offsets, and the top pass's global
-    // storage when the crossing nodes exceed its shared memory
-    DBuf split_, cross_, topk_, plan_, top_, gbox_, height_, llist_, lhdr_, tlist_, thdr_;
+    // crossing nodes) with their level offsets, record links (leaves, crossing
+    // nodes), export marks and lists with the export slots, and the top
+    // pass's global storage when the crossing nodes exceed shared memory
+    DBuf split_, cross_, topk_, plan_, top_, gbox_, height_, llist_, lhdr_, tlist_, thdr_, llink_, tlink_, lexp_,
+        nexp_, lexport_, gext_;
     // build scratch
     DBuf keys_, vals_, keys2_, vals2_, k64_, k64b_, metric_, ulc_, urc_, upar_, urx_, ury_, umark_,
         ubox_, uflag_, posb_, clen_, coff_, dfs_, ulpar_, scene_, partial_, scratch_, task_, tmpface_;
