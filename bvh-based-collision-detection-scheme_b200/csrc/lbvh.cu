@@ -254,6 +254,7 @@ struct Climb {
     float4 *ubox;
     unsigned *uflag;
     int *posb, *clen, *ulpar;
+    int *uheight;  // node height (leaves 0), for the refit plan
 };
 
 // Bottom-up construction (buildIntNodes, LBvhBuildKernels.cu:135-172; with
@@ -262,8 +263,8 @@ struct Climb {
 // leaves, or over all leaves of a forest when `leaves` is null, with
 // `prev_topo` null: a scene root has no father).  Internal nodes are
 // indexed by split.  The second thread to reach a node merges the child
-// boxes, records posb = distance from the bottom of its left chain and, at a
-// chain top, the chain length of the chain's leftmost leaf.
+// boxes, records its height and posb = distance from the bottom of its left
+// chain and, at a chain top, the chain length of the chain's leftmost leaf.
 template <bool kSeg>
 __global__ void __launch_bounds__(kThreads) k_climb(int T, int n, const int *__restrict__ leaves,
                                                     const int *__restrict__ seg,
@@ -307,6 +308,7 @@ __global__ void __launch_bounds__(kThreads) k_climb(int T, int n, const int *__r
             c.ubox[2 * cur + 1] = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.f);
             const int pb = (m & 1u) ? 0 : __ldcg(&c.posb[lc]) + 1;
             c.posb[cur] = pb;
+            c.uheight[cur] = 1 + max((m & 1u) ? 0 : __ldcg(&c.uheight[lc]), (m & 2u) ? 0 : __ldcg(&c.uheight[rc]));
             l = rx - 1;
             r = ry;
             if (kSeg) bd = ((l < 0 || seg[l] != sub) ? 2 : 0) | ((r == T - 1 || seg[r + 1] != sub) ? 1 : 0);
@@ -381,7 +383,8 @@ __global__ void k_leaf_links(int T, const unsigned *__restrict__ coff, const int
 // Internal nodes in DFS order (reorderIntNode, LBvhBuildKernels.cu:202-217).
 __global__ void k_write_nodes(int nint, int T, Climb c, const int *__restrict__ dfs,
                               const unsigned *__restrict__ coff, const int *__restrict__ clen,
-                              const int *__restrict__ leafscene, float4 *nrec, int4 *topo, int2 *nrange) {
+                              const int *__restrict__ leafscene, float4 *nrec, int4 *topo, int2 *nrange,
+                              int *height) {
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nint; u += gridDim.x * blockDim.x) {
         if (scene_end(leafscene, u, T)) continue;
         int d = dfs[u];
@@ -390,6 +393,7 @@ __global__ void k_write_nodes(int nint, int T, Climb c, const int *__restrict__ 
         int rx = c.urx[u], ry = c.ury[u];
         topo[d] = make_int4((m & 1u) ? lc : dfs[lc], (m & 2u) ? rc : dfs[rc], p < 0 ? -1 : dfs[p], (int)m);
         nrange[d] = make_int2(rx, ry);
+        height[d] = c.uheight[u];
         float4 lo = c.ubox[2 * u], hi = c.ubox[2 * u + 1];
         lo.w = __int_as_float(rx);
         hi.w = __int_as_float(scene_end(leafscene, ry, T) ? -1 : lca_of(ry + 1, T, coff, clen));
@@ -1162,7 +1166,7 @@ LBvh::~LBvh() {
                     &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &flagbuf_,
                     &ctr_, &scene_of_, &leafscene_, &sbox_, &tiles_, &nrec16_, &split_, &cross_, &topk_,
                     &plan_, &top_, &gbox_, &height_, &llist_, &lhdr_, &tlist_,
-                    &thdr_, &llink_, &tlink_, &lexp_, &nexp_, &lexport_, &gext_};
+                    &thdr_, &llink_, &tlink_, &lexp_, &nexp_, &lexport_, &gext_, &uheight_};
     for (DBuf *b : bufs) b->release();
     if (h_ctr_) cudaFreeHost(h_ctr_);
 }
@@ -1202,6 +1206,7 @@ bvhcd_status LBvh::ensure_capacity(int T, int V) {
     BV_TRY(top_.reserve(sizeof(int4) * n));
     BV_TRY(gbox_.reserve(sizeof(float) * 6 * n));
     BV_TRY(height_.reserve(sizeof(int) * n));
+    BV_TRY(uheight_.reserve(sizeof(int) * n));
     BV_TRY(llist_.reserve(sizeof(int4) * (n + kRefitW)));
     BV_TRY(lhdr_.reserve(sizeof(int) * kLevelHdr * (n / kRefitW + 2)));
     BV_TRY(tlist_.reserve(sizeof(int4) * n));
@@ -1299,12 +1304,12 @@ bvhcd_status LBvh::scene_box(cudaStream_t s) {
 
 static Climb make_climb(const DBuf &ulc, const DBuf &urc, const DBuf &upar, const DBuf &urx,
                         const DBuf &ury, const DBuf &umark, const DBuf &ubox, const DBuf &uflag,
-                        const DBuf &posb, const DBuf &clen, const DBuf &ulpar) {
+                        const DBuf &posb, const DBuf &clen, const DBuf &ulpar, const DBuf &uheight) {
     Climb c;
     c.ulc = ulc.as<int>(); c.urc = urc.as<int>(); c.upar = upar.as<int>();
     c.urx = urx.as<int>(); c.ury = ury.as<int>(); c.umark = umark.as<unsigned>();
     c.ubox = ubox.as<float4>(); c.uflag = uflag.as<unsigned>(); c.posb = posb.as<int>();
-    c.clen = clen.as<int>(); c.ulpar = ulpar.as<int>();
+    c.clen = clen.as<int>(); c.ulpar = ulpar.as<int>(); c.uheight = uheight.as<int>();
     return c;
 }
 
@@ -1345,10 +1350,10 @@ bvhcd_status LBvh::build(cudaStream_t s) {
             k_single_leaf<<<1, 32, 0, s>>>(lca_.as<int>(), lrec_.as<float4>()); note_launch();
             BV_TRY(cudaGetLastError());
             built_ = true;
-            return refit_plan(s);
+            return refit_plan(s, true);
         }
     }
-    Climb c = make_climb(ulc_, urc_, upar_, urx_, ury_, umark_, ubox_, uflag_, posb_, clen_, ulpar_);
+    Climb c = make_climb(ulc_, urc_, upar_, urx_, ury_, umark_, ubox_, uflag_, posb_, clen_, ulpar_, uheight_);
     BV_TRY(cudaMemsetAsync(uflag_.p, 0, sizeof(unsigned) * (size_t)T, s));
     BV_TRY(cudaMemsetAsync(clen_.as<int>() + T, 0, sizeof(int), s));
     if (leafscene)
@@ -1367,10 +1372,10 @@ bvhcd_status LBvh::build(cudaStream_t s) {
                                                   lrec_.as<float4>()); note_launch();
     k_write_nodes<<<grid_for(T - 1), kThreads, 0, s>>>(T - 1, T, c, dfs_.as<int>(), coff_.as<unsigned>(),
                                                        clen_.as<int>(), leafscene, nrec_.as<float4>(),
-                                                       topo_.as<int4>(), nrange_.as<int2>()); note_launch();
+                                                       topo_.as<int4>(), nrange_.as<int2>(), height_.as<int>()); note_launch();
     BV_TRY(cudaGetLastError());
     built_ = true;
-    return refit_plan(s);
+    return refit_plan(s, true);
 }
 
 bvhcd_status LBvh::copy_state_from(const LBvh &src, cudaStream_t s) {
@@ -1435,8 +1440,9 @@ bvhcd_status LBvh::set_scenes(int S, const int32_t *off) {
 }
 
 // The refit plan of the current topology (see k_heights, k_plan_split,
-// k_plan_write, k_plan_local, k_plan_top).
-bvhcd_status LBvh::refit_plan(cudaStream_t s) {
+// k_plan_write, k_plan_local, k_plan_top).  heights_known: the build's climb
+// has written every node's height already.
+bvhcd_status LBvh::refit_plan(cudaStream_t s, bool heights_known) {
     const int nint = T_ - S_;  // internal nodes: one tree of n - 1 per scene of n leaves
     const int nb = (T_ + kRefitW - 1) / kRefitW;
     if (T_ <= 0) return BVHCD_OK;
@@ -1445,10 +1451,12 @@ bvhcd_status LBvh::refit_plan(cudaStream_t s) {
     if (nint > 0) {
         BV_TRY(cudaMemsetAsync(nexp_.p, 0xFF, sizeof(int) * (size_t)nint, s));
         BV_TRY(cudaMemsetAsync(plan_.p, 0xFF, sizeof(int4) * (size_t)T_, s));
-        BV_TRY(cudaMemsetAsync(height_.p, 0, sizeof(int) * (size_t)nint, s));
-        BV_TRY(cudaMemsetAsync(refit_flag_.p, 0, sizeof(unsigned) * (size_t)nint, s));
-        k_heights<<<grid_for(T_), kThreads, 0, s>>>(T_, lrec_.as<float4>(), topo_.as<int4>(),
-                                                    refit_flag_.as<unsigned>(), height_.as<int>()); note_launch();
+        if (!heights_known) {
+            BV_TRY(cudaMemsetAsync(height_.p, 0, sizeof(int) * (size_t)nint, s));
+            BV_TRY(cudaMemsetAsync(refit_flag_.p, 0, sizeof(unsigned) * (size_t)nint, s));
+            k_heights<<<grid_for(T_), kThreads, 0, s>>>(T_, lrec_.as<float4>(), topo_.as<int4>(),
+                                                        refit_flag_.as<unsigned>(), height_.as<int>()); note_launch();
+        }
         k_plan_split<<<grid_for(nint), kThreads, 0, s>>>(nint, topo_.as<int4>(), nrange_.as<int2>(),
                                                          split_.as<int>(), cross_.as<unsigned>()); note_launch();
         BV_TRY(scan_u32(cross_.as<unsigned>(), topk_.as<unsigned>(), nint, false, ctr_.as<unsigned>() + C_TOPK,
@@ -1549,7 +1557,7 @@ bvhcd_status LBvh::restructure(cudaStream_t s) {
     if (st != BVHCD_OK) return st;
     // 10 confined rebuild
     k_metrics<<<grid_for(T), kThreads, 0, s>>>(T, code_.as<unsigned>(), metric_.as<int>()); note_launch();
-    Climb c = make_climb(ulc_, urc_, upar_, urx_, ury_, umark_, ubox_, uflag_, posb_, clen_, ulpar_);
+    Climb c = make_climb(ulc_, urc_, upar_, urx_, ury_, umark_, ubox_, uflag_, posb_, clen_, ulpar_, uheight_);
     BV_TRY(cudaMemsetAsync(uflag_.p, 0, sizeof(unsigned) * (size_t)T, s));
     BV_TRY(cudaMemsetAsync(clen_.p, 0, sizeof(int) * (size_t)(T + 1), s));
     k_climb<true><<<grid_for(nr), kThreads, 0, s>>>(T, nr, task_.as<int>(), leafroot_.as<int>(),
@@ -1566,7 +1574,8 @@ bvhcd_status LBvh::restructure(cudaStream_t s) {
                                                  nrange_.as<int2>(), lrec_.as<float4>()); note_launch();
     BV_TRY(cudaGetLastError());
     opt_tag_ = 1;
-    return refit_plan(s);
+    // the confined rebuild can change the heights of the subtrees' ancestors
+    return refit_plan(s, false);
 }
 
 bvhcd_status LBvh::node_fp16(cudaStream_t s) {

@@ -142,7 +142,7 @@ class LBvh {
     bvhcd_status upload(const bvhcd_scene &scene, cudaStream_t s);
     bvhcd_status build(cudaStream_t s);
     bvhcd_status refit(cudaStream_t s);
-    bvhcd_status refit_plan(cudaStream_t s);
+    bvhcd_status refit_plan(cudaStream_t s, bool heights_known);
     bvhcd_status restructure(cudaStream_t s);
     bvhcd_status scene_box(cudaStream_t s);
     bvhcd_status climb_and_order(cudaStream_t s);
@@ -165,7 +165,7 @@ class LBvh {
     // nodes), export marks and lists with the export slots, and the top
     // pass's global storage when the crossing nodes exceed shared memory
     DBuf split_, cross_, topk_, plan_, top_, gbox_, height_, llist_, lhdr_, tlist_, thdr_, llink_, tlink_, lexp_,
-        nexp_, lexport_, gext_;
+        nexp_, lexport_, gext_, uheight_;
     // build scratch
     DBuf keys_, vals_, keys2_, vals2_, k64_, k64b_, metric_, ulc_, urc_, upar_, urx_, ury_, umark_,
         ubox_, uflag_, posb_, clen_, coff_, dfs_, ulpar_, scene_, partial_, scratch_, task_, tmpface_;
