@@ -456,30 +456,80 @@ __global__ void __launch_bounds__(kB) k_balance_scan(FArgs a) {
 // pureReorderLooseFrontsWithLog (BvttFrontReorderKernels.cu:12-24): counting
 // sort scatter of both fronts by node id.  Holes left by chunked emission are
 // skipped; the sorted fronts' sizes are the per-node count totals.
-__global__ void __launch_bounds__(kThreads) k_reorder(FArgs a) {
+//
+// Tiles of kReorderTile entries: each CTA first groups its tile by key
+// (node, internal or external front) in a shared-memory hash table, taking
+// each entry's rank within its key; then one global atomic per distinct key
+// reserves the key's run in the sorted front; then every entry is written at
+// run start + rank.  Neighbouring primitives share most front nodes, so a
+// tile holds far fewer keys than entries: the cursor atomics (which
+// serialise on the nodes near the root) drop by that factor, and a key's
+// entries land next to each other.
+constexpr int kReorderThreads = 256;
+constexpr int kReorderPer = 8;                                   // entries per thread per tile
+constexpr int kReorderTile = kReorderThreads * kReorderPer;      // 2048
+constexpr int kReorderSlots = 2 * kReorderTile;                  // hash slots (load factor <= 1/2)
+constexpr unsigned kEmptyKey = 0xffffffffu;
+
+__global__ void __launch_bounds__(kReorderThreads) k_reorder(FArgs a) {
+    __shared__ unsigned skey[kReorderSlots], scnt[kReorderSlots], sbase[kReorderSlots];
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.ctr[a.out_int_slot] = a.log.intbeg[a.T];
         a.ctr[a.out_ext_slot] = a.log.extbeg[a.T];
     }
-    const unsigned stride = gridDim.x * blockDim.x, total = ni + ne;
-    unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
-    int2 nxt = q < total ? (q < ni ? __ldcs(&a.in_int[q]) : __ldcs(&a.in_ext[q - ni])) : make_int2(-1, -1);
-    for (; q < total; q += stride) {
-        const bool is_int = q < ni;
-        const int2 e = nxt;  // prefetched one step ahead
-        const unsigned qn = q + stride;
-        if (qn < total) nxt = qn < ni ? __ldcs(&a.in_int[qn]) : __ldcs(&a.in_ext[qn - ni]);
-        if (e.x < 0) continue;  // hole
-        const unsigned key = ((unsigned)e.y << 1) | (is_int ? 0u : 1u);
-        if (is_int) {
-            unsigned pos = a.log.intbeg[e.y] + node_add(a.log.intcnt, key, e.y);
-            if (pos < a.cap_int) a.out_int[pos] = e;
-        } else {
-            unsigned pos = a.log.extbeg[e.y] + node_add(a.log.extcnt, key, e.y);
-            if (pos < a.cap_ext) a.out_ext[pos] = e;
+    const unsigned total = ni + ne;
+    const unsigned ntiles = (total + kReorderTile - 1) / kReorderTile;
+    for (unsigned tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        for (int i = threadIdx.x; i < kReorderSlots; i += kReorderThreads) {
+            skey[i] = kEmptyKey;
+            scnt[i] = 0u;
         }
+        __syncthreads();
+        int2 e[kReorderPer];
+        unsigned slot[kReorderPer], rank[kReorderPer];
+#pragma unroll
+        for (int j = 0; j < kReorderPer; j++) {
+            const unsigned q = tile * kReorderTile + j * kReorderThreads + threadIdx.x;
+            e[j] = q < total ? (q < ni ? __ldcs(&a.in_int[q]) : __ldcs(&a.in_ext[q - ni])) : make_int2(-1, -1);
+            if (e[j].x >= 0) e[j].x |= (q < ni ? 0 : (int)0x80000000);  // front tag in the sign bit, for now
+        }
+#pragma unroll
+        for (int j = 0; j < kReorderPer; j++) {
+            slot[j] = kEmptyKey;
+            if (e[j].x == -1) continue;  // hole (a tagged entry is never -1: its index is below 2^31 - 1)
+            const unsigned key = ((unsigned)e[j].y << 1) | ((unsigned)e[j].x >> 31);
+            unsigned h = (key * 2654435761u) >> 20;  // 12 bits: kReorderSlots = 4096
+            for (int probe = 0; probe < kReorderSlots; probe++, h = (h + 1) & (kReorderSlots - 1)) {
+                const unsigned prev = atomicCAS(&skey[h], kEmptyKey, key);
+                if (prev == kEmptyKey || prev == key) break;
+            }
+            slot[j] = h;
+            rank[j] = atomicAdd(&scnt[h], 1u);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kReorderSlots; i += kReorderThreads) {
+            const unsigned key = skey[i];
+            if (key == kEmptyKey) continue;
+            const int node = (int)(key >> 1);
+            if (key & 1u) sbase[i] = a.log.extbeg[node] + atomicAdd(a.log.extcnt + node, scnt[i]);
+            else sbase[i] = a.log.intbeg[node] + atomicAdd(a.log.intcnt + node, scnt[i]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kReorderPer; j++) {
+            if (slot[j] == kEmptyKey) continue;
+            const bool is_ext = e[j].x < 0;
+            const int2 v = make_int2(e[j].x & 0x7fffffff, e[j].y);
+            const unsigned pos = sbase[slot[j]] + rank[j];
+            if (!is_ext) {
+                if (pos < a.cap_int) a.out_int[pos] = v;
+            } else if (pos < a.cap_ext) {
+                a.out_ext[pos] = v;
+            }
+        }
+        __syncthreads();  // the table is cleared for the next tile
     }
 }
 
@@ -907,7 +957,7 @@ bvhcd_status Front::reorder(cudaStream_t s) {
     a.in_int_slot = 2 * nx; a.in_ext_slot = 2 * nx + 1;
     a.out_int_slot = 2 * cur_; a.out_ext_slot = 2 * cur_ + 1;
     a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
-    k_reorder<<<RESIDENT(k_reorder), kThreads, 0, s>>>(a); note_launch();
+    k_reorder<<<RESIDENT_B(k_reorder, kReorderThreads), kReorderThreads, 0, s>>>(a); note_launch();
     return cuda_status(cudaGetLastError());
 }
 
