@@ -154,6 +154,29 @@ __device__ __forceinline__ void em_close(const FArgs &a, Em &em) {
     if (a.work) chunk_close(a.work, a.cap_work, em.wk);
 }
 
+// The front scans walk their n entries grid-stride (the whole grid then works
+// on a narrow window of the node-sorted front at any time, which keeps the
+// records it reads in L2), but with no more lanes than n / kScanMinPer:
+// chunked emission leaves up to kChunk - 1 reserved but unused slots per
+// emitting lane and stream, and those holes count against the capacity.  With
+// at least kScanMinPer entries per lane they stay below 7/32 of the input
+// however small the front is next to the grid (one entry per lane would
+// reserve eight slots per entry).  The traversal kernels (generation, sprout)
+// keep one work item per lane: an item is a whole traversal, and their holes
+// are at most seven per item and stream.
+constexpr unsigned kScanMinPer = 32;
+struct Spread {
+    unsigned start, stride;  // this lane's first item (n: none); the lanes at work
+};
+template <unsigned kMin>
+__device__ __forceinline__ Spread spread(unsigned n) {
+    const unsigned grid = gridDim.x * blockDim.x;
+    unsigned lanes = ((n + kMin - 1) / kMin + 31u) & ~31u;
+    lanes = lanes < 32u ? 32u : lanes < grid ? lanes : grid;
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    return Spread{t < lanes ? t : n, lanes};
+}
+
 // Stackless traversal from tagged node `st` until tagged node `stop`
 // (the loop shared by genLooseIntraFrontsWithLog,
 // Mine/collision/bvtt_front/BvttFrontGenerateKernels.cu:65-88, the sprout
@@ -306,6 +329,7 @@ __device__ __forceinline__ void take_ents(Batch<kU> &dst, const Batch<kU> &src) 
 // for one round trip (the records) instead of two (entries, then records).
 
 
+
 // Traversal below overlapping internal front nodes (the sprout half of
 // maintainIntLooseIntraFrontsWithLog, BvttFrontPruneSproutKernels.cu:32-56,
 // with kFront; keepIntLooseIntraFronts, BvttFrontKeepKernels.cu:21-42, and the
@@ -334,12 +358,11 @@ template <int kU, int kB>
 __global__ void __launch_bounds__(kB) k_maintain_int_scan(FArgs a) {
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
-    const unsigned stride = gridDim.x * blockDim.x;
-    const unsigned q_start = blockIdx.x * blockDim.x + threadIdx.x;
+    const Spread sp = spread<kScanMinPer>(ni);
     Batch<kU> b, nb;
-    load_ents(a, q_start, stride, ni, ni, b);
-    for (unsigned q0 = q_start; q0 < ni; q0 += kU * stride, take_ents(b, nb)) {
-        load_ents(a, q0 + kU * stride, stride, ni, ni, nb);
+    load_ents(a, sp.start, sp.stride, ni, ni, b);
+    for (unsigned q0 = sp.start; q0 < ni; q0 += kU * sp.stride, take_ents(b, nb)) {
+        load_ents(a, q0 + kU * sp.stride, sp.stride, ni, ni, nb);
         load_recs(a, b);
 #pragma unroll
         for (int k = 0; k < kU; k++) {
@@ -361,12 +384,11 @@ template <int kU, int kB>
 __global__ void __launch_bounds__(kB) k_maintain_ext(FArgs a) {
     Em em;
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
-    const unsigned stride = gridDim.x * blockDim.x;
-    const unsigned q_start = blockIdx.x * blockDim.x + threadIdx.x;
+    const Spread sp = spread<kScanMinPer>(ne);
     Batch<kU> b, nb;
-    load_ents(a, q_start, stride, 0, ne, b);
-    for (unsigned q0 = q_start; q0 < ne; q0 += kU * stride, take_ents(b, nb)) {
-        load_ents(a, q0 + kU * stride, stride, 0, ne, nb);
+    load_ents(a, sp.start, sp.stride, 0, ne, b);
+    for (unsigned q0 = sp.start; q0 < ne; q0 += kU * sp.stride, take_ents(b, nb)) {
+        load_ents(a, q0 + kU * sp.stride, sp.stride, 0, ne, nb);
         load_recs(a, b);
 #pragma unroll
         for (int k = 0; k < kU; k++) {
@@ -400,12 +422,11 @@ __global__ void __launch_bounds__(kB) k_keep_scan(FArgs a) {
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
-    const unsigned stride = gridDim.x * blockDim.x;
-    const unsigned q_start = blockIdx.x * blockDim.x + threadIdx.x;
+    const Spread sp = spread<kScanMinPer>(ni + ne);
     Batch<kU> b, nb;
-    load_ents(a, q_start, stride, ni, ni + ne, b);
-    for (unsigned q0 = q_start; q0 < ni + ne; q0 += kU * stride, take_ents(b, nb)) {
-        load_ents(a, q0 + kU * stride, stride, ni, ni + ne, nb);
+    load_ents(a, sp.start, sp.stride, ni, ni + ne, b);
+    for (unsigned q0 = sp.start; q0 < ni + ne; q0 += kU * sp.stride, take_ents(b, nb)) {
+        load_ents(a, q0 + kU * sp.stride, sp.stride, ni, ni + ne, nb);
         load_recs(a, b);
 #pragma unroll
         for (int k = 0; k < kU; k++) {
@@ -426,13 +447,12 @@ __global__ void __launch_bounds__(kB) k_balance_scan(FArgs a) {
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
-    const unsigned stride = gridDim.x * blockDim.x;
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[a.out_int_slot] = a.ctr[a.in_int_slot];
-    const unsigned q_start = blockIdx.x * blockDim.x + threadIdx.x;
+    const Spread sp = spread<kScanMinPer>(ni + ne);
     Batch<kU> b, nb;
-    load_ents(a, q_start, stride, ni, ni + ne, b);
-    for (unsigned q0 = q_start; q0 < ni + ne; q0 += kU * stride, take_ents(b, nb)) {
-        load_ents(a, q0 + kU * stride, stride, ni, ni + ne, nb);
+    load_ents(a, sp.start, sp.stride, ni, ni + ne, b);
+    for (unsigned q0 = sp.start; q0 < ni + ne; q0 += kU * sp.stride, take_ents(b, nb)) {
+        load_ents(a, q0 + kU * sp.stride, sp.stride, ni, ni + ne, nb);
         load_recs(a, b);
 #pragma unroll
         for (int k = 0; k < kU; k++) {
