@@ -29,7 +29,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "capacit
 EXPORTED = [
     "bvhcd_status_string", "bvhcd_device_check", "bvhcd_bvh_create", "bvhcd_bvh_destroy",
     "bvhcd_bvh_maintain", "bvhcd_bvh_sizes", "bvhcd_bvh_opt_tag", "bvhcd_bvh_export",
-    "bvhcd_bvh_request_restructure",
+    "bvhcd_bvh_request_restructure", "bvhcd_bvh_stage_positions",
     "bvhcd_front_create", "bvhcd_front_destroy", "bvhcd_front_maintain", "bvhcd_front_stats_get",
     "bvhcd_front_pairs", "bvhcd_front_device_results", "bvhcd_front_export",
     "bvhcd_schedule_heuristic", "bvhcd_frame", "bvhcd_profile_enable", "bvhcd_profile_read",
@@ -123,6 +123,7 @@ def lib():
             "bvhcd_bvh_opt_tag": (ctypes.c_int, [vp, ctypes.POINTER(i32)]),
             "bvhcd_bvh_export": (ctypes.c_int, [vp] + [vp] * 7 + [vp]),
             "bvhcd_bvh_request_restructure": (ctypes.c_int, [vp, vp, i32, vp]),
+            "bvhcd_bvh_stage_positions": (ctypes.c_int, [vp, vp, i32, vp, ctypes.POINTER(vp)]),
             "bvhcd_front_create": (ctypes.c_int, [vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
             "bvhcd_front_destroy": (ctypes.c_int, [vp]),
             "bvhcd_front_maintain": (ctypes.c_int, [vp, ctypes.c_int, vp]),
@@ -208,9 +209,25 @@ def device_check(device: int = 0) -> bool:
     return bool(ok.value)
 
 
+class StagedPositions:
+    """Positions copied to one of an LBvh's staging buffers by
+    LBvh.stage_positions: pass it as `pos` (with faces on the GPU) to the
+    next maintain / frame."""
+
+    def __init__(self, ptr: int, num_vertices: int):
+        self.ptr, self.num_vertices = int(ptr), int(num_vertices)
+
+
 def _scene(pos, faces, faces_static=False):
     """Scene struct plus the objects that keep its buffers alive."""
     keep = []
+    if isinstance(pos, StagedPositions):
+        import torch
+        assert isinstance(faces, torch.Tensor) and faces.is_cuda and faces.dtype == torch.int32, \
+            "staged positions go with faces on the GPU"
+        faces = faces.contiguous()
+        keep.append(faces)
+        return Scene(pos.ptr, faces.data_ptr(), pos.num_vertices, faces.shape[0], 1, int(faces_static)), keep
     try:
         import torch
         is_t = isinstance(pos, torch.Tensor)
@@ -262,6 +279,27 @@ class LBvh:
         self._keep = keep
         _check(lib().bvhcd_bvh_maintain(self._h, int(op), ctypes.byref(sc), _stream_ptr(stream)),
                "bvh maintain")
+
+    def stage_positions(self, pos, copy_stream=None) -> "StagedPositions":
+        """bvhcd_bvh_stage_positions: copy the next frame's positions (a
+        host array; pinned for an asynchronous copy) to a staging buffer on
+        copy_stream; pass the result as the next maintain / frame's `pos`."""
+        try:
+            import torch
+            is_t = isinstance(pos, torch.Tensor)
+        except ImportError:
+            is_t = False
+        if is_t:
+            assert not pos.is_cuda and pos.dtype == torch.float32 and pos.is_contiguous()
+            ptr, nv = pos.data_ptr(), pos.shape[0]
+        else:
+            pos = np.ascontiguousarray(pos, dtype=np.float32)
+            ptr, nv = pos.ctypes.data, pos.shape[0]
+        self._stage_keep = pos
+        out = ctypes.c_void_p()
+        _check(lib().bvhcd_bvh_stage_positions(self._h, ctypes.c_void_p(ptr), int(nv), _stream_ptr(copy_stream),
+                                               ctypes.byref(out)), "stage positions")
+        return StagedPositions(out.value, nv)
 
     def profile(self, on: bool = True):
         """Record CUDA events around every stage (Logger::recordSection)."""

@@ -221,6 +221,12 @@ bvhcd_status bvhcd_schedule_heuristic(int32_t frame, int32_t start_frame, int32_
     return BVHCD_OK;
 }
 
+bvhcd_status bvhcd_bvh_stage_positions(bvhcd_bvh *bvh, const float *host_pos, int32_t num_vertices,
+                                       void *copy_stream, const float **staged) {
+    if (!bvh) return BVHCD_INVALID_ARG;
+    return bvh->impl.stage_positions(host_pos, num_vertices, as_stream(copy_stream), staged);
+}
+
 bvhcd_status bvhcd_frame(bvhcd_bvh *bvh, bvhcd_front *front, int32_t frame, int32_t start_frame,
                          const bvhcd_scene *scene, void *stream) {
     int32_t b, f;
@@ -369,6 +375,7 @@ bvhcd_status bvhcd_frame_graph(bvhcd_bvh *bvh, bvhcd_front *front, const bvhcd_s
     if (!bvh || !front || !scene || !stream) return BVHCD_INVALID_ARG;
     if (&bvh->impl != front->impl.bvh()) return BVHCD_INVALID_ARG;
     if (!scene->on_device || bvh->impl.restr_enabled() || front->impl.auto_grow()) return BVHCD_INVALID_ARG;
+    if (bvh->impl.is_staged(scene->pos)) return BVHCD_INVALID_ARG;  // staging buffers alternate
     if (bvh_op < BVHCD_BVH_BUILD || bvh_op > BVHCD_BVH_UPDATE) return BVHCD_INVALID_ARG;
     if (front_op < BVHCD_FRONT_PURE_BVH_CD || front_op > BVHCD_FRONT_RESTRUCTURE) return BVHCD_INVALID_ARG;
     cudaStream_t s = as_stream(stream);

@@ -1168,7 +1168,40 @@ LBvh::~LBvh() {
                     &plan_, &top_, &gbox_, &height_, &llist_, &lhdr_, &tlist_,
                     &thdr_, &llink_, &tlink_, &lexp_, &nexp_, &lexport_, &gext_, &uheight_};
     for (DBuf *b : bufs) b->release();
+    for (int k = 0; k < 2; k++) {
+        stage_[k].release();
+        if (stage_ready_[k]) cudaEventDestroy(stage_ready_[k]);
+        if (stage_free_[k]) cudaEventDestroy(stage_free_[k]);
+    }
     if (h_ctr_) cudaFreeHost(h_ctr_);
+}
+
+// Double-buffered position upload (see bvhcd_bvh_stage_positions).  Buffer k
+// is free once the stream that used it has passed the start of the maintain
+// that took the other buffer (stage_free_[k], recorded there).
+bvhcd_status LBvh::stage_positions(const float *host, int nv, cudaStream_t copy, const float **staged) {
+    if (!staged || nv < 0 || (nv > 0 && !host)) return BVHCD_INVALID_ARG;
+    if (stage_pending_) return BVHCD_NOT_READY;
+    for (int k = 0; k < 2; k++) {
+        if (!stage_ready_[k]) BV_TRY(cudaEventCreateWithFlags(&stage_ready_[k], cudaEventDisableTiming));
+        if (!stage_free_[k]) BV_TRY(cudaEventCreateWithFlags(&stage_free_[k], cudaEventDisableTiming));
+    }
+    const int k = stage_next_;
+    const size_t bytes = sizeof(float) * 3 * (size_t)(nv > 0 ? nv : 1);
+    if (stage_[k].bytes < bytes) {
+        BV_TRY(cudaStreamSynchronize(copy));
+        BV_TRY(cudaEventSynchronize(stage_free_[k]));
+        stage_[k].release();
+        BV_TRY(stage_[k].reserve(bytes));
+    }
+    BV_TRY(cudaStreamWaitEvent(copy, stage_free_[k], 0));
+    if (nv > 0)
+        BV_TRY(cudaMemcpyAsync(stage_[k].p, host, sizeof(float) * 3 * (size_t)nv, cudaMemcpyHostToDevice, copy));
+    BV_TRY(cudaEventRecord(stage_ready_[k], copy));
+    *staged = stage_[k].as<float>();
+    stage_next_ = 1 - k;
+    stage_pending_ = true;
+    return BVHCD_OK;
 }
 
 bvhcd_status LBvh::init() {
@@ -1275,6 +1308,12 @@ bvhcd_status LBvh::upload(const bvhcd_scene &sc, cudaStream_t s) {
     bvhcd_status st = ensure_capacity(sc.num_faces, sc.num_vertices);
     if (st != BVHCD_OK) return st;
     if (sc.on_device) {
+        if (is_staged(sc.pos)) {
+            const int k = sc.pos == stage_[0].as<float>() ? 0 : 1;
+            BV_TRY(cudaStreamWaitEvent(s, stage_ready_[k], 0));
+            BV_TRY(cudaEventRecord(stage_free_[1 - k], s));
+            stage_pending_ = false;
+        }
         vptr_ = sc.pos;
         fptr_ = sc.faces;
     } else {

@@ -89,6 +89,8 @@ class LBvh {
     bvhcd_status init();
     bvhcd_status maintain(bvhcd_bvh_op op, const bvhcd_scene &scene, cudaStream_t s);
     bvhcd_status maintain_tree(bvhcd_bvh_op op, const bvhcd_scene &scene, cudaStream_t s);
+    bvhcd_status stage_positions(const float *host, int nv, cudaStream_t copy, const float **staged);
+    bool is_staged(const float *p) const { return p && (p == stage_[0].as<float>() || p == stage_[1].as<float>()); }
     bvhcd_status export_tree(int32_t *inode, float *ibox, int32_t *leaf, float *lbox, int32_t *lca,
                              uint32_t *codes, int32_t *primmap, cudaStream_t s) const;
     bvhcd_status request_restructure(const int32_t *roots, int32_t n, cudaStream_t s);
@@ -178,6 +180,11 @@ class LBvh {
     DBuf scene_of_, leafscene_, sbox_, tiles_;
     DBuf ctr_;
     unsigned *h_ctr_ = nullptr;  // pinned
+    // double-buffered position uploads: copy done / buffer free events
+    DBuf stage_[2];
+    cudaEvent_t stage_ready_[2] = {nullptr, nullptr}, stage_free_[2] = {nullptr, nullptr};
+    int stage_next_ = 0;
+    bool stage_pending_ = false;
     Profiler prof_;
 };
 

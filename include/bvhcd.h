@@ -122,6 +122,20 @@ bvhcd_status bvhcd_bvh_maintain(bvhcd_bvh *bvh, bvhcd_bvh_op op, const bvhcd_sce
                                 void *stream);
 bvhcd_status bvhcd_bvh_sizes(const bvhcd_bvh *bvh, int32_t *prims, int32_t *ext_nodes,
                              int32_t *int_nodes);
+/* Copies the next frame's positions (host memory, num_vertices x 3 floats;
+ * pinned memory lets the copy run asynchronously) into one of two device
+ * staging buffers of the handle, on copy_stream, and returns the buffer's
+ * device address in *staged.  A bvhcd_bvh_maintain or bvhcd_frame whose
+ * scene has pos == that address (on_device = 1, faces on the device) first
+ * makes its own stream wait for the copy, so the upload of frame f + 1 runs
+ * while frame f computes; a buffer is refilled only after the frames that
+ * read it.  One staged frame may be outstanding: a second call before a
+ * maintain used the first returns BVHCD_NOT_READY.  Not for
+ * bvhcd_frame_graph (its scene pointers are fixed).  The reference uploads
+ * each frame's positions before the frame runs
+ * (Mine/Frameworks/CudaProject/CudaProjectApp.cpp:49-52, Scene::getFormatedData). */
+bvhcd_status bvhcd_bvh_stage_positions(bvhcd_bvh *bvh, const float *host_pos, int32_t num_vertices,
+                                       void *copy_stream, const float **staged);
 bvhcd_status bvhcd_bvh_opt_tag(const bvhcd_bvh *bvh, int32_t *tag);
 /* Marks subtrees (internal nodes by DFS id, host array) as degraded, the
  * marks the front-quality check leaves in BvhRestrLog
