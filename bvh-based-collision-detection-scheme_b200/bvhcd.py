@@ -30,7 +30,7 @@ EXPORTED = [
     "bvhcd_status_string", "bvhcd_device_check", "bvhcd_bvh_create", "bvhcd_bvh_destroy",
     "bvhcd_bvh_maintain", "bvhcd_bvh_sizes", "bvhcd_bvh_opt_tag", "bvhcd_bvh_export",
     "bvhcd_bvh_request_restructure", "bvhcd_bvh_stage_positions",
-    "bvhcd_front_create", "bvhcd_front_destroy", "bvhcd_front_maintain", "bvhcd_front_stats_get",
+    "bvhcd_front_create", "bvhcd_front_create_inter", "bvhcd_front_destroy", "bvhcd_front_maintain", "bvhcd_front_stats_get",
     "bvhcd_front_pairs", "bvhcd_front_device_results", "bvhcd_front_export",
     "bvhcd_schedule_heuristic", "bvhcd_frame", "bvhcd_profile_enable", "bvhcd_profile_read",
     "bvhcd_launch_count", "bvhcd_morton_order_noalloc", "bvhcd_bvh_set_scenes", "bvhcd_frame_graph",
@@ -125,6 +125,7 @@ def lib():
             "bvhcd_bvh_request_restructure": (ctypes.c_int, [vp, vp, i32, vp]),
             "bvhcd_bvh_stage_positions": (ctypes.c_int, [vp, vp, i32, vp, ctypes.POINTER(vp)]),
             "bvhcd_front_create": (ctypes.c_int, [vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
+            "bvhcd_front_create_inter": (ctypes.c_int, [vp, vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
             "bvhcd_front_destroy": (ctypes.c_int, [vp]),
             "bvhcd_front_maintain": (ctypes.c_int, [vp, ctypes.c_int, vp]),
             "bvhcd_front_stats_get": (ctypes.c_int, [vp, ctypes.POINTER(FrontStats), vp]),
@@ -353,18 +354,25 @@ class LBvh:
 
 
 class BvttFront:
-    """BvttFrontLooseIntra over a borrowed LBvh: maintain(op) per frame."""
+    """BvttFrontLooseIntra over a borrowed LBvh: maintain(op) per frame.
+    With rigid= another LBvh, BvttFrontLooseInter: the rigid BVH's triangles
+    traverse `bvh` (the deformable one); pairs are (deformable id, rigid id)."""
 
     def __init__(self, bvh: LBvh, int_front_capacity: int = 2_300_000,
                  ext_front_capacity: int = 2_300_000, pair_capacity: int = 1_600_000,
                  cull_adjacent: bool = True, narrow_phase: bool = True, auto_grow: bool = False,
-                 precision: int = 0):
+                 precision: int = 0, rigid: "LBvh" = None):
         cfg = FrontConfig(int(int_front_capacity), int(ext_front_capacity), int(pair_capacity),
                           int(cull_adjacent), int(narrow_phase), int(auto_grow), int(precision))
         h = ctypes.c_void_p()
-        _check(lib().bvhcd_front_create(bvh.handle, ctypes.byref(cfg), ctypes.byref(h)), "front create")
+        if rigid is None:
+            _check(lib().bvhcd_front_create(bvh.handle, ctypes.byref(cfg), ctypes.byref(h)), "front create")
+        else:
+            _check(lib().bvhcd_front_create_inter(bvh.handle, rigid.handle, ctypes.byref(cfg), ctypes.byref(h)),
+                   "inter front create")
         self._h = h
         self._bvh = bvh
+        self._rigid = rigid
 
     @property
     def handle(self):

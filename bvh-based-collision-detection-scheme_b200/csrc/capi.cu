@@ -30,7 +30,7 @@ struct bvhcd_front {
     const int32_t *g_faces = nullptr;
     int g_T = -1, g_V = -1, g_scenes = -1, g_shapes = -1;  // layout / launch-shape epochs
     bool g_warm = false;
-    bvhcd_front(bvhcd::LBvh *b, const bvhcd_front_config &c) : impl(b, c) {}
+    bvhcd_front(bvhcd::LBvh *b, const bvhcd_front_config &c, bvhcd::LBvh *trav = nullptr) : impl(b, c, trav) {}
     ~bvhcd_front() { drop_graphs(); }
     void drop_graphs() {
         for (FrameGraph &g : graphs)
@@ -53,7 +53,8 @@ bool same_state(const bvhcd::LBvh::HostState &a, const bvhcd::LBvh::HostState &b
            a.vptr == b.vptr && a.fptr == b.fptr;
 }
 bool same_state(const bvhcd::Front::HostState &a, const bvhcd::Front::HostState &b) {
-    return a.cur == b.cur && a.last_op == b.last_op && a.has_front == b.has_front && a.int_swapped == b.int_swapped;
+    return a.cur == b.cur && a.last_op == b.last_op && a.has_front == b.has_front && a.int_swapped == b.int_swapped &&
+           a.log_counted == b.log_counted;
 }
 }  // namespace
 
@@ -144,6 +145,22 @@ bvhcd_status bvhcd_front_create(bvhcd_bvh *bvh, const bvhcd_front_config *cfg, b
     if (!bvh || !cfg || !out) return BVHCD_INVALID_ARG;
     *out = nullptr;
     bvhcd_front *h = new (std::nothrow) bvhcd_front(&bvh->impl, *cfg);
+    if (!h) return BVHCD_OUT_OF_MEMORY;
+    bvhcd_status st = h->impl.init();
+    if (st != BVHCD_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return BVHCD_OK;
+}
+
+bvhcd_status bvhcd_front_create_inter(bvhcd_bvh *deformable, bvhcd_bvh *rigid, const bvhcd_front_config *cfg,
+                                      bvhcd_front **out) {
+    if (!deformable || !rigid || !cfg || !out || deformable == rigid) return BVHCD_INVALID_ARG;
+    if (cfg->precision || deformable->impl.num_scenes() != 1 || rigid->impl.num_scenes() != 1) return BVHCD_INVALID_ARG;
+    *out = nullptr;
+    bvhcd_front *h = new (std::nothrow) bvhcd_front(&deformable->impl, *cfg, &rigid->impl);
     if (!h) return BVHCD_OUT_OF_MEMORY;
     bvhcd_status st = h->impl.init();
     if (st != BVHCD_OK) {
@@ -250,14 +267,14 @@ bvhcd_status bvhcd_bvh_copy_state(bvhcd_bvh *dst, const bvhcd_bvh *src, void *st
 
 bvhcd_status bvhcd_front_copy_state(bvhcd_front *dst, const bvhcd_front *src, void *stream) {
     if (!dst || !src) return BVHCD_INVALID_ARG;
-    if (dst->impl.bvh() == src->impl.bvh()) return BVHCD_INVALID_ARG;  // two fronts on one BVH share counters
+    if (dst->impl.inter() || src->impl.inter()) return BVHCD_INVALID_ARG;
     dst->drop_graphs();
     return dst->impl.copy_state_from(src->impl, as_stream(stream));
 }
 
 bvhcd_status bvhcd_learner_create(bvhcd_bvh *bvh, bvhcd_front *front, int32_t max_subtree_leaves,
                                   bvhcd_learner **out) {
-    if (!bvh || !front || !out || &bvh->impl != front->impl.bvh()) return BVHCD_INVALID_ARG;
+    if (!bvh || !front || !out || &bvh->impl != front->impl.bvh() || front->impl.inter()) return BVHCD_INVALID_ARG;
     bvhcd_learner *l = new (std::nothrow) bvhcd_learner(&bvh->impl, &front->impl, max_subtree_leaves);
     if (!l) return BVHCD_OUT_OF_MEMORY;
     bvhcd_status st = l->impl.init();
@@ -374,7 +391,8 @@ bvhcd_status bvhcd_frame_graph(bvhcd_bvh *bvh, bvhcd_front *front, const bvhcd_s
                                int32_t front_op, void *stream) {
     if (!bvh || !front || !scene || !stream) return BVHCD_INVALID_ARG;
     if (&bvh->impl != front->impl.bvh()) return BVHCD_INVALID_ARG;
-    if (!scene->on_device || bvh->impl.restr_enabled() || front->impl.auto_grow()) return BVHCD_INVALID_ARG;
+    if (!scene->on_device || bvh->impl.restr_enabled() || front->impl.auto_grow() || front->impl.inter())
+        return BVHCD_INVALID_ARG;
     if (bvh->impl.is_staged(scene->pos)) return BVHCD_INVALID_ARG;  // staging buffers alternate
     if (bvh_op < BVHCD_BVH_BUILD || bvh_op > BVHCD_BVH_UPDATE) return BVHCD_INVALID_ARG;
     if (front_op < BVHCD_FRONT_PURE_BVH_CD || front_op > BVHCD_FRONT_RESTRUCTURE) return BVHCD_INVALID_ARG;

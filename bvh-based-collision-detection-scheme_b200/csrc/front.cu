@@ -38,6 +38,11 @@ inline unsigned grid_for(int64_t n) {
 
 struct FArgs {
     const float4 *nrec, *lrec;
+    // records of the traversing primitives: the tree's own leaves (an intra
+    // front), or the leaves of another BVH (an inter front, whose primitives
+    // start at the root, root_tag, instead of their own leaf's escape link)
+    const float4 *prec;
+    int nprim, inter, root_tag;
     const uint4 *nrec16;   // FP16 node records, or null for the FP32 ones
     const int2 *nrange;
     const int4 *topo;
@@ -243,10 +248,15 @@ __device__ __forceinline__ int4 prim_face(const FArgs &a, int prim) {
 template <bool kFront>
 __global__ void __launch_bounds__(kThreads) k_generate(FArgs a) {
     Em em;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.T - 1; i += gridDim.x * blockDim.x) {
+    // an intra front: primitive i traverses from its own leaf's escape link
+    // (the primitives to its right); an inter front: every primitive of the
+    // other BVH from the root (genLooseInterFrontsWithLog,
+    // BvttFrontGenerateKernels.cu:92-124, which skips the last one)
+    const int n = a.inter ? a.nprim : a.T - 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 plo, phi;
-        ldg8(a.lrec + 2 * i, plo, phi);
-        traverse<kFront>(a, em, i, plo, phi, prim_face(a, i), __float_as_int(phi.w), -1);
+        ldg8(a.prec + 2 * i, plo, phi);
+        traverse<kFront>(a, em, i, plo, phi, prim_face(a, i), a.inter ? a.root_tag : __float_as_int(phi.w), -1);
     }
     em_close(a, em);
 }
@@ -307,7 +317,7 @@ __device__ __forceinline__ void load_recs(const FArgs &a, Batch<kU> &b) {
 #pragma unroll
     for (int k = 0; k < kU; k++) {
         if (!b.v[k]) continue;
-        ldg8(a.lrec + 2 * b.e[k].x, b.plo[k], b.phi[k]);
+        ldg8(a.prec + 2 * b.e[k].x, b.plo[k], b.phi[k]);
         if (b.in_int[k]) {
             node_rec(a, b.e[k].y, b.nlo[k], b.nhi[k]);
         } else {
@@ -343,7 +353,7 @@ __global__ void __launch_bounds__(kB) k_sprout(FArgs a) {
         const int2 e = a.work[q];
         if (e.x < 0) continue;  // hole
         float4 plo, phi;
-        ldg8(a.lrec + 2 * e.x, plo, phi);
+        ldg8(a.prec + 2 * e.x, plo, phi);
         float4 nlo, nhi;
         node_rec(a, e.y, nlo, nhi);
         traverse<kFront>(a, em, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, node_rangex(a, e.y, nlo)),
@@ -648,10 +658,14 @@ __device__ __forceinline__ v3 vload(const float *v, int i) {
 // simpleNarrowPhase (Mine/collision/narrow_phase/narrow_phase.cu:8-24):
 // keeps the pairs whose triangles intersect, as original triangle ids, and
 // counts the valid broad-phase pairs (the pair list has holes).  Without
-// kTest it only counts.
+// kTest it only counts.  A pair is (traversing primitive, leaf): the
+// primitive's triangle from (psface, pverts), the leaf's from (sface, verts)
+// -- the same mesh for an intra front, the other BVH's for an inter front,
+// whose hits are written leaf first (the reference's inter pair order).
 template <bool kTest, int kB>
-__global__ void __launch_bounds__(kB) k_narrow(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
-                                                     const float *__restrict__ verts, unsigned *ctr,
+__global__ void __launch_bounds__(kB) k_narrow(const int2 *__restrict__ pairs, const int4 *__restrict__ psface,
+                                                     const float *__restrict__ pverts, const int4 *__restrict__ sface,
+                                                     const float *__restrict__ verts, int leaf_first, unsigned *ctr,
                                                      unsigned cap_pairs, int2 *hits, unsigned cap_hits) {
     const unsigned n = min(ctr[C_PAIRS], cap_pairs);
     unsigned valid = 0;
@@ -660,10 +674,11 @@ __global__ void __launch_bounds__(kB) k_narrow(const int2 *__restrict__ pairs, c
         if (p.x < 0) continue;  // hole
         ++valid;
         if (!kTest) continue;
-        int4 a = __ldg(&sface[p.x]), b = __ldg(&sface[p.y]);
-        if (tritri_sat32(vload(verts, a.x), vload(verts, a.y), vload(verts, a.z), vload(verts, b.x),
+        int4 a = __ldg(&psface[p.x]), b = __ldg(&sface[p.y]);
+        if (tritri_sat32(vload(pverts, a.x), vload(pverts, a.y), vload(pverts, a.z), vload(verts, b.x),
                          vload(verts, b.y), vload(verts, b.z)))
-            emit(hits, ctr + C_HITS, cap_hits, make_int2(a.w, b.w), ctr + C_OVERFLOW, 8u);
+            emit(hits, ctr + C_HITS, cap_hits, leaf_first ? make_int2(b.w, a.w) : make_int2(a.w, b.w),
+                 ctr + C_OVERFLOW, 8u);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) valid += __shfl_xor_sync(0xffffffffu, valid, o);
@@ -799,14 +814,16 @@ __global__ void k_pair_flags(const int2 *__restrict__ pairs, const unsigned *__r
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n_all; q += gridDim.x * blockDim.x)
         flags[q] = (q < n && pairs[q].x >= 0) ? 1u : 0u;
 }
-__global__ void k_pair_scatter(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
-                               const unsigned *__restrict__ ctr, unsigned cap, const unsigned *__restrict__ flags,
-                               const unsigned *__restrict__ pos, int2 *out) {
+__global__ void k_pair_scatter(const int2 *__restrict__ pairs, const int4 *__restrict__ psface,
+                               const int4 *__restrict__ sface, int leaf_first, const unsigned *__restrict__ ctr,
+                               unsigned cap, const unsigned *__restrict__ flags, const unsigned *__restrict__ pos,
+                               int2 *out) {
     const unsigned n = min(ctr[C_PAIRS], cap);
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
         if (flags[q]) {
             const int2 p = pairs[q];
-            out[pos[q]] = make_int2(__ldg(&sface[p.x]).w, __ldg(&sface[p.y]).w);
+            const int a = __ldg(&psface[p.x]).w, b = __ldg(&sface[p.y]).w;
+            out[pos[q]] = leaf_first ? make_int2(b, a) : make_int2(a, b);
         }
 }
 
@@ -864,7 +881,7 @@ Front::~Front() {
     for (auto &set : front_)
         for (auto &b : set) b.release();
     DBuf *bufs[] = {&pairs_, &hits_, &outbuf_, &work_, &intcnt_, &extcnt_, &intbeg_, &extbeg_, &intback_,
-                    &extback_, &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_};
+                    &extback_, &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_, &fctr_};
     for (DBuf *b : bufs) b->release();
 }
 
@@ -888,6 +905,8 @@ bvhcd_status Front::init() {
     FR_TRY(hits_.reserve(sizeof(int2) * (size_t)pcap_));
     FR_TRY(work_.reserve(sizeof(int2) * (size_t)fcap_[0]));
     FR_TRY(counts64_.reserve(sizeof(int64_t) * 2));
+    FR_TRY(fctr_.reserve(sizeof(unsigned) * C_NUM));
+    FR_TRY(cudaMemset(fctr_.p, 0, sizeof(unsigned) * C_NUM));
     return ensure_node_capacity(bvh_->T() > 0 ? bvh_->T() : 1);
 }
 
@@ -926,14 +945,19 @@ FrontLog Front::log() const {
 
 // The work list's capacity is what its buffer holds, never a front capacity
 // that may have grown past it.
-static FArgs make_args(const LBvh *bvh, const FrontLog &log, int cull, const DBuf &work) {
+static FArgs make_args(const LBvh *bvh, const LBvh *trav, unsigned *ctr, const FrontLog &log, int cull,
+                       const DBuf &work) {
     const int64_t cap_work = (int64_t)(work.bytes / sizeof(int2));
     Tree t = bvh->tree();
     FArgs a;
     a.nrec = t.nrec; a.lrec = t.lrec; a.topo = t.topo; a.lca = t.lca; a.sface = t.sface;
     a.nrec16 = t.nrec16; a.nrange = t.nrange;
+    a.prec = trav ? trav->tree().lrec : t.lrec;
+    a.nprim = trav ? trav->T() : t.T;
+    a.inter = trav ? 1 : 0;
+    a.root_tag = t.T >= 2 ? 0 : 1;  // internal node 0, or the single leaf
     a.log = log;
-    a.ctr = bvh->counters();
+    a.ctr = ctr;
     a.in_int = a.in_ext = nullptr;
     a.out_int = a.out_ext = nullptr;
     a.in_int_slot = C_INT0; a.in_ext_slot = C_EXT0; a.out_int_slot = C_INT1; a.out_ext_slot = C_EXT1;
@@ -942,7 +966,7 @@ static FArgs make_args(const LBvh *bvh, const FrontLog &log, int cull, const DBu
     a.cap_pairs = 0;
     a.work = work.as<int2>();
     a.cap_work = (unsigned)(cap_work < 0xffffffffLL ? cap_work : 0xffffffffLL);
-    a.cull = cull;
+    a.cull = trav ? 0 : cull;  // vertex sharing means nothing across two meshes
     a.T = t.T;
     return a;
 }
@@ -970,7 +994,7 @@ bvhcd_status Front::reorder(cudaStream_t s) {
     FrontLog l = log();
     FR_TRY(log_prepare(l, T, scratch_.p, s));
     FR_TRY(log_clear(l, T, s));
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_);
+    FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
     const int nx = 1 - cur_;
     a.in_int = front_[nx][0].as<int2>(); a.in_ext = front_[nx][1].as<int2>();
     a.out_int = front_[cur_][0].as<int2>(); a.out_ext = front_[cur_][1].as<int2>();
@@ -978,21 +1002,22 @@ bvhcd_status Front::reorder(cudaStream_t s) {
     a.out_int_slot = 2 * cur_; a.out_ext_slot = 2 * cur_ + 1;
     a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
     k_reorder<<<RESIDENT_B(k_reorder, kReorderThreads), kReorderThreads, 0, s>>>(a); note_launch();
+    log_counted_ = true;  // the scatter counted every entry again
     return cuda_status(cudaGetLastError());
 }
 
 // Emission into the other buffer set; the caller reorders back.
 bvhcd_status Front::generate(cudaStream_t s, bool pure) {
     const int T = bvh_->T();
-    unsigned *ctr = bvh_->counters();
+    unsigned *ctr = counters();
     FrontLog l = log();
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_);
+    FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
     a.pairs = pairs_.as<int2>();
     a.cap_pairs = (unsigned)pcap_;
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
     if (pure) {
         StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_PURE_BVH_CD, s);
-        k_generate<false><<<grid_for(T), kThreads, 0, s>>>(a); note_launch();
+        k_generate<false><<<grid_for(a.inter ? a.nprim : T), kThreads, 0, s>>>(a); note_launch();
         return cuda_status(cudaGetLastError());
     }
     FR_TRY(log_clear(l, T, s));
@@ -1003,13 +1028,15 @@ bvhcd_status Front::generate(cudaStream_t s, bool pure) {
     FR_TRY(cudaMemsetAsync(ctr + 2 * nx, 0, 2 * sizeof(unsigned), s));
     {
         StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_GENERATE, s);
-        k_generate<true><<<grid_for(T), kThreads, 0, s>>>(a); note_launch();
+        k_generate<true><<<grid_for(a.inter ? a.nprim : T), kThreads, 0, s>>>(a); note_launch();
     }
     FR_TRY(cudaGetLastError());
     bvhcd_status st = reorder(s);
     if (st != BVHCD_OK) return st;
     has_front_ = true;
-    if (bvh_->restr_enabled()) return snapshot(s);
+    seen_epoch_[0] = bvh_->topo_epoch();
+    seen_epoch_[1] = trav()->topo_epoch();
+    if (bvh_->restr_enabled() && !inter()) return snapshot(s);
     return BVHCD_OK;
 }
 
@@ -1040,10 +1067,10 @@ bvhcd_status Front::check_quality(cudaStream_t s) {
 // reorder back.
 bvhcd_status Front::update_kernels(cudaStream_t s) {
     const int T = bvh_->T();
-    unsigned *ctr = bvh_->counters();
+    unsigned *ctr = counters();
     FrontLog l = log();
     FR_TRY(log_clear(l, T, s));
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_);
+    FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
     const int nx = 1 - cur_;
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
     a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
@@ -1067,7 +1094,7 @@ bvhcd_status Front::update_kernels(cudaStream_t s) {
 bvhcd_status Front::prune_sprout(cudaStream_t s) {
     bvhcd_status st = update_kernels(s);
     if (st != BVHCD_OK) return st;
-    if (bvh_->restr_enabled() && quality_check_) {
+    if (bvh_->restr_enabled() && quality_check_ && !inter()) {
         st = check_quality(s);
         if (st != BVHCD_OK) return st;
     }
@@ -1076,8 +1103,8 @@ bvhcd_status Front::prune_sprout(cudaStream_t s) {
 
 bvhcd_status Front::keep(cudaStream_t s) {
     StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_KEEP, s);
-    unsigned *ctr = bvh_->counters();
-    FArgs a = make_args(bvh_, log(), cfg_.cull_adjacent, work_);
+    unsigned *ctr = counters();
+    FArgs a = make_args(bvh_, trav_, counters(), log(), cfg_.cull_adjacent, work_);
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
     a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
     a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
@@ -1094,11 +1121,19 @@ bvhcd_status Front::keep(cudaStream_t s) {
 // it is; only the internal front moves to the other buffer.
 bvhcd_status Front::balance_kernels(cudaStream_t s) {
     const int T = bvh_->T();
-    unsigned *ctr = bvh_->counters();
+    unsigned *ctr = counters();
     FrontLog l = log();
-    FR_TRY(log_prepare(l, T, scratch_.p, s));
+    // A balance leaves a node's entries counted in two halves (intcnt from
+    // the front of its bucket, intback from the back) and the external counts
+    // cleared, but it moves no entry to another node: the begins it started
+    // from still hold, and a balance that follows one (with only keeps in
+    // between) starts from them again.  The reference scans the counts every
+    // time (BvttFrontLooseIntra.cu:286), which places a second balance's
+    // entries over one another; its schedules never run two in a row.
+    if (log_counted_) FR_TRY(log_prepare(l, T, scratch_.p, s));
     FR_TRY(log_clear(l, T, s));
-    FArgs a = make_args(bvh_, l, cfg_.cull_adjacent, work_);
+    log_counted_ = false;
+    FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
     const int nx = 1 - cur_;
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
     a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
@@ -1118,7 +1153,7 @@ bvhcd_status Front::balance(cudaStream_t s) {
     StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_BALANCE, s);
     bvhcd_status st = balance_kernels(s);
     if (st != BVHCD_OK) return st;
-    unsigned *ctr = bvh_->counters();
+    unsigned *ctr = counters();
     const int nx = 1 - cur_;
     // swap the internal front buffers of the two sets, keep the external one
     std::swap(front_[0][0], front_[1][0]);
@@ -1129,7 +1164,7 @@ bvhcd_status Front::balance(cudaStream_t s) {
 
 bvhcd_status Front::narrow(cudaStream_t s, bool test) {
     StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_NARROW, s);
-    unsigned *ctr = bvh_->counters();
+    unsigned *ctr = counters();
     FR_TRY(cudaMemsetAsync(ctr + C_HITS, 0, sizeof(unsigned), s));
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));
     const Shape sh = shape_[BVHCD_SHAPE_NARROW];
@@ -1138,11 +1173,13 @@ bvhcd_status Front::narrow(cudaStream_t s, bool test) {
         LAUNCH_ITEM(k_narrow_prec, true, sh, s, pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
                     (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_);
     else if (test)
-        LAUNCH_ITEM(k_narrow, true, sh, s, pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
-                    (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_);
+        LAUNCH_ITEM(k_narrow, true, sh, s, pairs_.as<int2>(), trav()->tree().sface, trav()->verts(),
+                    bvh_->tree().sface, bvh_->verts(), inter() ? 1 : 0, ctr, (unsigned)pcap_, hits_.as<int2>(),
+                    (unsigned)pcap_);
     else
-        LAUNCH_ITEM(k_narrow, false, sh, s, pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
-                    (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_);
+        LAUNCH_ITEM(k_narrow, false, sh, s, pairs_.as<int2>(), trav()->tree().sface, trav()->verts(),
+                    bvh_->tree().sface, bvh_->verts(), inter() ? 1 : 0, ctr, (unsigned)pcap_, hits_.as<int2>(),
+                    (unsigned)pcap_);
     return cuda_status(cudaGetLastError());
 }
 
@@ -1159,7 +1196,7 @@ bvhcd_status Front::run(bvhcd_front_op op, cudaStream_t s) {
 
 bvhcd_status Front::grow_and_check(cudaStream_t s, bool *overflowed) {
     unsigned h[C_NUM];
-    FR_TRY(cudaMemcpyAsync(h, bvh_->counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaMemcpyAsync(h, counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
     FR_TRY(cudaStreamSynchronize(s));
     *overflowed = h[C_OVERFLOW] != 0;
     if (!*overflowed) return BVHCD_OK;
@@ -1199,29 +1236,39 @@ bvhcd_status Front::grow_and_check(cudaStream_t s, bool *overflowed) {
         FR_TRY(hits_.reserve(sizeof(int2) * (size_t)npc));
         pcap_ = npc;
     }
-    FR_TRY(cudaMemsetAsync(bvh_->counters() + C_OVERFLOW, 0, sizeof(unsigned), s));
+    FR_TRY(cudaMemsetAsync(counters() + C_OVERFLOW, 0, sizeof(unsigned), s));
     return BVHCD_OK;
 }
 
 // BvttFrontLooseIntra::maintain (BvttFrontLooseIntra.cu:69-126)
 bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     if (op < BVHCD_FRONT_PURE_BVH_CD || op > BVHCD_FRONT_RESTRUCTURE) return BVHCD_INVALID_ARG;
-    if (!bvh_->built()) return BVHCD_NOT_READY;
+    if (!bvh_->built() || !trav()->built()) return BVHCD_NOT_READY;
+    if (inter() && (bvh_->num_scenes() != 1 || trav_->num_scenes() != 1)) return BVHCD_INVALID_ARG;
     const int T = bvh_->T();
     bvhcd_status st = ensure_node_capacity(T);
     if (st != BVHCD_OK) return st;
-    bvh_->set_updated(false);
+    if (!inter()) bvh_->set_updated(false);  // an inter front leaves the deformable BVH's restructure marks alone
     bvhcd_front_op run_op = op;
     // front override after a BVH build or restructure (:75-110): the front
     // is regenerated in both cases
     if (bvh_->restr_enabled() && (bvh_->opt_tag() == 2 || bvh_->opt_tag() == 1)) run_op = BVHCD_FRONT_GENERATE;
+    // an inter front's entries name both trees' leaves: after a build or a
+    // restructure of either (the rigid one included, which the reference does
+    // not check) it is regenerated
+    if (inter() && has_front_ && (seen_epoch_[0] != bvh_->topo_epoch() || seen_epoch_[1] != trav_->topo_epoch()) &&
+        run_op != BVHCD_FRONT_PURE_BVH_CD)
+        run_op = BVHCD_FRONT_GENERATE;
     if (op == BVHCD_FRONT_RESTRUCTURE) run_op = BVHCD_FRONT_GENERATE;
     // a front operation needs a front: the first one is generated
     if (!has_front_ && (run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER || run_op == BVHCD_FRONT_KEEP))
         run_op = BVHCD_FRONT_GENERATE;
-    unsigned *ctr = bvh_->counters();
+    // a deformable BVH of one leaf has no internal node for the front
+    // operations to climb to: its inter front is generated every frame
+    if (inter() && T == 1 && run_op != BVHCD_FRONT_PURE_BVH_CD) run_op = BVHCD_FRONT_GENERATE;
+    unsigned *ctr = counters();
     FR_TRY(cudaMemsetAsync(ctr + C_OVERFLOW, 0, sizeof(unsigned), s));
-    if (T < 2) {
+    if (inter() ? (T < 1 || trav_->T() < 1) : T < 2) {
         FR_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned) * 6, s));
         FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));
         last_op_ = run_op;
@@ -1256,9 +1303,9 @@ bvhcd_status Front::copy_state_from(const Front &src, cudaStream_t s) {
     if (st != BVHCD_OK) return st;
     const DBuf *from[] = {&src.front_[0][0], &src.front_[0][1], &src.front_[1][0], &src.front_[1][1], &src.pairs_,
                           &src.hits_, &src.work_, &src.intcnt_, &src.extcnt_, &src.intbeg_, &src.extbeg_,
-                          &src.intback_, &src.extback_, &src.snapshot_, &src.counts64_};
+                          &src.intback_, &src.extback_, &src.snapshot_, &src.counts64_, &src.fctr_};
     DBuf *to[] = {&front_[0][0], &front_[0][1], &front_[1][0], &front_[1][1], &pairs_, &hits_, &work_, &intcnt_,
-                  &extcnt_, &intbeg_, &extbeg_, &intback_, &extback_, &snapshot_, &counts64_};
+                  &extcnt_, &intbeg_, &extbeg_, &intback_, &extback_, &snapshot_, &counts64_, &fctr_};
     for (size_t k = 0; k < sizeof(to) / sizeof(to[0]); k++) FR_TRY(to[k]->copy_from(*from[k], s));
     fcap_[0] = src.fcap_[0];
     fcap_[1] = src.fcap_[1];
@@ -1267,6 +1314,7 @@ bvhcd_status Front::copy_state_from(const Front &src, cudaStream_t s) {
     last_op_ = src.last_op_;
     has_front_ = src.has_front_;
     int_swapped_ = src.int_swapped_;
+    log_counted_ = src.log_counted_;
     for (int k = 0; k < BVHCD_SHAPE_COUNT; k++) shape_[k] = src.shape_[k];
     shape_epoch_++;
     return cuda_status(cudaGetLastError());
@@ -1355,7 +1403,7 @@ bvhcd_status Front::autotune(int repeats, bvhcd_launch_shapes *chosen, double *b
         prof->on = prof_on;
         if (st != BVHCD_OK) return st;
         last_op_ = BVHCD_FRONT_GENERATE;
-        k_counts64<<<1, 32, 0, s>>>(bvh_->counters(), (unsigned)pcap_, (unsigned)pcap_, counts64_.as<int64_t>());
+        k_counts64<<<1, 32, 0, s>>>(counters(), (unsigned)pcap_, (unsigned)pcap_, counts64_.as<int64_t>());
         note_launch();
         FR_TRY(cudaGetLastError());
         FR_TRY(cudaStreamSynchronize(s));
@@ -1367,7 +1415,7 @@ bvhcd_status Front::autotune(int repeats, bvhcd_launch_shapes *chosen, double *b
 
 bvhcd_status Front::stats(bvhcd_front_stats *st, cudaStream_t s) {
     unsigned h[C_NUM];
-    FR_TRY(cudaMemcpyAsync(h, bvh_->counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaMemcpyAsync(h, counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
     FR_TRY(cudaStreamSynchronize(s));
     *st = bvhcd_front_stats{};
     st->int_front = h[2 * cur_];
@@ -1390,12 +1438,13 @@ bvhcd_status Front::compact_pairs(cudaStream_t s) {
     FR_TRY(cflag_.reserve(sizeof(unsigned) * 2 * n));
     FR_TRY(cscratch_.reserve(scan_scratch_bytes((int64_t)n)));
     unsigned *flags = cflag_.as<unsigned>(), *pos = flags + n;
-    unsigned *ctr = bvh_->counters();
+    unsigned *ctr = counters();
     k_pair_flags<<<grid_for((int64_t)n), kThreads, 0, s>>>(pairs_.as<int2>(), ctr, (unsigned)pcap_, (unsigned)n, flags);
     note_launch();
     FR_TRY(scan_u32(flags, pos, (int64_t)n, false, ctr + C_COMPACT, cscratch_.p, s));
-    k_pair_scatter<<<kFrontBlocks, kThreads, 0, s>>>(pairs_.as<int2>(), bvh_->tree().sface, ctr, (unsigned)pcap_,
-                                                     flags, pos, outbuf_.as<int2>());
+    k_pair_scatter<<<kFrontBlocks, kThreads, 0, s>>>(pairs_.as<int2>(), trav()->tree().sface, bvh_->tree().sface,
+                                                     inter() ? 1 : 0, ctr, (unsigned)pcap_, flags, pos,
+                                                     outbuf_.as<int2>());
     note_launch();
     return cuda_status(cudaGetLastError());
 }
@@ -1410,7 +1459,7 @@ bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, 
         src = outbuf_.as<int2>();
     }
     unsigned h[C_NUM];
-    FR_TRY(cudaMemcpyAsync(h, bvh_->counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaMemcpyAsync(h, counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
     FR_TRY(cudaStreamSynchronize(s));
     int64_t n = which ? (int64_t)h[C_HITS] : (int64_t)h[C_COMPACT];
     if (n > pcap_) n = pcap_;
@@ -1429,9 +1478,9 @@ bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, 
 // (which = 1), in the order bvhcd_front_pairs returns them.
 bvhcd_status Front::contacts(int which, float *out, int64_t cap, int64_t *count, int64_t *flagged, bool out_dev,
                              cudaStream_t s) {
-    if (which < 0 || which > 1 || cap < 0) return BVHCD_INVALID_ARG;
+    if (which < 0 || which > 1 || cap < 0 || inter()) return BVHCD_INVALID_ARG;
     const int2 *list = hits_.as<int2>();
-    unsigned *ctr = bvh_->counters();
+    unsigned *ctr = counters();
     const unsigned *cnt = ctr + C_HITS;
     if (which == 1) {
         bvhcd_status st = compact_pairs(s);
@@ -1472,7 +1521,7 @@ bvhcd_status Front::contacts(int which, float *out, int64_t cap, int64_t *count,
 bvhcd_status Front::export_front(int which, int32_t *out, int64_t cap, int64_t *count, cudaStream_t s) {
     if (which < 0 || which > 1) return BVHCD_INVALID_ARG;
     unsigned h[C_NUM];
-    FR_TRY(cudaMemcpyAsync(h, bvh_->counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaMemcpyAsync(h, counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
     FR_TRY(cudaStreamSynchronize(s));
     int64_t n = h[2 * cur_ + which];
     if (n > fcap_[which]) n = fcap_[which];

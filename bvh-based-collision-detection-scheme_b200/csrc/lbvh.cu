@@ -1389,6 +1389,7 @@ bvhcd_status LBvh::build(cudaStream_t s) {
             k_single_leaf<<<1, 32, 0, s>>>(lca_.as<int>(), lrec_.as<float4>()); note_launch();
             BV_TRY(cudaGetLastError());
             built_ = true;
+            topo_epoch_++;
             return refit_plan(s, true);
         }
     }
@@ -1414,6 +1415,7 @@ bvhcd_status LBvh::build(cudaStream_t s) {
                                                        topo_.as<int4>(), nrange_.as<int2>(), height_.as<int>()); note_launch();
     BV_TRY(cudaGetLastError());
     built_ = true;
+    topo_epoch_++;
     return refit_plan(s, true);
 }
 
@@ -1444,6 +1446,7 @@ bvhcd_status LBvh::copy_state_from(const LBvh &src, cudaStream_t s) {
     fptr_ = src.fptr_ == src.faces_.as<int>() ? faces_.as<int>() : src.fptr_;
     S_ = src.S_; ntiles_ = src.ntiles_; h_off_ = src.h_off_;
     epoch_++;
+    topo_epoch_++;
     return cuda_status(cudaGetLastError());
 }
 
@@ -1613,6 +1616,7 @@ bvhcd_status LBvh::restructure(cudaStream_t s) {
                                                  nrange_.as<int2>(), lrec_.as<float4>()); note_launch();
     BV_TRY(cudaGetLastError());
     opt_tag_ = 1;
+    topo_epoch_++;
     // the confined rebuild can change the heights of the subtrees' ancestors
     return refit_plan(s, false);
 }

@@ -124,6 +124,9 @@ class LBvh {
     int V() const { return V_; }
     bool built() const { return built_; }
     int opt_tag() const { return opt_tag_; }
+    // advances whenever the topology (and so the leaf order) changes: build,
+    // restructure, state copy
+    int topo_epoch() const { return topo_epoch_; }
     const float *verts() const { return vptr_; }
     const int *faces() const { return fptr_; }
     bool restr_enabled() const { return cfg_.enable_restr != 0; }
@@ -175,7 +178,7 @@ class LBvh {
     DBuf intrange_, rtroot_, intmark_, extrange_, extmark_, leafroot_, flagbuf_;
     // batched scenes: S_ scenes, triangle offsets, per-triangle scene id,
     // per-slot scene id, per-scene boxes, box-reduction tiles
-    int S_ = 1, ntiles_ = 0, epoch_ = 0;
+    int S_ = 1, ntiles_ = 0, epoch_ = 0, topo_epoch_ = 0;
     std::vector<int> h_off_;
     DBuf scene_of_, leafscene_, sbox_, tiles_;
     DBuf ctr_;
@@ -190,7 +193,9 @@ class LBvh {
 
 class Front {
   public:
-    Front(LBvh *bvh, const bvhcd_front_config &cfg) : bvh_(bvh), cfg_(cfg) {}
+    // trav: null for an intra front (the BVH's own triangles traverse it), or
+    // the BVH whose triangles traverse `bvh` (an inter front)
+    Front(LBvh *bvh, const bvhcd_front_config &cfg, LBvh *trav = nullptr) : bvh_(bvh), trav_(trav), cfg_(cfg) {}
     ~Front();
     bvhcd_status init();
     bvhcd_status maintain(bvhcd_front_op op, cudaStream_t s);
@@ -204,16 +209,18 @@ class Front {
 
     // Host-side state a maintain() call advances (see LBvh::HostState);
     // int_swapped: balance() exchanged the internal-front buffers of the two
-    // sets an odd number of times.
+    // sets an odd number of times; log_counted: the log's per-node counts
+    // describe the current front (a balance leaves only its begins valid).
     struct HostState {
         int cur, last_op;
-        bool has_front, int_swapped;
+        bool has_front, int_swapped, log_counted;
     };
-    HostState host_state() const { return HostState{cur_, last_op_, has_front_, int_swapped_}; }
+    HostState host_state() const { return HostState{cur_, last_op_, has_front_, int_swapped_, log_counted_}; }
     void set_host_state(const HostState &h) {
         cur_ = h.cur;
         last_op_ = h.last_op;
         has_front_ = h.has_front;
+        log_counted_ = h.log_counted;
         if (h.int_swapped != int_swapped_) {
             std::swap(front_[0][0], front_[1][0]);
             int_swapped_ = h.int_swapped;
@@ -221,6 +228,9 @@ class Front {
     }
     bool auto_grow() const { return cfg_.auto_grow != 0; }
     LBvh *bvh() const { return bvh_; }
+    bool inter() const { return trav_ != nullptr; }
+    const LBvh *trav() const { return trav_ ? trav_ : bvh_; }
+    unsigned *counters() const { return fctr_.as<unsigned>(); }
     bvhcd_status copy_state_from(const Front &src, cudaStream_t s);
     const FrontLog front_log() const { return log(); }
     // the front-quality check of an UPDATE (checkFrontQuality) marks
@@ -250,6 +260,9 @@ class Front {
     FrontLog log() const;
 
     LBvh *bvh_;
+    LBvh *trav_ = nullptr;
+    int seen_epoch_[2] = {-1, -1};  // topology epochs of bvh_ and trav() at the last generation
+    DBuf fctr_;                     // this front's device counters (CounterSlot)
     bvhcd_front_config cfg_;
     int capT_ = 0;
     int cur_ = 0;  // which buffer set holds the current front
@@ -263,6 +276,7 @@ class Front {
     int shape_epoch_ = 0;
     bool has_front_ = false;
     bool int_swapped_ = false;
+    bool log_counted_ = true;
     bool quality_check_ = true;
     DBuf front_[2][2];  // [set][0 int, 1 ext] int2 entries
     int64_t fcap_[2] = {0, 0};

@@ -164,6 +164,22 @@ bvhcd_status bvhcd_bvh_export(const bvhcd_bvh *bvh, int32_t *inode, float *ibox,
  * applyCpResults(uint*, uint2*) (:63-67) -> bvhcd_front_pairs(which = 0). */
 bvhcd_status bvhcd_front_create(bvhcd_bvh *bvh, const bvhcd_front_config *cfg,
                                 bvhcd_front **out);
+/* Inter-object front: replaces BvttFrontLooseInter
+ * (Mine/collision/bvtt_front/BvttFrontLooseInter.cu:16-331) over a deformable
+ * BVH and a rigid one (LBvhRigid, Mine/collision/lbvh/LBvhRigid.cu: the same
+ * build and refit without restructuring -- an ordinary BVH handle here).  The
+ * rigid BVH's triangles traverse the deformable BVH; every front operation of
+ * bvhcd_front_maintain applies (RESTRUCTURE, and a build or restructure of
+ * either BVH, regenerate the front).  Pairs are (deformable triangle id, rigid
+ * triangle id), as the reference writes them; every rigid triangle takes part
+ * (the reference's generation skips the last one).  narrow_phase runs the
+ * triangle test across the two meshes (the reference's inter front has no
+ * narrow phase); cull_adjacent does not apply; precision must be 0.  Both
+ * BVHs must hold one scene and stay alive, unmoved, while the front lives;
+ * not for bvhcd_frame_graph, bvhcd_front_contacts, bvhcd_front_copy_state or
+ * the learner. */
+bvhcd_status bvhcd_front_create_inter(bvhcd_bvh *deformable, bvhcd_bvh *rigid, const bvhcd_front_config *cfg,
+                                      bvhcd_front **out);
 bvhcd_status bvhcd_front_destroy(bvhcd_front *front);
 bvhcd_status bvhcd_front_maintain(bvhcd_front *front, bvhcd_front_op op, void *stream);
 /* Synchronises `stream`. */

@@ -249,6 +249,7 @@ struct orc_pipe {
     int updated, opt_tag, num_rt_subtree, num_rt_int;
     /* front log (FlOrderLog) */
     unsigned *intcnt, *extcnt, *intbeg, *extbeg, *intback, *extback;
+    int log_stale;            /* counts split by a balance; begins still hold */
     float *snapshot;
     /* fronts (current) and pairs */
     pvec intf, extf, pairs, hits;
@@ -725,6 +726,7 @@ static void orc_reorder_fronts(orc_pipe *p) {
     pv_free(&p->intf); pv_free(&p->extf);
     p->intf = ni;
     p->extf = ne;
+    p->log_stale = 0;
 }
 
 /* frontSnapshot (BvttFrontGenerateKernels.cu:26-32) */
@@ -866,8 +868,14 @@ static void orc_keep(orc_pipe *p) {
  * non-overlapping entries fill each node bucket from the front, overlapping
  * ones from the back and are traversed; the external front is kept. */
 static void orc_balance(orc_pipe *p) {
-    log_prepare(p);
+    /* A balance splits each node's count into front and back halves and
+     * clears the external counts without moving an entry to another node,
+     * so the begins it started from still hold for a following balance
+     * (the reference rescans the split counts there, :286, and overlaps
+     * entries; its schedules never run two balances in a row). */
+    if (!p->log_stale) log_prepare(p);
     log_clear(p);
+    p->log_stale = 1;
     p->pairs.n = 0;
     pvec ni = {0};
     pv_reserve(&ni, p->intf.n);

@@ -136,6 +136,42 @@ def narrow(pairs, faces, pos, exact=False):
     return hit
 
 
+def _joined(fa, va, fb, vb):
+    fa = np.asarray(fa, dtype=np.int32).reshape(-1, 3)
+    fb = np.asarray(fb, dtype=np.int32).reshape(-1, 3)
+    va = np.asarray(va, dtype=np.float32).reshape(-1, 3)
+    vb = np.asarray(vb, dtype=np.float32).reshape(-1, 3)
+    return np.concatenate([fa, fb + va.shape[0]]), np.concatenate([va, vb])
+
+
+def brute_inter_pairs(fa, va, fb, vb) -> np.ndarray:
+    """Every (a, b), a a triangle of mesh A and b one of mesh B, whose FP32
+    AABBs overlap (touching counts), as sorted rows.  This is the pair set of
+    an inter front over a deformable mesh A and an obstacle mesh B: the
+    obstacle's primitives traverse A's BVH from the root and report each
+    overlapping leaf, with no adjacency culling between the two meshes
+    (genLooseInterFrontsWithLog, Mine/collision/bvtt_front/
+    BvttFrontGenerateKernels.cu:92-124; pureBvhInterCD, BvhCDKernels.cu:51-76).
+    Sweep and prune over the two meshes joined, keeping the pairs across."""
+    faces, pos = _joined(fa, va, fb, vb)
+    ta = np.asarray(fa).reshape(-1, 3).shape[0]
+    p = brute_pairs(faces, pos, False)
+    q = p[(p[:, 0] < ta) & (p[:, 1] >= ta)].copy()
+    q[:, 1] -= ta
+    return q
+
+
+def inter_narrow(pairs, fa, va, fb, vb) -> np.ndarray:
+    """FP32 SAT hit mask over (a, b) pairs of an inter front, the obstacle's
+    triangle b as the first operand, as the inter front's narrow phase calls
+    the test (the traversing primitive first)."""
+    faces, pos = _joined(fa, va, fb, vb)
+    ta = np.asarray(fa).reshape(-1, 3).shape[0]
+    pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
+    q = np.stack([pairs[:, 1] + ta, pairs[:, 0]], axis=1)
+    return narrow(q, faces, pos)
+
+
 def ref_narrow(pairs, faces, pos):
     R = ref_lib()
     if R is None:

@@ -9,7 +9,7 @@ sides, so its hit set must match exactly too.
 import numpy as np
 import pytest
 
-from treecheck import check_tree
+from treecheck import check_tree, pick_roots
 
 pytestmark = pytest.mark.gpu
 
@@ -91,19 +91,23 @@ def test_front_is_node_ordered(cuda, lib_built, cloth_c1):
         assert np.all(np.diff(nodes) >= 0), "counting sort must order entries by node"
 
 
-def _pick_roots(tree, frac=0.25, lo=16, hi=512):
-    inode = tree["inode"]
-    size = inode[:, 5] - inode[:, 4] + 1
-    covered = np.zeros(inode.shape[0] + 1, bool)
-    chosen, total = [], 0
-    for d in range(inode.shape[0]):
-        if lo <= size[d] <= hi and not covered[d]:
-            chosen.append(d)
-            covered[d:d + size[d] - 1] = True
-            total += size[d] - 1
-            if total >= frac * inode.shape[0]:
-                break
-    return np.array(chosen, np.int32)
+def test_any_operation_order(cuda, lib_built, oracle, cloth_c1):
+    """Front operations in orders the reference's schedules never produce: two
+    balances in a row, keeps between balances, a balance right after
+    generation.  Fronts (as multisets) and pairs equal the oracle's; pairs
+    equal the brute-force set."""
+    faces, frames = cloth_c1
+    order = [(0, 1), (1, 3), (1, 3), (1, 4), (1, 3), (1, 2), (1, 3), (1, 4), (1, 4), (1, 3), (1, 3), (1, 2)]
+    bvh, front = _new(lib_built, faces.shape[0], frames[0].shape[0], restr=False)
+    p = oracle.Pipeline(False, True, True)
+    for f, (b, fr) in enumerate(order):
+        bvh.maintain(b, frames[f], faces)
+        front.maintain(fr)
+        p.frame(faces, frames[f], b, fr)
+        for which in (0, 1):
+            assert np.array_equal(sorted_rows(front.export(which)), sorted_rows(p.front(which))), (f, which)
+        assert np.array_equal(canon(front.pairs()), oracle.brute_pairs(faces, frames[f], 1)), f
+        assert np.array_equal(canon(front.pairs(narrow=True)), canon(p.pairs(narrow=True))), f
 
 
 def test_restructure_parity(cuda, lib_built, oracle, cloth_c1):
@@ -122,7 +126,7 @@ def test_restructure_parity(cuda, lib_built, oracle, cloth_c1):
         assert not check_tree(bvh.export(), T)
         assert np.array_equal(canon(front.pairs()), canon(p.pairs())), f
         if f == 2:
-            roots = _pick_roots(p.tree())
+            roots = pick_roots(p.tree())
             bvh.request_restructure(roots)
             p.mark_restructure(roots)
         if f == 3:

@@ -6,7 +6,7 @@ checks."""
 import numpy as np
 import pytest
 
-from treecheck import check_tree
+from treecheck import check_tree, pick_roots
 
 
 def _run_pipeline(po, faces, frames, cull, restr=True, marks=()):
@@ -36,6 +36,22 @@ def test_pipeline_pairs_equal_brute_force(oracle, cloth_c1, cull):
         assert np.array_equal(hits, pairs[keep])
 
 
+# front operations in orders the reference's schedules never produce: two
+# balances in a row, keeps between balances, a balance right after generation
+ANY_ORDER = [(0, 1), (1, 3), (1, 3), (1, 4), (1, 3), (1, 2), (1, 3), (1, 4), (1, 4), (1, 3), (1, 3), (1, 2)]
+
+
+def test_pipeline_any_operation_order(oracle, cloth_c1):
+    faces, frames = cloth_c1
+    p = oracle.Pipeline(False, True, True)
+    for f, (b, fr) in enumerate(ANY_ORDER):
+        p.frame(faces, frames[f], b, fr)
+        assert np.array_equal(oracle.canon_pairs(p.pairs()), oracle.brute_pairs(faces, frames[f], 1)), f
+        for which in (0, 1):
+            fr_ = p.front(which)
+            assert len(np.unique(fr_, axis=0)) == len(fr_), (f, which)
+
+
 def test_schedule_table(oracle):
     # STATIC_MANDATORY with divergent marks, BenchmarkLogic.hpp:102-117
     got = [oracle.schedule(f) for f in range(26)]
@@ -48,24 +64,9 @@ def test_schedule_table(oracle):
     assert got == exp
 
 
-def _pick_roots(tree, frac=0.25, lo=16, hi=512):
-    inode = tree["inode"]
-    size = inode[:, 5] - inode[:, 4] + 1
-    covered = np.zeros(inode.shape[0] + 1, bool)
-    chosen, total = [], 0
-    for d in range(inode.shape[0]):
-        if lo <= size[d] <= hi and not covered[d]:
-            chosen.append(d)
-            covered[d:d + size[d] - 1] = True
-            total += size[d] - 1
-            if total >= frac * inode.shape[0]:
-                break
-    return np.array(chosen, np.int32)
-
-
 def test_restructure_keeps_pairs_and_tree(oracle, cloth_c1):
     faces, frames = cloth_c1
-    res = _run_pipeline(oracle, faces, frames[:6], 1, marks={2: _pick_roots})
+    res = _run_pipeline(oracle, faces, frames[:6], 1, marks={2: pick_roots})
     info, pairs, _, tree = res[3]
     assert info["opt_tag"] == 1, "the marked subtrees must be restructured"
     assert info["num_rt_int"] * 8 >= faces.shape[0] - 1
@@ -77,7 +78,7 @@ def test_restructure_keeps_pairs_and_tree(oracle, cloth_c1):
     codes = tree["codes"]
     leaf_root = np.zeros(faces.shape[0], np.int64)
     inode = tree["inode"]
-    for r in _pick_roots(res[2][3]):
+    for r in pick_roots(res[2][3]):
         lo, hi = inode[r, 4], inode[r, 5]
         assert np.all(np.diff(codes[lo:hi + 1].astype(np.int64)) >= 0)
 
@@ -85,7 +86,7 @@ def test_restructure_keeps_pairs_and_tree(oracle, cloth_c1):
 def test_restructure_decision_thresholds(oracle, cloth_c1):
     faces, frames = cloth_c1
     # a handful of marked nodes: fewer than 1/8 of the internal nodes -> refit
-    res = _run_pipeline(oracle, faces, frames[:5], 1, marks={2: lambda t: _pick_roots(t, frac=0.01)})
+    res = _run_pipeline(oracle, faces, frames[:5], 1, marks={2: lambda t: pick_roots(t, frac=0.01)})
     assert res[3][0]["opt_tag"] == 0
     # more than half -> rebuild
     res = _run_pipeline(oracle, faces, frames[:5], 1, marks={2: lambda t: np.array([0], np.int32)})
@@ -154,3 +155,37 @@ def test_morton_codes_known_values(oracle):
     codes = np.zeros(2, np.uint32)
     oracle.lib().orc_morton_codes(2, faces, verts, box, codes)
     assert codes[0] == 0 and codes[1] == (1 << 30) - 1
+
+
+def _boxes(faces, verts):
+    t = np.asarray(verts, np.float32)[np.asarray(faces)]
+    return t.min(axis=1), t.max(axis=1)
+
+
+def test_inter_pairs_equal_all_pairs_enumeration(oracle):
+    """The inter oracle (sweep and prune over two joined meshes) against every
+    pair of boxes tested, on meshes whose vertex ids overlap numerically."""
+    rng = np.random.default_rng(21)
+    va = rng.uniform(0, 1, (300, 3)).astype(np.float32)
+    vb = rng.uniform(0.3, 1.3, (200, 3)).astype(np.float32)
+    fa = rng.integers(0, 300, (400, 3)).astype(np.int32)
+    fb = rng.integers(0, 200, (250, 3)).astype(np.int32)
+    va[:, 2] *= 0.05  # thin slabs: a sparse set of pairs
+    vb[:, 2] *= 0.05
+    lo_a, hi_a = _boxes(fa, va)
+    lo_b, hi_b = _boxes(fb, vb)
+    ov = np.all((lo_a[:, None, :] <= hi_b[None, :, :]) & (lo_b[None, :, :] <= hi_a[:, None, :]), axis=2)
+    exp = np.argwhere(ov).astype(np.int64)
+    got = oracle.brute_inter_pairs(fa, va, fb, vb)
+    assert 0 < exp.shape[0] < ov.size
+    assert np.array_equal(got, exp)
+    # the SAT takes the obstacle's triangle first
+    hit = oracle.inter_narrow(got, fa, va, fb, vb)
+    n = got.shape[0]
+    P = vb[fb[got[:, 1]]].reshape(n, 9)
+    Q = va[fa[got[:, 0]]].reshape(n, 9)
+    assert np.array_equal(hit, _narrow_batch(oracle.narrow, P, Q))
+    # either mesh empty: no pairs
+    empty = np.zeros((0, 3), np.int32)
+    assert oracle.brute_inter_pairs(empty, va, fb, vb).shape == (0, 2)
+    assert oracle.brute_inter_pairs(fa, va, empty, vb).shape == (0, 2)

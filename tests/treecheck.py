@@ -71,3 +71,20 @@ def check_tree(t, T):
             np.array_equal(ibox[:, 3:], np.maximum(cb_hi_l, cb_hi_r))):
         errs.append("internal box is not the exact union of its children")
     return errs
+
+
+def pick_roots(tree, frac=0.25, lo=16, hi=512):
+    """Disjoint subtrees (DFS ids) of lo..hi leaves covering about `frac` of
+    the internal nodes: restructure marks for the tests."""
+    inode = tree["inode"]
+    size = inode[:, 5] - inode[:, 4] + 1
+    covered = np.zeros(inode.shape[0] + 1, bool)
+    chosen, total = [], 0
+    for d in range(inode.shape[0]):
+        if lo <= size[d] <= hi and not covered[d]:
+            chosen.append(d)
+            covered[d:d + size[d] - 1] = True
+            total += size[d] - 1
+            if total >= frac * inode.shape[0]:
+                break
+    return np.array(chosen, np.int32)
