@@ -178,12 +178,13 @@ def run_ours(args):
         dist.barrier()
     value = dev_ms / (K * world)
 
-    e2e = roof = batched = fp16 = None
+    e2e = roof = batched = fp16 = inter = None
     if not args.only_value:
         e2e = e2e_pass(bvhcd, torch, pipeline, host, faces, dfaces, flush, hits_host, stream, W, K, V, world)
         # roofline of the dominant stage, from a stage-timed replay
         roof = roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
         fp16 = fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
+        inter = inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, st)
     learned = None
     if not args.only_value and not args.no_batched:
         del dev, host, flush
@@ -216,6 +217,7 @@ def run_ours(args):
             "roofline": roof,
             "clocks": clk.summary(),
             "fp16_node_boxes": fp16,
+            "inter_rigid_obstacle": inter,
             "batched": batched,
             "learned": learned,
         }
@@ -285,6 +287,13 @@ def front_bytes(st_prev, st, T, uniq_nodes):
     return 8 * st_prev + 32 * T + 32 * uniq_nodes + 8 * st
 
 
+# DRAM bytes (read + write) of one k_keep_scan launch on this workload, from an
+# ncu capture (dram__bytes_read.sum 146.3 MB + dram__bytes_write.sum 3.6 MB)
+KEEP_SCAN_DRAM_BYTES = 149.9e6
+KEEP_SCAN_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_keep_scan launch, "
+                         "profiles/k_keep_scan_cloth512_sphere.md")
+
+
 def roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
     """Replays the frames with stage events on; the stage with the largest
     total time is the dominant one.  For it: average event duration per
@@ -319,7 +328,8 @@ def roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
     achieved = algo / (avg_keep_ms * 1e-3) / 1e9 if avg_keep_ms > 0 else 0.0
     return {"kernel": "k_keep (front_keep stage)", "bound": "hbm", "achieved": round(achieved, 1),
             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": kind,
-            "traffic": None, "algorithmic_bytes_per_launch": int(algo),
+            "traffic": KEEP_SCAN_DRAM_BYTES, "traffic_source": KEEP_SCAN_DRAM_SOURCE,
+            "algorithmic_bytes_per_launch": int(algo),
             "avg_launch_ms": round(avg_keep_ms, 4),
             "dominant_stage": dom[0],
             "stage_ms_per_call": {k: round(v[0] / v[1], 4) for k, v in times.items() if v[1]},
@@ -470,6 +480,65 @@ def _batched_on(bvhcd, torch, args, world, B, sizes, off, faces, vidx, T, V, S, 
         "pairs_equal_plain_last_frame": bool(equal),
         "shard": {"ranks": world, "scenes_this_rank": int(S), "triangles_this_rank": int(T)},
     }
+
+
+def inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, single):
+    """The same frames with the sphere as a rigid obstacle: the cloth in its own
+    BVH with an intra front, the sphere in a rigid BVH (refit every frame) and
+    an inter front between them, both fronts on the reference's schedule.
+    Device ms per frame, timed as `value`; the last frame's pair counts of the
+    two fronts plus the sphere's own (static) pairs must equal the single
+    front's over the joined scene."""
+    Vc = 512 * 512
+    Tc = 2 * 511 * 511
+    assert int(faces[:Tc].max()) < Vc and int(faces[Tc:].min()) >= Vc
+    cfaces = dfaces[:Tc].contiguous()
+    sfaces = (dfaces[Tc:] - Vc).contiguous()
+    Ts, Vs = faces.shape[0] - Tc, dev.shape[1] - Vc
+    cbvh = bvhcd.LBvh(Tc, Vc, enable_restr=True)
+    sbvh = bvhcd.LBvh(Ts, Vs, enable_restr=False)
+    intra = bvhcd.BvttFront(cbvh, cull_adjacent=True, narrow_phase=True, auto_grow=False, **CAPS)
+    inter = bvhcd.BvttFront(cbvh, rigid=sbvh, narrow_phase=True, auto_grow=False, **CAPS)
+    own = bvhcd.BvttFront(sbvh, cull_adjacent=True, narrow_phase=True, auto_grow=False, **CAPS)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def frame(f):
+        b, fr = bvhcd.schedule(f)
+        cbvh.maintain(b, dev[f][:Vc], cfaces, stream=stream, faces_static=f > 0)
+        intra.maintain(fr, stream=stream)
+        sbvh.maintain(bvhcd.BVH_BUILD if f == 0 else bvhcd.BVH_REFIT, dev[f][Vc:], sfaces, stream=stream,
+                      faces_static=f > 0)
+        inter.maintain(fr, stream=stream)
+
+    for f in range(W):
+        frame(f)
+    own.maintain(bvhcd.FRONT_GENERATE, stream=stream)  # the static sphere's own pairs, once
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    torch.cuda.synchronize()
+    for i in range(K):
+        flush.zero_()
+        starts[i].record(stream)
+        frame(W + i)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    ms = float(sum(a.elapsed_time(b) for a, b in zip(starts, ends))) / K
+    si, sx, so = intra.stats(), inter.stats(), own.stats()
+    if si["overflow"] or sx["overflow"] or so["overflow"]:
+        raise RuntimeError(f"inter leg overflow: {si} {sx} {so}")
+    pairs = [si["broad_pairs"] + sx["broad_pairs"] + so["broad_pairs"],
+             si["narrow_hits"] + sx["narrow_hits"] + so["narrow_hits"]]
+    for h in (own, inter, intra):
+        h.close()
+    sbvh.close()
+    cbvh.close()
+    return {"workload": f"cloth 512x512 ({Tc} triangles, own BVH, intra front) with the icosphere ({Ts} triangles) "
+                        "as a rigid obstacle BVH refit every frame, inter front between them",
+            "value": round(ms, 4), "unit": "ms/frame",
+            "pairs_last_frame": {"cloth_self": [si["broad_pairs"], si["narrow_hits"]],
+                                 "cloth_sphere": [sx["broad_pairs"], sx["narrow_hits"]],
+                                 "sphere_self": [so["broad_pairs"], so["narrow_hits"]]},
+            "pairs_equal_single_front": pairs == [single["broad_pairs"], single["narrow_hits"]]}
 
 
 def fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):

@@ -483,25 +483,41 @@ __global__ void __launch_bounds__(kB) k_balance_scan(FArgs a) {
     em_close(a, em);
 }
 
-// pureReorderLooseFrontsWithLog (BvttFrontReorderKernels.cu:12-24): counting
-// sort scatter of both fronts by node id.  Holes left by chunked emission are
-// skipped; the sorted fronts' sizes are the per-node count totals.
+// pureReorderLooseFrontsWithLog (BvttFrontReorderKernels.cu:12-24): a
+// counting sort scatter of both fronts by node.  Holes left by chunked
+// emission are skipped; the sorted fronts' sizes are the per-node count
+// totals.
+//
+// The sort key is the node's group of 2^kReorderShift consecutive DFS ids,
+// not the node itself: the order only serves the locality of the scans that
+// read the front next (their node records then come from a few lines per
+// warp), and the per-node counts the emission kept are what the quality
+// check, the snapshot and a balance's buckets use.  A group's run starts at
+// the begin of its first node (the scan of the per-node counts), so no count
+// is recomputed and the counts stay as the emission left them.
 //
 // Tiles of kReorderTile entries: each CTA first groups its tile by key
-// (node, internal or external front) in a shared-memory hash table, taking
+// (group, internal or external front) in a shared-memory hash table, taking
 // each entry's rank within its key; then one global atomic per distinct key
 // reserves the key's run in the sorted front; then every entry is written at
-// run start + rank.  Neighbouring primitives share most front nodes, so a
-// tile holds far fewer keys than entries: the cursor atomics (which
-// serialise on the nodes near the root) drop by that factor, and a key's
-// entries land next to each other.
+// run start + rank.  Neighbouring primitives share most front nodes and a
+// group holds several nodes, so a tile holds far fewer keys than entries:
+// the cursor atomics (which serialise on the groups near the root) drop by
+// that factor, and a key's entries land next to each other.
 constexpr int kReorderThreads = 256;
 constexpr int kReorderPer = 8;                                   // entries per thread per tile
 constexpr int kReorderTile = kReorderThreads * kReorderPer;      // 2048
 constexpr int kReorderSlots = 2 * kReorderTile;                  // hash slots (load factor <= 1/2)
 constexpr unsigned kEmptyKey = 0xffffffffu;
 
-__global__ void __launch_bounds__(kReorderThreads) k_reorder(FArgs a) {
+#ifndef BVHCD_REORDER_SHIFT
+#define BVHCD_REORDER_SHIFT 2
+#endif
+constexpr int kReorderShift = BVHCD_REORDER_SHIFT;  // 4 nodes (128 bytes of node records) per group
+
+inline size_t reorder_groups(int T) { return ((size_t)T >> kReorderShift) + 2; }
+
+__global__ void __launch_bounds__(kReorderThreads) k_reorder(FArgs a, unsigned *cur_int, unsigned *cur_ext) {
     __shared__ unsigned skey[kReorderSlots], scnt[kReorderSlots], sbase[kReorderSlots];
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
@@ -529,7 +545,7 @@ __global__ void __launch_bounds__(kReorderThreads) k_reorder(FArgs a) {
         for (int j = 0; j < kReorderPer; j++) {
             slot[j] = kEmptyKey;
             if (e[j].x == -1) continue;  // hole (a tagged entry is never -1: its index is below 2^31 - 1)
-            const unsigned key = ((unsigned)e[j].y << 1) | ((unsigned)e[j].x >> 31);
+            const unsigned key = (((unsigned)e[j].y >> kReorderShift) << 1) | ((unsigned)e[j].x >> 31);
             unsigned h = (key * 2654435761u) >> 20;  // 12 bits: kReorderSlots = 4096
             for (int probe = 0; probe < kReorderSlots; probe++, h = (h + 1) & (kReorderSlots - 1)) {
                 const unsigned prev = atomicCAS(&skey[h], kEmptyKey, key);
@@ -542,9 +558,10 @@ __global__ void __launch_bounds__(kReorderThreads) k_reorder(FArgs a) {
         for (int i = threadIdx.x; i < kReorderSlots; i += kReorderThreads) {
             const unsigned key = skey[i];
             if (key == kEmptyKey) continue;
-            const int node = (int)(key >> 1);
-            if (key & 1u) sbase[i] = a.log.extbeg[node] + atomicAdd(a.log.extcnt + node, scnt[i]);
-            else sbase[i] = a.log.intbeg[node] + atomicAdd(a.log.intcnt + node, scnt[i]);
+            const unsigned g = key >> 1;
+            const unsigned first = g << kReorderShift;
+            if (key & 1u) sbase[i] = a.log.extbeg[first] + atomicAdd(cur_ext + g, scnt[i]);
+            else sbase[i] = a.log.intbeg[first] + atomicAdd(cur_int + g, scnt[i]);
         }
         __syncthreads();
 #pragma unroll
@@ -881,7 +898,7 @@ Front::~Front() {
     for (auto &set : front_)
         for (auto &b : set) b.release();
     DBuf *bufs[] = {&pairs_, &hits_, &outbuf_, &work_, &intcnt_, &extcnt_, &intbeg_, &extbeg_, &intback_,
-                    &extback_, &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_, &fctr_};
+                    &extback_, &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_, &fctr_, &rcur_};
     for (DBuf *b : bufs) b->release();
 }
 
@@ -921,6 +938,7 @@ bvhcd_status Front::ensure_node_capacity(int T) {
     FR_TRY(extback_.reserve(sizeof(unsigned) * n));
     FR_TRY(snapshot_.reserve(sizeof(float) * n));
     FR_TRY(scratch_.reserve(scan_scratch_bytes((int64_t)n)));
+    FR_TRY(rcur_.reserve(sizeof(unsigned) * 2 * reorder_groups(T)));
     FR_TRY(cudaMemset(intcnt_.p, 0, sizeof(unsigned) * n));
     FR_TRY(cudaMemset(extcnt_.p, 0, sizeof(unsigned) * n));
     FR_TRY(cudaMemset(intbeg_.p, 0, sizeof(unsigned) * n));
@@ -993,7 +1011,8 @@ bvhcd_status Front::reorder(cudaStream_t s) {
     const int T = bvh_->T();
     FrontLog l = log();
     FR_TRY(log_prepare(l, T, scratch_.p, s));
-    FR_TRY(log_clear(l, T, s));
+    const size_t ng = reorder_groups(T);
+    FR_TRY(cudaMemsetAsync(rcur_.p, 0, sizeof(unsigned) * 2 * ng, s));
     FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
     const int nx = 1 - cur_;
     a.in_int = front_[nx][0].as<int2>(); a.in_ext = front_[nx][1].as<int2>();
@@ -1001,8 +1020,10 @@ bvhcd_status Front::reorder(cudaStream_t s) {
     a.in_int_slot = 2 * nx; a.in_ext_slot = 2 * nx + 1;
     a.out_int_slot = 2 * cur_; a.out_ext_slot = 2 * cur_ + 1;
     a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
-    k_reorder<<<RESIDENT_B(k_reorder, kReorderThreads), kReorderThreads, 0, s>>>(a); note_launch();
-    log_counted_ = true;  // the scatter counted every entry again
+    k_reorder<<<RESIDENT_B(k_reorder, kReorderThreads), kReorderThreads, 0, s>>>(a, rcur_.as<unsigned>(),
+                                                                                 rcur_.as<unsigned>() + ng);
+    note_launch();
+    log_counted_ = true;  // the emission before it counted every entry
     return cuda_status(cudaGetLastError());
 }
 

@@ -283,6 +283,7 @@ class Front {
     DBuf pairs_, hits_, outbuf_, work_, cbuf_, cflag_, cscratch_;
     int64_t pcap_ = 0;
     DBuf intcnt_, extcnt_, intbeg_, extbeg_, intback_, extback_, snapshot_, scratch_, counts64_;
+    DBuf rcur_;  // reorder cursors, one per group of 2^kReorderShift nodes and front
 };
 
 }  // namespace bvhcd

@@ -88,7 +88,8 @@ def test_front_is_node_ordered(cuda, lib_built, cloth_c1):
     front.maintain(lib_built.FRONT_GENERATE)
     for which in (0, 1):
         nodes = front.export(which)[:, 1]
-        assert np.all(np.diff(nodes) >= 0), "counting sort must order entries by node"
+        # the counting sort orders entries by groups of 16 consecutive node ids
+        assert np.all(np.diff(nodes >> 4) >= 0), "counting sort must order entries by node group"
 
 
 def test_any_operation_order(cuda, lib_built, oracle, cloth_c1):
