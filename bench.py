@@ -178,13 +178,14 @@ def run_ours(args):
         dist.barrier()
     value = dev_ms / (K * world)
 
-    e2e = roof = batched = fp16 = inter = None
+    e2e = roof = batched = fp16 = inter = boxes = None
     if not args.only_value:
         e2e = e2e_pass(bvhcd, torch, pipeline, host, faces, dfaces, flush, hits_host, stream, W, K, V, world)
         # roofline of the dominant stage, from a stage-timed replay
         roof = roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
         fp16 = fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
         inter = inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, st)
+        boxes = box_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
     learned = None
     if not args.only_value and not args.no_batched:
         del dev, host, flush
@@ -218,6 +219,7 @@ def run_ours(args):
             "clocks": clk.summary(),
             "fp16_node_boxes": fp16,
             "inter_rigid_obstacle": inter,
+            "box_scene": boxes,
             "batched": batched,
             "learned": learned,
         }
@@ -539,6 +541,52 @@ def inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, single):
                                  "cloth_sphere": [sx["broad_pairs"], sx["narrow_hits"]],
                                  "sphere_self": [so["broad_pairs"], so["narrow_hits"]]},
             "pairs_equal_single_front": pairs == [single["broad_pairs"], single["narrow_hits"]]}
+
+
+def box_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
+    """The same frames given as primitive boxes (ARCSimSceneData input): each
+    triangle's box swept over frames f and f + 1, computed on the device
+    outside the timed region as a simulator would hand them over, read in
+    place (FP32).  Broad phase only (a box scene has no triangles to test)."""
+    F = dev.shape[0]
+    fl = dfaces.long()
+    boxes = torch.empty((F, T, 6), dtype=torch.float32, device="cuda")
+    for f in range(F):
+        a = dev[f][fl]                      # T x 3 x 3
+        b = dev[min(f + 1, F - 1)][fl]
+        boxes[f, :, :3] = torch.minimum(a.amin(dim=1), b.amin(dim=1))
+        boxes[f, :, 3:] = torch.maximum(a.amax(dim=1), b.amax(dim=1))
+    bvh = bvhcd.LBvh(T, 0, enable_restr=True)
+    front = bvhcd.BvttFront(bvh, cull_adjacent=True, narrow_phase=False, auto_grow=False, **CAPS)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def frame(f):
+        b, fr = bvhcd.schedule(f)
+        bvh.maintain_boxes(b, boxes[f], dfaces, stream=stream, faces_static=f > 0)
+        front.maintain(fr, stream=stream)
+
+    for f in range(W):
+        frame(f)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    torch.cuda.synchronize()
+    for i in range(K):
+        flush.zero_()
+        starts[i].record(stream)
+        frame(W + i)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    ms = float(sum(a.elapsed_time(b) for a, b in zip(starts, ends))) / K
+    st = front.stats()
+    if st["overflow"]:
+        raise RuntimeError(f"box leg overflow: {st}")
+    front.close()
+    bvh.close()
+    del boxes
+    torch.cuda.empty_cache()
+    return {"workload": f"the bench frames as {T} swept triangle boxes (frames f and f + 1), FP32, device-resident",
+            "value": round(ms, 4), "unit": "ms/frame", "narrow_phase": False,
+            "front_sizes_last_frame": [st["int_front"], st["ext_front"]], "pairs_last_frame": st["broad_pairs"]}
 
 
 def fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):

@@ -29,7 +29,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "capacit
 EXPORTED = [
     "bvhcd_status_string", "bvhcd_device_check", "bvhcd_bvh_create", "bvhcd_bvh_destroy",
     "bvhcd_bvh_maintain", "bvhcd_bvh_sizes", "bvhcd_bvh_opt_tag", "bvhcd_bvh_export",
-    "bvhcd_bvh_request_restructure", "bvhcd_bvh_stage_positions",
+    "bvhcd_bvh_request_restructure", "bvhcd_bvh_stage_positions", "bvhcd_bvh_maintain_boxes",
     "bvhcd_front_create", "bvhcd_front_create_inter", "bvhcd_front_destroy", "bvhcd_front_maintain", "bvhcd_front_stats_get",
     "bvhcd_front_pairs", "bvhcd_front_device_results", "bvhcd_front_export",
     "bvhcd_schedule_heuristic", "bvhcd_frame", "bvhcd_profile_enable", "bvhcd_profile_read",
@@ -73,6 +73,11 @@ class Scene(ctypes.Structure):
     _fields_ = [("pos", ctypes.c_void_p), ("faces", ctypes.c_void_p),
                 ("num_vertices", ctypes.c_int32), ("num_faces", ctypes.c_int32),
                 ("on_device", ctypes.c_int32), ("faces_static", ctypes.c_int32)]
+
+
+class BoxScene(ctypes.Structure):
+    _fields_ = [("boxes", ctypes.c_void_p), ("faces", ctypes.c_void_p), ("num_faces", ctypes.c_int32),
+                ("boxes_f64", ctypes.c_int32), ("on_device", ctypes.c_int32), ("faces_static", ctypes.c_int32)]
 
 
 class LaunchShapes(ctypes.Structure):
@@ -124,6 +129,7 @@ def lib():
             "bvhcd_bvh_export": (ctypes.c_int, [vp] + [vp] * 7 + [vp]),
             "bvhcd_bvh_request_restructure": (ctypes.c_int, [vp, vp, i32, vp]),
             "bvhcd_bvh_stage_positions": (ctypes.c_int, [vp, vp, i32, vp, ctypes.POINTER(vp)]),
+            "bvhcd_bvh_maintain_boxes": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(BoxScene), vp]),
             "bvhcd_front_create": (ctypes.c_int, [vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
             "bvhcd_front_create_inter": (ctypes.c_int, [vp, vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
             "bvhcd_front_destroy": (ctypes.c_int, [vp]),
@@ -249,6 +255,29 @@ def _scene(pos, faces, faces_static=False):
     return sc, keep
 
 
+def _box_scene(boxes, faces, faces_static=False):
+    """Box-scene struct (T x 6 boxes, FP32 or FP64; T x 3 faces) plus the
+    objects that keep its buffers alive."""
+    try:
+        import torch
+        is_t = isinstance(boxes, torch.Tensor)
+    except ImportError:
+        is_t = False
+    if is_t:
+        assert boxes.is_cuda and faces.is_cuda, "tensors must live on the GPU"
+        assert boxes.dtype in (torch.float32, torch.float64) and faces.dtype == torch.int32
+        boxes = boxes.contiguous()
+        faces = faces.contiguous()
+        f64 = int(boxes.dtype == torch.float64)
+        return BoxScene(boxes.data_ptr(), faces.data_ptr(), faces.shape[0], f64, 1, int(faces_static)), [boxes, faces]
+    boxes = np.asarray(boxes)
+    f64 = int(boxes.dtype == np.float64)
+    boxes = np.ascontiguousarray(boxes, dtype=np.float64 if f64 else np.float32).reshape(-1, 6)
+    faces = np.ascontiguousarray(faces, dtype=np.int32).reshape(-1, 3)
+    assert boxes.shape[0] == faces.shape[0]
+    return BoxScene(boxes.ctypes.data, faces.ctypes.data, faces.shape[0], f64, 0, int(faces_static)), [boxes, faces]
+
+
 class LBvh:
     """LBvhFixedDeformable: maintain(BUILD | REFIT | UPDATE, scene) per frame."""
 
@@ -280,6 +309,14 @@ class LBvh:
         self._keep = keep
         _check(lib().bvhcd_bvh_maintain(self._h, int(op), ctypes.byref(sc), _stream_ptr(stream)),
                "bvh maintain")
+
+    def maintain_boxes(self, op: int, boxes, faces, stream=None, faces_static=False):
+        """maintain(scheme, ARCSimSceneData): the primitives given as boxes
+        (T x 6: min xyz, max xyz; FP64 boxes are rounded outward to FP32)."""
+        sc, keep = _box_scene(boxes, faces, faces_static)
+        self._keep = keep
+        _check(lib().bvhcd_bvh_maintain_boxes(self._h, int(op), ctypes.byref(sc), _stream_ptr(stream)),
+               "bvh maintain boxes")
 
     def stage_positions(self, pos, copy_stream=None) -> "StagedPositions":
         """bvhcd_bvh_stage_positions: copy the next frame's positions (a

@@ -50,7 +50,7 @@ inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s
 
 bool same_state(const bvhcd::LBvh::HostState &a, const bvhcd::LBvh::HostState &b) {
     return a.T == b.T && a.V == b.V && a.opt_tag == b.opt_tag && a.built == b.built && a.updated == b.updated &&
-           a.vptr == b.vptr && a.fptr == b.fptr;
+           a.box_input == b.box_input && a.vptr == b.vptr && a.bptr == b.bptr && a.fptr == b.fptr;
 }
 bool same_state(const bvhcd::Front::HostState &a, const bvhcd::Front::HostState &b) {
     return a.cur == b.cur && a.last_op == b.last_op && a.has_front == b.has_front && a.int_swapped == b.int_swapped &&
@@ -107,6 +107,11 @@ bvhcd_status bvhcd_bvh_destroy(bvhcd_bvh *bvh) {
 bvhcd_status bvhcd_bvh_maintain(bvhcd_bvh *bvh, bvhcd_bvh_op op, const bvhcd_scene *scene, void *stream) {
     if (!bvh || !scene) return BVHCD_INVALID_ARG;
     return bvh->impl.maintain(op, *scene, as_stream(stream));
+}
+
+bvhcd_status bvhcd_bvh_maintain_boxes(bvhcd_bvh *bvh, bvhcd_bvh_op op, const bvhcd_box_scene *scene, void *stream) {
+    if (!bvh || !scene) return BVHCD_INVALID_ARG;
+    return bvh->impl.maintain_boxes(op, *scene, as_stream(stream));
 }
 
 bvhcd_status bvhcd_bvh_sizes(const bvhcd_bvh *bvh, int32_t *prims, int32_t *ext_nodes, int32_t *int_nodes) {

@@ -120,6 +120,32 @@ __device__ __forceinline__ void tri_box(const float3 &a, const float3 &b, const 
     hi.z = fmaxf(fmaxf(fmaxf(-3.402823466e+38f, a.z), b.z), c.z);
 }
 
+// Where the primitives' boxes come from: triangles (vertex ids and vertex
+// positions), or a scene given as one FP32 box per primitive (min xyz, max
+// xyz; the reference's ARCSimSceneData, Mine/world/Scene.h:39-45), whose
+// faces only give the vertex ids for adjacency culling.
+struct PrimSrc {
+    const int *faces;
+    const float *verts;  // null for a box scene
+    const float *boxes;  // null for triangles
+};
+// box of primitive t (its original id)
+__device__ __forceinline__ void prim_box(const PrimSrc &p, int t, float4 &lo, float4 &hi) {
+    if (p.boxes) {
+        const float *b = p.boxes + 6 * (size_t)t;
+        lo = make_float4(__ldg(b), __ldg(b + 1), __ldg(b + 2), 0.f);
+        hi = make_float4(__ldg(b + 3), __ldg(b + 4), __ldg(b + 5), 0.f);
+    } else {
+        tri_box(load_vert(p.verts, __ldg(p.faces + 3 * (size_t)t)), load_vert(p.verts, __ldg(p.faces + 3 * (size_t)t + 1)),
+                load_vert(p.verts, __ldg(p.faces + 3 * (size_t)t + 2)), lo, hi);
+    }
+}
+// the same from a slot's stored face (x, y, z vertex ids, w original id)
+__device__ __forceinline__ void face_box(const PrimSrc &p, const int4 &f, float4 &lo, float4 &hi) {
+    if (p.boxes) prim_box(p, f.w, lo, hi);
+    else tri_box(load_vert(p.verts, f.x), load_vert(p.verts, f.y), load_vert(p.verts, f.z), lo, hi);
+}
+
 // 30-bit Morton code of a box centre normalised by the scene box
 // (calcMCs, LBvhBuildKernels.cu:76-91; morton3D/expandBits,
 // Mine/utility/CudaDeviceUtils.cu:82-130).  IEEE operations only, no

@@ -1266,6 +1266,8 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     if (op < BVHCD_FRONT_PURE_BVH_CD || op > BVHCD_FRONT_RESTRUCTURE) return BVHCD_INVALID_ARG;
     if (!bvh_->built() || !trav()->built()) return BVHCD_NOT_READY;
     if (inter() && (bvh_->num_scenes() != 1 || trav_->num_scenes() != 1)) return BVHCD_INVALID_ARG;
+    // a box scene has no triangles to test
+    if (cfg_.narrow_phase && (bvh_->box_input() || trav()->box_input())) return BVHCD_INVALID_ARG;
     const int T = bvh_->T();
     bvhcd_status st = ensure_node_capacity(T);
     if (st != BVHCD_OK) return st;
@@ -1499,7 +1501,7 @@ bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, 
 // (which = 1), in the order bvhcd_front_pairs returns them.
 bvhcd_status Front::contacts(int which, float *out, int64_t cap, int64_t *count, int64_t *flagged, bool out_dev,
                              cudaStream_t s) {
-    if (which < 0 || which > 1 || cap < 0 || inter()) return BVHCD_INVALID_ARG;
+    if (which < 0 || which > 1 || cap < 0 || inter() || bvh_->box_input()) return BVHCD_INVALID_ARG;
     const int2 *list = hits_.as<int2>();
     unsigned *ctr = counters();
     const unsigned *cnt = ctr + C_HITS;

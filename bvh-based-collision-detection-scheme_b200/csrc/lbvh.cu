@@ -72,26 +72,20 @@ __device__ __forceinline__ void block_box(float (&mn)[3], float (&mx)[3], float 
     }
 }
 
-__device__ __forceinline__ void box_of_range(int first, int end, int step, const int *__restrict__ faces,
-                                             const float *__restrict__ verts, float (&mn)[3],
+__device__ __forceinline__ void box_of_range(int first, int end, int step, const PrimSrc &p, float (&mn)[3],
                                              float (&mx)[3]) {
     for (int t = first; t < end; t += step) {
-        float3 a = load_vert(verts, __ldg(faces + 3 * (size_t)t));
-        float3 b = load_vert(verts, __ldg(faces + 3 * (size_t)t + 1));
-        float3 c = load_vert(verts, __ldg(faces + 3 * (size_t)t + 2));
         float4 lo, hi;
-        tri_box(a, b, c, lo, hi);
+        prim_box(p, t, lo, hi);
         mn[0] = fminf(mn[0], lo.x); mn[1] = fminf(mn[1], lo.y); mn[2] = fminf(mn[2], lo.z);
         mx[0] = fmaxf(mx[0], hi.x); mx[1] = fmaxf(mx[1], hi.y); mx[2] = fmaxf(mx[2], hi.z);
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_box_partial(int T, const int *__restrict__ faces,
-                                                          const float *__restrict__ verts,
-                                                          float *partial) {
+__global__ void __launch_bounds__(kThreads) k_box_partial(int T, PrimSrc p, float *partial) {
     float mn[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
     float mx[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
-    box_of_range(blockIdx.x * blockDim.x + threadIdx.x, T, gridDim.x * blockDim.x, faces, verts, mn, mx);
+    box_of_range(blockIdx.x * blockDim.x + threadIdx.x, T, gridDim.x * blockDim.x, p, mn, mx);
     __shared__ float out[6];
     block_box(mn, mx, out);
     if (threadIdx.x < 6) partial[6 * blockIdx.x + threadIdx.x] = out[threadIdx.x];
@@ -140,13 +134,12 @@ __global__ void k_sbox_init(int S, float *sbox) {
 // Per-scene boxes: one block per tile {scene, first, end} of one scene's
 // triangles; the tile's box is merged into its scene's with the atomics above
 // (min/max are exact, so the box equals the scene's own reduction).
-__global__ void __launch_bounds__(kThreads) k_sbox_tiles(const int4 *__restrict__ tiles,
-                                                         const int *__restrict__ faces,
-                                                         const float *__restrict__ verts, float *sbox) {
+__global__ void __launch_bounds__(kThreads) k_sbox_tiles(const int4 *__restrict__ tiles, PrimSrc p,
+                                                         float *sbox) {
     const int4 tl = tiles[blockIdx.x];
     float mn[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
     float mx[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
-    box_of_range(tl.y + threadIdx.x, tl.z, blockDim.x, faces, verts, mn, mx);
+    box_of_range(tl.y + threadIdx.x, tl.z, blockDim.x, p, mn, mx);
     __shared__ float out[6];
     block_box(mn, mx, out);
     if (threadIdx.x < 3) atomic_min_f32(sbox + 6 * tl.x + threadIdx.x, out[threadIdx.x]);
@@ -154,16 +147,12 @@ __global__ void __launch_bounds__(kThreads) k_sbox_tiles(const int4 *__restrict_
 }
 
 // 64-bit keys (scene << 30 | 30-bit code of the triangle in its scene's box).
-__global__ void k_morton_seg(int T, const int *__restrict__ faces, const float *__restrict__ verts,
-                             const int *__restrict__ scene_of, const float *__restrict__ sbox,
+__global__ void k_morton_seg(int T, PrimSrc p, const int *__restrict__ scene_of, const float *__restrict__ sbox,
                              unsigned long long *keys, int *vals) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
         const int sc = __ldg(scene_of + t);
-        float3 a = load_vert(verts, __ldg(faces + 3 * (size_t)t));
-        float3 b = load_vert(verts, __ldg(faces + 3 * (size_t)t + 1));
-        float3 c = load_vert(verts, __ldg(faces + 3 * (size_t)t + 2));
         float4 lo, hi;
-        tri_box(a, b, c, lo, hi);
+        prim_box(p, t, lo, hi);
         float box[6];
 #pragma unroll
         for (int k = 0; k < 6; k++) box[k] = __ldg(sbox + 6 * sc + k);
@@ -173,17 +162,13 @@ __global__ void k_morton_seg(int T, const int *__restrict__ faces, const float *
 }
 
 // ---------------------------------------------------------------- build
-__global__ void k_morton(int T, const int *__restrict__ faces, const float *__restrict__ verts,
-                         const float *__restrict__ scene, unsigned *keys, int *vals) {
+__global__ void k_morton(int T, PrimSrc p, const float *__restrict__ scene, unsigned *keys, int *vals) {
     __shared__ float s[6];
     if (threadIdx.x < 6) s[threadIdx.x] = scene[threadIdx.x];
     __syncthreads();
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
-        float3 a = load_vert(verts, __ldg(faces + 3 * (size_t)t));
-        float3 b = load_vert(verts, __ldg(faces + 3 * (size_t)t + 1));
-        float3 c = load_vert(verts, __ldg(faces + 3 * (size_t)t + 2));
         float4 lo, hi;
-        tri_box(a, b, c, lo, hi);
+        prim_box(p, t, lo, hi);
         keys[t] = morton_box(lo, hi, s);
         vals[t] = t;
     }
@@ -193,45 +178,48 @@ __global__ void k_morton(int T, const int *__restrict__ faces, const float *__re
 // Mine/utility/CudaKernelUtils.cu:28-32; buildPrimitives,
 // LBvhBuildKernels.cu:114-133, here storing the vertex ids too;
 // calcExtNodeSplitMetrics, Mine/collision/lbvh/BvhExtNode.cu:128-134).
-__device__ __forceinline__ void write_leaf(int i, int t, unsigned k, int metric_i,
-                                           const int *__restrict__ faces, const float *__restrict__ verts,
+__device__ __forceinline__ void write_leaf(int i, int t, unsigned k, int metric_i, const PrimSrc &p,
                                            int4 *sface, int *primmap, unsigned *code, int *metric,
                                            float4 *lrec) {
-    int4 f = make_int4(__ldg(faces + 3 * (size_t)t), __ldg(faces + 3 * (size_t)t + 1),
-                       __ldg(faces + 3 * (size_t)t + 2), t);
+    int4 f = make_int4(__ldg(p.faces + 3 * (size_t)t), __ldg(p.faces + 3 * (size_t)t + 1),
+                       __ldg(p.faces + 3 * (size_t)t + 2), t);
     sface[i] = f;
     primmap[t] = i;
     code[i] = k;
     metric[i] = metric_i;
     float4 lo, hi;
-    tri_box(load_vert(verts, f.x), load_vert(verts, f.y), load_vert(verts, f.z), lo, hi);
+    face_box(p, f, lo, hi);
     lrec[2 * i] = lo;
     lrec[2 * i + 1] = hi;
 }
 
-__global__ void k_leaves(int T, const unsigned *__restrict__ keys, const int *__restrict__ vals,
-                         const int *__restrict__ faces, const float *__restrict__ verts,
+__global__ void k_leaves(int T, const unsigned *__restrict__ keys, const int *__restrict__ vals, PrimSrc p,
                          int4 *sface, int *primmap, unsigned *code, int *metric, float4 *lrec) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) {
         const unsigned k = keys[i];
-        write_leaf(i, vals[i], k, (i != T - 1) ? split_metric(k, keys[i + 1]) : 33, faces, verts, sface,
-                   primmap, code, metric, lrec);
+        write_leaf(i, vals[i], k, (i != T - 1) ? split_metric(k, keys[i + 1]) : 33, p, sface, primmap, code,
+                   metric, lrec);
     }
 }
 
 // Leaves of a forest: the scene id of every slot goes to leafscene (the
 // metric across a scene boundary is never read: the boundary decides).
 __global__ void k_leaves_seg(int T, const unsigned long long *__restrict__ keys, const int *__restrict__ vals,
-                             const int *__restrict__ faces, const float *__restrict__ verts,
-                             int4 *sface, int *primmap, unsigned *code, int *metric, float4 *lrec,
+                             PrimSrc p, int4 *sface, int *primmap, unsigned *code, int *metric, float4 *lrec,
                              int *leafscene) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) {
         const unsigned long long k = keys[i];
         const unsigned c = (unsigned)(k & 0x3fffffffu);
         leafscene[i] = (int)(k >> 30);
         const int m = (i != T - 1) ? split_metric(c, (unsigned)(keys[i + 1] & 0x3fffffffu)) : 33;
-        write_leaf(i, vals[i], c, m, faces, verts, sface, primmap, code, metric, lrec);
+        write_leaf(i, vals[i], c, m, p, sface, primmap, code, metric, lrec);
     }
+}
+
+// FP64 primitive boxes (min xyz, max xyz) to FP32, rounded outward
+__global__ void k_boxes_f64(int64_t n, const double *__restrict__ in, float *out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (i % 6) < 3 ? __double2float_rd(in[i]) : __double2float_ru(in[i]);
 }
 
 __global__ void k_single_leaf(int *lca, float4 *lrec) {
@@ -808,8 +796,7 @@ __device__ void refit_top(const RefitTop &g, float4 *nrec, float *smem, int *sof
 // One CTA per block of kRefitW leaves: leaf boxes, then the block's local
 // nodes level by level from its level-sorted list, all in shared memory,
 // then its exports; the last CTA to finish runs the crossing nodes.
-__global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *__restrict__ sface,
-                                                            const float *__restrict__ verts,
+__global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *__restrict__ sface, PrimSrc p,
                                                             const int4 *__restrict__ plan,
                                                             const int4 *__restrict__ llist,
                                                             const int2 *__restrict__ llink,
@@ -836,7 +823,7 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
         const int4 f = __ldg(&sface[L0 + t]);
         const int2 lk = __ldg(&llink[L0 + t]);
         float4 lo, hi;
-        tri_box(load_vert(verts, f.x), load_vert(verts, f.y), load_vert(verts, f.z), lo, hi);
+        face_box(p, f, lo, hi);
         box_store6(sb + 6 * t, lo, hi);
         lo.w = __int_as_float(lk.x);
         hi.w = __int_as_float(lk.y);
@@ -966,7 +953,7 @@ __global__ void k_rs_flags(int T, const int *__restrict__ leafroot, unsigned *fl
 }
 // calcRestrMCs + selectPrimitives (:37-66): (subtree root, Morton) keys
 __global__ void k_rs_select(int T, const int *__restrict__ leafroot, const unsigned *__restrict__ pos,
-                            const int4 *__restrict__ sface, const float *__restrict__ verts,
+                            const int4 *__restrict__ sface, PrimSrc p,
                             const float *__restrict__ scene, unsigned long long *keys, int *task,
                             int *vals) {
     __shared__ float sc[6];
@@ -977,7 +964,7 @@ __global__ void k_rs_select(int T, const int *__restrict__ leafroot, const unsig
         if (rt > 0) {
             int4 f = sface[s];
             float4 lo, hi;
-            tri_box(load_vert(verts, f.x), load_vert(verts, f.y), load_vert(verts, f.z), lo, hi);
+            face_box(p, f, lo, hi);
             unsigned q = pos[s];
             keys[q] = ((unsigned long long)(unsigned)rt << 32) | morton_box(lo, hi, sc);
             task[q] = s;
@@ -1327,16 +1314,67 @@ bvhcd_status LBvh::upload(const bvhcd_scene &sc, cudaStream_t s) {
         vptr_ = verts_.as<float>();
         fptr_ = faces_.as<int>();
     }
-    if (built_ && sc.num_faces != T_) built_ = false;
+    // a tree built over a box scene is rebuilt for triangles
+    if (built_ && (sc.num_faces != T_ || box_input_)) built_ = false;
+    box_input_ = false;
+    bptr_ = nullptr;
     T_ = sc.num_faces;
     V_ = sc.num_vertices;
+    return BVHCD_OK;
+}
+
+// ARCSimSceneData input (LBvhFixedDeformable::maintain(scheme, const
+// ARCSimSceneData&), LBvhFixedDeformable.cu:89-112): the primitives' boxes
+// are given.  FP64 boxes are rounded outward, so the FP32 box the tree holds
+// contains the given one (the reference converts to nearest,
+// buildPrimitivesARCSim / refitExtNodeARCSim, LBvhBuildKernels.cu:35-50,
+// LBvhUpdateKernels.cu:11-22).
+bvhcd_status LBvh::upload_boxes(const bvhcd_box_scene &sc, cudaStream_t s) {
+    if (sc.num_faces < 0) return BVHCD_INVALID_ARG;
+    if (sc.num_faces > 0 && (!sc.boxes || !sc.faces)) return BVHCD_INVALID_ARG;
+    bvhcd_status st = ensure_capacity(sc.num_faces, 0);
+    if (st != BVHCD_OK) return st;
+    const size_t T = (size_t)sc.num_faces;
+    const bool convert = sc.boxes_f64 != 0;
+    if (convert || !sc.on_device) BV_TRY(boxes_.reserve(sizeof(float) * 6 * (T > 0 ? T : 1)));
+    if (sc.on_device) {
+        fptr_ = sc.faces;
+        if (convert && T) {
+            k_boxes_f64<<<grid_for((int64_t)(6 * T)), kThreads, 0, s>>>((int64_t)(6 * T),
+                                                                       static_cast<const double *>(sc.boxes),
+                                                                       boxes_.as<float>()); note_launch();
+            BV_TRY(cudaGetLastError());
+        }
+        bptr_ = convert ? boxes_.as<float>() : static_cast<const float *>(sc.boxes);
+    } else {
+        bool same = sc.faces_static && built_ && fptr_ == faces_.as<int>() && T_ == sc.num_faces;
+        if (!same && T)
+            BV_TRY(cudaMemcpyAsync(faces_.p, sc.faces, sizeof(int) * 3 * T, cudaMemcpyHostToDevice, s));
+        fptr_ = faces_.as<int>();
+        if (convert && T) {
+            BV_TRY(boxes64_.reserve(sizeof(double) * 6 * T));
+            BV_TRY(cudaMemcpyAsync(boxes64_.p, sc.boxes, sizeof(double) * 6 * T, cudaMemcpyHostToDevice, s));
+            k_boxes_f64<<<grid_for((int64_t)(6 * T)), kThreads, 0, s>>>((int64_t)(6 * T), boxes64_.as<double>(),
+                                                                       boxes_.as<float>()); note_launch();
+            BV_TRY(cudaGetLastError());
+        } else if (T) {
+            BV_TRY(cudaMemcpyAsync(boxes_.p, sc.boxes, sizeof(float) * 6 * T, cudaMemcpyHostToDevice, s));
+        }
+        bptr_ = boxes_.as<float>();
+    }
+    // a tree built over triangles is rebuilt for boxes
+    if (built_ && (sc.num_faces != T_ || !box_input_)) built_ = false;
+    box_input_ = true;
+    vptr_ = nullptr;
+    T_ = sc.num_faces;
+    V_ = 0;
     return BVHCD_OK;
 }
 
 bvhcd_status LBvh::scene_box(cudaStream_t s) {
     int g = (int)grid_for(T_);
     if (g > 4096) g = 4096;
-    k_box_partial<<<g, kThreads, 0, s>>>(T_, fptr_, vptr_, partial_.as<float>()); note_launch();
+    k_box_partial<<<g, kThreads, 0, s>>>(T_, src(), partial_.as<float>()); note_launch();
     k_box_final<<<1, kThreads, 0, s>>>(g, partial_.as<float>(), scene_.as<float>()); note_launch();
     return cuda_status(cudaGetLastError());
 }
@@ -1362,26 +1400,26 @@ bvhcd_status LBvh::build(cudaStream_t s) {
         // a forest of S_ scenes: per-scene boxes, (scene, code) keys
         if (T != h_off_[S_]) return BVHCD_INVALID_ARG;
         k_sbox_init<<<1, kThreads, 0, s>>>(S_, sbox_.as<float>()); note_launch();
-        k_sbox_tiles<<<ntiles_, kThreads, 0, s>>>(tiles_.as<int4>(), fptr_, vptr_, sbox_.as<float>()); note_launch();
-        k_morton_seg<<<grid_for(T), kThreads, 0, s>>>(T, fptr_, vptr_, scene_of_.as<int>(), sbox_.as<float>(),
+        k_sbox_tiles<<<ntiles_, kThreads, 0, s>>>(tiles_.as<int4>(), src(), sbox_.as<float>()); note_launch();
+        k_morton_seg<<<grid_for(T), kThreads, 0, s>>>(T, src(), scene_of_.as<int>(), sbox_.as<float>(),
                                                       k64_.as<unsigned long long>(), vals_.as<int>()); note_launch();
         int sbits = 0;
         while ((1 << sbits) < S_) sbits++;
         BV_TRY(radix_sort_u64(k64_.as<unsigned long long>(), vals_.as<int>(), k64b_.as<unsigned long long>(),
                               vals2_.as<int>(), T, 30 + sbits, scratch_.p, s));
         leafscene = leafscene_.as<int>();
-        k_leaves_seg<<<grid_for(T), kThreads, 0, s>>>(T, k64_.as<unsigned long long>(), vals_.as<int>(), fptr_,
-                                                      vptr_, sface_.as<int4>(), primmap_.as<int>(),
+        k_leaves_seg<<<grid_for(T), kThreads, 0, s>>>(T, k64_.as<unsigned long long>(), vals_.as<int>(), src(),
+                                                      sface_.as<int4>(), primmap_.as<int>(),
                                                       code_.as<unsigned>(), metric_.as<int>(),
                                                       lrec_.as<float4>(), leafscene); note_launch();
     } else {
         bvhcd_status st = scene_box(s);
         if (st != BVHCD_OK) return st;
-        k_morton<<<grid_for(T), kThreads, 0, s>>>(T, fptr_, vptr_, scene_.as<float>(), keys_.as<unsigned>(),
+        k_morton<<<grid_for(T), kThreads, 0, s>>>(T, src(), scene_.as<float>(), keys_.as<unsigned>(),
                                                   vals_.as<int>()); note_launch();
         BV_TRY(radix_sort_u32(keys_.as<unsigned>(), vals_.as<int>(), keys2_.as<unsigned>(), vals2_.as<int>(),
                               T, 30, scratch_.p, s));
-        k_leaves<<<grid_for(T), kThreads, 0, s>>>(T, keys_.as<unsigned>(), vals_.as<int>(), fptr_, vptr_,
+        k_leaves<<<grid_for(T), kThreads, 0, s>>>(T, keys_.as<unsigned>(), vals_.as<int>(), src(),
                                                   sface_.as<int4>(), primmap_.as<int>(), code_.as<unsigned>(),
                                                   metric_.as<int>(), lrec_.as<float4>()); note_launch();
         if (T == 1) {
@@ -1423,14 +1461,14 @@ bvhcd_status LBvh::copy_state_from(const LBvh &src, cudaStream_t s) {
     if (&src == this) return BVHCD_OK;
     if (src.cfg_.enable_restr != cfg_.enable_restr || src.cfg_.node_box_fp16 != cfg_.node_box_fp16)
         return BVHCD_INVALID_ARG;
-    const DBuf *from[] = {&src.verts_, &src.faces_, &src.nrec_, &src.lrec_, &src.topo_, &src.nrange_, &src.lca_,
+    const DBuf *from[] = {&src.verts_, &src.faces_, &src.boxes_, &src.nrec_, &src.lrec_, &src.topo_, &src.nrange_, &src.lca_,
                           &src.sface_, &src.primmap_, &src.code_, &src.refit_flag_, &src.intrange_, &src.rtroot_,
                           &src.intmark_, &src.extrange_, &src.extmark_, &src.leafroot_, &src.ctr_,
                           &src.scene_of_, &src.leafscene_, &src.sbox_, &src.tiles_, &src.scene_, &src.nrec16_,
                           &src.split_, &src.cross_, &src.topk_, &src.plan_, &src.top_,
                           &src.height_, &src.llist_, &src.lhdr_, &src.tlist_, &src.thdr_,
                           &src.llink_, &src.tlink_, &src.lexport_, &src.gext_};
-    DBuf *to[] = {&verts_, &faces_, &nrec_, &lrec_, &topo_, &nrange_, &lca_, &sface_, &primmap_, &code_,
+    DBuf *to[] = {&verts_, &faces_, &boxes_, &nrec_, &lrec_, &topo_, &nrange_, &lca_, &sface_, &primmap_, &code_,
                   &refit_flag_, &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &ctr_,
                   &scene_of_, &leafscene_, &sbox_, &tiles_, &scene_, &nrec16_, &split_, &cross_, &topk_,
                   &plan_, &top_, &height_, &llist_, &lhdr_, &tlist_, &thdr_, &llink_, &tlink_,
@@ -1444,6 +1482,8 @@ bvhcd_status LBvh::copy_state_from(const LBvh &src, cudaStream_t s) {
     // input read in place stays where it is; an owned copy maps to this handle's copy
     vptr_ = src.vptr_ == src.verts_.as<float>() ? verts_.as<float>() : src.vptr_;
     fptr_ = src.fptr_ == src.faces_.as<int>() ? faces_.as<int>() : src.fptr_;
+    bptr_ = src.bptr_ && src.bptr_ == src.boxes_.as<float>() ? boxes_.as<float>() : src.bptr_;
+    box_input_ = src.box_input_;
     S_ = src.S_; ntiles_ = src.ntiles_; h_off_ = src.h_off_;
     epoch_++;
     topo_epoch_++;
@@ -1536,7 +1576,7 @@ bvhcd_status LBvh::refit(cudaStream_t s) {
     g.gbox = gbox_.as<float>();
     g.done = ctr_.as<unsigned>() + C_REFIT_DONE;
     const int nb = (T + kRefitW - 1) / kRefitW;
-    k_refit<<<nb, kRefitThreads, kLocalSmem, s>>>(T, sface_.as<int4>(), vptr_, plan_.as<int4>(), llist_.as<int4>(),
+    k_refit<<<nb, kRefitThreads, kLocalSmem, s>>>(T, sface_.as<int4>(), src(), plan_.as<int4>(), llist_.as<int4>(),
                                                   llink_.as<int2>(), lexport_.as<int4>(), lhdr_.as<int>(),
                                                   lrec_.as<float4>(), nrec_.as<float4>(), gext_.as<float>(), g); note_launch();
     return cuda_status(cudaGetLastError());
@@ -1581,7 +1621,7 @@ bvhcd_status LBvh::restructure(cudaStream_t s) {
     unsigned *pos = keys2_.as<unsigned>();
     k_rs_flags<<<grid_for(T), kThreads, 0, s>>>(T, leafroot_.as<int>(), flag); note_launch();
     BV_TRY(scan_u32(flag, pos, T, false, ctr + C_RT_SUBTREES + 2, scratch_.p, s));
-    k_rs_select<<<grid_for(T), kThreads, 0, s>>>(T, leafroot_.as<int>(), pos, sface_.as<int4>(), vptr_,
+    k_rs_select<<<grid_for(T), kThreads, 0, s>>>(T, leafroot_.as<int>(), pos, sface_.as<int4>(), src(),
                                                  scene_.as<float>(), k64_.as<unsigned long long>(),
                                                  task_.as<int>(), vals_.as<int>()); note_launch();
     const int nr = rt_intnodes_ + rt_subtrees_;  // leaves = internal nodes + subtrees
@@ -1642,6 +1682,22 @@ bvhcd_status LBvh::maintain_tree(bvhcd_bvh_op op, const bvhcd_scene &scene, cuda
     bool was_built = built_;
     bvhcd_status st = upload(scene, s);
     if (st != BVHCD_OK) return st;
+    return maintain_ops(op, prevT, was_built, s);
+}
+
+bvhcd_status LBvh::maintain_boxes(bvhcd_bvh_op op, const bvhcd_box_scene &scene, cudaStream_t s) {
+    if (op < BVHCD_BVH_BUILD || op > BVHCD_BVH_UPDATE) return BVHCD_INVALID_ARG;
+    if (S_ > 1 && scene.num_faces != h_off_[S_]) return BVHCD_INVALID_ARG;
+    int prevT = T_;
+    bool was_built = built_;
+    bvhcd_status st = upload_boxes(scene, s);
+    if (st != BVHCD_OK) return st;
+    st = maintain_ops(op, prevT, was_built, s);
+    if (st != BVHCD_OK) return st;
+    return node_fp16(s);
+}
+
+bvhcd_status LBvh::maintain_ops(bvhcd_bvh_op op, int prevT, bool was_built, cudaStream_t s) {
     opt_tag_ = 0;
     if (cfg_.enable_restr && updated_ && was_built && built_ && prevT == T_ && T_ >= 2)
         return restructure(s);
@@ -1777,9 +1833,9 @@ bvhcd_status morton_order_noalloc(const float *verts, const int *faces, int T, u
     // every scratch word read below is written earlier in the same call
     int g = (int)grid_for(T);
     if (g > 4096) g = 4096;
-    k_box_partial<<<g, kThreads, 0, s>>>(T, faces, verts, partial); note_launch();
+    k_box_partial<<<g, kThreads, 0, s>>>(T, PrimSrc{faces, verts, nullptr}, partial); note_launch();
     k_box_final<<<1, kThreads, 0, s>>>(g, partial, scene); note_launch();
-    k_morton<<<grid_for(T), kThreads, 0, s>>>(T, faces, verts, scene, codes, order); note_launch();
+    k_morton<<<grid_for(T), kThreads, 0, s>>>(T, PrimSrc{faces, verts, nullptr}, scene, codes, order); note_launch();
     BV_TRY(cudaGetLastError());
     BV_TRY(radix_sort_u32(codes, order, keys_alt, vals_alt, T, 30, sort_scratch, s));
     return BVHCD_OK;

@@ -89,6 +89,9 @@ class LBvh {
     bvhcd_status init();
     bvhcd_status maintain(bvhcd_bvh_op op, const bvhcd_scene &scene, cudaStream_t s);
     bvhcd_status maintain_tree(bvhcd_bvh_op op, const bvhcd_scene &scene, cudaStream_t s);
+    // the same for a scene of primitive boxes (no positions)
+    bvhcd_status maintain_boxes(bvhcd_bvh_op op, const bvhcd_box_scene &scene, cudaStream_t s);
+    bool box_input() const { return box_input_; }
     bvhcd_status stage_positions(const float *host, int nv, cudaStream_t copy, const float **staged);
     bool is_staged(const float *p) const { return p && (p == stage_[0].as<float>() || p == stage_[1].as<float>()); }
     bvhcd_status export_tree(int32_t *inode, float *ibox, int32_t *leaf, float *lbox, int32_t *lca,
@@ -107,16 +110,18 @@ class LBvh {
     // restores the state its capture ended with after every replay.
     struct HostState {
         int T, V, opt_tag, rt_subtrees, rt_intnodes;
-        bool built, updated;
-        const float *vptr;
+        bool built, updated, box_input;
+        const float *vptr, *bptr;
         const int *fptr;
     };
     HostState host_state() const {
-        return HostState{T_, V_, opt_tag_, rt_subtrees_, rt_intnodes_, built_, updated_, vptr_, fptr_};
+        return HostState{T_, V_, opt_tag_, rt_subtrees_, rt_intnodes_, built_, updated_, box_input_, vptr_, bptr_,
+                         fptr_};
     }
     void set_host_state(const HostState &h) {
         T_ = h.T; V_ = h.V; opt_tag_ = h.opt_tag; rt_subtrees_ = h.rt_subtrees; rt_intnodes_ = h.rt_intnodes;
-        built_ = h.built; updated_ = h.updated; vptr_ = h.vptr; fptr_ = h.fptr;
+        built_ = h.built; updated_ = h.updated; box_input_ = h.box_input; vptr_ = h.vptr; bptr_ = h.bptr;
+        fptr_ = h.fptr;
     }
 
     Tree tree() const;
@@ -145,6 +150,9 @@ class LBvh {
   private:
     bvhcd_status ensure_capacity(int T, int V);
     bvhcd_status upload(const bvhcd_scene &scene, cudaStream_t s);
+    bvhcd_status upload_boxes(const bvhcd_box_scene &scene, cudaStream_t s);
+    bvhcd_status maintain_ops(bvhcd_bvh_op op, int prevT, bool was_built, cudaStream_t s);
+    PrimSrc src() const { return PrimSrc{fptr_, vptr_, bptr_}; }
     bvhcd_status build(cudaStream_t s);
     bvhcd_status refit(cudaStream_t s);
     bvhcd_status refit_plan(cudaStream_t s, bool heights_known);
@@ -159,8 +167,11 @@ class LBvh {
     int opt_tag_ = 0, rt_subtrees_ = 0, rt_intnodes_ = 0;
     const float *vptr_ = nullptr;
     const int *fptr_ = nullptr;
-    // owned copies of host input
-    DBuf verts_, faces_;
+    const float *bptr_ = nullptr;  // FP32 primitive boxes of a box scene
+    bool box_input_ = false;
+    // owned copies of host input (boxes_: a box scene's FP32 boxes, boxes64_:
+    // its FP64 boxes before rounding)
+    DBuf verts_, faces_, boxes_, boxes64_;
     // tree
     DBuf nrec_, lrec_, topo_, nrange_, lca_, sface_, primmap_, code_, refit_flag_, nrec16_;
     // refit plan (a function of the topology): split of each internal node,

@@ -87,6 +87,24 @@ typedef struct {
     int32_t faces_static;  /* 1: faces unchanged since the last call (skip their copy) */
 } bvhcd_scene;
 
+/* A scene given as one axis-aligned box per primitive instead of triangles:
+ * ARCSimSceneData{fsize, faces, boxes} (Mine/world/Scene.h:39-45), boxes a
+ * simulator computed itself (for instance swept over its time step).  The
+ * boxes take the place of the triangles' boxes everywhere (scene box, Morton
+ * codes of their centres, leaves, refit, restructure); the faces give the
+ * vertex ids for adjacency culling and the original ids of the pairs.  There
+ * are no positions, so a front over such a BVH runs the broad phase only
+ * (narrow_phase = 0). */
+typedef struct {
+    const void *boxes;     /* T x 6: min x, y, z, max x, y, z; FP32, or FP64 with boxes_f64 */
+    const int32_t *faces;  /* T x 3 vertex ids */
+    int32_t num_faces;
+    int32_t boxes_f64;     /* 1: FP64 boxes, rounded outward to FP32 (min down, max up), so the
+                              FP32 box contains the given one; the reference converts to nearest */
+    int32_t on_device;     /* 1: device pointers (FP32 boxes read in place); 0: host, copied */
+    int32_t faces_static;  /* 1: faces unchanged since the last call (skip their copy) */
+} bvhcd_box_scene;
+
 /* Stats the reference logs per frame in inspectResults
  * (Mine/collision/bvtt_front/BvttFrontLooseIntra.cu:50-61). */
 typedef struct {
@@ -120,6 +138,13 @@ bvhcd_status bvhcd_bvh_create(const bvhcd_bvh_config *cfg, bvhcd_bvh **out);
 bvhcd_status bvhcd_bvh_destroy(bvhcd_bvh *bvh);
 bvhcd_status bvhcd_bvh_maintain(bvhcd_bvh *bvh, bvhcd_bvh_op op, const bvhcd_scene *scene,
                                 void *stream);
+/* maintain(scheme, const ARCSimSceneData&) (Mine/collision/lbvh/
+ * LBvhFixedDeformable.cu:89-112, with the *ARCSim kernels of
+ * LBvhBuildKernels.cu:10-52 and LBvhUpdateKernels.cu:11-32): the same
+ * operations on a box scene.  A handle may switch between box and triangle
+ * scenes at a BUILD. */
+bvhcd_status bvhcd_bvh_maintain_boxes(bvhcd_bvh *bvh, bvhcd_bvh_op op, const bvhcd_box_scene *scene,
+                                      void *stream);
 bvhcd_status bvhcd_bvh_sizes(const bvhcd_bvh *bvh, int32_t *prims, int32_t *ext_nodes,
                              int32_t *int_nodes);
 /* Copies the next frame's positions (host memory, num_vertices x 3 floats;
