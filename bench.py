@@ -178,7 +178,7 @@ def run_ours(args):
         dist.barrier()
     value = dev_ms / (K * world)
 
-    e2e = roof = batched = fp16 = inter = boxes = None
+    e2e = roof = batched = fp16 = inter = boxes = prox = None
     if not args.only_value:
         e2e = e2e_pass(bvhcd, torch, pipeline, host, faces, dfaces, flush, hits_host, stream, W, K, V, world)
         # roofline of the dominant stage, from a stage-timed replay
@@ -186,6 +186,7 @@ def run_ours(args):
         fp16 = fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
         inter = inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, st)
         boxes = box_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
+        prox = proximity_pass(bvhcd, torch, front, stream)
     learned = None
     if not args.only_value and not args.no_batched:
         del dev, host, flush
@@ -220,6 +221,7 @@ def run_ours(args):
             "fp16_node_boxes": fp16,
             "inter_rigid_obstacle": inter,
             "box_scene": boxes,
+            "proximity": prox,
             "batched": batched,
             "learned": learned,
         }
@@ -587,6 +589,37 @@ def box_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
     return {"workload": f"the bench frames as {T} swept triangle boxes (frames f and f + 1), FP32, device-resident",
             "value": round(ms, 4), "unit": "ms/frame", "narrow_phase": False,
             "front_sizes_last_frame": [st["int_front"], st["ext_front"]], "pairs_last_frame": st["broad_pairs"]}
+
+
+def proximity_pass(bvhcd, torch, front, stream, thickness=1e-3, reps=5):
+    """Vertex-face / edge-edge proximities (FP64) of the last frame's broad
+    pairs through bvhcd_front_proximity into a device buffer: CUDA-event time
+    of the call (a counting pass, a scan, the host reading the total, the
+    writing pass), the record count and the pairs evaluated."""
+    import ctypes
+    L = bvhcd.lib()
+    n = ctypes.c_int64()
+    st = L.bvhcd_front_proximity(front.handle, None, float(thickness), None, 0, ctypes.byref(n), 1,
+                                 ctypes.c_void_p(stream.cuda_stream))
+    if st not in (0, 3):
+        raise RuntimeError(f"proximity: status {st}")
+    cap = max(int(n.value), 1)
+    buf = torch.empty(cap * bvhcd.PROX_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    times = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        st = L.bvhcd_front_proximity(front.handle, None, float(thickness), ctypes.c_void_p(buf.data_ptr()), cap,
+                                     ctypes.byref(n), 1, ctypes.c_void_p(stream.cuda_stream))
+        b.record(stream)
+        torch.cuda.synchronize()
+        if st != 0:
+            raise RuntimeError(f"proximity: status {st}")
+        times.append(a.elapsed_time(b))
+    pairs = front.stats()["broad_pairs"]
+    return {"thickness": thickness, "pairs": int(pairs), "records": int(n.value),
+            "ms_per_call": round(statistics.median(times), 4), "unit": "ms", "arithmetic": "f64",
+            "pairs_per_s": round(pairs / (statistics.median(times) * 1e-3), 1)}
 
 
 def fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):

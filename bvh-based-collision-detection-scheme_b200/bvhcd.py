@@ -31,7 +31,7 @@ EXPORTED = [
     "bvhcd_bvh_maintain", "bvhcd_bvh_sizes", "bvhcd_bvh_opt_tag", "bvhcd_bvh_export",
     "bvhcd_bvh_request_restructure", "bvhcd_bvh_stage_positions", "bvhcd_bvh_maintain_boxes",
     "bvhcd_front_create", "bvhcd_front_create_inter", "bvhcd_front_destroy", "bvhcd_front_maintain", "bvhcd_front_stats_get",
-    "bvhcd_front_pairs", "bvhcd_front_device_results", "bvhcd_front_export",
+    "bvhcd_front_pairs", "bvhcd_front_device_results", "bvhcd_front_export", "bvhcd_front_proximity",
     "bvhcd_schedule_heuristic", "bvhcd_frame", "bvhcd_profile_enable", "bvhcd_profile_read",
     "bvhcd_launch_count", "bvhcd_morton_order_noalloc", "bvhcd_bvh_set_scenes", "bvhcd_frame_graph",
     "bvhcd_front_get_shapes", "bvhcd_front_set_shapes", "bvhcd_front_autotune",
@@ -73,6 +73,12 @@ class Scene(ctypes.Structure):
     _fields_ = [("pos", ctypes.c_void_p), ("faces", ctypes.c_void_p),
                 ("num_vertices", ctypes.c_int32), ("num_faces", ctypes.c_int32),
                 ("on_device", ctypes.c_int32), ("faces_static", ctypes.c_int32)]
+
+
+# bvhcd_proximity
+PROX_DTYPE = np.dtype([("pair", np.int32), ("kind", np.int32), ("fa", np.int32), ("fb", np.int32),
+                       ("dist", np.float64), ("n", np.float64, 3), ("w", np.float64, 4)], align=True)
+assert PROX_DTYPE.itemsize == 80
 
 
 class BoxScene(ctypes.Structure):
@@ -133,6 +139,8 @@ def lib():
             "bvhcd_front_create": (ctypes.c_int, [vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
             "bvhcd_front_create_inter": (ctypes.c_int, [vp, vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
             "bvhcd_front_destroy": (ctypes.c_int, [vp]),
+            "bvhcd_front_proximity": (ctypes.c_int, [vp, vp, ctypes.c_double, vp, ctypes.c_int64,
+                                                     ctypes.POINTER(ctypes.c_int64), i32, vp]),
             "bvhcd_front_maintain": (ctypes.c_int, [vp, ctypes.c_int, vp]),
             "bvhcd_front_stats_get": (ctypes.c_int, [vp, ctypes.POINTER(FrontStats), vp]),
             "bvhcd_front_pairs": (ctypes.c_int, [vp, i32, vp, i64, ctypes.POINTER(i64), i32, vp]),
@@ -454,6 +462,27 @@ class BvttFront:
         out = np.zeros((max(n.value, 1), 2), np.int32)
         _check(lib().bvhcd_front_export(self._h, int(which), out.ctypes.data, n.value, ctypes.byref(n),
                                         _stream_ptr(stream)), "front export")
+        return out[:n.value]
+
+    def proximity(self, thickness: float, pos=None, stream=None) -> np.ndarray:
+        """Vertex-face and edge-edge proximities of the broad pairs within
+        `thickness` (bvhcd_front_proximity), a structured array of PROX_DTYPE
+        records ordered by pair.  pos: CUDA tensor of positions, or None for
+        the BVH's own."""
+        ptr = None
+        if pos is not None:
+            import torch
+            assert isinstance(pos, torch.Tensor) and pos.is_cuda and pos.dtype == torch.float32
+            pos = pos.contiguous()
+            ptr = pos.data_ptr()
+        n = ctypes.c_int64()
+        st = lib().bvhcd_front_proximity(self._h, ptr, float(thickness), None, 0, ctypes.byref(n), 0,
+                                         _stream_ptr(stream))
+        if st not in (0, 3):
+            _check(st, "proximity")
+        out = np.zeros(max(n.value, 1), dtype=PROX_DTYPE)
+        _check(lib().bvhcd_front_proximity(self._h, ptr, float(thickness), out.ctypes.data, n.value, ctypes.byref(n),
+                                           0, _stream_ptr(stream)), "proximity")
         return out[:n.value]
 
     def contacts(self, which: int = 0, stream=None):

@@ -265,6 +265,12 @@ bvhcd_status bvhcd_front_contacts(bvhcd_front *front, int32_t which, float *out,
     return front->impl.contacts(which, out, cap, count, flagged, out_on_device != 0, as_stream(stream));
 }
 
+bvhcd_status bvhcd_front_proximity(bvhcd_front *front, const float *pos, double thickness, bvhcd_proximity *out,
+                                   int64_t cap, int64_t *count, int32_t out_on_device, void *stream) {
+    if (!front) return BVHCD_INVALID_ARG;
+    return front->impl.proximity(pos, thickness, out, cap, count, out_on_device != 0, as_stream(stream));
+}
+
 bvhcd_status bvhcd_bvh_copy_state(bvhcd_bvh *dst, const bvhcd_bvh *src, void *stream) {
     if (!dst || !src) return BVHCD_INVALID_ARG;
     return dst->impl.copy_state_from(src->impl, as_stream(stream));

@@ -13,6 +13,7 @@
 
 #include "pipeline.h"
 #include "tritri.cuh"
+#include "proximity.cuh"
 #include "prims.cuh"
 
 namespace bvhcd {
@@ -898,7 +899,8 @@ Front::~Front() {
     for (auto &set : front_)
         for (auto &b : set) b.release();
     DBuf *bufs[] = {&pairs_, &hits_, &outbuf_, &work_, &intcnt_, &extcnt_, &intbeg_, &extbeg_, &intback_,
-                    &extback_, &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_, &fctr_, &rcur_};
+                    &extback_, &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_, &fctr_, &rcur_,
+                    &pxbuf_, &pxout_};
     for (DBuf *b : bufs) b->release();
 }
 
@@ -1495,6 +1497,105 @@ bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, 
     FR_TRY(cudaStreamSynchronize(s));
     if (h[C_OVERFLOW] & (which ? 8u : 4u)) return BVHCD_CAPACITY_EXCEEDED;
     return n > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
+}
+
+namespace {
+// Proximities of the compacted broad pairs (bvhcd_front_proximity): a first
+// pass counts each pair's records (0 past the last pair, up to the capacity),
+// a scan turns the counts into offsets, a second pass writes the records
+// there, so they come ordered by pair and, inside a pair, by feature.
+template <bool kWrite>
+__global__ void k_proximity(const int2 *__restrict__ list, const unsigned *__restrict__ cnt, unsigned cap,
+                            const int *__restrict__ fa, const float *__restrict__ va, const int *__restrict__ fb,
+                            const float *__restrict__ vb, int same_mesh, double h, unsigned *counts,
+                            const unsigned *__restrict__ offs, bvhcd_proximity *out, unsigned long long ocap) {
+    const unsigned n = min(*cnt, cap);
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < cap; q += gridDim.x * blockDim.x) {
+        if (q >= n) {
+            if (!kWrite) counts[q] = 0u;
+            continue;
+        }
+        if (kWrite && counts[q] == 0u) continue;  // most pairs have no proximity
+        const int2 p = list[q];
+        int ia[3], ib[3];
+        prec::d3 pa[3], pb[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            ia[k] = __ldg(fa + 3 * (size_t)p.x + k);
+            ib[k] = __ldg(fb + 3 * (size_t)p.y + k);
+            const float3 x = load_vert(va, ia[k]), y = load_vert(vb, ib[k]);
+            pa[k] = prec::mk(x.x, x.y, x.z);
+            pb[k] = prec::mk(y.x, y.y, y.z);
+        }
+        if (!kWrite) {
+            unsigned c = 0;
+            prox::triangle_pair(ia, pa, ib, pb, same_mesh != 0, h, [&](const prox::Hit &) { ++c; });
+            counts[q] = c;
+        } else {
+            unsigned long long o = offs[q];
+            prox::triangle_pair(ia, pa, ib, pb, same_mesh != 0, h, [&](const prox::Hit &r) {
+                if (o < ocap) {
+                    bvhcd_proximity &x = out[o];
+                    x.pair = (int)q;
+                    x.kind = r.kind;
+                    x.fa = r.fa;
+                    x.fb = r.fb;
+                    x.dist = r.d;
+                    x.n[0] = r.n.x;
+                    x.n[1] = r.n.y;
+                    x.n[2] = r.n.z;
+                    for (int k = 0; k < 4; k++) x.w[k] = r.w[k];
+                }
+                ++o;
+            });
+        }
+    }
+}
+}  // namespace
+
+bvhcd_status Front::proximity(const float *pos, double h, bvhcd_proximity *out, int64_t cap, int64_t *count,
+                              bool out_dev, cudaStream_t s) {
+    if (cap < 0 || !(h >= 0.0) || (inter() && pos)) return BVHCD_INVALID_ARG;
+    if (!bvh_->built() || !trav()->built() || !has_front_) return BVHCD_NOT_READY;
+    const float *va = pos ? pos : bvh_->verts();
+    const float *vb = inter() ? trav_->verts() : va;
+    if (!va || !vb) return BVHCD_INVALID_ARG;  // a box scene has no positions of its own
+    if (count) *count = 0;
+    if (pcap_ <= 0) return BVHCD_OK;
+    bvhcd_status st = compact_pairs(s);
+    if (st != BVHCD_OK) return st;
+    const size_t n = (size_t)pcap_;
+    FR_TRY(pxbuf_.reserve(sizeof(unsigned) * (2 * n + 1)));
+    FR_TRY(cscratch_.reserve(scan_scratch_bytes((int64_t)n)));
+    unsigned *counts = pxbuf_.as<unsigned>(), *offs = counts + n, *total = offs + n;
+    const int2 *list = outbuf_.as<int2>();
+    const unsigned *cnt = counters() + C_COMPACT;
+    const unsigned g = RESIDENT((k_proximity<false>));
+    k_proximity<false><<<g, kThreads, 0, s>>>(list, cnt, (unsigned)pcap_, bvh_->faces(), va, trav()->faces(), vb,
+                                              inter() ? 0 : 1, h, counts, nullptr, nullptr, 0ull);
+    note_launch();
+    FR_TRY(cudaGetLastError());
+    FR_TRY(scan_u32(counts, offs, (int64_t)n, false, total, cscratch_.p, s));
+    unsigned htot = 0;
+    FR_TRY(cudaMemcpyAsync(&htot, total, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaStreamSynchronize(s));
+    if (count) *count = (int64_t)htot;
+    const int64_t m = (int64_t)htot < cap ? (int64_t)htot : cap;
+    if (out && m > 0) {
+        bvhcd_proximity *dst = out;
+        if (!out_dev) {
+            FR_TRY(pxout_.reserve(sizeof(bvhcd_proximity) * (size_t)m));
+            dst = pxout_.as<bvhcd_proximity>();
+        }
+        k_proximity<true><<<g, kThreads, 0, s>>>(list, cnt, (unsigned)pcap_, bvh_->faces(), va, trav()->faces(), vb,
+                                                 inter() ? 0 : 1, h, counts, offs, dst, (unsigned long long)m);
+        note_launch();
+        FR_TRY(cudaGetLastError());
+        if (!out_dev)
+            FR_TRY(cudaMemcpyAsync(out, dst, sizeof(bvhcd_proximity) * (size_t)m, cudaMemcpyDeviceToHost, s));
+        FR_TRY(cudaStreamSynchronize(s));
+    }
+    return (int64_t)htot > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
 }
 
 // Contact points of the hits (which = 0) or distances of the broad pairs

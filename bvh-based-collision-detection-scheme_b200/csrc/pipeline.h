@@ -214,6 +214,8 @@ class Front {
     bvhcd_status pairs(int which, int32_t *out, int64_t cap, int64_t *count, bool out_dev,
                        cudaStream_t s);
     bvhcd_status export_front(int which, int32_t *out, int64_t cap, int64_t *count, cudaStream_t s);
+    bvhcd_status proximity(const float *pos, double thickness, bvhcd_proximity *out, int64_t cap, int64_t *count,
+                           bool out_dev, cudaStream_t s);
     bvhcd_status contacts(int which, float *out, int64_t cap, int64_t *count, int64_t *flagged, bool out_dev,
                           cudaStream_t s);
     bvhcd_status device_results(const int32_t **hits, const int64_t **counts);
@@ -295,6 +297,7 @@ class Front {
     int64_t pcap_ = 0;
     DBuf intcnt_, extcnt_, intbeg_, extbeg_, intback_, extback_, snapshot_, scratch_, counts64_;
     DBuf rcur_;  // reorder cursors, one per group of 2^kReorderShift nodes and front
+    DBuf pxbuf_, pxout_;  // proximity counts / offsets / total; records for a host destination
 };
 
 }  // namespace bvhcd

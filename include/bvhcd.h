@@ -294,6 +294,35 @@ bvhcd_status bvhcd_morton_order_noalloc(const float *pos, const int32_t *faces, 
  * maintain rebuilds either way. */
 bvhcd_status bvhcd_bvh_set_scenes(bvhcd_bvh *bvh, int32_t num_scenes, const int32_t *tri_offsets);
 
+/* ---- Proximities of the broad pairs (no counterpart in the reference's
+ * pipeline: it carries signed_vf_distance and signed_ee_distance,
+ * Mine/utility/CudaDeviceUtils.cu:163-193, the measures a cloth solver builds
+ * its repulsion constraints from, but never calls them).  For every broad
+ * pair, in the order of bvhcd_front_pairs(which = 0), every vertex-face and
+ * edge-edge feature pair of the two triangles whose signed distance is within
+ * `thickness` and whose closest points lie inside both features (all
+ * barycentric weights non-negative), skipping feature pairs that share a
+ * vertex id.  FP64 from the FP32 positions.  Records come ordered by pair,
+ * then kind, then feature. */
+typedef struct {
+    int32_t pair;    /* index of the pair in bvhcd_front_pairs(which = 0) order */
+    int32_t kind;    /* 0: vertex fa of the first triangle against the second's face;
+                        1: vertex fb of the second triangle against the first's face;
+                        2: edge fa of the first (its vertices fa, fa + 1 mod 3) against edge fb of the second */
+    int32_t fa, fb;  /* feature indices, -1 where the kind has none */
+    double dist;     /* signed distance along n (vertex minus face / first edge minus second) */
+    double n[3];     /* unit normal: the face's for kinds 0 and 1, the two edges' cross product for 2 */
+    double w[4];     /* weights as signed_vf_distance (1, -b0, -b1, -b2 over the face) and
+                        signed_ee_distance (a0, a1 on the first edge, -b0, -b1 on the second) give them */
+} bvhcd_proximity;
+/* pos: device positions (V x 3 FP32) of the front's BVH, or NULL for the
+ * positions of its last maintain (required for a box scene, which has none;
+ * NULL for an inter front, which uses each BVH's own).  out: host, or device
+ * with out_on_device; *count receives the full count (CAPACITY_EXCEEDED and
+ * the first cap records when it exceeds cap).  Synchronises `stream`. */
+bvhcd_status bvhcd_front_proximity(bvhcd_front *front, const float *pos, double thickness, bvhcd_proximity *out,
+                                   int64_t cap, int64_t *count, int32_t out_on_device, void *stream);
+
 /* ---- Contact points and distances (precision mode extension; the
  * reference's narrow phase returns a hit flag only, narrow_phase.cu:8-24).
  * which = 0: for every hit, in the order bvhcd_front_pairs(which = 1) returns

@@ -89,6 +89,16 @@ double orc_tri_distance64(const float *p9, const float *q9);
 void orc_precision_pairs(int64_t n, const int *pairs, const int *faces, const float *verts,
                          unsigned char *hit64, double *contact4, double *dist);
 
+/* Proximities of a pair list (proximity_oracle.c): the layout of
+ * bvhcd_proximity.  Pairs index faces fa (first) and fb (second); returns the
+ * count and writes up to cap records in the kernel's order. */
+typedef struct {
+    int32_t pair, kind, fa, fb;
+    double dist, n[3], w[4];
+} orc_prox;
+int64_t orc_proximity(int64_t n, const int *pairs, const int *fa, const float *va, const int *fb, const float *vb,
+                      int same_mesh, double h, orc_prox *out, int64_t cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,6 +57,9 @@ def lib():
         L.orc_pipe_set_reference_permutation.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_precision_pairs.argtypes = [ctypes.c_int64, _i32p, _i32p, _f32p, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_proximity.restype = ctypes.c_int64
+        L.orc_proximity.argtypes = [ctypes.c_int64, _i32p, _i32p, _f32p, _i32p, _f32p, ctypes.c_int,
+                                    ctypes.c_double, ctypes.c_void_p, ctypes.c_int64]
         L.orc_tritri_sat64.restype = ctypes.c_int
         L.orc_tritri_sat64.argtypes = [_f32p, _f32p]
         L.orc_contact64.restype = ctypes.c_int
@@ -170,6 +173,26 @@ def inter_narrow(pairs, fa, va, fb, vb) -> np.ndarray:
     pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
     q = np.stack([pairs[:, 1] + ta, pairs[:, 0]], axis=1)
     return narrow(q, faces, pos)
+
+
+PROX_DTYPE = np.dtype([("pair", np.int32), ("kind", np.int32), ("fa", np.int32), ("fb", np.int32),
+                       ("dist", np.float64), ("n", np.float64, 3), ("w", np.float64, 4)], align=True)
+
+
+def proximity(pairs, fa, va, fb=None, vb=None, h=0.0):
+    """Proximity records of a pair list (first triangle from (fa, va), second
+    from (fb, vb); one mesh when fb is None), in the kernel's order."""
+    same = fb is None
+    if same:
+        fb, vb = fa, va
+    pairs = np.ascontiguousarray(np.asarray(pairs).reshape(-1, 2), dtype=np.int32)
+    args = [np.ascontiguousarray(fa, dtype=np.int32), np.ascontiguousarray(va, dtype=np.float32),
+            np.ascontiguousarray(fb, dtype=np.int32), np.ascontiguousarray(vb, dtype=np.float32)]
+    L = lib()
+    n = L.orc_proximity(pairs.shape[0], pairs, *args, int(same), float(h), None, 0)
+    out = np.zeros(max(n, 1), dtype=PROX_DTYPE)
+    L.orc_proximity(pairs.shape[0], pairs, *args, int(same), float(h), out.ctypes.data, n)
+    return out[:n]
 
 
 def ref_narrow(pairs, faces, pos):
