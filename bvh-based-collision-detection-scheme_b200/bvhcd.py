@@ -29,7 +29,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "capacit
 EXPORTED = [
     "bvhcd_status_string", "bvhcd_device_check", "bvhcd_bvh_create", "bvhcd_bvh_destroy",
     "bvhcd_bvh_maintain", "bvhcd_bvh_sizes", "bvhcd_bvh_opt_tag", "bvhcd_bvh_export",
-    "bvhcd_bvh_request_restructure", "bvhcd_bvh_stage_positions", "bvhcd_bvh_maintain_boxes",
+    "bvhcd_bvh_request_restructure", "bvhcd_bvh_stage_positions", "bvhcd_bvh_maintain_boxes", "bvhcd_obj_read",
     "bvhcd_front_create", "bvhcd_front_create_inter", "bvhcd_front_destroy", "bvhcd_front_maintain", "bvhcd_front_stats_get",
     "bvhcd_front_pairs", "bvhcd_front_device_results", "bvhcd_front_export", "bvhcd_front_proximity",
     "bvhcd_schedule_heuristic", "bvhcd_frame", "bvhcd_profile_enable", "bvhcd_profile_read",
@@ -136,6 +136,8 @@ def lib():
             "bvhcd_bvh_request_restructure": (ctypes.c_int, [vp, vp, i32, vp]),
             "bvhcd_bvh_stage_positions": (ctypes.c_int, [vp, vp, i32, vp, ctypes.POINTER(vp)]),
             "bvhcd_bvh_maintain_boxes": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(BoxScene), vp]),
+            "bvhcd_obj_read": (ctypes.c_int, [ctypes.c_char_p, vp, i32, vp, i32, ctypes.POINTER(i32),
+                                              ctypes.POINTER(i32)]),
             "bvhcd_front_create": (ctypes.c_int, [vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
             "bvhcd_front_create_inter": (ctypes.c_int, [vp, vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
             "bvhcd_front_destroy": (ctypes.c_int, [vp]),
@@ -528,6 +530,28 @@ class BvttFront:
         _check(lib().bvhcd_front_device_results(self._h, ctypes.byref(hits), ctypes.byref(counts)),
                "device results")
         return hits.value, counts.value
+
+
+def load_obj(path: str):
+    """(positions V x 3 float32, faces T x 3 int32) of a Wavefront OBJ file
+    (bvhcd_obj_read: polygons fan-triangulated, vertex ids as the file
+    shares them)."""
+    V, T = ctypes.c_int32(), ctypes.c_int32()
+    p = os.fsencode(path)
+    _check(lib().bvhcd_obj_read(p, None, 0, None, 0, ctypes.byref(V), ctypes.byref(T)), f"read {path}")
+    pos = np.zeros((max(V.value, 1), 3), np.float32)
+    faces = np.zeros((max(T.value, 1), 3), np.int32)
+    _check(lib().bvhcd_obj_read(p, pos.ctypes.data, V.value, faces.ctypes.data, T.value, ctypes.byref(V),
+                                ctypes.byref(T)), f"read {path}")
+    return pos[:V.value], faces[:T.value]
+
+
+def obj_frames(pattern: str, start: int, count: int):
+    """The frames of a benchmark sequence, one OBJ file per frame named by a
+    printf pattern (CDBenchmarkSettings::file_name: pattern % frame for
+    frames start .. start + count - 1); yields (positions, faces)."""
+    for f in range(start, start + count):
+        yield load_obj(pattern % f)
 
 
 def frame(bvh: LBvh, front: BvttFront, f: int, start: int, pos, faces, stream=None, faces_static=False):

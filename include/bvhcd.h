@@ -323,6 +323,21 @@ typedef struct {
 bvhcd_status bvhcd_front_proximity(bvhcd_front *front, const float *pos, double thickness, bvhcd_proximity *out,
                                    int64_t cap, int64_t *count, int32_t out_on_device, void *stream);
 
+/* ---- Mesh files.  Reads a Wavefront OBJ file -- the format of the reference's
+ * benchmark frames, loaded per frame by Scene::update / addMesh
+ * (Mine/world/Scene.cpp:14-43) through assimp with triangulation
+ * (Mine/utility/ModelReader.hpp:23-27) -- into positions (V x 3) and faces
+ * (T x 3, 0-based): v records and f records (v, v/vt, v//vn, v/vt/vn corners,
+ * negative ids relative to the vertices read so far), polygons split into a
+ * fan around their first corner, other records skipped.  Vertex ids stay as
+ * the file shares them (assimp's OBJ import gives every face corner its own
+ * vertex, which leaves nothing for adjacency culling).  With pos / faces NULL
+ * only the counts are returned; CAPACITY_EXCEEDED when a count exceeds its
+ * capacity (the first vcap / fcap records are written).  INVALID_ARG for a
+ * missing file or a malformed v or f record.  Host only. */
+bvhcd_status bvhcd_obj_read(const char *path, float *pos, int32_t vcap, int32_t *faces, int32_t fcap,
+                            int32_t *num_vertices, int32_t *num_faces);
+
 /* ---- Contact points and distances (precision mode extension; the
  * reference's narrow phase returns a hit flag only, narrow_phase.cu:8-24).
  * which = 0: for every hit, in the order bvhcd_front_pairs(which = 1) returns
