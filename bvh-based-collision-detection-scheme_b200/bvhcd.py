@@ -32,6 +32,7 @@ EXPORTED = [
     "bvhcd_bvh_request_restructure", "bvhcd_bvh_stage_positions", "bvhcd_bvh_maintain_boxes", "bvhcd_obj_read",
     "bvhcd_front_create", "bvhcd_front_create_inter", "bvhcd_front_destroy", "bvhcd_front_maintain", "bvhcd_front_stats_get",
     "bvhcd_front_pairs", "bvhcd_front_device_results", "bvhcd_front_export", "bvhcd_front_proximity",
+    "bvhcd_front_pairs_async", "bvhcd_host_alloc", "bvhcd_host_free",
     "bvhcd_schedule_heuristic", "bvhcd_frame", "bvhcd_profile_enable", "bvhcd_profile_read",
     "bvhcd_launch_count", "bvhcd_morton_order_noalloc", "bvhcd_bvh_set_scenes", "bvhcd_frame_graph",
     "bvhcd_front_get_shapes", "bvhcd_front_set_shapes", "bvhcd_front_autotune",
@@ -141,6 +142,9 @@ def lib():
             "bvhcd_front_create": (ctypes.c_int, [vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
             "bvhcd_front_create_inter": (ctypes.c_int, [vp, vp, ctypes.POINTER(FrontConfig), ctypes.POINTER(vp)]),
             "bvhcd_front_destroy": (ctypes.c_int, [vp]),
+            "bvhcd_front_pairs_async": (ctypes.c_int, [vp, i32, vp, ctypes.c_int64, vp, vp]),
+            "bvhcd_host_alloc": (ctypes.c_int, [ctypes.c_int64, ctypes.POINTER(vp)]),
+            "bvhcd_host_free": (ctypes.c_int, [vp]),
             "bvhcd_front_proximity": (ctypes.c_int, [vp, vp, ctypes.c_double, vp, ctypes.c_int64,
                                                      ctypes.POINTER(ctypes.c_int64), i32, vp]),
             "bvhcd_front_maintain": (ctypes.c_int, [vp, ctypes.c_int, vp]),
@@ -466,6 +470,12 @@ class BvttFront:
                                         _stream_ptr(stream)), "front export")
         return out[:n.value]
 
+    def pairs_async(self, dst: "HostPairs", narrow: bool = False, stream=None):
+        """Enqueues the pairs' copy into `dst` (bvhcd_front_pairs_async); no
+        synchronisation."""
+        _check(lib().bvhcd_front_pairs_async(self._h, int(narrow), ctypes.c_void_p(dst.pairs_ptr), dst.cap,
+                                             ctypes.c_void_p(dst.count_ptr), _stream_ptr(stream)), "pairs async")
+
     def proximity(self, thickness: float, pos=None, stream=None) -> np.ndarray:
         """Vertex-face and edge-edge proximities of the broad pairs within
         `thickness` (bvhcd_front_proximity), a structured array of PROX_DTYPE
@@ -530,6 +540,48 @@ class BvttFront:
         _check(lib().bvhcd_front_device_results(self._h, ctypes.byref(hits), ctypes.byref(counts)),
                "device results")
         return hits.value, counts.value
+
+
+class HostPairs:
+    """Mapped pinned host memory for `cap` pairs and their count, the target
+    of BvttFront.pairs_async (bvhcd_host_alloc)."""
+
+    def __init__(self, cap: int):
+        self.cap = int(cap)
+        p = ctypes.c_void_p()
+        _check(lib().bvhcd_host_alloc(8 * self.cap + 64, ctypes.byref(p)), "host alloc")
+        self._p = p
+        buf = (ctypes.c_char * (8 * self.cap + 64)).from_address(p.value)
+        self._count = np.frombuffer(buf, dtype=np.int64, count=1, offset=0)
+        self._pairs = np.frombuffer(buf, dtype=np.int32, count=2 * self.cap, offset=64).reshape(-1, 2)
+
+    @property
+    def count_ptr(self):
+        return self._p.value
+
+    @property
+    def pairs_ptr(self):
+        return self._p.value + 64
+
+    def read(self) -> np.ndarray:
+        """The pairs written by the last completed pairs_async (the caller
+        synchronises first)."""
+        return self._pairs[:min(int(self._count[0]), self.cap)].copy()
+
+    @property
+    def count(self) -> int:
+        return int(self._count[0])
+
+    def close(self):
+        if self._p:
+            lib().bvhcd_host_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def load_obj(path: str):

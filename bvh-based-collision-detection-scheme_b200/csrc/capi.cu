@@ -265,6 +265,24 @@ bvhcd_status bvhcd_front_contacts(bvhcd_front *front, int32_t which, float *out,
     return front->impl.contacts(which, out, cap, count, flagged, out_on_device != 0, as_stream(stream));
 }
 
+bvhcd_status bvhcd_front_pairs_async(bvhcd_front *front, int32_t which, int32_t *host_out, int64_t cap,
+                                     int64_t *host_count, void *stream) {
+    if (!front) return BVHCD_INVALID_ARG;
+    return front->impl.pairs_async(which, host_out, cap, host_count, as_stream(stream));
+}
+
+bvhcd_status bvhcd_host_alloc(int64_t bytes, void **ptr) {
+    if (!ptr || bytes < 0) return BVHCD_INVALID_ARG;
+    *ptr = nullptr;
+    cudaError_t e = cudaHostAlloc(ptr, (size_t)(bytes > 0 ? bytes : 1), cudaHostAllocMapped | cudaHostAllocPortable);
+    return bvhcd::cuda_status(e);
+}
+
+bvhcd_status bvhcd_host_free(void *ptr) {
+    if (!ptr) return BVHCD_OK;
+    return bvhcd::cuda_status(cudaFreeHost(ptr));
+}
+
 bvhcd_status bvhcd_front_proximity(bvhcd_front *front, const float *pos, double thickness, bvhcd_proximity *out,
                                    int64_t cap, int64_t *count, int32_t out_on_device, void *stream) {
     if (!front) return BVHCD_INVALID_ARG;

@@ -1658,6 +1658,43 @@ bvhcd_status Front::export_front(int which, int32_t *out, int64_t cap, int64_t *
     return n > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
 }
 
+namespace {
+// The pairs and their count into mapped host memory (bvhcd_front_pairs_async).
+__global__ void k_pairs_to_host(const int2 *__restrict__ src, const unsigned *__restrict__ cnt, unsigned pcap,
+                                int2 *out, int64_t cap, int64_t *count) {
+    const unsigned n = min(*cnt, pcap);
+    const int64_t m = (int64_t)n < cap ? (int64_t)n : cap;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x)
+        out[q] = src[q];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *count = (int64_t)n;
+}
+}  // namespace
+
+bvhcd_status Front::pairs_async(int which, int32_t *host_out, int64_t cap, int64_t *host_count, cudaStream_t s) {
+    if (which < 0 || which > 1 || cap < 0 || !host_count || (cap > 0 && !host_out)) return BVHCD_INVALID_ARG;
+    void *dout = nullptr, *dcnt = nullptr;
+    if (cudaHostGetDevicePointer(&dcnt, host_count, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return BVHCD_INVALID_ARG;  // not mapped host memory
+    }
+    if (cap > 0 && cudaHostGetDevicePointer(&dout, host_out, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return BVHCD_INVALID_ARG;
+    }
+    const int2 *src = hits_.as<int2>();
+    const unsigned *cnt = counters() + C_HITS;
+    if (!which) {
+        bvhcd_status st = compact_pairs(s);
+        if (st != BVHCD_OK) return st;
+        src = outbuf_.as<int2>();
+        cnt = counters() + C_COMPACT;
+    }
+    k_pairs_to_host<<<kFrontBlocks, kThreads, 0, s>>>(src, cnt, (unsigned)pcap_, static_cast<int2 *>(dout), cap,
+                                                      static_cast<int64_t *>(dcnt));
+    note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
 bvhcd_status Front::device_results(const int32_t **hits, const int64_t **counts) {
     if (hits) *hits = hits_.as<int32_t>();
     if (counts) *counts = counts64_.as<int64_t>();

@@ -219,6 +219,7 @@ class Front {
     bvhcd_status contacts(int which, float *out, int64_t cap, int64_t *count, int64_t *flagged, bool out_dev,
                           cudaStream_t s);
     bvhcd_status device_results(const int32_t **hits, const int64_t **counts);
+    bvhcd_status pairs_async(int which, int32_t *host_out, int64_t cap, int64_t *host_count, cudaStream_t s);
 
     // Host-side state a maintain() call advances (see LBvh::HostState);
     // int_swapped: balance() exchanged the internal-front buffers of the two

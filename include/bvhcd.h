@@ -222,6 +222,20 @@ bvhcd_status bvhcd_front_pairs(bvhcd_front *front, int32_t which, int32_t *out, 
  * the last maintain on its stream; valid until the next maintain.  No sync. */
 bvhcd_status bvhcd_front_device_results(bvhcd_front *front, const int32_t **hit_pairs,
                                         const int64_t **counts);
+/* Asynchronous read-back: enqueues on `stream` a kernel that writes the pairs
+ * (which as in bvhcd_front_pairs, the same order) and their count straight
+ * into host memory from bvhcd_host_alloc, so nothing synchronises and the
+ * next frame can be enqueued at once; the results are valid once the stream
+ * has passed this point (an event).  At most cap pairs are written;
+ * *host_count receives the full count.  No counterpart in the reference,
+ * whose applyCpResults / inspectResults copy synchronously
+ * (BvttFrontLooseIntra.cu:50-67). */
+bvhcd_status bvhcd_front_pairs_async(bvhcd_front *front, int32_t which, int32_t *host_out, int64_t cap,
+                                     int64_t *host_count, void *stream);
+/* Pinned host memory mapped into the device's address space (for
+ * bvhcd_front_pairs_async), and its release. */
+bvhcd_status bvhcd_host_alloc(int64_t bytes, void **ptr);
+bvhcd_status bvhcd_host_free(void *ptr);
 /* Copies the current front (sorted-prim, node) entries; which = 0 internal,
  * 1 external.  Synchronises `stream`. */
 bvhcd_status bvhcd_front_export(bvhcd_front *front, int32_t which, int32_t *out, int64_t cap,

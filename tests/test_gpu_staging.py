@@ -76,3 +76,34 @@ def test_graph_frames_refuse_staged_positions(cuda, lib_built):
         bvhcd.frame_graph(bvh, front, staged, torch.from_numpy(faces).cuda(), bvhcd.BVH_BUILD,
                           bvhcd.FRONT_GENERATE, stream=s)
     assert err.value.status == 1  # BVHCD_INVALID_ARG
+
+
+def test_pairs_async_equal_synchronous_read(cuda, lib_built):
+    """bvhcd_front_pairs_async writes the same pairs, in the same order, as
+    bvhcd_front_pairs, into mapped host memory with no synchronisation;
+    capacity and unmapped memory behave as documented."""
+    import ctypes
+    bvhcd = lib_built
+    import scenes
+    faces, frames = scenes.cloth_over_sphere_frames(48, frames=4, sphere_freq=8)
+    T, V = faces.shape[0], frames[0].shape[0]
+    bvh = bvhcd.LBvh(T, V, enable_restr=True)
+    front = bvhcd.BvttFront(bvh, int_front_capacity=2_000_000, ext_front_capacity=2_000_000, pair_capacity=500_000)
+    bufs = [bvhcd.HostPairs(500_000) for _ in range(2)]
+    small = bvhcd.HostPairs(10)
+    stream = cuda.cuda.Stream()
+    for f, pos in enumerate(frames):
+        bvhcd.frame(bvh, front, f, 0, pos, faces, stream=stream)
+        front.pairs_async(bufs[0], narrow=False, stream=stream)
+        front.pairs_async(bufs[1], narrow=True, stream=stream)
+        front.pairs_async(small, narrow=False, stream=stream)
+        stream.synchronize()
+        broad, hits = front.pairs(narrow=False, stream=stream), front.pairs(narrow=True, stream=stream)
+        assert np.array_equal(bufs[0].read(), broad) and np.array_equal(bufs[1].read(), hits), f
+        assert small.count == broad.shape[0] and np.array_equal(small.read(), broad[:10])
+    pageable = np.zeros(4, np.int64)
+    st = bvhcd.lib().bvhcd_front_pairs_async(front.handle, 0, ctypes.c_void_p(pageable.ctypes.data + 16), 1,
+                                             ctypes.c_void_p(pageable.ctypes.data), None)
+    assert st == 1  # INVALID_ARG: not mapped host memory
+    for b in bufs + [small]:
+        b.close()
