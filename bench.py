@@ -308,10 +308,14 @@ def front_bytes(st_prev, st, T, uniq_nodes):
     return 8 * st_prev + 32 * T + 32 * uniq_nodes + 8 * st
 
 
-# DRAM bytes (read + write) of one k_keep_scan launch on this workload, from an
-# ncu capture (dram__bytes_read.sum 146.3 MB + dram__bytes_write.sum 3.6 MB)
-KEEP_SCAN_DRAM_BYTES = 149.9e6
-KEEP_SCAN_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_keep_scan launch, "
+# DRAM bytes (read + write) per keep on this workload, from an ncu capture of
+# its kernels: a full keep (k_keep_scan writing every expiry) 163.8 MB, a
+# selecting keep (k_keep_select 50.6 MB + k_keep_scan over the selected entries
+# 54.0 MB) 104.6 MB; the reference's schedule runs 2 full and 7 selecting keeps
+# per 12 frames, 117.8 MB per keep on average
+KEEP_SCAN_DRAM_BYTES = 117.8e6
+KEEP_SCAN_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_keep_scan / k_keep_select, "
+                         "averaged over the schedule's full and selecting keeps, "
                          "profiles/k_keep_scan_cloth512_sphere.md")
 
 
@@ -333,13 +337,22 @@ def roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
         flush.zero_()
         b, fr = bvhcd.schedule(f)
         bvhcd.frame(bvh, front, f, 0, dev[f], dfaces, stream=stream, faces_static=f > 0)
-        if f >= W and fr == bvhcd.FRONT_KEEP and n_keep < 3:
-            # algorithmic bytes of this keep launch: front entries, prim records,
-            # unique nodes referenced by the front, pairs written
+        if f >= W and fr == bvhcd.FRONT_KEEP:
+            # algorithmic bytes of this keep: a full keep reads every entry, the
+            # primitive record once per primitive and each referenced node
+            # record once, writes every entry's expiry and the pairs; a
+            # selecting keep reads every expiry, then for each tested entry its
+            # list index (written and read), the entry, both records and the
+            # new expiry, and writes the pairs
             st = front.stats(stream)
-            fi, fe = front.export(0, stream), front.export(1, stream)
-            uniq = len(np.unique(fi[:, 1])) + len(np.unique(fe[:, 1]))
-            keep_bytes += 8 * (st["int_front"] + st["ext_front"]) + 32 * T + 32 * uniq + 8 * st["broad_pairs"]
+            F = st["int_front"] + st["ext_front"]
+            tested = st["keep_tested"]
+            if tested >= F:
+                fi, fe = front.export(0, stream), front.export(1, stream)
+                uniq = len(np.unique(fi[:, 1])) + len(np.unique(fe[:, 1]))
+                keep_bytes += 12 * F + 32 * T + 32 * uniq + 8 * st["broad_pairs"]
+            else:
+                keep_bytes += 4 * F + tested * (4 + 4 + 8 + 64 + 4) + 8 * st["broad_pairs"]
             n_keep += 1
     times = bvh.stage_times()
     dom = max(times.items(), key=lambda kv: kv[1][0])

@@ -100,7 +100,7 @@ class FrontStats(ctypes.Structure):
                 ("overflow", ctypes.c_int32), ("bvh_opt_tag", ctypes.c_int32),
                 ("front_op_run", ctypes.c_int32), ("restr_pending", ctypes.c_int32),
                 ("num_rt_subtrees", ctypes.c_int32), ("num_rt_int_nodes", ctypes.c_int32),
-                ("flagged", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
+                ("flagged", ctypes.c_int32), ("keep_tested", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

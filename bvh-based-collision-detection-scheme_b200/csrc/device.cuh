@@ -63,13 +63,16 @@ enum CounterSlot {
     C_OVERFLOW = 6,           // bit0 int front, bit1 ext front, bit2 pairs, bit3 hits,
                               // bit4 traversal bound hit, bit5 sprout work list
     C_RT_SUBTREES = 7, C_RT_INTNODES = 8,
+    C_KSEL = 9,               // keep: front entries selected for a test (the rest wait on their expiries)
     C_WORK = 10,              // overlapping internal entries queued for traversal
     C_PAIRS_VALID = 11,       // broad-phase pairs (C_PAIRS counts reserved slots, holes included)
     C_COMPACT = 12,           // compaction cursor of the pair export
     C_FLAGGED = 13,           // precision mode: pairs re-decided in FP64
     C_TOPK = 14,              // refit plan: nodes whose leaf range crosses a refit block
     C_REFIT_DONE = 15,        // refit: leaf blocks finished (the last one runs the crossing nodes)
-    C_NUM = 16
+    C_DELTA = 16,             // refit: largest change of a leaf box coordinate (FP32 bits, rounded up)
+    C_MOTION = 17,            // refit: sum of those changes since the last build (FP32 bits, rounded up)
+    C_NUM = 18
 };
 
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }

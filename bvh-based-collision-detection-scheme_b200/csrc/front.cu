@@ -61,6 +61,15 @@ struct FArgs {
     unsigned cap_work;
     int cull;
     int T;
+    // keep-time expiries (keep only): motion is the tree's accumulated box
+    // motion (FP32 bits); the _in arrays give each entry's expiry (read by
+    // k_keep_select), the _out arrays receive the expiries of the entries
+    // tested; ksel lists the entries to test (indices into [0, F_int + F_ext)),
+    // or is null to test every entry
+    const unsigned *motion;
+    const float *iexp_in, *xexp_in;
+    float *iexp_out, *xexp_out;
+    const unsigned *ksel;
 };
 
 // A node's box and escape link: from the FP32 record ({lo.xyz, rangex},
@@ -295,19 +304,22 @@ __device__ __forceinline__ int prune_up(const FArgs &a, int n, int top, const fl
 template <int kU>
 struct Batch {
     int2 e[kU];
+    unsigned qi[kU];  // the entry's index in [0, F_int + F_ext)
     bool v[kU], in_int[kU];
     float4 plo[kU], phi[kU], nlo[kU], nhi[kU];
 };
 
 // entries q0 + k*stride (internal ones first in the index space, then
 // external ones)
-template <int kU>
+template <int kU, bool kKeep = false>
 __device__ __forceinline__ void load_ents(const FArgs &a, unsigned q0, unsigned stride, unsigned ni,
                                           unsigned total, Batch<kU> &b) {
 #pragma unroll
     for (int k = 0; k < kU; k++) {
-        const unsigned q = q0 + k * stride;
-        b.v[k] = q < total;
+        const unsigned p = q0 + k * stride;
+        b.v[k] = p < total;
+        const unsigned q = (kKeep && a.ksel && b.v[k]) ? __ldg(a.ksel + p) : p;
+        if (kKeep) b.qi[k] = q;
         b.in_int[k] = q < ni;
         b.e[k] = b.v[k] ? (b.in_int[k] ? __ldcs(&a.in_int[q]) : __ldcs(&a.in_ext[q - ni])) : make_int2(0, 0);
     }
@@ -326,11 +338,12 @@ __device__ __forceinline__ void load_recs(const FArgs &a, Batch<kU> &b) {
         }
     }
 }
-template <int kU>
+template <int kU, bool kKeep = false>
 __device__ __forceinline__ void take_ents(Batch<kU> &dst, const Batch<kU> &src) {
 #pragma unroll
     for (int k = 0; k < kU; k++) {
         dst.e[k] = src.e[k];
+        if (kKeep) dst.qi[k] = src.qi[k];
         dst.v[k] = src.v[k];
         dst.in_int[k] = src.in_int[k];
     }
@@ -426,24 +439,128 @@ __global__ void __launch_bounds__(kB) k_maintain_ext(FArgs a) {
     em_close(a, em);
 }
 
+// Keep-time expiries.  Between two refits every box of a tree moves by at
+// most the largest change of a leaf box coordinate (a node's box is a min /
+// max of leaf boxes); the refit sums those changes, rounded up, into the
+// tree's motion M.  A keep that finds an entry's boxes apart by a gap g (a
+// lower bound, rounded down, along their most separated axis) gives it the
+// expiry M + g / 2: while the motion stays below it the boxes stay apart and
+// the entry has nothing to emit.  An external entry of two triangles that
+// share a vertex never gives a pair while the faces stay the same (expiry
+// +inf); an entry that overlaps is tested every time (expiry -1).
+__device__ __forceinline__ float box_gap(const float4 &alo, const float4 &ahi, const float4 &blo, const float4 &bhi) {
+    float g = fmaxf(__fsub_rd(blo.x, ahi.x), __fsub_rd(alo.x, bhi.x));
+    g = fmaxf(g, fmaxf(__fsub_rd(blo.y, ahi.y), __fsub_rd(alo.y, bhi.y)));
+    return fmaxf(g, fmaxf(__fsub_rd(blo.z, ahi.z), __fsub_rd(alo.z, bhi.z)));
+}
+
+// The entries whose expiry the motion has reached, as a list of indices into
+// [0, F_int + F_ext).  The expiries are read as a stream and nothing else of a
+// waiting entry is touched.  A block takes tiles of kSelPer x 256 entries,
+// each warp kSelPer runs of 32: ballots count a warp's picks, a block scan in
+// shared memory places the warps, one atomic per tile reserves its run.
+constexpr int kSelPer = 8;
+__global__ void __launch_bounds__(kThreads) k_keep_select(FArgs a, unsigned *list, unsigned *count) {
+    __shared__ unsigned wsum[kThreads / 32], tbase;
+    const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
+    const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
+    const unsigned total = ni + ne;
+    const float M = __uint_as_float(*a.motion);
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr unsigned kTile = kSelPer * kThreads;
+    for (unsigned t0 = blockIdx.x * kTile; t0 < total; t0 += gridDim.x * kTile) {
+        float ex[kSelPer];
+#pragma unroll
+        for (int r = 0; r < kSelPer; r++) {  // every load of the tile in flight at once
+            const unsigned q = t0 + (warp * kSelPer + r) * 32u + lane;
+            ex[r] = q >= total ? 3.402823466e+38f : q < ni ? __ldcs(a.iexp_in + q) : __ldcs(a.xexp_in + (q - ni));
+        }
+        unsigned m[kSelPer], n = 0;
+#pragma unroll
+        for (int r = 0; r < kSelPer; r++) {
+            m[r] = __ballot_sync(0xffffffffu, !(M < ex[r]));
+            n += __popc(m[r]);
+        }
+        if (lane == 0) wsum[warp] = n;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned s = 0;
+            for (int w = 0; w < kThreads / 32; w++) {
+                const unsigned c = wsum[w];
+                wsum[w] = s;
+                s += c;
+            }
+            tbase = s ? atomicAdd(count, s) : 0u;
+        }
+        __syncthreads();
+        unsigned pos = tbase + wsum[warp];
+#pragma unroll
+        for (int r = 0; r < kSelPer; r++) {
+            if ((m[r] >> lane) & 1u) list[pos + __popc(m[r] & ((1u << lane) - 1u))] = t0 + (warp * kSelPer + r) * 32u + lane;
+            pos += __popc(m[r]);
+        }
+        __syncthreads();  // wsum and tbase are reused by the next tile
+    }
+}
+
+// An emission without per-lane chunks: the converged lanes that emit at the
+// same time take consecutive slots with one atomic, so nothing is reserved
+// unused (the selected keep runs few entries per lane, where chunks would
+// leave holes in most slots).
+__device__ __forceinline__ void put_dense(int2 *buf, unsigned *ctr, unsigned cap, const int2 &v, unsigned *ovf,
+                                          unsigned bit) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned b = 0;
+    if (g.thread_rank() == 0) b = atomicAdd(ctr, g.size());
+    const unsigned slot = g.shfl(b, 0) + g.thread_rank();
+    if (slot < cap) buf[slot] = v;
+    else atomicOr(ovf, bit);
+}
+
 // keepIntLooseIntraFronts / keepExtLooseIntraFronts (BvttFrontKeepKernels.cu:11-58)
-// in one index space: [0, F_int) internal entries, then external ones.
+// in one index space: [0, F_int) internal entries, then external ones; with
+// a selection list, only the listed entries, spread over every lane and
+// emitted densely.  With expiries out, every entry tested gets its new
+// expiry.
 template <int kU, int kB>
 __global__ void __launch_bounds__(kB) k_keep_scan(FArgs a) {
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
-    const Spread sp = spread<kScanMinPer>(ni + ne);
+    const unsigned total = a.ksel ? min(a.ctr[C_KSEL], ni + ne) : ni + ne;
+    const float M = a.motion ? __uint_as_float(*a.motion) : 0.f;
+    const Spread sp = a.ksel ? spread<1>(total) : spread<kScanMinPer>(total);
     Batch<kU> b, nb;
-    load_ents(a, sp.start, sp.stride, ni, ni + ne, b);
-    for (unsigned q0 = sp.start; q0 < ni + ne; q0 += kU * sp.stride, take_ents(b, nb)) {
-        load_ents(a, q0 + kU * sp.stride, sp.stride, ni, ni + ne, nb);
+    load_ents<kU, true>(a, sp.start, sp.stride, ni, total, b);
+    for (unsigned q0 = sp.start; q0 < total; q0 += kU * sp.stride, take_ents<kU, true>(b, nb)) {
+        load_ents<kU, true>(a, q0 + kU * sp.stride, sp.stride, ni, total, nb);
         load_recs(a, b);
 #pragma unroll
         for (int k = 0; k < kU; k++) {
-            if (!b.v[k] || !overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k])) continue;
-            if (b.in_int[k]) emit_work(a, em, b.e[k]);
-            else emit_pair(a, em, b.e[k].x, prim_face(a, b.e[k].x), b.e[k].y);
+            if (!b.v[k]) continue;
+            const bool ov = overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k]);
+            if (b.in_int[k]) {
+                if (a.iexp_out)
+                    a.iexp_out[b.qi[k]] =
+                        ov ? -1.f : __fadd_rd(M, __fmul_rd(box_gap(b.plo[k], b.phi[k], b.nlo[k], b.nhi[k]), 0.5f));
+                if (ov) {
+                    if (a.ksel) put_dense(a.work, a.ctr + C_WORK, a.cap_work, b.e[k], a.ctr + C_OVERFLOW, 32u);
+                    else emit_work(a, em, b.e[k]);
+                }
+                continue;
+            }
+            if (!a.xexp_out) {
+                if (ov) emit_pair(a, em, b.e[k].x, prim_face(a, b.e[k].x), b.e[k].y);
+                continue;
+            }
+            const bool adj = a.cull && covertex(prim_face(a, b.e[k].x), __ldg(&a.sface[b.e[k].y]));
+            a.xexp_out[b.qi[k] - ni] =
+                adj ? 3.402823466e+38f
+                    : (ov ? -1.f : __fadd_rd(M, __fmul_rd(box_gap(b.plo[k], b.phi[k], b.nlo[k], b.nhi[k]), 0.5f)));
+            if (ov && !adj) {
+                if (a.ksel) put_dense(a.pairs, a.ctr + C_PAIRS, a.cap_pairs, b.e[k], a.ctr + C_OVERFLOW, 4u);
+                else chunk_put(a.pairs, a.ctr + C_PAIRS, a.cap_pairs, em.pr, b.e[k], a.ctr + C_OVERFLOW, 4u);
+            }
         }
     }
     em_close(a, em);
@@ -900,7 +1017,7 @@ Front::~Front() {
         for (auto &b : set) b.release();
     DBuf *bufs[] = {&pairs_, &hits_, &outbuf_, &work_, &intcnt_, &extcnt_, &intbeg_, &extbeg_, &intback_,
                     &extback_, &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_, &fctr_, &rcur_,
-                    &pxbuf_, &pxout_};
+                    &pxbuf_, &pxout_, &iexp_, &xexp_, &ksel_};
     for (DBuf *b : bufs) b->release();
 }
 
@@ -923,6 +1040,9 @@ bvhcd_status Front::init() {
     FR_TRY(pairs_.reserve(sizeof(int2) * (size_t)pcap_));
     FR_TRY(hits_.reserve(sizeof(int2) * (size_t)pcap_));
     FR_TRY(work_.reserve(sizeof(int2) * (size_t)fcap_[0]));
+    FR_TRY(iexp_.reserve(sizeof(float) * (size_t)fcap_[0]));
+    FR_TRY(xexp_.reserve(sizeof(float) * (size_t)fcap_[1]));
+    FR_TRY(ksel_.reserve(sizeof(unsigned) * (size_t)(fcap_[0] + fcap_[1])));
     FR_TRY(counts64_.reserve(sizeof(int64_t) * 2));
     FR_TRY(fctr_.reserve(sizeof(unsigned) * C_NUM));
     FR_TRY(cudaMemset(fctr_.p, 0, sizeof(unsigned) * C_NUM));
@@ -988,6 +1108,10 @@ static FArgs make_args(const LBvh *bvh, const LBvh *trav, unsigned *ctr, const F
     a.cap_work = (unsigned)(cap_work < 0xffffffffLL ? cap_work : 0xffffffffLL);
     a.cull = trav ? 0 : cull;  // vertex sharing means nothing across two meshes
     a.T = t.T;
+    a.motion = nullptr;
+    a.iexp_in = a.xexp_in = nullptr;
+    a.iexp_out = a.xexp_out = nullptr;
+    a.ksel = nullptr;
     return a;
 }
 
@@ -1013,6 +1137,7 @@ bvhcd_status Front::reorder(cudaStream_t s) {
     const int T = bvh_->T();
     FrontLog l = log();
     FR_TRY(log_prepare(l, T, scratch_.p, s));
+    exp_valid_ = false;  // the fronts move
     const size_t ng = reorder_groups(T);
     FR_TRY(cudaMemsetAsync(rcur_.p, 0, sizeof(unsigned) * 2 * ng, s));
     FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
@@ -1135,7 +1260,30 @@ bvhcd_status Front::keep(cudaStream_t s) {
     a.cap_pairs = (unsigned)pcap_;
     FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
     FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
+    // expiries: an intra front over FP32 node boxes (an inter front's
+    // primitives move with another tree; FP16 boxes move by their rounding too)
+    const bool expiries = !inter() && !cfg_.precision && !bvh_->tree().nrec16;
+    if (exp_epoch_ != bvh_->topo_epoch() || exp_faces_ != bvh_->faces_epoch()) exp_valid_ = false;
+    if (expiries) {
+        a.motion = bvh_->counters() + C_MOTION;
+        a.iexp_out = iexp_.as<float>();
+        a.xexp_out = xexp_.as<float>();
+        if (exp_valid_) {
+            a.iexp_in = iexp_.as<float>();
+            a.xexp_in = xexp_.as<float>();
+            FR_TRY(cudaMemsetAsync(ctr + C_KSEL, 0, sizeof(unsigned), s));
+            k_keep_select<<<RESIDENT(k_keep_select), kThreads, 0, s>>>(a, ksel_.as<unsigned>(), ctr + C_KSEL);
+            note_launch();
+            a.ksel = ksel_.as<unsigned>();
+        }
+    }
+    last_keep_sel_ = a.ksel != nullptr;
     LAUNCH_SCAN(k_keep_scan, shape_[BVHCD_SHAPE_KEEP], s, a);
+    if (expiries) {
+        exp_valid_ = true;
+        exp_epoch_ = bvh_->topo_epoch();
+        exp_faces_ = bvh_->faces_epoch();
+    }
     LAUNCH_ITEM(k_sprout, false, shape_[BVHCD_SHAPE_SPROUT], s, a);
     return cuda_status(cudaGetLastError());
 }
@@ -1156,6 +1304,7 @@ bvhcd_status Front::balance_kernels(cudaStream_t s) {
     if (log_counted_) FR_TRY(log_prepare(l, T, scratch_.p, s));
     FR_TRY(log_clear(l, T, s));
     log_counted_ = false;
+    exp_valid_ = false;  // the internal front moves
     FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
     const int nx = 1 - cur_;
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
@@ -1250,7 +1399,17 @@ bvhcd_status Front::grow_and_check(cudaStream_t s, bool *overflowed) {
             // every work item comes from one internal entry of the input front
             work_.release();
             FR_TRY(work_.reserve(sizeof(int2) * (size_t)nc));
+            iexp_.release();
+            FR_TRY(iexp_.reserve(sizeof(float) * (size_t)nc));
+        } else {
+            xexp_.release();
+            FR_TRY(xexp_.reserve(sizeof(float) * (size_t)nc));
         }
+        exp_valid_ = false;
+    }
+    if ((size_t)(fcap_[0] + fcap_[1]) * sizeof(unsigned) > ksel_.bytes) {
+        ksel_.release();
+        FR_TRY(ksel_.reserve(sizeof(unsigned) * (size_t)(fcap_[0] + fcap_[1])));
     }
     if (npc != pcap_) {
         pairs_.release();
@@ -1340,6 +1499,7 @@ bvhcd_status Front::copy_state_from(const Front &src, cudaStream_t s) {
     has_front_ = src.has_front_;
     int_swapped_ = src.int_swapped_;
     log_counted_ = src.log_counted_;
+    exp_valid_ = false;
     for (int k = 0; k < BVHCD_SHAPE_COUNT; k++) shape_[k] = src.shape_[k];
     shape_epoch_++;
     return cuda_status(cudaGetLastError());
@@ -1454,6 +1614,7 @@ bvhcd_status Front::stats(bvhcd_front_stats *st, cudaStream_t s) {
     st->num_rt_subtrees = bvh_->last_rt_subtrees();
     st->num_rt_int_nodes = bvh_->last_rt_intnodes();
     st->flagged = (int32_t)h[C_FLAGGED];
+    st->keep_tested = last_keep_sel_ ? (int32_t)h[C_KSEL] : (int32_t)(h[2 * cur_] + h[2 * cur_ + 1]);
     return BVHCD_OK;
 }
 

@@ -463,6 +463,8 @@ __device__ __forceinline__ void box_empty(float4 &lo, float4 &hi) {
     hi = make_float4(-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f, 0.f);
 }
 // boxes as 6 floats (24 bytes, 8-byte aligned): three 64-bit accesses
+// |b - a| rounded up
+__device__ __forceinline__ float box_change(float a, float b) { return fmaxf(__fsub_ru(b, a), __fsub_ru(a, b)); }
 __device__ __forceinline__ void box_store6(float *b, const float4 &lo, const float4 &hi) {
     float2 *q = reinterpret_cast<float2 *>(b);
     q[0] = make_float2(lo.x, lo.y);
@@ -716,6 +718,8 @@ struct RefitTop {
     const float *gext;  // 2 export slots per crossing node
     float *gbox;        // crossing-node slots when shared memory is too small
     unsigned *done;     // leaf blocks finished
+    unsigned *delta;    // largest leaf box change of this refit (FP32 bits)
+    unsigned *motion;   // accumulated leaf box change (FP32 bits)
 };
 
 // The crossing nodes, run by the CTA that finished last: a node's slot
@@ -806,14 +810,21 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
     extern __shared__ __align__(16) float sb[];  // boxes: the block's leaves, then its nodes
     int *slist = reinterpret_cast<int *>(sb + 12 * kRefitW);
     __shared__ int sofs[kLevelHdr], hmax, last;
+    __shared__ unsigned sdelta;
     const int L0 = blockIdx.x * kRefitW;
     const int nl = min(kRefitW, T - L0);
     const int *hdr = lhdr + (size_t)blockIdx.x * kLevelHdr;
-    if (threadIdx.x == 0) hmax = 0;
+    if (threadIdx.x == 0) {
+        hmax = 0;
+        sdelta = 0u;
+    }
     const int L = __ldg(&hdr[0]);
     const int nloc = L >= 0 ? __ldg(&hdr[2 + L]) : 0;
     if (L >= 0 && threadIdx.x <= L + 1) sofs[threadIdx.x] = __ldg(&hdr[1 + threadIdx.x]);
     int4 w[kRefitSlots];
+    // the largest change of a leaf box coordinate, rounded up: a bound on how
+    // far any box of the tree moved (a node's box is a min / max of leaf boxes)
+    float dmax = 0.f;
 #pragma unroll
     for (int i = 0; i < kRefitSlots; i++) {
         const int t = threadIdx.x + i * kRefitThreads;
@@ -822,13 +833,19 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
         if (t >= nl) continue;
         const int4 f = __ldg(&sface[L0 + t]);
         const int2 lk = __ldg(&llink[L0 + t]);
+        const float4 olo = __ldcg(lrec + 2 * (size_t)(L0 + t)), ohi = __ldcg(lrec + 2 * (size_t)(L0 + t) + 1);
         float4 lo, hi;
         face_box(p, f, lo, hi);
+        dmax = fmaxf(dmax, fmaxf(box_change(olo.x, lo.x), fmaxf(box_change(olo.y, lo.y), box_change(olo.z, lo.z))));
+        dmax = fmaxf(dmax, fmaxf(box_change(ohi.x, hi.x), fmaxf(box_change(ohi.y, hi.y), box_change(ohi.z, hi.z))));
         box_store6(sb + 6 * t, lo, hi);
         lo.w = __int_as_float(lk.x);
         hi.w = __int_as_float(lk.y);
         stg8(lrec + 2 * (size_t)(L0 + t), lo, hi);
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&sdelta, __float_as_uint(dmax));  // non-negative: bit order
     __syncthreads();
     if (L >= 0) {
         run_levels<kRefitThreads>(sofs, L, __ldg(&hdr[kHdrNarrow]), [&](int t) {
@@ -881,7 +898,11 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
             rec_store_box(nrec + 2 * (size_t)e[i].x, lo, hi);
         }
     }
-    if (gridDim.x == 1) return;  // one block: no node crosses
+    if (gridDim.x == 1) {  // one block: no node crosses
+        if (threadIdx.x == 0)
+            *g.motion = __float_as_uint(__fadd_ru(__uint_as_float(*g.motion), __uint_as_float(sdelta)));
+        return;
+    }
     const int nex = __ldg(&hdr[kHdrCount]);
     for (int x = threadIdx.x; x < nex; x += blockDim.x) {
         const int4 ex = __ldg(&lexport[(size_t)L0 + x]);
@@ -895,6 +916,7 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
     // the last CTA to finish runs the crossing nodes
     __syncthreads();
     if (threadIdx.x == 0) {
+        atomicMax(g.delta, sdelta);
         __threadfence();
         last = atomicAdd(g.done, 1u) == gridDim.x - 1;
     }
@@ -902,7 +924,11 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
     if (!last) return;
     __threadfence();
     refit_top(g, nrec, sb, sofs);
-    if (threadIdx.x == 0) *g.done = 0u;
+    if (threadIdx.x == 0) {
+        *g.done = 0u;
+        const float d = __uint_as_float(atomicExch(g.delta, 0u));
+        *g.motion = __float_as_uint(__fadd_ru(__uint_as_float(*g.motion), d));
+    }
 }
 
 // ---------------------------------------------------------------- FP16 node records
@@ -1302,12 +1328,14 @@ bvhcd_status LBvh::upload(const bvhcd_scene &sc, cudaStream_t s) {
             stage_pending_ = false;
         }
         vptr_ = sc.pos;
+        if (fptr_ != sc.faces || !sc.faces_static) faces_epoch_++;
         fptr_ = sc.faces;
     } else {
         if (sc.num_vertices)
             BV_TRY(cudaMemcpyAsync(verts_.p, sc.pos, sizeof(float) * 3 * (size_t)sc.num_vertices,
                                    cudaMemcpyHostToDevice, s));
         bool same = sc.faces_static && built_ && fptr_ == faces_.as<int>() && T_ == sc.num_faces;
+        if (!same) faces_epoch_++;
         if (!same && sc.num_faces)
             BV_TRY(cudaMemcpyAsync(faces_.p, sc.faces, sizeof(int) * 3 * (size_t)sc.num_faces,
                                    cudaMemcpyHostToDevice, s));
@@ -1338,6 +1366,7 @@ bvhcd_status LBvh::upload_boxes(const bvhcd_box_scene &sc, cudaStream_t s) {
     const bool convert = sc.boxes_f64 != 0;
     if (convert || !sc.on_device) BV_TRY(boxes_.reserve(sizeof(float) * 6 * (T > 0 ? T : 1)));
     if (sc.on_device) {
+        if (fptr_ != sc.faces || !sc.faces_static) faces_epoch_++;
         fptr_ = sc.faces;
         if (convert && T) {
             k_boxes_f64<<<grid_for((int64_t)(6 * T)), kThreads, 0, s>>>((int64_t)(6 * T),
@@ -1348,6 +1377,7 @@ bvhcd_status LBvh::upload_boxes(const bvhcd_box_scene &sc, cudaStream_t s) {
         bptr_ = convert ? boxes_.as<float>() : static_cast<const float *>(sc.boxes);
     } else {
         bool same = sc.faces_static && built_ && fptr_ == faces_.as<int>() && T_ == sc.num_faces;
+        if (!same) faces_epoch_++;
         if (!same && T)
             BV_TRY(cudaMemcpyAsync(faces_.p, sc.faces, sizeof(int) * 3 * T, cudaMemcpyHostToDevice, s));
         fptr_ = faces_.as<int>();
@@ -1394,6 +1424,8 @@ bvhcd_status LBvh::build(cudaStream_t s) {
     StageScope prof_scope(&prof_, BVHCD_STAGE_BVH_BUILD, s);
     const int T = T_;
     built_ = false;
+    // a new topology: the accumulated box motion starts again
+    BV_TRY(cudaMemsetAsync(ctr_.as<unsigned>() + C_DELTA, 0, 2 * sizeof(unsigned), s));
     if (T == 0) { built_ = true; return BVHCD_OK; }
     int *leafscene = nullptr;
     if (S_ > 1) {
@@ -1487,6 +1519,7 @@ bvhcd_status LBvh::copy_state_from(const LBvh &src, cudaStream_t s) {
     S_ = src.S_; ntiles_ = src.ntiles_; h_off_ = src.h_off_;
     epoch_++;
     topo_epoch_++;
+    faces_epoch_++;
     return cuda_status(cudaGetLastError());
 }
 
@@ -1575,6 +1608,8 @@ bvhcd_status LBvh::refit(cudaStream_t s) {
     g.gext = gext_.as<float>();
     g.gbox = gbox_.as<float>();
     g.done = ctr_.as<unsigned>() + C_REFIT_DONE;
+    g.delta = ctr_.as<unsigned>() + C_DELTA;
+    g.motion = ctr_.as<unsigned>() + C_MOTION;
     const int nb = (T + kRefitW - 1) / kRefitW;
     k_refit<<<nb, kRefitThreads, kLocalSmem, s>>>(T, sface_.as<int4>(), src(), plan_.as<int4>(), llist_.as<int4>(),
                                                   llink_.as<int2>(), lexport_.as<int4>(), lhdr_.as<int>(),
@@ -1657,6 +1692,9 @@ bvhcd_status LBvh::restructure(cudaStream_t s) {
     BV_TRY(cudaGetLastError());
     opt_tag_ = 1;
     topo_epoch_++;
+    // a new topology (the refit above saw leaves change slots): the
+    // accumulated box motion starts again
+    BV_TRY(cudaMemsetAsync(ctr_.as<unsigned>() + C_DELTA, 0, 2 * sizeof(unsigned), s));
     // the confined rebuild can change the heights of the subtrees' ancestors
     return refit_plan(s, false);
 }

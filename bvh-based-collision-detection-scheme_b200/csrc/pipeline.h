@@ -132,6 +132,8 @@ class LBvh {
     // advances whenever the topology (and so the leaf order) changes: build,
     // restructure, state copy
     int topo_epoch() const { return topo_epoch_; }
+    // advances whenever the faces (vertex ids) may have changed
+    int faces_epoch() const { return faces_epoch_; }
     const float *verts() const { return vptr_; }
     const int *faces() const { return fptr_; }
     bool restr_enabled() const { return cfg_.enable_restr != 0; }
@@ -189,7 +191,7 @@ class LBvh {
     DBuf intrange_, rtroot_, intmark_, extrange_, extmark_, leafroot_, flagbuf_;
     // batched scenes: S_ scenes, triangle offsets, per-triangle scene id,
     // per-slot scene id, per-scene boxes, box-reduction tiles
-    int S_ = 1, ntiles_ = 0, epoch_ = 0, topo_epoch_ = 0;
+    int S_ = 1, ntiles_ = 0, epoch_ = 0, topo_epoch_ = 0, faces_epoch_ = 0;
     std::vector<int> h_off_;
     DBuf scene_of_, leafscene_, sbox_, tiles_;
     DBuf ctr_;
@@ -226,15 +228,20 @@ class Front {
     // sets an odd number of times; log_counted: the log's per-node counts
     // describe the current front (a balance leaves only its begins valid).
     struct HostState {
-        int cur, last_op;
-        bool has_front, int_swapped, log_counted;
+        int cur, last_op, exp_epoch, exp_faces;
+        bool has_front, int_swapped, log_counted, exp_valid;
     };
-    HostState host_state() const { return HostState{cur_, last_op_, has_front_, int_swapped_, log_counted_}; }
+    HostState host_state() const {
+        return HostState{cur_, last_op_, exp_epoch_, exp_faces_, has_front_, int_swapped_, log_counted_, exp_valid_};
+    }
     void set_host_state(const HostState &h) {
         cur_ = h.cur;
         last_op_ = h.last_op;
+        exp_epoch_ = h.exp_epoch;
+        exp_faces_ = h.exp_faces;
         has_front_ = h.has_front;
         log_counted_ = h.log_counted;
+        exp_valid_ = h.exp_valid;
         if (h.int_swapped != int_swapped_) {
             std::swap(front_[0][0], front_[1][0]);
             int_swapped_ = h.int_swapped;
@@ -291,6 +298,13 @@ class Front {
     bool has_front_ = false;
     bool int_swapped_ = false;
     bool log_counted_ = true;
+    // keep-time expiries of the front entries (one float per entry of the
+    // current set's internal / external front), valid until the fronts move,
+    // the tree's topology changes or new faces arrive; ksel_: the entries a
+    // keep selects for a test
+    DBuf iexp_, xexp_, ksel_;
+    bool exp_valid_ = false, last_keep_sel_ = false;
+    int exp_epoch_ = -1, exp_faces_ = -1;
     bool quality_check_ = true;
     DBuf front_[2][2];  // [set][0 int, 1 ext] int2 entries
     int64_t fcap_[2] = {0, 0};

@@ -119,7 +119,9 @@ typedef struct {
     int32_t num_rt_subtrees; /* restructure decision inputs (LBvhFixedDeformable.cu:240-241) */
     int32_t num_rt_int_nodes;
     int32_t flagged;         /* precision mode: pairs the narrow phase re-decided in FP64 */
-    int32_t reserved[5];
+    int32_t keep_tested;     /* entries the last KEEP tested: all of them, or those whose
+                                expiry had come (the others cannot have changed state) */
+    int32_t reserved[4];
 } bvhcd_front_stats;
 
 typedef struct bvhcd_bvh bvhcd_bvh;

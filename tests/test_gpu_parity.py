@@ -64,7 +64,7 @@ def test_pipeline_parity_over_schedule(cuda, lib_built, oracle, cloth_c1, cull):
     p = oracle.Pipeline(True, bool(cull), True)
     for f, pos in enumerate(frames):
         b, fr = lib_built.schedule(f)
-        bvh.maintain(b, pos, faces)
+        bvh.maintain(b, pos, faces, faces_static=f > 0)  # unchanged faces: keeps may skip entries
         front.maintain(fr)
         p.frame(faces, pos, b, fr)
         st, info = front.stats(), p.info()
@@ -108,6 +108,28 @@ def test_any_operation_order(cuda, lib_built, oracle, cloth_c1):
         for which in (0, 1):
             assert np.array_equal(sorted_rows(front.export(which)), sorted_rows(p.front(which))), (f, which)
         assert np.array_equal(canon(front.pairs()), oracle.brute_pairs(faces, frames[f], 1)), f
+        assert np.array_equal(canon(front.pairs(narrow=True)), canon(p.pairs(narrow=True))), f
+
+
+@pytest.mark.parametrize("step", [1, 4])
+def test_long_keep_runs(cuda, lib_built, oracle, step):
+    """A generation followed by keeps only, with the motion per frame scaled by
+    `step` (frames skipped): the keep's expiries must never hold back an entry
+    whose boxes have come to overlap.  Fronts and pairs equal the oracle's
+    every frame."""
+    import scenes
+    faces, frames = scenes.cloth_over_sphere_frames(64, frames=1 + 12 * step, sphere_freq=8)
+    frames = frames[::step]
+    bvh, front = _new(lib_built, faces.shape[0], frames[0].shape[0], restr=False)
+    p = oracle.Pipeline(False, True, True)
+    for f, pos in enumerate(frames):
+        op = (0, 1) if f == 0 else (1, 4)
+        bvh.maintain(op[0], pos, faces, faces_static=f > 0)
+        front.maintain(op[1])
+        p.frame(faces, pos, *op)
+        for which in (0, 1):
+            assert np.array_equal(sorted_rows(front.export(which)), sorted_rows(p.front(which))), (f, which)
+        assert np.array_equal(canon(front.pairs()), canon(p.pairs())), f
         assert np.array_equal(canon(front.pairs(narrow=True)), canon(p.pairs(narrow=True))), f
 
 
