@@ -271,9 +271,9 @@ def evaluate(torch, weights, n, frames, seed, check_every=1, decide_every=3):
         for f in range(frames):
             ev[2 * f].record()
             if mode == "heuristic":
-                bvhcd.frame(bvh, front, f, 0, dpos[f], dfaces)
+                bvhcd.frame(bvh, front, f, 0, dpos[f], dfaces, faces_static=f > 0)
             elif mode == "cycle":
-                bvh.maintain(bvhcd.BVH_BUILD if f == 0 else bvhcd.BVH_REFIT, dpos[f], dfaces)
+                bvh.maintain(bvhcd.BVH_BUILD if f == 0 else bvhcd.BVH_REFIT, dpos[f], dfaces, faces_static=f > 0)
                 front.maintain(bvhcd.FRONT_GENERATE if f == 0 else cycle_front_op(f))
             else:
                 tag, op = lrn.frame(dpos[f], dfaces, f)
