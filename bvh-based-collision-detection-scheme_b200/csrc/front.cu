@@ -553,7 +553,8 @@ __global__ void __launch_bounds__(kB) k_keep_scan(FArgs a) {
                 if (ov) emit_pair(a, em, b.e[k].x, prim_face(a, b.e[k].x), b.e[k].y);
                 continue;
             }
-            const bool adj = a.cull && covertex(prim_face(a, b.e[k].x), __ldg(&a.sface[b.e[k].y]));
+            // (faces are read only for overlapping entries; a separated one waits on its gap)
+            const bool adj = ov && a.cull && covertex(prim_face(a, b.e[k].x), __ldg(&a.sface[b.e[k].y]));
             a.xexp_out[b.qi[k] - ni] =
                 adj ? 3.402823466e+38f
                     : (ov ? -1.f : __fadd_rd(M, __fmul_rd(box_gap(b.plo[k], b.phi[k], b.nlo[k], b.nhi[k]), 0.5f)));
