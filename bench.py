@@ -316,7 +316,7 @@ def front_bytes(st_prev, st, T, uniq_nodes):
 KEEP_SCAN_DRAM_BYTES = 117.8e6
 KEEP_SCAN_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_keep_scan / k_keep_select, "
                          "averaged over the schedule's full and selecting keeps, "
-                         "profiles/k_keep_scan_cloth512_sphere.md")
+                         "the keep-stage capture summarised under profiles/")
 
 
 def roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
