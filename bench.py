@@ -112,9 +112,12 @@ def dist_setup():
     return world, rank, local
 
 
+CLOTH = 512  # cloth side in vertices (--cloth; 512 is the headline workload)
+
+
 def make_frames(n):
     import scenes
-    return scenes.cloth_over_sphere_frames(512, n)
+    return scenes.cloth_over_sphere_frames(CLOTH, n)
 
 
 def run_ours(args):
@@ -168,7 +171,7 @@ def run_ours(args):
     per = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     dev_ms = float(sum(per))
     st = front.stats()
-    if st["overflow"]:
+    if st["overflow_any"]:  # sticky: any overflow in any warm-up or timed frame
         raise RuntimeError(f"front/pair capacity overflow during the bench: {st}")
     if world > 1:
         t = torch.tensor([dev_ms], device="cuda")
@@ -177,11 +180,12 @@ def run_ours(args):
         dist.barrier()
     value = dev_ms / (K * world)
 
-    e2e = roof = batched = fp16 = inter = boxes = prox = None
+    e2e = roof = batched = fp16 = inter = boxes = prox = grow = None
     if not args.only_value:
         e2e = e2e_pass(bvhcd, torch, pipeline, host, faces, dfaces, flush, stream, W, K, V, world)
         # roofline of the dominant stage, from a stage-timed replay
         roof = roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
+        grow = autogrow_pass(bvhcd, torch, dev, dfaces, stream, W, K, T)
         fp16 = fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
         inter = inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, st)
         boxes = box_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
@@ -202,7 +206,7 @@ def run_ours(args):
             "metric": METRIC, "value": round(value, 4), "unit": "ms/frame", "n_gpus": world,
             "steps": K, "warmup": W, "ms_per_step": round(value * world, 4), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "triangles": T, "vertices": V,
+            "config": {"workload": WORKLOAD if CLOTH == 512 else f"cloth{CLOTH}_over_icosphere45", "triangles": T, "vertices": V,
                        "frames_timed": K, "schedule": "build/12, front cycle 6 (STATIC_MANDATORY, divergent marks)",
                        "restructure": "quality-triggered (enabled)", "adjacency_culling": True,
                        "narrow_phase": "fp32 17-axis SAT",
@@ -217,6 +221,7 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "roofline": roof,
             "clocks": clk.summary(),
+            "auto_grow": grow,
             "fp16_node_boxes": fp16,
             "inter_rigid_obstacle": inter,
             "box_scene": boxes,
@@ -300,74 +305,146 @@ def e2e_pass(bvhcd, torch, pipeline, host, faces, dfaces, flush, stream, W, K, V
             "pairs_equal_synchronous_read": same}
 
 
-def front_bytes(st_prev, st, T, uniq_nodes):
-    """Algorithmic bytes of one front traversal stage (keep / update):
-    8 B per input front entry, 12 B per output entry (entry + per-node count),
-    32 B per primitive record, 32 B per unique tree record touched, 8 B per
-    pair written."""
-    return 8 * st_prev + 32 * T + 32 * uniq_nodes + 8 * st
+# Per-stage DRAM traffic (read + write bytes per call) of this workload, from
+# the ncu captures summarised in the profiles folder: the file lists, per
+# stage, the summed dram__bytes of that stage's kernels per call.
+STAGE_TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_per_stage_cloth512_sphere.txt")
 
 
-# DRAM bytes (read + write) per keep on this workload, from an ncu capture of
-# its kernels: a full keep (k_keep_scan writing every expiry) 163.8 MB, a
-# selecting keep (k_keep_select 50.6 MB + k_keep_scan over the selected entries
-# 54.0 MB) 104.6 MB; the reference's schedule runs 2 full and 7 selecting keeps
-# per 12 frames, 117.8 MB per keep on average
-KEEP_SCAN_DRAM_BYTES = 117.8e6
-KEEP_SCAN_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_keep_scan / k_keep_select, "
-                         "averaged over the schedule's full and selecting keeps, "
-                         "the keep-stage capture summarised under profiles/")
+def _stage_traffic():
+    out = {}
+    try:
+        with open(STAGE_TRAFFIC_FILE) as f:
+            for line in f:
+                line = line.split("#", 1)[0].split()
+                if len(line) == 2:
+                    out[line[0]] = float(line[1])
+    except OSError:
+        pass
+    return out
+
+
+def _uniq_nodes(front):
+    """Distinct tree records a front references (internal nodes of the
+    internal front, leaves of the external one): the U of the algorithmic-
+    bytes formulas, counted on the exported front (a lower bound of the
+    records a traversal touches)."""
+    fi, fe = front.export(0), front.export(1)
+    return len(np.unique(fi[:, 1])) + len(np.unique(fe[:, 1]))
+
+
+def stage_bytes(stage, T, V, F_in, F_out, U, P, H, pairs=None, faces=None, passes=4):
+    """Algorithmic bytes of one call of a stage, per the hot-path scope
+    table's measurement formulas (FP32 records):
+      refit   12V + 12T + 24T + 24(T-1)*3 + 8(T-1)
+      build   refit + 8T + 16T per radix pass + 16T + 8T
+      front maintenance (generate / update / keep / balance)
+              8 F_in + 12 F_out + 24T + 32U + 8P
+      reorder 16F + 4(2T) + 4(2T)*2
+      narrow  8P + 12 T_touched + 12 V_touched + 8H"""
+    refit = 12 * V + 12 * T + 24 * T + 24 * (T - 1) * 3 + 8 * (T - 1)
+    if stage == "bvh_refit":
+        return refit
+    if stage == "bvh_build":
+        return refit + 8 * T + 16 * T * passes + 16 * T + 8 * T
+    if stage in ("front_generate", "front_update", "front_keep", "front_balance"):
+        return 8 * F_in + 12 * F_out + 24 * T + 32 * U + 8 * P
+    if stage == "front_reorder":
+        return 16 * F_out + 4 * 2 * T + 4 * 2 * T * 2
+    if stage == "narrow":
+        tt = len(np.unique(pairs)) if pairs is not None and len(pairs) else 0
+        vt = len(np.unique(faces[np.unique(pairs)])) if tt else 0
+        return 8 * P + 12 * tt + 12 * vt + 8 * H
+    return None
 
 
 def roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
-    """Replays the frames with stage events on; the stage with the largest
-    total time is the dominant one.  For it: average event duration per
-    launch, algorithmic bytes per launch, fraction of the measured HBM copy
-    bandwidth."""
+    """Replays the frames with stage events on and reads the stage times after
+    every frame.  For every stage: calls, average event time per call,
+    algorithmic bytes per call (stage_bytes, with this run's front sizes,
+    pair counts and distinct records), achieved GB/s and its fraction of the
+    measured HBM copy bandwidth, and the DRAM traffic per call from the ncu
+    capture of the stage's kernels.  The top-level figures are those of the
+    dominant stage (the largest total time over the timed frames)."""
     peak, kind = _peaks()
-    bvh = bvhcd.LBvh(T, dev.shape[1], enable_restr=True)
+    V = dev.shape[1]
+    traffic = _stage_traffic()
+    bvh = bvhcd.LBvh(T, V, enable_restr=True)
     front = bvhcd.BvttFront(bvh, cull_adjacent=True, narrow_phase=True, auto_grow=False, **CAPS)
     bvh.profile(True)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    n_keep = 0
-    keep_bytes = 0.0
+    acc = {}   # stage -> [ms, calls, bytes]
+    prev = None
+    U = 0
     for f in range(W + K):
-        if f == W:
-            bvh.stage_times(reset=True)
         flush.zero_()
-        b, fr = bvhcd.schedule(f)
         bvhcd.frame(bvh, front, f, 0, dev[f], dfaces, stream=stream, faces_static=f > 0)
-        if f >= W and fr == bvhcd.FRONT_KEEP:
-            # algorithmic bytes of this keep: a full keep reads every entry, the
-            # primitive record once per primitive and each referenced node
-            # record once, writes every entry's expiry and the pairs; a
-            # selecting keep reads every expiry, then for each tested entry its
-            # list index (written and read), the entry, both records and the
-            # new expiry, and writes the pairs
-            st = front.stats(stream)
-            F = st["int_front"] + st["ext_front"]
-            tested = st["keep_tested"]
-            if tested >= F:
-                fi, fe = front.export(0, stream), front.export(1, stream)
-                uniq = len(np.unique(fi[:, 1])) + len(np.unique(fe[:, 1]))
-                keep_bytes += 12 * F + 32 * T + 32 * uniq + 8 * st["broad_pairs"]
+        times = bvh.stage_times(reset=True)
+        st = front.stats(stream)
+        F = st["int_front"] + st["ext_front"]
+        op = st["front_op_run"]
+        if op in (bvhcd.FRONT_GENERATE, bvhcd.FRONT_UPDATE, bvhcd.FRONT_REORDER) or prev is None:
+            U = _uniq_nodes(front)
+        if f < W:
+            prev = st
+            continue
+        F_prev = prev["int_front"] + prev["ext_front"]
+        P, H = st["broad_pairs"], st["narrow_hits"]
+        hits = None
+        for stage, (ms, calls) in times.items():
+            if not calls:
+                continue
+            if stage == "front_generate":
+                b = stage_bytes(stage, T, V, 0, F, U, P, H)
+            elif stage == "front_update":
+                b = stage_bytes(stage, T, V, F_prev, F, U, P, H)
+            elif stage == "front_keep":
+                b = stage_bytes(stage, T, V, F, 0, U, P, H)
+            elif stage == "front_balance":
+                b = stage_bytes(stage, T, V, F, st["int_front"], U, P, H)
+            elif stage == "front_reorder":
+                b = stage_bytes(stage, T, V, F, F, U, P, H)
+            elif stage == "narrow":
+                if hits is None:
+                    hits = front.pairs()
+                b = stage_bytes(stage, T, V, 0, 0, U, P, H, pairs=hits, faces=faces)
             else:
-                keep_bytes += 4 * F + tested * (4 + 4 + 8 + 64 + 4) + 8 * st["broad_pairs"]
-            n_keep += 1
-    times = bvh.stage_times()
-    dom = max(times.items(), key=lambda kv: kv[1][0])
-    keep_ms, keep_calls = times["front_keep"]
-    avg_keep_ms = keep_ms / max(keep_calls, 1)
-    algo = keep_bytes / max(n_keep, 1)
-    achieved = algo / (avg_keep_ms * 1e-3) / 1e9 if avg_keep_ms > 0 else 0.0
-    return {"kernel": "k_keep (front_keep stage)", "bound": "hbm", "achieved": round(achieved, 1),
-            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": kind,
-            "traffic": KEEP_SCAN_DRAM_BYTES, "traffic_source": KEEP_SCAN_DRAM_SOURCE,
-            "algorithmic_bytes_per_launch": int(algo),
-            "avg_launch_ms": round(avg_keep_ms, 4),
-            "dominant_stage": dom[0],
-            "stage_ms_per_call": {k: round(v[0] / v[1], 4) for k, v in times.items() if v[1]},
-            "stage_total_ms": {k: round(v[0], 3) for k, v in times.items() if v[1]}}
+                b = stage_bytes(stage, T, V, 0, 0, U, P, H)
+            a = acc.setdefault(stage, [0.0, 0, 0.0, b is not None])
+            a[0] += ms
+            a[1] += calls
+            a[2] += (b or 0) * calls
+        prev = st
+    front.close()
+    bvh.close()
+    stages = {}
+    for stage, (ms, calls, byts, has_bytes) in acc.items():
+        avg = ms / calls
+        e = {"calls": calls, "avg_launch_ms": round(avg, 4), "total_ms": round(ms, 3)}
+        if has_bytes:
+            algo = byts / calls
+            ach = algo / (avg * 1e-3) / 1e9
+            e.update({"algorithmic_bytes_per_call": int(algo), "achieved": round(ach, 1),
+                      "frac": round(ach / peak, 4)})
+        tr = traffic.get(stage)
+        e["traffic"] = tr
+        stages[stage] = e
+    dom = max(stages.items(), key=lambda kv: kv[1]["total_ms"])
+    d = dom[1]
+    maint = [k for k in ("front_keep", "front_update", "front_balance", "front_reorder") if k in stages]
+    m_bytes = sum(stages[k]["algorithmic_bytes_per_call"] * stages[k]["calls"] for k in maint)
+    m_ms = sum(stages[k]["total_ms"] for k in maint)
+    return {"kernel": f"{dom[0]} stage", "bound": "hbm", "achieved": d.get("achieved"), "peak": peak,
+            "unit": "GB/s", "frac": d.get("frac"), "peak_source": kind,
+            "traffic": d.get("traffic"),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the stage's kernels per call "
+                              "(profiles/dram_per_stage_cloth512_sphere.txt)",
+            "algorithmic_bytes_per_launch": d.get("algorithmic_bytes_per_call"),
+            "avg_launch_ms": d["avg_launch_ms"], "dominant_stage": dom[0],
+            "front_maintenance": {"stages": maint, "achieved": round(m_bytes / (m_ms * 1e-3) / 1e9, 1) if m_ms else None,
+                                  "frac": round(m_bytes / (m_ms * 1e-3) / 1e9 / peak, 4) if m_ms else None},
+            "U": "distinct records the front references (exported front; a lower bound)",
+            "stages": stages}
 
 
 def _pct(xs, q):
@@ -436,7 +513,7 @@ def _batched_on(bvhcd, torch, args, world, B, sizes, off, faces, vidx, T, V, S, 
     launches = bvhcd.launch_count() - l0
     per = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     st = front.stats()
-    if st["overflow"]:
+    if st["overflow_any"]:
         raise RuntimeError(f"batched front/pair capacity overflow: {st}")
     batched_pairs = (front.pairs(), front.pairs(narrow=True))
     total_ms = float(sum(per))
@@ -558,7 +635,7 @@ def inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, single):
     torch.cuda.synchronize()
     ms = float(sum(a.elapsed_time(b) for a, b in zip(starts, ends))) / K
     si, sx, so = intra.stats(), inter.stats(), own.stats()
-    if si["overflow"] or sx["overflow"] or so["overflow"]:
+    if si["overflow_any"] or sx["overflow_any"] or so["overflow_any"]:
         raise RuntimeError(f"inter leg overflow: {si} {sx} {so}")
     pairs = [si["broad_pairs"] + sx["broad_pairs"] + so["broad_pairs"],
              si["narrow_hits"] + sx["narrow_hits"] + so["narrow_hits"]]
@@ -573,6 +650,43 @@ def inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, single):
                                  "cloth_sphere": [sx["broad_pairs"], sx["narrow_hits"]],
                                  "sphere_self": [so["broad_pairs"], so["narrow_hits"]]},
             "pairs_equal_single_front": pairs == [single["broad_pairs"], single["narrow_hits"]]}
+
+
+def autogrow_pass(bvhcd, torch, dev, dfaces, stream, W, K, T):
+    """The same device-resident frames through fronts with the two
+    auto_grow modes an integrator can pick: 2 (deferred: each maintain copies
+    its counters to pinned host memory, a later one acts on an overflow; no
+    synchronisation) and 1 (grow and replay inside the call: every maintain
+    reads the counters back).  The capacities are the bench's, so nothing
+    overflows; both give the main loop's pairs."""
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = {}
+    for mode, name in ((2, "deferred"), (1, "sync")):
+        bvh = bvhcd.LBvh(T, dev.shape[1], enable_restr=True)
+        front = bvhcd.BvttFront(bvh, cull_adjacent=True, narrow_phase=True, auto_grow=mode, **CAPS)
+        for f in range(W):
+            bvhcd.frame(bvh, front, f, 0, dev[f], dfaces, stream=stream, faces_static=f > 0)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(K):
+            flush.zero_()
+            starts[i].record(stream)
+            bvhcd.frame(bvh, front, W + i, 0, dev[W + i], dfaces, stream=stream, faces_static=True)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        st = front.stats()
+        if st["overflow_any"]:
+            raise RuntimeError(f"auto_grow {mode} leg overflow: {st}")
+        out[name] = {"auto_grow": mode,
+                     "value": round(float(sum(a.elapsed_time(b) for a, b in zip(starts, ends))) / K, 4),
+                     "unit": "ms/frame", "host_wall_ms_per_frame": round(wall * 1e3 / K, 4),
+                     "pairs_last_frame": [st["broad_pairs"], st["narrow_hits"]]}
+        front.close()
+        bvh.close()
+    return out
 
 
 def box_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
@@ -610,7 +724,7 @@ def box_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
     torch.cuda.synchronize()
     ms = float(sum(a.elapsed_time(b) for a, b in zip(starts, ends))) / K
     st = front.stats()
-    if st["overflow"]:
+    if st["overflow_any"]:
         raise RuntimeError(f"box leg overflow: {st}")
     front.close()
     bvh.close()
@@ -670,7 +784,7 @@ def fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
         ends[i].record(stream)
     torch.cuda.synchronize()
     st = front.stats()
-    if st["overflow"]:
+    if st["overflow_any"]:
         raise RuntimeError(f"fp16 leg overflow: {st}")
     ms = float(sum(a.elapsed_time(b) for a, b in zip(starts, ends))) / K
     front.close()
@@ -746,7 +860,7 @@ def run_reference(args):
             "n_gpus": world, "steps": n, "warmup": W, "ms_per_step": round(value, 3),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "triangles": int(faces.shape[0]), "vertices": int(frames[0].shape[0])},
+            "config": {"workload": WORKLOAD if CLOTH == 512 else f"cloth{CLOTH}_over_icosphere45", "triangles": int(faces.shape[0]), "vertices": int(frames[0].shape[0])},
             "cpu_baseline": {"value": round(value, 3), "unit": "ms/frame", "cores": cores, "kind": "port",
                              "sample": f"frames {W}..{W + n - 1} timed after {W} warm-up frames"
                                        f"{' (stopped at the time budget)' if n < K else ''}"},
@@ -765,12 +879,16 @@ def main():
                     help="time the device-resident frames only (no e2e / roofline replay); for profiling")
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-scene batched leg")
+    ap.add_argument("--cloth", type=int, default=512,
+                    help="cloth side in vertices; 512 is the headline workload, smaller sides are for profiling")
     ap.add_argument("--batched-frames", type=int, default=30)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-scheduler leg")
     ap.add_argument("--learned-frames", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    global CLOTH
+    CLOTH = args.cloth
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:
         print(json.dumps(out), flush=True)

@@ -100,7 +100,8 @@ class FrontStats(ctypes.Structure):
                 ("overflow", ctypes.c_int32), ("bvh_opt_tag", ctypes.c_int32),
                 ("front_op_run", ctypes.c_int32), ("restr_pending", ctypes.c_int32),
                 ("num_rt_subtrees", ctypes.c_int32), ("num_rt_int_nodes", ctypes.c_int32),
-                ("flagged", ctypes.c_int32), ("keep_tested", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4)]
+                ("flagged", ctypes.c_int32), ("keep_tested", ctypes.c_int32), ("overflow_any", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 3)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -411,8 +412,11 @@ class BvttFront:
 
     def __init__(self, bvh: LBvh, int_front_capacity: int = 2_300_000,
                  ext_front_capacity: int = 2_300_000, pair_capacity: int = 1_600_000,
-                 cull_adjacent: bool = True, narrow_phase: bool = True, auto_grow: bool = False,
+                 cull_adjacent: bool = True, narrow_phase: bool = True, auto_grow: int = 0,
                  precision: int = 0, rigid: "LBvh" = None):
+        """auto_grow: 0 off, 1 (or True) grow and replay in the same call
+        (synchronises every maintain), 2 deferred (no synchronisation; a later
+        maintain grows and regenerates)."""
         cfg = FrontConfig(int(int_front_capacity), int(ext_front_capacity), int(pair_capacity),
                           int(cull_adjacent), int(narrow_phase), int(auto_grow), int(precision))
         h = ctypes.c_void_p()

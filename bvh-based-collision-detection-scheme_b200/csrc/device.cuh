@@ -72,7 +72,8 @@ enum CounterSlot {
     C_REFIT_DONE = 15,        // refit: leaf blocks finished (the last one runs the crossing nodes)
     C_DELTA = 16,             // refit: largest change of a leaf box coordinate (FP32 bits, rounded up)
     C_MOTION = 17,            // refit: sum of those changes since the last build (FP32 bits, rounded up)
-    C_NUM = 18
+    C_OVF_STICKY = 18,        // C_OVERFLOW bits of every maintain since the front was created
+    C_NUM = 19
 };
 
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }

@@ -963,6 +963,22 @@ __global__ void k_pair_scatter(const int2 *__restrict__ pairs, const int4 *__res
         }
 }
 
+// Start of a maintain: the previous maintain's overflow bits join the sticky
+// record, and the bits that say the current front is incomplete (an entry or
+// a traversal was lost: bits 0, 1, 4, 5) carry over when this maintain works
+// from that front (keep, update, balance), since its results are then
+// incomplete too; a generation starts clean.
+// The carried bits are joined by bit 6, which says that this maintain's own
+// results (pairs, hits) are incomplete because its input front was.
+constexpr unsigned kFrontLossBits = 1u | 2u | 16u | 32u | 64u;
+__global__ void k_ovf_roll(unsigned *ctr, unsigned carry) {
+    if (threadIdx.x == 0) {
+        const unsigned o = ctr[C_OVERFLOW];
+        ctr[C_OVF_STICKY] |= o;
+        ctr[C_OVERFLOW] = (o & carry) ? ((o & carry) | 64u) : 0u;
+    }
+}
+
 __global__ void k_counts64(const unsigned *__restrict__ ctr, unsigned cap_pairs, unsigned cap_hits,
                            int64_t *out) {
     if (threadIdx.x == 0) {
@@ -1020,6 +1036,9 @@ Front::~Front() {
                     &extback_, &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_, &fctr_, &rcur_,
                     &pxbuf_, &pxout_, &iexp_, &xexp_, &ksel_};
     for (DBuf *b : bufs) b->release();
+    for (int k = 0; k < kSnap; k++)
+        if (snap_ev_[k]) cudaEventDestroy(snap_ev_[k]);
+    if (h_snap_) cudaFreeHost(h_snap_);
 }
 
 bvhcd_status Front::init() {
@@ -1030,6 +1049,7 @@ bvhcd_status Front::init() {
     }
     if (cfg_.int_front_capacity <= 0 || cfg_.ext_front_capacity <= 0 || cfg_.pair_capacity <= 0)
         return BVHCD_INVALID_ARG;
+    if (cfg_.auto_grow < 0 || cfg_.auto_grow > 2) return BVHCD_INVALID_ARG;
     if (cfg_.int_front_capacity > 0x7fffffffLL || cfg_.ext_front_capacity > 0x7fffffffLL ||
         cfg_.pair_capacity > 0x7fffffffLL)
         return BVHCD_INVALID_ARG;
@@ -1373,6 +1393,57 @@ bvhcd_status Front::grow_and_check(cudaStream_t s, bool *overflowed) {
     FR_TRY(cudaStreamSynchronize(s));
     *overflowed = h[C_OVERFLOW] != 0;
     if (!*overflowed) return BVHCD_OK;
+    bvhcd_status st = grow_from(h, s);
+    if (st != BVHCD_OK) return st;
+    FR_TRY(cudaMemsetAsync(counters() + C_OVERFLOW, 0, sizeof(unsigned), s));
+    return BVHCD_OK;
+}
+
+// Deferred capacity check (auto_grow = 2): the counters of each of the last
+// kSnap maintains are copied into pinned host memory on the work stream, each
+// copy with an event.  A maintain looks at the copies whose events have
+// completed (it waits only for the slot it is about to reuse, a maintain
+// kSnap - 1 calls back); one that shows an overflow in a maintain made since
+// the last regeneration grows the buffers from its counts and makes this
+// maintain regenerate the front.  No synchronisation in the steady state;
+// the frames between the overflow and the regeneration report it.
+bvhcd_status Front::deferred_check(cudaStream_t s, bool *regen) {
+    *regen = false;
+    if (!h_snap_) {
+        FR_TRY(cudaMallocHost(reinterpret_cast<void **>(&h_snap_), sizeof(unsigned) * C_NUM * kSnap));
+        for (int k = 0; k < kSnap; k++) FR_TRY(cudaEventCreateWithFlags(&snap_ev_[k], cudaEventDisableTiming));
+    }
+    const int reuse = (int)(seq_ % kSnap);
+    for (int k = 0; k < kSnap; k++) {
+        if (snap_seq_[k] < 0) continue;
+        cudaError_t q = cudaEventQuery(snap_ev_[k]);
+        if (q == cudaErrorNotReady && k == reuse) q = cudaEventSynchronize(snap_ev_[k]);
+        if (q == cudaErrorNotReady) continue;
+        FR_TRY(q);
+        const unsigned *h = h_snap_ + (size_t)k * C_NUM;
+        if (h[C_OVERFLOW] != 0 && snap_seq_[k] >= regen_seq_) {
+            bvhcd_status st = grow_from(h, s);  // (synchronises s: rare)
+            if (st != BVHCD_OK) return st;
+            *regen = true;
+        }
+        snap_seq_[k] = -1;
+    }
+    if (*regen) regen_seq_ = seq_;
+    return BVHCD_OK;
+}
+
+bvhcd_status Front::deferred_snapshot(cudaStream_t s) {
+    const int k = (int)(seq_ % kSnap);
+    FR_TRY(cudaMemcpyAsync(h_snap_ + (size_t)k * C_NUM, counters(), sizeof(unsigned) * C_NUM,
+                           cudaMemcpyDeviceToHost, s));
+    FR_TRY(cudaEventRecord(snap_ev_[k], s));
+    snap_seq_[k] = seq_++;
+    return BVHCD_OK;
+}
+
+// Buffers grown to the sizes the counters `h` of an overflowed maintain ask
+// for (reserved slots, so at least the true sizes), half as much again.
+bvhcd_status Front::grow_from(const unsigned *h, cudaStream_t s) {
     int64_t need_int = (int64_t)(h[C_INT0] > h[C_INT1] ? h[C_INT0] : h[C_INT1]);
     int64_t need_ext = (int64_t)(h[C_EXT0] > h[C_EXT1] ? h[C_EXT0] : h[C_EXT1]);
     int64_t need_pairs = (int64_t)(h[C_PAIRS] > h[C_HITS] ? h[C_PAIRS] : h[C_HITS]);
@@ -1419,7 +1490,6 @@ bvhcd_status Front::grow_and_check(cudaStream_t s, bool *overflowed) {
         FR_TRY(hits_.reserve(sizeof(int2) * (size_t)npc));
         pcap_ = npc;
     }
-    FR_TRY(cudaMemsetAsync(counters() + C_OVERFLOW, 0, sizeof(unsigned), s));
     return BVHCD_OK;
 }
 
@@ -1434,6 +1504,11 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     bvhcd_status st = ensure_node_capacity(T);
     if (st != BVHCD_OK) return st;
     if (!inter()) bvh_->set_updated(false);  // an inter front leaves the deformable BVH's restructure marks alone
+    bool regen = false;
+    if (cfg_.auto_grow == 2) {
+        st = deferred_check(s, &regen);
+        if (st != BVHCD_OK) return st;
+    }
     bvhcd_front_op run_op = op;
     // front override after a BVH build or restructure (:75-110): the front
     // is regenerated in both cases
@@ -1451,14 +1526,19 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     // a deformable BVH of one leaf has no internal node for the front
     // operations to climb to: its inter front is generated every frame
     if (inter() && T == 1 && run_op != BVHCD_FRONT_PURE_BVH_CD) run_op = BVHCD_FRONT_GENERATE;
+    // a deferred check found an earlier overflow: the buffers have grown, the
+    // front is made again
+    if (regen && run_op != BVHCD_FRONT_PURE_BVH_CD) run_op = BVHCD_FRONT_GENERATE;
     unsigned *ctr = counters();
-    FR_TRY(cudaMemsetAsync(ctr + C_OVERFLOW, 0, sizeof(unsigned), s));
+    const bool from_front =
+        run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER || run_op == BVHCD_FRONT_KEEP;
+    k_ovf_roll<<<1, 32, 0, s>>>(ctr, from_front ? kFrontLossBits : 0u); note_launch();
     if (inter() ? (T < 1 || trav_->T() < 1) : T < 2) {
         FR_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned) * 6, s));
         FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));
         last_op_ = run_op;
         if (run_op != BVHCD_FRONT_PURE_BVH_CD) has_front_ = true;
-        return BVHCD_OK;
+        return cfg_.auto_grow == 2 ? deferred_snapshot(s) : BVHCD_OK;
     }
     // With auto_grow the stage is replayed after growing the buffers.  The
     // stage's input (the tree and the front in set cur_) is intact when an
@@ -1469,7 +1549,7 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
         if (st != BVHCD_OK) return st;
         st = narrow(s, cfg_.narrow_phase != 0);  // without the test it only counts the pairs
         if (st != BVHCD_OK) return st;
-        if (!cfg_.auto_grow) break;
+        if (cfg_.auto_grow != 1) break;
         bool ovf = false;
         st = grow_and_check(s, &ovf);
         if (st != BVHCD_OK) return st;
@@ -1479,7 +1559,8 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     }
     last_op_ = run_op;
     k_counts64<<<1, 32, 0, s>>>(ctr, (unsigned)pcap_, (unsigned)pcap_, counts64_.as<int64_t>()); note_launch();
-    return cuda_status(cudaGetLastError());
+    FR_TRY(cudaGetLastError());
+    return cfg_.auto_grow == 2 ? deferred_snapshot(s) : BVHCD_OK;
 }
 
 bvhcd_status Front::copy_state_from(const Front &src, cudaStream_t s) {
@@ -1609,6 +1690,7 @@ bvhcd_status Front::stats(bvhcd_front_stats *st, cudaStream_t s) {
     st->broad_pairs = h[C_PAIRS_VALID];
     st->narrow_hits = h[C_HITS];
     st->overflow = (int32_t)h[C_OVERFLOW];
+    st->overflow_any = (int32_t)(h[C_OVERFLOW] | h[C_OVF_STICKY]);
     st->bvh_opt_tag = bvh_->opt_tag();
     st->front_op_run = last_op_;
     st->restr_pending = bvh_->updated() ? 1 : 0;
@@ -1657,7 +1739,8 @@ bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, 
         FR_TRY(cudaMemcpyAsync(out, src, sizeof(int2) * (size_t)m,
                                out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
     FR_TRY(cudaStreamSynchronize(s));
-    if (h[C_OVERFLOW] & (which ? 8u : 4u)) return BVHCD_CAPACITY_EXCEEDED;
+    // lost pairs or hits, or a front (this maintain's input or its traversals) that lost entries
+    if (h[C_OVERFLOW] & (which ? (4u | 8u | 16u | 32u | 64u) : (4u | 16u | 32u | 64u))) return BVHCD_CAPACITY_EXCEEDED;
     return n > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
 }
 

@@ -277,6 +277,9 @@ class Front {
     bvhcd_status check_quality(cudaStream_t s);
     bvhcd_status snapshot(cudaStream_t s);
     bvhcd_status grow_and_check(cudaStream_t s, bool *overflowed);
+    bvhcd_status grow_from(const unsigned *h, cudaStream_t s);
+    bvhcd_status deferred_check(cudaStream_t s, bool *regen);
+    bvhcd_status deferred_snapshot(cudaStream_t s);
     bvhcd_status compact_pairs(cudaStream_t s);
     FrontLog log() const;
 
@@ -313,6 +316,15 @@ class Front {
     DBuf intcnt_, extcnt_, intbeg_, extbeg_, intback_, extback_, snapshot_, scratch_, counts64_;
     DBuf rcur_;  // reorder cursors, one per group of 2^kReorderShift nodes and front
     DBuf pxbuf_, pxout_;  // proximity counts / offsets / total; records for a host destination
+    // deferred capacity check (auto_grow = 2): counter copies of the last
+    // kSnap maintains in pinned host memory, one event each; the maintain
+    // number of each copy (-1: looked at); maintains counted; the maintain
+    // that last regenerated after an overflow
+    static constexpr int kSnap = 3;
+    unsigned *h_snap_ = nullptr;
+    cudaEvent_t snap_ev_[kSnap] = {nullptr, nullptr, nullptr};
+    long long snap_seq_[kSnap] = {-1, -1, -1};
+    long long seq_ = 0, regen_seq_ = 0;
 };
 
 }  // namespace bvhcd

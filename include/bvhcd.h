@@ -69,7 +69,20 @@ typedef struct {
     int64_t pair_capacity;       /* reference default 1,600,000 */
     int32_t cull_adjacent;       /* drop pairs sharing a vertex id (covertex) */
     int32_t narrow_phase;        /* run the tri-tri test after the broad phase */
-    int32_t auto_grow;           /* on overflow: grow buffers and replay (syncs) */
+    int32_t auto_grow;           /* what an overflow of a front, pair or hit buffer does:
+                                    0: nothing (reported in the stats; the front and the
+                                       results of that maintain and of the ones working
+                                       from its front are incomplete until a GENERATE);
+                                    1: grow the buffers and replay the stage in the same
+                                       call -- complete results every call, but each
+                                       maintain reads the counters back (synchronises);
+                                    2: deferred -- no synchronisation: each maintain copies
+                                       its counters to pinned host memory with an event,
+                                       and a later maintain that finds a completed copy
+                                       showing an overflow grows the buffers and
+                                       regenerates the front; the maintains in between
+                                       report the overflow (stats, CAPACITY_EXCEEDED from
+                                       bvhcd_front_pairs) */
     int32_t precision;           /* 0: the reference's FP32 narrow phase; 1: FP32 where
                                     certain, FP64 for the pairs it flags (hits equal an
                                     FP64 evaluation of every pair), FP64 contact points /
@@ -112,7 +125,11 @@ typedef struct {
     int64_t ext_front;       /* F_ext */
     int64_t broad_pairs;     /* cpNum */
     int64_t narrow_hits;     /* actualCpNum */
-    int32_t overflow;        /* bit0 int front, bit1 ext front, bit2 pairs */
+    int32_t overflow;        /* this maintain: bit0 int front, bit1 ext front, bit2 pairs,
+                                bit3 hits, bit4 traversal bound, bit5 sprout work list,
+                                bit6 the front it worked from had lost entries (bits 0,
+                                1, 4, 5 carry over from maintain to maintain until a
+                                GENERATE) */
     int32_t bvh_opt_tag;     /* 0 refit, 1 restructure, 2 build (BvhRestrLog.h:59) */
     int32_t front_op_run;    /* the front operation that actually ran */
     int32_t restr_pending;   /* quality check marked the BVH for restructuring */
@@ -121,7 +138,9 @@ typedef struct {
     int32_t flagged;         /* precision mode: pairs the narrow phase re-decided in FP64 */
     int32_t keep_tested;     /* entries the last KEEP tested: all of them, or those whose
                                 expiry had come (the others cannot have changed state) */
-    int32_t reserved[4];
+    int32_t overflow_any;    /* the overflow bits of every maintain since the front was
+                                created (sticky; a replay of auto_grow = 1 clears its own) */
+    int32_t reserved[3];
 } bvhcd_front_stats;
 
 typedef struct bvhcd_bvh bvhcd_bvh;
@@ -288,7 +307,11 @@ bvhcd_status bvhcd_launch_count(int64_t *n);
  * BVHCD_NOALLOC_MAX_FACES; larger requests return BVHCD_CAPACITY_EXCEEDED
  * without touching the GPU.  The first call on a device looks up that array's
  * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture.  Calls share the array: two calls whose work overlaps on
+ * stream capture.  Under CUDA's lazy module loading the library's device code,
+ * and with it the array, is loaded on a device at the first use of any of its
+ * kernels there -- possibly this call -- which allocates and synchronises
+ * once: make the first call during initialisation, not in the loop that must
+ * not allocate.  Calls share the array: two calls whose work overlaps on
  * the GPU (different streams, or different host threads) race and must be
  * serialised by the caller.  Asynchronous on `stream`. */
 #define BVHCD_NOALLOC_MAX_FACES 1048576

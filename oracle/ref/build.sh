@@ -1,6 +1,7 @@
 #!/bin/sh
 # Builds, from the reference's own sources where they lie in the reference
-# tree (default /root/reference; override with REF_ROOT):
+# tree (REF_ROOT; by default the directory `reference` beside the checkout of
+# this repository):
 #   oracle/_ref/libref_tritri.so -- the gProximity triangle-pair predicate;
 #   oracle/_ref/ref_emu_driver   -- the reference's collision pipeline as host
 #                                   C++ (Makefile.refemu).
@@ -8,7 +9,7 @@
 # reference tree is absent (the GPU box has only the prebuilt files).
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF_ROOT=${REF_ROOT:-/root/reference}
+REF_ROOT=${REF_ROOT:-$(cd "$HERE/../../.." && pwd)/reference}
 OUT="$HERE/../_ref"
 GP="$REF_ROOT/Source/Externals/inc/gProximity"
 if [ ! -f "$GP/cuda_intersect_tritri.h" ]; then

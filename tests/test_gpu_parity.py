@@ -131,6 +131,52 @@ def test_long_keep_runs(cuda, lib_built, oracle, step):
             assert np.array_equal(sorted_rows(front.export(which)), sorted_rows(p.front(which))), (f, which)
         assert np.array_equal(canon(front.pairs()), canon(p.pairs())), f
         assert np.array_equal(canon(front.pairs(narrow=True)), canon(p.pairs(narrow=True))), f
+        st = front.stats()
+        if f >= 2:
+            # the keeps after the first one select by expiry: fewer entries tested than the front holds
+            assert 0 < st["keep_tested"] < st["int_front"] + st["ext_front"], (f, st)
+        elif f == 1:
+            assert st["keep_tested"] == st["int_front"] + st["ext_front"], (f, st)
+
+
+def _flat_grid(n):
+    xs = np.linspace(0.0, 1.0, n, dtype=np.float32)
+    gx, gy = np.meshgrid(xs, xs, indexing="ij")
+    verts = np.stack([gx.ravel(), gy.ravel(), np.zeros(n * n, np.float32)], axis=1).astype(np.float32)
+    faces = []
+    for i in range(n - 1):
+        for j in range(n - 1):
+            a, b, c, d = i * n + j, i * n + j + 1, (i + 1) * n + j, (i + 1) * n + j + 1
+            faces += [(a, b, d), (a, d, c)]
+    return np.asarray(faces, np.int32), verts
+
+
+def test_keep_expiry_catches_a_closing_gap(cuda, lib_built, oracle):
+    """A triangle falls onto a flat, still cloth by a small step per frame,
+    under keeps only (one generation on frame 0): its entries wait on their
+    expiries while the gap closes, and the pairs must equal the brute-force
+    set on every frame -- none may appear late, on the frame the boxes first
+    touch included."""
+    faces, verts = _flat_grid(24)
+    nv = verts.shape[0]
+    tri = np.array([[0.41, 0.43, 0.0], [0.55, 0.47, 0.0], [0.47, 0.58, 0.0]], np.float32)
+    faces = np.concatenate([faces, np.array([[nv, nv + 1, nv + 2]], np.int32)])
+    bvh, front = _new(lib_built, faces.shape[0], nv + 3, restr=False)
+    first = None
+    for f in range(40):
+        pos = np.concatenate([verts, tri + np.float32([0.0, 0.0, 0.2 - 0.0125 * f])]).astype(np.float32)
+        op = (0, 1) if f == 0 else (1, 4)
+        bvh.maintain(op[0], pos, faces, faces_static=f > 0)
+        front.maintain(op[1])
+        got = canon(front.pairs())
+        assert np.array_equal(got, oracle.brute_pairs(faces, pos, 1)), f
+        falling = faces.shape[0] - 1
+        if first is None and np.any(got == falling):
+            first = f
+        if f >= 2:
+            st = front.stats()
+            assert st["keep_tested"] < st["int_front"] + st["ext_front"], (f, st)
+    assert first == 16, first  # z = 0.2 - 0.0125 * 16 = 0 touches the cloth
 
 
 def test_restructure_parity(cuda, lib_built, oracle, cloth_c1):
@@ -247,22 +293,47 @@ def test_device_resident_input(cuda, lib_built, cloth_c1):
 
 
 def test_cloth_over_sphere_full_size(cuda, lib_built, oracle):
+    """The bench workload (512x512 cloth over a frequency-45 icosphere,
+    562,742 triangles) through a whole cycle of the reference's schedule --
+    build + generate (0), keeps, balance (5), prune/sprout (6), a restructure
+    forced through the public marks (8), the mandatory rebuild (12) -- with
+    the CPU oracle pipeline alongside.  Every frame: the broad set equals the
+    brute-force set of overlapping boxes, the hits equal the FP32 SAT over it,
+    sizes / op tags / front operation equal the oracle's; on the frames that
+    change the front, both fronts equal the oracle's as multisets."""
     import scenes
-    faces, frames = scenes.cloth_over_sphere_frames(512, 3)
+    faces, frames = scenes.cloth_over_sphere_frames(512, 14)
     T, V = faces.shape[0], frames[0].shape[0]
     assert T == 522242 + 40500
     caps = dict(int_front_capacity=40_000_000, ext_front_capacity=40_000_000, pair_capacity=8_000_000)
     bvh, front = _new(lib_built, T, V, caps=caps)
-    for f in range(3):
+    p = oracle.Pipeline(True, True, True)
+    ops = []
+    for f in range(14):
         b, fr = lib_built.schedule(f)
-        bvh.maintain(b, frames[f], faces)
+        bvh.maintain(b, frames[f], faces, faces_static=f > 0)
         front.maintain(fr)
-        st = front.stats()
-        assert st["overflow"] == 0
+        p.frame(faces, frames[f], b, fr)
+        st, info = front.stats(), p.info()
+        assert st["overflow"] == 0, f
+        assert st["bvh_opt_tag"] == info["opt_tag"] and st["front_op_run"] == info["front_op"], (f, st, info)
+        assert (st["int_front"], st["ext_front"]) == (info["F_int"], info["F_ext"]), (f, st, info)
+        assert (st["broad_pairs"], st["narrow_hits"]) == (info["P"], info["H"]), (f, st, info)
         pairs = canon(front.pairs())
         assert np.array_equal(pairs, oracle.brute_pairs(faces, frames[f], 1)), f
         hits = canon(front.pairs(narrow=True))
         keep = oracle.narrow(pairs, faces, frames[f]).astype(bool)
         assert np.array_equal(hits, pairs[keep]), f
         assert len(hits) > 0, "the cloth must cut the sphere"
+        ops.append((st["bvh_opt_tag"], st["front_op_run"]))
+        if f in (0, 5, 6, 8, 12):
+            for which in (0, 1):
+                assert np.array_equal(sorted_rows(front.export(which)), sorted_rows(p.front(which))), (f, which)
+        if f == 7:
+            roots = pick_roots(p.tree())
+            bvh.request_restructure(roots)
+            p.mark_restructure(roots)
+    assert ops[8] == (1, lib_built.FRONT_GENERATE), ops      # the forced restructure, then a regeneration
+    assert ops[12][1] == lib_built.FRONT_GENERATE, ops       # the mandatory rebuild (its tag stays 0, as the reference's)
+    assert ops[5][1] == lib_built.FRONT_REORDER and ops[6][1] == lib_built.FRONT_UPDATE, ops
     assert not check_tree(bvh.export(), T)

@@ -55,6 +55,31 @@ def test_noalloc_morton_order_matches_build(cuda, lib_built, cloth_c1):
         assert np.array_equal(order, exp_order)
 
 
+def test_noalloc_calls_allocate_nothing(cuda, lib_built, cloth_c1):
+    """After the first call on the device (which may load the library's
+    device code and with it the fixed array), further calls leave the device's
+    free memory unchanged: no allocation, by the library or anything it
+    calls."""
+    torch = cuda
+    faces, frames = cloth_c1
+    T = faces.shape[0]
+    dpos = torch.from_numpy(frames[3]).cuda()
+    dfaces = torch.from_numpy(faces).cuda()
+    codes = torch.empty(T, dtype=torch.int32, device="cuda")
+    order = torch.empty(T, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    args = [ctypes.c_void_p(dpos.data_ptr()), ctypes.c_void_p(dfaces.data_ptr()), T,
+            ctypes.c_void_p(codes.data_ptr()), ctypes.c_void_p(order.data_ptr()),
+            ctypes.c_void_p(stream.cuda_stream)]
+    assert lib_built.lib().bvhcd_morton_order_noalloc(*args) == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert lib_built.lib().bvhcd_morton_order_noalloc(*args) == 0
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_noalloc_rejects_sizes_beyond_its_array(cuda, lib_built):
     torch = cuda
     dummy = torch.zeros(1, dtype=torch.int32, device="cuda")
