@@ -40,7 +40,7 @@ EXPORTED = [
     "bvhcd_learner_create", "bvhcd_learner_destroy", "bvhcd_learner_set_params", "bvhcd_learner_get_params",
     "bvhcd_learner_frame", "bvhcd_learner_observe", "bvhcd_learner_cut", "bvhcd_learner_features",
     "bvhcd_learner_work", "bvhcd_mlp_gradient", "bvhcd_mlp_train", "bvhcd_mlp_predict",
-    "bvhcd_learner_set_decide_every", "bvhcd_front_contacts",
+    "bvhcd_learner_set_decide_every", "bvhcd_front_contacts", "bvhcd_debug_fail_alloc",
 ]
 
 MLP_PARAMS = 5443
@@ -101,7 +101,7 @@ class FrontStats(ctypes.Structure):
                 ("front_op_run", ctypes.c_int32), ("restr_pending", ctypes.c_int32),
                 ("num_rt_subtrees", ctypes.c_int32), ("num_rt_int_nodes", ctypes.c_int32),
                 ("flagged", ctypes.c_int32), ("keep_tested", ctypes.c_int32), ("overflow_any", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 3)]
+                ("nonfinite_input", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -158,6 +158,7 @@ def lib():
             "bvhcd_profile_enable": (ctypes.c_int, [vp, i32]),
             "bvhcd_profile_read": (ctypes.c_int, [vp, vp, vp, i32]),
             "bvhcd_launch_count": (ctypes.c_int, [ctypes.POINTER(i64)]),
+            "bvhcd_debug_fail_alloc": (ctypes.c_int, [i64]),
             "bvhcd_morton_order_noalloc": (ctypes.c_int, [vp, vp, i32, vp, vp, vp]),
             "bvhcd_bvh_set_scenes": (ctypes.c_int, [vp, i32, vp]),
             "bvhcd_frame_graph": (ctypes.c_int, [vp, vp, ctypes.POINTER(Scene), i32, i32, vp]),

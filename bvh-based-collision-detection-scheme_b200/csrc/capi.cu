@@ -510,6 +510,24 @@ void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace bvhcd
 
+namespace bvhcd {
+// allocations left before the chosen one fails (0: no fault planned)
+static std::atomic<long long> g_alloc_countdown{0};
+bool alloc_fault_due() {
+    long long c = g_alloc_countdown.load(std::memory_order_relaxed);
+    while (c > 0) {
+        if (g_alloc_countdown.compare_exchange_weak(c, c - 1, std::memory_order_relaxed)) return c == 1;
+    }
+    return false;
+}
+}  // namespace bvhcd
+
+extern "C" __attribute__((visibility("default"))) bvhcd_status bvhcd_debug_fail_alloc(int64_t n) {
+    if (n < 0) return BVHCD_INVALID_ARG;
+    bvhcd::g_alloc_countdown.store((long long)n, std::memory_order_relaxed);
+    return BVHCD_OK;
+}
+
 extern "C" __attribute__((visibility("default"))) bvhcd_status bvhcd_launch_count(int64_t *n) {
     if (!n) return BVHCD_INVALID_ARG;
     *n = bvhcd::launch_count();

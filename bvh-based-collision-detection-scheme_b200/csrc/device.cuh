@@ -73,7 +73,10 @@ enum CounterSlot {
     C_DELTA = 16,             // refit: largest change of a leaf box coordinate (FP32 bits, rounded up)
     C_MOTION = 17,            // refit: sum of those changes since the last build (FP32 bits, rounded up)
     C_OVF_STICKY = 18,        // C_OVERFLOW bits of every maintain since the front was created
-    C_NUM = 19
+    C_NF_ACC = 19,            // BVH: non-finite input seen by the blocks of the running check
+    C_NONFINITE = 20,         // BVH: 1 when the last maintain's input held a NaN or infinite coordinate
+    C_NF_DONE = 21,           // BVH: blocks of the build-time finiteness check finished
+    C_NUM = 22
 };
 
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
@@ -148,6 +151,20 @@ __device__ __forceinline__ void prim_box(const PrimSrc &p, int t, float4 &lo, fl
 __device__ __forceinline__ void face_box(const PrimSrc &p, const int4 &f, float4 &lo, float4 &hi) {
     if (p.boxes) prim_box(p, f.w, lo, hi);
     else tri_box(load_vert(p.verts, f.x), load_vert(p.verts, f.y), load_vert(p.verts, f.z), lo, hi);
+}
+// |x| <= FLT_MAX: false for NaN and for +-inf
+__device__ __forceinline__ bool finite1(float x) { return fabsf(x) <= 3.402823466e+38f; }
+__device__ __forceinline__ bool finite3(const float3 &v) { return finite1(v.x) & finite1(v.y) & finite1(v.z); }
+// face_box that also says whether every input coordinate was finite (the
+// box's min / max would drop a NaN, so the inputs themselves are tested)
+__device__ __forceinline__ bool face_box_fin(const PrimSrc &p, const int4 &f, float4 &lo, float4 &hi) {
+    if (p.boxes) {
+        prim_box(p, f.w, lo, hi);
+        return finite1(lo.x) & finite1(lo.y) & finite1(lo.z) & finite1(hi.x) & finite1(hi.y) & finite1(hi.z);
+    }
+    const float3 a = load_vert(p.verts, f.x), b = load_vert(p.verts, f.y), c = load_vert(p.verts, f.z);
+    tri_box(a, b, c, lo, hi);
+    return finite3(a) & finite3(b) & finite3(c);
 }
 
 // 30-bit Morton code of a box centre normalised by the scene box

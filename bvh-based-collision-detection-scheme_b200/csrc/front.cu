@@ -126,7 +126,8 @@ struct Em {
     Chunk fi, fe, pr, wk;  // internal front, external front, pairs, sprout work
 };
 
-__device__ __forceinline__ void chunk_put(int2 *buf, unsigned *ctr, unsigned cap, Chunk &c, const int2 &v,
+// Returns whether the entry was stored (false: past the capacity, flagged).
+__device__ __forceinline__ bool chunk_put(int2 *buf, unsigned *ctr, unsigned cap, Chunk &c, const int2 &v,
                                           unsigned *ovf, unsigned bit) {
     if (c.left == 0) {
         cg::coalesced_group g = cg::coalesced_threads();
@@ -137,8 +138,12 @@ __device__ __forceinline__ void chunk_put(int2 *buf, unsigned *ctr, unsigned cap
     }
     const unsigned slot = c.base++;
     --c.left;
-    if (slot < cap) buf[slot] = v;
-    else atomicOr(ovf, bit);
+    if (slot < cap) {
+        buf[slot] = v;
+        return true;
+    }
+    atomicOr(ovf, bit);
+    return false;
 }
 __device__ __forceinline__ void chunk_close(int2 *buf, unsigned cap, Chunk &c) {
     for (; c.left > 0; --c.left) {
@@ -147,13 +152,16 @@ __device__ __forceinline__ void chunk_close(int2 *buf, unsigned cap, Chunk &c) {
     }
 }
 
+// Only stored entries are counted: the per-node counts place the entries in
+// the ordered front (reorder, balance), so after an overflow the ordered
+// front holds exactly the entries that were kept and no unwritten slot.
 __device__ __forceinline__ void emit_int(const FArgs &a, Em &em, int prim, int node) {
-    chunk_put(a.out_int, a.ctr + a.out_int_slot, a.cap_int, em.fi, make_int2(prim, node), a.ctr + C_OVERFLOW, 1u);
-    node_add(a.log.intcnt, (unsigned)node, node);
+    if (chunk_put(a.out_int, a.ctr + a.out_int_slot, a.cap_int, em.fi, make_int2(prim, node), a.ctr + C_OVERFLOW, 1u))
+        node_add(a.log.intcnt, (unsigned)node, node);
 }
 __device__ __forceinline__ void emit_ext(const FArgs &a, Em &em, int prim, int leaf) {
-    chunk_put(a.out_ext, a.ctr + a.out_ext_slot, a.cap_ext, em.fe, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 2u);
-    node_add(a.log.extcnt, (unsigned)leaf, leaf);
+    if (chunk_put(a.out_ext, a.ctr + a.out_ext_slot, a.cap_ext, em.fe, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 2u))
+        node_add(a.log.extcnt, (unsigned)leaf, leaf);
 }
 __device__ __forceinline__ void emit_pair(const FArgs &a, Em &em, int prim, const int4 &pf, int leaf) {
     if (a.cull && covertex(pf, __ldg(&a.sface[leaf]))) return;
@@ -1387,12 +1395,12 @@ bvhcd_status Front::run(bvhcd_front_op op, cudaStream_t s) {
     }
 }
 
-bvhcd_status Front::grow_and_check(cudaStream_t s, bool *overflowed) {
+bvhcd_status Front::grow_and_check(cudaStream_t s, unsigned *ovf_bits) {
     unsigned h[C_NUM];
     FR_TRY(cudaMemcpyAsync(h, counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
     FR_TRY(cudaStreamSynchronize(s));
-    *overflowed = h[C_OVERFLOW] != 0;
-    if (!*overflowed) return BVHCD_OK;
+    *ovf_bits = h[C_OVERFLOW];
+    if (!*ovf_bits) return BVHCD_OK;
     bvhcd_status st = grow_from(h, s);
     if (st != BVHCD_OK) return st;
     FR_TRY(cudaMemsetAsync(counters() + C_OVERFLOW, 0, sizeof(unsigned), s));
@@ -1452,42 +1460,53 @@ bvhcd_status Front::grow_from(const unsigned *h, cudaStream_t s) {
         if (g > 0x7fffffffLL) g = 0x7fffffffLL;
         return g > cur ? g : cur;
     };
-    // the current front survives in set cur_: copy it into the grown buffers
-    int64_t nic = grow(need_int, fcap_[0]), nec = grow(need_ext, fcap_[1]), npc = grow(need_pairs, pcap_);
+    const int64_t nc[2] = {grow(need_int, fcap_[0]), grow(need_ext, fcap_[1])};
+    const int64_t npc = grow(need_pairs, pcap_);
+    const bool gf[2] = {nc[0] > fcap_[0], nc[1] > fcap_[1]}, gp = npc > pcap_;
+    // Every grown buffer is allocated before the handle changes: if one
+    // allocation fails the others are released and the front keeps its old,
+    // consistent buffers (no capacity ever exceeds the buffer behind it).
+    DBuf nf[2][2], nwork, niexp, nxexp, nksel, npairs, nhits;
+    DBuf *tmp[] = {&nf[0][0], &nf[0][1], &nf[1][0], &nf[1][1], &nwork, &niexp, &nxexp, &nksel, &npairs, &nhits};
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 2 && e == cudaSuccess; k++)
+        for (int set = 0; set < 2 && gf[k] && e == cudaSuccess; set++) e = nf[set][k].reserve(sizeof(int2) * (size_t)nc[k]);
+    // every work item comes from one internal entry of the input front
+    if (e == cudaSuccess && gf[0]) e = nwork.reserve(sizeof(int2) * (size_t)nc[0]);
+    if (e == cudaSuccess && gf[0]) e = niexp.reserve(sizeof(float) * (size_t)nc[0]);
+    if (e == cudaSuccess && gf[1]) e = nxexp.reserve(sizeof(float) * (size_t)nc[1]);
+    if (e == cudaSuccess && (gf[0] || gf[1])) e = nksel.reserve(sizeof(unsigned) * (size_t)(nc[0] + nc[1]));
+    if (e == cudaSuccess && gp) e = npairs.reserve(sizeof(int2) * (size_t)npc);
+    if (e == cudaSuccess && gp) e = nhits.reserve(sizeof(int2) * (size_t)npc);
+    // the current front survives in set cur_: copied into its grown buffers
+    for (int k = 0; k < 2 && e == cudaSuccess; k++)
+        if (gf[k]) e = cudaMemcpyAsync(nf[cur_][k].p, front_[cur_][k].p, sizeof(int2) * (size_t)fcap_[k],
+                                       cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // nothing queued still reads the old buffers
+    if (e != cudaSuccess) {
+        for (DBuf *b : tmp) b->release();
+        return cuda_status(e);
+    }
+    auto swap_in = [](DBuf &dst, DBuf &src) {
+        dst.release();
+        dst = src;
+        src = DBuf{};
+    };
     for (int k = 0; k < 2; k++) {
-        int64_t nc = k == 0 ? nic : nec;
-        if (nc == fcap_[k]) continue;
-        for (int set = 0; set < 2; set++) {
-            DBuf nb;
-            FR_TRY(nb.reserve(sizeof(int2) * (size_t)nc));
-            if (set == cur_) FR_TRY(cudaMemcpyAsync(nb.p, front_[set][k].p, sizeof(int2) * (size_t)fcap_[k],
-                                                    cudaMemcpyDeviceToDevice, s));
-            FR_TRY(cudaStreamSynchronize(s));
-            front_[set][k].release();
-            front_[set][k] = nb;
-        }
-        fcap_[k] = nc;
-        if (k == 0) {
-            // every work item comes from one internal entry of the input front
-            work_.release();
-            FR_TRY(work_.reserve(sizeof(int2) * (size_t)nc));
-            iexp_.release();
-            FR_TRY(iexp_.reserve(sizeof(float) * (size_t)nc));
-        } else {
-            xexp_.release();
-            FR_TRY(xexp_.reserve(sizeof(float) * (size_t)nc));
-        }
+        if (!gf[k]) continue;
+        for (int set = 0; set < 2; set++) swap_in(front_[set][k], nf[set][k]);
+        fcap_[k] = nc[k];
         exp_valid_ = false;
     }
-    if ((size_t)(fcap_[0] + fcap_[1]) * sizeof(unsigned) > ksel_.bytes) {
-        ksel_.release();
-        FR_TRY(ksel_.reserve(sizeof(unsigned) * (size_t)(fcap_[0] + fcap_[1])));
+    if (gf[0]) {
+        swap_in(work_, nwork);
+        swap_in(iexp_, niexp);
     }
-    if (npc != pcap_) {
-        pairs_.release();
-        hits_.release();
-        FR_TRY(pairs_.reserve(sizeof(int2) * (size_t)npc));
-        FR_TRY(hits_.reserve(sizeof(int2) * (size_t)npc));
+    if (gf[1]) swap_in(xexp_, nxexp);
+    if (gf[0] || gf[1]) swap_in(ksel_, nksel);
+    if (gp) {
+        swap_in(pairs_, npairs);
+        swap_in(hits_, nhits);
         pcap_ = npc;
     }
     return BVHCD_OK;
@@ -1550,12 +1569,15 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
         st = narrow(s, cfg_.narrow_phase != 0);  // without the test it only counts the pairs
         if (st != BVHCD_OK) return st;
         if (cfg_.auto_grow != 1) break;
-        bool ovf = false;
+        unsigned ovf = 0;
         st = grow_and_check(s, &ovf);
         if (st != BVHCD_OK) return st;
         if (!ovf) break;
-        // an UPDATE overwrote the front; start again from a generated front
-        if (run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER) run_op = BVHCD_FRONT_GENERATE;
+        // an UPDATE or a balance overwrote the front, or the front this
+        // maintain started from had lost entries: start again from a
+        // generated front
+        if (run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER || (ovf & (1u | 2u | 16u | 64u)))
+            run_op = BVHCD_FRONT_GENERATE;
     }
     last_op_ = run_op;
     k_counts64<<<1, 32, 0, s>>>(ctr, (unsigned)pcap_, (unsigned)pcap_, counts64_.as<int64_t>()); note_launch();
@@ -1680,9 +1702,18 @@ bvhcd_status Front::autotune(int repeats, bvhcd_launch_shapes *chosen, double *b
     return BVHCD_OK;
 }
 
+// 1 when the last maintain of this front's BVH (or, for an inter front, of
+// either BVH) was given a NaN or infinite coordinate; enqueued copies only
+static cudaError_t nonfinite_read(const LBvh *a, const LBvh *b, unsigned *h2, cudaStream_t s) {
+    cudaError_t e = cudaMemcpyAsync(h2, a->nonfinite_flag(), sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h2 + 1, b->nonfinite_flag(), sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    return e;
+}
+
 bvhcd_status Front::stats(bvhcd_front_stats *st, cudaStream_t s) {
-    unsigned h[C_NUM];
+    unsigned h[C_NUM], nf[2] = {0u, 0u};
     FR_TRY(cudaMemcpyAsync(h, counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(nonfinite_read(bvh_, trav(), nf, s));
     FR_TRY(cudaStreamSynchronize(s));
     *st = bvhcd_front_stats{};
     st->int_front = h[2 * cur_];
@@ -1691,6 +1722,7 @@ bvhcd_status Front::stats(bvhcd_front_stats *st, cudaStream_t s) {
     st->narrow_hits = h[C_HITS];
     st->overflow = (int32_t)h[C_OVERFLOW];
     st->overflow_any = (int32_t)(h[C_OVERFLOW] | h[C_OVF_STICKY]);
+    st->nonfinite_input = (nf[0] | nf[1]) ? 1 : 0;
     st->bvh_opt_tag = bvh_->opt_tag();
     st->front_op_run = last_op_;
     st->restr_pending = bvh_->updated() ? 1 : 0;
@@ -1727,9 +1759,15 @@ bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, 
         if (st != BVHCD_OK) return st;
         src = outbuf_.as<int2>();
     }
-    unsigned h[C_NUM];
+    unsigned h[C_NUM], nf[2] = {0u, 0u};
     FR_TRY(cudaMemcpyAsync(h, counters(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FR_TRY(nonfinite_read(bvh_, trav(), nf, s));
     FR_TRY(cudaStreamSynchronize(s));
+    // NaN / infinite input: no tree, front or pair of this frame means anything
+    if (nf[0] | nf[1]) {
+        if (count) *count = 0;
+        return BVHCD_INVALID_ARG;
+    }
     int64_t n = which ? (int64_t)h[C_HITS] : (int64_t)h[C_COMPACT];
     if (n > pcap_) n = pcap_;
     if (count) *count = n;

@@ -720,6 +720,8 @@ struct RefitTop {
     unsigned *done;     // leaf blocks finished
     unsigned *delta;    // largest leaf box change of this refit (FP32 bits)
     unsigned *motion;   // accumulated leaf box change (FP32 bits)
+    unsigned *nf_acc;   // a block saw a non-finite input coordinate
+    unsigned *nonfinite;  // the refit's verdict (written by the last block)
 };
 
 // The crossing nodes, run by the CTA that finished last: a node's slot
@@ -810,13 +812,14 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
     extern __shared__ __align__(16) float sb[];  // boxes: the block's leaves, then its nodes
     int *slist = reinterpret_cast<int *>(sb + 12 * kRefitW);
     __shared__ int sofs[kLevelHdr], hmax, last;
-    __shared__ unsigned sdelta;
+    __shared__ unsigned sdelta, snf;
     const int L0 = blockIdx.x * kRefitW;
     const int nl = min(kRefitW, T - L0);
     const int *hdr = lhdr + (size_t)blockIdx.x * kLevelHdr;
     if (threadIdx.x == 0) {
         hmax = 0;
         sdelta = 0u;
+        snf = 0u;
     }
     const int L = __ldg(&hdr[0]);
     const int nloc = L >= 0 ? __ldg(&hdr[2 + L]) : 0;
@@ -825,6 +828,7 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
     // the largest change of a leaf box coordinate, rounded up: a bound on how
     // far any box of the tree moved (a node's box is a min / max of leaf boxes)
     float dmax = 0.f;
+    bool nonfin = false;  // a NaN or infinite input coordinate
 #pragma unroll
     for (int i = 0; i < kRefitSlots; i++) {
         const int t = threadIdx.x + i * kRefitThreads;
@@ -835,7 +839,7 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
         const int2 lk = __ldg(&llink[L0 + t]);
         const float4 olo = __ldcg(lrec + 2 * (size_t)(L0 + t)), ohi = __ldcg(lrec + 2 * (size_t)(L0 + t) + 1);
         float4 lo, hi;
-        face_box(p, f, lo, hi);
+        nonfin |= !face_box_fin(p, f, lo, hi);
         dmax = fmaxf(dmax, fmaxf(box_change(olo.x, lo.x), fmaxf(box_change(olo.y, lo.y), box_change(olo.z, lo.z))));
         dmax = fmaxf(dmax, fmaxf(box_change(ohi.x, hi.x), fmaxf(box_change(ohi.y, hi.y), box_change(ohi.z, hi.z))));
         box_store6(sb + 6 * t, lo, hi);
@@ -846,6 +850,7 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
     if ((threadIdx.x & 31) == 0) atomicMax(&sdelta, __float_as_uint(dmax));  // non-negative: bit order
+    if (__any_sync(0xffffffffu, nonfin) && (threadIdx.x & 31) == 0) atomicOr(&snf, 1u);
     __syncthreads();
     if (L >= 0) {
         run_levels<kRefitThreads>(sofs, L, __ldg(&hdr[kHdrNarrow]), [&](int t) {
@@ -899,8 +904,10 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
         }
     }
     if (gridDim.x == 1) {  // one block: no node crosses
-        if (threadIdx.x == 0)
+        if (threadIdx.x == 0) {
             *g.motion = __float_as_uint(__fadd_ru(__uint_as_float(*g.motion), __uint_as_float(sdelta)));
+            *g.nonfinite = snf;
+        }
         return;
     }
     const int nex = __ldg(&hdr[kHdrCount]);
@@ -917,6 +924,7 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
     __syncthreads();
     if (threadIdx.x == 0) {
         atomicMax(g.delta, sdelta);
+        if (snf) atomicOr(g.nf_acc, 1u);
         __threadfence();
         last = atomicAdd(g.done, 1u) == gridDim.x - 1;
     }
@@ -928,6 +936,34 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
         *g.done = 0u;
         const float d = __uint_as_float(atomicExch(g.delta, 0u));
         *g.motion = __float_as_uint(__fadd_ru(__uint_as_float(*g.motion), d));
+        *g.nonfinite = atomicExch(g.nf_acc, 0u);
+    }
+}
+
+// Finiteness of a build's or restructure's input (the refit checks its own
+// inline): every coordinate of the n floats (positions, or a box scene's FP32
+// boxes); the last block to finish writes the verdict and clears the
+// accumulator, so the check needs no clearing launch.
+__global__ void __launch_bounds__(kThreads) k_check_finite(int64_t n, const float *__restrict__ x, unsigned *ctr) {
+    __shared__ unsigned snf;
+    __shared__ bool last;
+    if (threadIdx.x == 0) snf = 0u;
+    __syncthreads();
+    bool bad = false;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        bad |= !finite1(__ldg(x + i));
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&snf, 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (snf) atomicOr(ctr + C_NF_ACC, 1u);
+        __threadfence();
+        last = atomicAdd(ctr + C_NF_DONE, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        ctr[C_NF_DONE] = 0u;
+        ctr[C_NONFINITE] = atomicExch(ctr + C_NF_ACC, 0u);
     }
 }
 
@@ -1594,7 +1630,10 @@ bvhcd_status LBvh::refit_plan(cudaStream_t s, bool heights_known) {
 bvhcd_status LBvh::refit(cudaStream_t s) {
     StageScope prof_scope(&prof_, BVHCD_STAGE_BVH_REFIT, s);
     const int T = T_;
-    if (T == 0) return BVHCD_OK;
+    if (T == 0) {
+        BV_TRY(cudaMemsetAsync(ctr_.as<unsigned>() + C_NONFINITE, 0, sizeof(unsigned), s));
+        return BVHCD_OK;
+    }
     static const bool attrs = [] {
         cudaFuncSetAttribute(k_refit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLocalSmem);
         return true;
@@ -1610,6 +1649,8 @@ bvhcd_status LBvh::refit(cudaStream_t s) {
     g.done = ctr_.as<unsigned>() + C_REFIT_DONE;
     g.delta = ctr_.as<unsigned>() + C_DELTA;
     g.motion = ctr_.as<unsigned>() + C_MOTION;
+    g.nf_acc = ctr_.as<unsigned>() + C_NF_ACC;
+    g.nonfinite = ctr_.as<unsigned>() + C_NONFINITE;
     const int nb = (T + kRefitW - 1) / kRefitW;
     k_refit<<<nb, kRefitThreads, kLocalSmem, s>>>(T, sface_.as<int4>(), src(), plan_.as<int4>(), llist_.as<int4>(),
                                                   llink_.as<int2>(), lexport_.as<int4>(), lhdr_.as<int>(),
@@ -1737,10 +1778,31 @@ bvhcd_status LBvh::maintain_boxes(bvhcd_bvh_op op, const bvhcd_box_scene &scene,
 
 bvhcd_status LBvh::maintain_ops(bvhcd_bvh_op op, int prevT, bool was_built, cudaStream_t s) {
     opt_tag_ = 0;
-    if (cfg_.enable_restr && updated_ && was_built && built_ && prevT == T_ && T_ >= 2)
-        return restructure(s);
-    if (op == BVHCD_BVH_BUILD || !built_) return build(s);
+    if (cfg_.enable_restr && updated_ && was_built && built_ && prevT == T_ && T_ >= 2) {
+        bvhcd_status st = check_finite(s);
+        return st != BVHCD_OK ? st : restructure(s);
+    }
+    if (op == BVHCD_BVH_BUILD || !built_) {
+        bvhcd_status st = check_finite(s);
+        return st != BVHCD_OK ? st : build(s);
+    }
     return refit(s);  // UPDATE is refit: the reference marks updateIntNode deprecated (LBvhUpdateKernels.cu:88)
+}
+
+// The input of a build or restructure checked for NaN / infinite coordinates
+// (a refit checks inline); the verdict goes to the counter C_NONFINITE, which
+// the front's stats and pair export read.
+bvhcd_status LBvh::check_finite(cudaStream_t s) {
+    const float *x = box_input_ ? bptr_ : vptr_;
+    const int64_t n = box_input_ ? 6 * (int64_t)T_ : 3 * (int64_t)V_;
+    if (!x || n <= 0) {
+        BV_TRY(cudaMemsetAsync(ctr_.as<unsigned>() + C_NONFINITE, 0, sizeof(unsigned), s));
+        return BVHCD_OK;
+    }
+    int64_t g = (n + kThreads - 1) / kThreads;
+    if (g > kSms * 4) g = kSms * 4;
+    k_check_finite<<<(unsigned)g, kThreads, 0, s>>>(n, x, ctr_.as<unsigned>()); note_launch();
+    return cuda_status(cudaGetLastError());
 }
 
 bvhcd_status LBvh::request_restructure(const int32_t *roots, int32_t n, cudaStream_t s) {

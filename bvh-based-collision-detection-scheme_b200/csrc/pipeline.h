@@ -16,6 +16,10 @@
 
 namespace bvhcd {
 
+// Host-side fault injection for the tests (bvhcd_debug_fail_alloc): true when
+// the device allocation about to be made is the one chosen to fail.
+bool alloc_fault_due();
+
 // Device buffer owned by a handle.
 struct DBuf {
     void *p = nullptr;
@@ -25,7 +29,7 @@ struct DBuf {
         if (p) cudaFree(p);
         p = nullptr;
         bytes = 0;
-        cudaError_t e = cudaMalloc(&p, n);
+        cudaError_t e = alloc_fault_due() ? cudaErrorMemoryAllocation : cudaMalloc(&p, n);
         if (e == cudaSuccess) bytes = n;
         return e;
     }
@@ -145,6 +149,9 @@ class LBvh {
     void set_updated(bool u) { updated_ = u; }
     bool updated() const { return updated_; }
     unsigned *counters() const { return ctr_.as<unsigned>(); }
+    // this BVH's device word saying the last maintain's input held a NaN or
+    // infinite coordinate
+    const unsigned *nonfinite_flag() const { return ctr_.as<unsigned>() + C_NONFINITE; }
     int last_rt_subtrees() const { return rt_subtrees_; }
     int last_rt_intnodes() const { return rt_intnodes_; }
     Profiler *profiler() { return &prof_; }
@@ -162,6 +169,7 @@ class LBvh {
     bvhcd_status scene_box(cudaStream_t s);
     bvhcd_status climb_and_order(cudaStream_t s);
     bvhcd_status node_fp16(cudaStream_t s);
+    bvhcd_status check_finite(cudaStream_t s);
 
     bvhcd_bvh_config cfg_;
     int T_ = 0, V_ = 0, capT_ = 0, capV_ = 0;
@@ -276,7 +284,7 @@ class Front {
     bvhcd_status narrow(cudaStream_t s, bool test);
     bvhcd_status check_quality(cudaStream_t s);
     bvhcd_status snapshot(cudaStream_t s);
-    bvhcd_status grow_and_check(cudaStream_t s, bool *overflowed);
+    bvhcd_status grow_and_check(cudaStream_t s, unsigned *ovf_bits);
     bvhcd_status grow_from(const unsigned *h, cudaStream_t s);
     bvhcd_status deferred_check(cudaStream_t s, bool *regen);
     bvhcd_status deferred_snapshot(cudaStream_t s);

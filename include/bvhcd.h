@@ -140,7 +140,13 @@ typedef struct {
                                 expiry had come (the others cannot have changed state) */
     int32_t overflow_any;    /* the overflow bits of every maintain since the front was
                                 created (sticky; a replay of auto_grow = 1 clears its own) */
-    int32_t reserved[3];
+    int32_t nonfinite_input; /* 1: the last maintain of the front's BVH (either BVH of an
+                                inter front) was given a NaN or infinite coordinate; the
+                                frame's tree, front and pairs mean nothing, and
+                                bvhcd_front_pairs returns BVHCD_INVALID_ARG.  The reference
+                                does not check (its CUDA error checks exit the process,
+                                Mine/utility/CudaThrustUtils.hpp:9-11). */
+    int32_t reserved[2];
 } bvhcd_front_stats;
 
 typedef struct bvhcd_bvh bvhcd_bvh;
@@ -291,6 +297,13 @@ bvhcd_status bvhcd_profile_read(bvhcd_bvh *bvh, double *ms, int64_t *calls, int3
  * for benchmarks; no reference counterpart beyond the per-kernel timers of
  * Mine/system/CudaDevice/CudaKernelLauncher.cu:54-69). */
 bvhcd_status bvhcd_launch_count(int64_t *n);
+
+/* Fault injection for tests (no counterpart in the reference, whose
+ * allocation failures end the process in checkCudaErrors): the n-th device
+ * allocation the library makes from now on (n >= 1) fails as if the device
+ * were out of memory, so the call that makes it returns BVHCD_OUT_OF_MEMORY;
+ * n = 0 cancels a planned fault.  Host-side only: nothing reaches the GPU. */
+bvhcd_status bvhcd_debug_fail_alloc(int64_t n);
 
 /* ---- Morton order without device allocation.  No counterpart in the
  * reference.  For callers that may not allocate device memory once they are
