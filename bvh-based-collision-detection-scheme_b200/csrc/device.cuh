@@ -10,8 +10,9 @@
 //                         starts at s); escape = lca[s+1], the next node in
 //                         DFS order after the leaf.
 //   nrec[2d], nrec[2d+1]  internal record, one 32-byte sector:
-//                         {min.xyz, rangex}, {max.xyz, escape}
-//                         escape = lca[rangey+1].
+//                         {min.xyz, rangex | leftleaf << 31}, {max.xyz, escape}
+//                         escape = lca[rangey+1]; leftleaf = the left child is
+//                         the leaf rangex (else it is node d + 1).
 //   sface[s]              int4 {v0, v1, v2, original triangle id}
 //   lca[0..T]             tagged DFS entry per leaf (node<<1, or leaf<<1|1),
 //                         lca[T] = -1, the reference's escape links

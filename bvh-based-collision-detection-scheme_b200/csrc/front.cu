@@ -72,8 +72,8 @@ struct FArgs {
     const unsigned *ksel;
 };
 
-// A node's box and escape link: from the FP32 record ({lo.xyz, rangex},
-// {hi.xyz, escape}), or, with FP16 node boxes, from the 16-byte record {min.xyz,
+// A node's box and escape link: from the FP32 record ({lo.xyz, rangex |
+// leftleaf << 31}, {hi.xyz, escape}), or, with FP16 node boxes, from the 16-byte record {min.xyz,
 // max.xyz as halves rounded outward, escape}.  The FP16 box contains the FP32
 // one, so a traversal on it visits a superset of the nodes and still tests
 // every overlapping leaf in FP32: the pair set does not change.
@@ -88,9 +88,9 @@ __device__ __forceinline__ void node_rec(const FArgs &a, int n, float4 &lo, floa
         ldg8(a.nrec + 2 * n, lo, hi);
     }
 }
-// the node's leftmost leaf (its lo.w in the FP32 record)
+// the node's leftmost leaf (lo.w of the FP32 record without its bit 31)
 __device__ __forceinline__ int node_rangex(const FArgs &a, int n, const float4 &lo) {
-    return a.nrec16 ? __ldg(&a.nrange[n]).x : __float_as_int(lo.w);
+    return a.nrec16 ? __ldg(&a.nrange[n]).x : (__float_as_int(lo.w) & 0x7fffffff);
 }
 
 // Per-node counter increment aggregated over the converged lanes of a warp
@@ -200,15 +200,34 @@ __device__ __forceinline__ Spread spread(unsigned n) {
     return Spread{t < lanes ? t : n, lanes};
 }
 
+// left child of internal node d, tagged: the FP32 record carries it (bit 31
+// of lo.w set: the left child is the leaf rangex; clear: it is node d + 1,
+// the next id in DFS order); the FP16 record does not, so there it comes
+// from the range and the leaf's parent
+__device__ __forceinline__ int left_child_tagged(const FArgs &a, int d, const float4 &lo) {
+    if (!a.nrec16) {
+        const int w = __float_as_int(lo.w);
+        return w < 0 ? (((w & 0x7fffffff) << 1) | 1) : ((d + 1) << 1);
+    }
+    const int rx = __ldg(&a.nrange[d]).x;
+    const int last = __float_as_int(__ldg(reinterpret_cast<const float *>(a.lrec) + 8 * (size_t)rx + 3));
+    return last == d ? ((rx << 1) | 1) : ((d + 1) << 1);
+}
+
 // Stackless traversal from tagged node `st` until tagged node `stop`
 // (the loop shared by genLooseIntraFrontsWithLog,
 // Mine/collision/bvtt_front/BvttFrontGenerateKernels.cu:65-88, the sprout
 // half of maintainIntLooseIntraFrontsWithLog,
 // BvttFrontPruneSproutKernels.cu:34-56, keepIntLooseIntraFronts,
 // BvttFrontKeepKernels.cu:26-42, and pureBvhSelfCD, BvhCDKernels.cu:30-47):
-// walk the left spine of an internal node by DFS id while the box overlaps,
-// up to the parent of its leftmost leaf; a node that stops overlapping is a
-// front node and is left through its escape link.
+// the reference walks the left spine of an internal node by DFS id while the
+// box overlaps, up to the parent of its leftmost leaf; a node that stops
+// overlapping is a front node and is left through its escape link.  Here
+// every step reads one 32-byte record, a leaf's or a node's, and moves to
+// the escape link (a leaf, or a node that does not overlap) or to the left
+// child (an overlapping node): the same visits in the same order, with one
+// loop body for all lanes of a warp and no leaf record read ahead at each
+// spine.
 template <bool kFront>
 __device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const float4 &plo,
                                          const float4 &phi, const int4 &pf, int st, int stop) {
@@ -220,41 +239,22 @@ __device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const
             atomicOr(a.ctr + C_OVERFLOW, 16u);
             return;
         }
-        int leaf;
-        float4 llo, lhi;
+        const int id = st >> 1;
+        float4 lo, hi;
+        if (st & 1) ldg8(a.lrec + 2 * id, lo, hi);
+        else node_rec(a, id, lo, hi);
+        const bool ov = overlap(lo, hi, plo, phi);
         if (st & 1) {
-            leaf = st >> 1;
-            ldg8(a.lrec + 2 * leaf, llo, lhi);
+            if (ov) emit_pair(a, em, prim, pf, id);
+            if (kFront) emit_ext(a, em, prim, id);
+            st = __float_as_int(hi.w);
+        } else if (!ov) {
+            if (kFront) emit_int(a, em, prim, id);
+            st = __float_as_int(hi.w);
         } else {
-            int n = st >> 1;
-            float4 nlo, nhi;
-            node_rec(a, n, nlo, nhi);
-            leaf = node_rangex(a, n, nlo);
-            ldg8(a.lrec + 2 * leaf, llo, lhi);
-            const int last = __float_as_int(llo.w);  // parent of the leftmost leaf
-            bool stopped = false;
-            while (true) {
-                if (!overlap(nlo, nhi, plo, phi)) { stopped = true; break; }
-                if (n >= last) break;
-                ++n;
-                node_rec(a, n, nlo, nhi);
-            }
-            if (stopped) {
-                if (kFront) emit_int(a, em, prim, n);
-                st = __float_as_int(nhi.w);
-                continue;
-            }
+            st = left_child_tagged(a, id, lo);
         }
-        if (overlap(llo, lhi, plo, phi)) emit_pair(a, em, prim, pf, leaf);
-        if (kFront) emit_ext(a, em, prim, leaf);
-        st = __float_as_int(lhi.w);
     }
-}
-
-// left child of internal node d, tagged, and its escape
-__device__ __forceinline__ int left_child_tagged(const FArgs &a, int d, int rx) {
-    const int last = __float_as_int(__ldg(reinterpret_cast<const float *>(a.lrec) + 8 * (size_t)rx + 3));
-    return last == d ? ((rx << 1) | 1) : ((d + 1) << 1);
 }
 
 __device__ __forceinline__ int4 prim_face(const FArgs &a, int prim) {
@@ -378,8 +378,7 @@ __global__ void __launch_bounds__(kB) k_sprout(FArgs a) {
         ldg8(a.prec + 2 * e.x, plo, phi);
         float4 nlo, nhi;
         node_rec(a, e.y, nlo, nhi);
-        traverse<kFront>(a, em, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, node_rangex(a, e.y, nlo)),
-                         __float_as_int(nhi.w));
+        traverse<kFront>(a, em, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, nlo), __float_as_int(nhi.w));
     }
     em_close(a, em);
 }
@@ -481,12 +480,15 @@ __global__ void __launch_bounds__(kThreads) k_keep_select(FArgs a, unsigned *lis
 #pragma unroll
         for (int r = 0; r < kSelPer; r++) {  // every load of the tile in flight at once
             const unsigned q = t0 + (warp * kSelPer + r) * 32u + lane;
-            ex[r] = q >= total ? 3.402823466e+38f : q < ni ? __ldcs(a.iexp_in + q) : __ldcs(a.xexp_in + (q - ni));
+            ex[r] = q >= total ? 0.f : q < ni ? __ldcs(a.iexp_in + q) : __ldcs(a.xexp_in + (q - ni));
         }
         unsigned m[kSelPer], n = 0;
 #pragma unroll
         for (int r = 0; r < kSelPer; r++) {
-            m[r] = __ballot_sync(0xffffffffu, !(M < ex[r]));
+            // past the end nothing is picked, whatever the motion (an infinite
+            // input coordinate makes it infinite)
+            const unsigned q = t0 + (warp * kSelPer + r) * 32u + lane;
+            m[r] = __ballot_sync(0xffffffffu, q < total && !(M < ex[r]));
             n += __popc(m[r]);
         }
         if (lane == 0) wsum[warp] = n;
@@ -625,16 +627,24 @@ __global__ void __launch_bounds__(kB) k_balance_scan(FArgs a) {
 //
 // Tiles of kReorderTile entries: each CTA first groups its tile by key
 // (group, internal or external front) in a shared-memory hash table, taking
-// each entry's rank within its key; then one global atomic per distinct key
-// reserves the key's run in the sorted front; then every entry is written at
-// run start + rank.  Neighbouring primitives share most front nodes and a
-// group holds several nodes, so a tile holds far fewer keys than entries:
-// the cursor atomics (which serialise on the groups near the root) drop by
-// that factor, and a key's entries land next to each other.
-constexpr int kReorderThreads = 256;
+// each entry's rank within its key and listing the slots it filled; then one
+// global atomic per distinct key reserves the key's run in the sorted front;
+// then every entry is written at run start + rank.  Neighbouring primitives
+// share most front nodes and a group holds several nodes, so a tile holds
+// far fewer keys than entries: the cursor atomics (which serialise on the
+// groups near the root) drop by that factor, and a key's entries land next to
+// each other.  Only the listed slots are visited to place the runs and to
+// clear the table for the next tile (a tile fills a few hundred of its
+// slots), and the table is cleared whole once per CTA.
+#ifndef BVHCD_REORDER_THREADS
+#define BVHCD_REORDER_THREADS 256
+#endif
+constexpr int kReorderThreads = BVHCD_REORDER_THREADS;
 constexpr int kReorderPer = 8;                                   // entries per thread per tile
-constexpr int kReorderTile = kReorderThreads * kReorderPer;      // 2048
+constexpr int kReorderTile = kReorderThreads * kReorderPer;
 constexpr int kReorderSlots = 2 * kReorderTile;                  // hash slots (load factor <= 1/2)
+constexpr int kReorderHashShift = 32 - (kReorderThreads == 512 ? 13 : 12);
+static_assert(kReorderSlots == (1 << (32 - kReorderHashShift)), "hash width");
 constexpr unsigned kEmptyKey = 0xffffffffu;
 
 #ifndef BVHCD_REORDER_SHIFT
@@ -645,21 +655,26 @@ constexpr int kReorderShift = BVHCD_REORDER_SHIFT;  // 4 nodes (128 bytes of nod
 inline size_t reorder_groups(int T) { return ((size_t)T >> kReorderShift) + 2; }
 
 __global__ void __launch_bounds__(kReorderThreads) k_reorder(FArgs a, unsigned *cur_int, unsigned *cur_ext) {
-    __shared__ unsigned skey[kReorderSlots], scnt[kReorderSlots], sbase[kReorderSlots];
+    extern __shared__ unsigned rsm[];
+    unsigned *skey = rsm, *scnt = rsm + kReorderSlots, *sbase = rsm + 2 * kReorderSlots;
+    unsigned short *sused = reinterpret_cast<unsigned short *>(rsm + 3 * kReorderSlots);  // filled slots (< 2^16)
+    __shared__ unsigned nused[2];
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.ctr[a.out_int_slot] = a.log.intbeg[a.T];
         a.ctr[a.out_ext_slot] = a.log.extbeg[a.T];
     }
+    for (int i = threadIdx.x; i < kReorderSlots; i += kReorderThreads) {
+        skey[i] = kEmptyKey;
+        scnt[i] = 0u;
+    }
+    if (threadIdx.x == 0) nused[0] = nused[1] = 0u;
+    __syncthreads();
     const unsigned total = ni + ne;
     const unsigned ntiles = (total + kReorderTile - 1) / kReorderTile;
-    for (unsigned tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        for (int i = threadIdx.x; i < kReorderSlots; i += kReorderThreads) {
-            skey[i] = kEmptyKey;
-            scnt[i] = 0u;
-        }
-        __syncthreads();
+    unsigned par = 0;
+    for (unsigned tile = blockIdx.x; tile < ntiles; tile += gridDim.x, par ^= 1u) {
         int2 e[kReorderPer];
         unsigned slot[kReorderPer], rank[kReorderPer];
 #pragma unroll
@@ -673,22 +688,25 @@ __global__ void __launch_bounds__(kReorderThreads) k_reorder(FArgs a, unsigned *
             slot[j] = kEmptyKey;
             if (e[j].x == -1) continue;  // hole (a tagged entry is never -1: its index is below 2^31 - 1)
             const unsigned key = (((unsigned)e[j].y >> kReorderShift) << 1) | ((unsigned)e[j].x >> 31);
-            unsigned h = (key * 2654435761u) >> 20;  // 12 bits: kReorderSlots = 4096
+            unsigned h = (key * 2654435761u) >> kReorderHashShift;
             for (int probe = 0; probe < kReorderSlots; probe++, h = (h + 1) & (kReorderSlots - 1)) {
                 const unsigned prev = atomicCAS(&skey[h], kEmptyKey, key);
+                if (prev == kEmptyKey) sused[atomicAdd(&nused[par], 1u)] = (unsigned short)h;
                 if (prev == kEmptyKey || prev == key) break;
             }
             slot[j] = h;
             rank[j] = atomicAdd(&scnt[h], 1u);
         }
+        if (threadIdx.x == 0) nused[par ^ 1u] = 0u;  // the next tile's list (last read before this tile's first barrier)
         __syncthreads();
-        for (int i = threadIdx.x; i < kReorderSlots; i += kReorderThreads) {
-            const unsigned key = skey[i];
-            if (key == kEmptyKey) continue;
+        const unsigned nu = nused[par];
+        for (unsigned i = threadIdx.x; i < nu; i += kReorderThreads) {
+            const unsigned h = sused[i];
+            const unsigned key = skey[h];
             const unsigned g = key >> 1;
             const unsigned first = g << kReorderShift;
-            if (key & 1u) sbase[i] = a.log.extbeg[first] + atomicAdd(cur_ext + g, scnt[i]);
-            else sbase[i] = a.log.intbeg[first] + atomicAdd(cur_int + g, scnt[i]);
+            if (key & 1u) sbase[h] = a.log.extbeg[first] + atomicAdd(cur_ext + g, scnt[h]);
+            else sbase[h] = a.log.intbeg[first] + atomicAdd(cur_int + g, scnt[h]);
         }
         __syncthreads();
 #pragma unroll
@@ -703,9 +721,18 @@ __global__ void __launch_bounds__(kReorderThreads) k_reorder(FArgs a, unsigned *
                 a.out_ext[pos] = v;
             }
         }
-        __syncthreads();  // the table is cleared for the next tile
+        // the filled slots are emptied for the next tile (the scatter reads only sbase)
+        for (unsigned i = threadIdx.x; i < nu; i += kReorderThreads) {
+            const unsigned h = sused[i];
+            skey[h] = kEmptyKey;
+            scnt[h] = 0u;
+        }
+        __syncthreads();
     }
 }
+
+constexpr size_t kReorderSmem = sizeof(unsigned) * 3 * kReorderSlots + sizeof(unsigned short) * kReorderTile;
+static_assert(kReorderSlots <= 65536, "slot indices are listed as 16-bit values");
 
 // frontSnapshot (BvttFrontGenerateKernels.cu:26-32)
 __global__ void k_snapshot(int nint, const int2 *__restrict__ nrange, const unsigned *__restrict__ intbeg,
@@ -1176,8 +1203,15 @@ bvhcd_status Front::reorder(cudaStream_t s) {
     a.in_int_slot = 2 * nx; a.in_ext_slot = 2 * nx + 1;
     a.out_int_slot = 2 * cur_; a.out_ext_slot = 2 * cur_ + 1;
     a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
-    k_reorder<<<RESIDENT_B(k_reorder, kReorderThreads), kReorderThreads, 0, s>>>(a, rcur_.as<unsigned>(),
-                                                                                 rcur_.as<unsigned>() + ng);
+    static const unsigned grid = [] {
+        cudaFuncSetAttribute(k_reorder, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kReorderSmem);
+        int nb = 0, dev = 0, sms = kSms;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_reorder, kReorderThreads, kReorderSmem);
+        return (unsigned)((nb > 0 ? nb : 1) * sms);
+    }();
+    k_reorder<<<grid, kReorderThreads, kReorderSmem, s>>>(a, rcur_.as<unsigned>(), rcur_.as<unsigned>() + ng);
     note_launch();
     log_counted_ = true;  // the emission before it counted every entry
     return cuda_status(cudaGetLastError());

@@ -383,7 +383,7 @@ __global__ void k_write_nodes(int nint, int T, Climb c, const int *__restrict__ 
         nrange[d] = make_int2(rx, ry);
         height[d] = c.uheight[u];
         float4 lo = c.ubox[2 * u], hi = c.ubox[2 * u + 1];
-        lo.w = __int_as_float(rx);
+        lo.w = __int_as_float(rx | ((m & 1u) ? (int)0x80000000 : 0));  // bit 31: the left child is leaf rx
         hi.w = __int_as_float(scene_end(leafscene, ry, T) ? -1 : lca_of(ry + 1, T, coff, clen));
         nrec[2 * d] = lo;
         nrec[2 * d + 1] = hi;
@@ -1101,7 +1101,7 @@ __global__ void k_rs_write(int nr, int T, const int *__restrict__ task, const in
             topo[d] = make_int4((m & 1u) ? lc : dfs[lc], (m & 2u) ? rc : dfs[rc], par, (int)m);
             nrange[d] = make_int2(rx, ry);
             float4 lo = c.ubox[2 * u], hi = c.ubox[2 * u + 1];
-            lo.w = __int_as_float(rx);
+            lo.w = __int_as_float(rx | ((m & 1u) ? (int)0x80000000 : 0));  // bit 31: the left child is leaf rx
             hi.w = __int_as_float(lca[ry + 1]);
             nrec[2 * d] = lo;
             nrec[2 * d + 1] = hi;

@@ -124,3 +124,51 @@ def test_fp16_node_boxes_c2_brute(cuda, lib_built, oracle):
         front.maintain(op)
         assert front.stats()["overflow"] == 0
         assert np.array_equal(oracle.canon_pairs(front.pairs()), oracle.brute_pairs(faces, frames[f], 1)), f
+
+
+@pytest.mark.parametrize("z_noise", [0.0, 0.8])
+def test_stacked_layers_full_size_against_exact_predicate(cuda, lib_built, oracle, z_noise):
+    """The precision configuration at its stated size: four stacked 512x512
+    cloths (2,088,968 triangles) 1e-3 apart with in-plane shear -- as stated
+    (z_noise 0: flat layers, every broad pair coplanar inside a layer) and
+    with a grazing vertical jitter of up to 0.8 gaps (layers cut each other).
+    FP16 outward-rounded node records, precision = 1.  Every frame: the broad
+    set equals the sweep-and-prune set of overlapping FP32 boxes and the hits
+    equal the exact (expansion-arithmetic) tri-tri predicate over it; on the
+    last frame the contact points and distances are within 1e-5 of the FP64
+    oracle, relative to the pair's size."""
+    import scenes
+    faces, frames = scenes.stacked_layers_frames(512, 4, 3, z_noise=z_noise)
+    T, V = faces.shape[0], frames[0].shape[0]
+    assert T == 2_088_968
+    bvh = lib_built.LBvh(T, V, enable_restr=False, node_box_fp16=True)
+    front = lib_built.BvttFront(bvh, 80_000_000, 60_000_000, 16_000_000, cull_adjacent=True, narrow_phase=True,
+                                precision=1)
+    for f in range(3):
+        b, fr = lib_built.schedule(f)
+        bvh.maintain(b, frames[f], faces, faces_static=f > 0)
+        front.maintain(fr)
+        st = front.stats()
+        assert st["overflow"] == 0, (f, st)
+        broad = oracle.canon_pairs(front.pairs())
+        exp = oracle.brute_pairs(faces, frames[f], 1)
+        assert np.array_equal(broad, exp), f
+        exact = oracle.narrow(exp, faces, frames[f], exact=True).astype(bool)
+        hits = oracle.canon_pairs(front.pairs(narrow=True))
+        assert np.array_equal(hits, exp[exact]), f
+    print(f"z_noise {z_noise}: {len(broad)} broad pairs, {len(hits)} hits, {st['flagged']} flagged")
+    if z_noise:
+        h = front.pairs(narrow=True)
+        c, _ = front.contacts(0)
+        _, con, _ = oracle.precision_pairs(h, faces, frames[2])
+        both = ~np.isnan(con[:, 0]) & ~np.isnan(c[:, 0])
+        assert both.sum() > 0.9 * len(h)
+        e = np.abs(c[both, :3].astype(np.float64) - con[both, :3]).max(axis=1) / _scale(faces, frames[2], h)[both]
+        assert float(e.max()) <= 1e-5, float(e.max())
+        bp = front.pairs()
+        d, _ = front.contacts(1)
+        hit64, _, dist = oracle.precision_pairs(bp, faces, frames[2])
+        assert np.array_equal(d[:, 3] == 0, hit64)
+        dd = ~hit64
+        ed = np.abs(d[dd, 3].astype(np.float64) - dist[dd]) / _scale(faces, frames[2], bp)[dd]
+        assert float(ed.max()) <= 1e-5, float(ed.max())
