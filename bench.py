@@ -190,9 +190,13 @@ def run_ours(args):
         inter = inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, st)
         boxes = box_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T)
         prox = proximity_pass(bvhcd, torch, front, stream)
-    learned = None
-    if not args.only_value and not args.no_batched:
+    learned = prec = prec_keep = None
+    if not args.only_value and not args.no_precision:
         del dev, host, flush
+        torch.cuda.empty_cache()
+        prec, prec_keep = precision_pass(bvhcd, torch, stream, args)
+    if not args.only_value and not args.no_batched:
+        dev = host = flush = None
         torch.cuda.empty_cache()
         batched = batched_pass(bvhcd, torch, args, world, rank)
     if not args.only_value and not args.no_learned:
@@ -202,6 +206,8 @@ def run_ours(args):
     out = None
     if rank == 0:
         cpu = cpu_baseline(faces, frames, args) if world == 1 and not args.no_cpu_baseline else None
+        if prec is not None and cpu is not None:
+            prec["cpu_check"] = precision_check(prec_keep)
         out = {
             "metric": METRIC, "value": round(value, 4), "unit": "ms/frame", "n_gpus": world,
             "steps": K, "warmup": W, "ms_per_step": round(value * world, 4), "higher_is_better": False,
@@ -223,6 +229,7 @@ def run_ours(args):
             "clocks": clk.summary(),
             "auto_grow": grow,
             "fp16_node_boxes": fp16,
+            "precision": prec,
             "inter_rigid_obstacle": inter,
             "box_scene": boxes,
             "proximity": prox,
@@ -639,6 +646,8 @@ def inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, single):
         raise RuntimeError(f"inter leg overflow: {si} {sx} {so}")
     pairs = [si["broad_pairs"] + sx["broad_pairs"] + so["broad_pairs"],
              si["narrow_hits"] + sx["narrow_hits"] + so["narrow_hits"]]
+    restr = inter_restructure_timing(bvhcd, torch, cbvh, sbvh, intra, inter, dev[W + K - 1], cfaces, sfaces, Vc,
+                                     flush, stream)
     for h in (own, inter, intra):
         h.close()
     sbvh.close()
@@ -649,7 +658,58 @@ def inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, single):
             "pairs_last_frame": {"cloth_self": [si["broad_pairs"], si["narrow_hits"]],
                                  "cloth_sphere": [sx["broad_pairs"], sx["narrow_hits"]],
                                  "sphere_self": [so["broad_pairs"], so["narrow_hits"]]},
-            "pairs_equal_single_front": pairs == [single["broad_pairs"], single["narrow_hits"]]}
+            "pairs_equal_single_front": pairs == [single["broad_pairs"], single["narrow_hits"]],
+            "front_restructure": restr}
+
+
+def _restructure_roots(inode, frac=0.2, lo=16, hi=512):
+    """Disjoint subtrees (DFS ids) of lo..hi leaves covering about `frac` of
+    the internal nodes, in DFS order: the marks a front-quality check leaves."""
+    size = inode[:, 5] - inode[:, 4] + 1
+    covered = np.zeros(inode.shape[0] + 1, bool)
+    chosen, total = [], 0
+    for d in range(inode.shape[0]):
+        if lo <= size[d] <= hi and not covered[d]:
+            chosen.append(d)
+            covered[d:d + size[d] - 1] = True
+            total += size[d] - 1
+            if total >= frac * inode.shape[0]:
+                break
+    return np.array(chosen, np.int32)
+
+
+def inter_restructure_timing(bvhcd, torch, cbvh, sbvh, intra, inter, pos, cfaces, sfaces, Vc, flush, stream):
+    """The inter front after a restructure of the cloth's BVH (subtrees
+    covering a fifth of its internal nodes marked, as a quality check would):
+    CUDA-event time of the front restructure (valid entries kept, the
+    restructured subtrees re-sprouted: BvttFrontLooseInter::restructure)
+    against a regeneration of the same front on the same trees, and whether
+    the two give the same pairs."""
+    cbvh.request_restructure(_restructure_roots(cbvh.export()["inode"]), stream=stream)
+    cbvh.maintain(bvhcd.BVH_REFIT, pos[:Vc], cfaces, stream=stream, faces_static=True)
+    tag = cbvh.opt_tag()
+    intra.maintain(bvhcd.FRONT_KEEP, stream=stream)
+    sbvh.maintain(bvhcd.BVH_REFIT, pos[Vc:], sfaces, stream=stream, faces_static=True)
+    out = {"bvh_opt_tag": tag}
+    for name, op in (("resprout", bvhcd.FRONT_KEEP), ("regenerate", bvhcd.FRONT_GENERATE)):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        inter.maintain(op, stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        st = inter.stats(stream)
+        out[name] = {"ms": round(a.elapsed_time(b), 4), "front_op_run": st["front_op_run"],
+                     "pairs": st["broad_pairs"], "fronts": [st["int_front"], st["ext_front"]]}
+        out[name + "_pairs"] = bvhcd_canon(inter.pairs(stream=stream))
+    out["pairs_equal"] = bool(np.array_equal(out.pop("resprout_pairs"), out.pop("regenerate_pairs")))
+    out["speedup"] = round(out["regenerate"]["ms"] / out["resprout"]["ms"], 3) if out["resprout"]["ms"] else None
+    return out
+
+
+def bvhcd_canon(p):
+    p = np.asarray(p, dtype=np.int64).reshape(-1, 2)
+    return p[np.lexsort((p[:, 1], p[:, 0]))]
 
 
 def autogrow_pass(bvhcd, torch, dev, dfaces, stream, W, K, T):
@@ -794,6 +854,110 @@ def fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
             "pairs_last_frame": [st["broad_pairs"], st["narrow_hits"]]}
 
 
+# front / pair capacities of the two stacked-layer runs (the grazing layers hold
+# about 63 front entries per triangle)
+PREC_CAPS = {0.0: dict(int_front_capacity=60_000_000, ext_front_capacity=40_000_000, pair_capacity=8_000_000),
+             0.8: dict(int_front_capacity=130_000_000, ext_front_capacity=90_000_000, pair_capacity=16_000_000)}
+
+
+def precision_pass(bvhcd, torch, stream, args):
+    """The precision configuration: four stacked 512x512 cloths (2,088,968
+    triangles) 1e-3 apart with a seeded in-plane shear (scenes.
+    stacked_layers_frames), 50 frames, FP16 outward-rounded node records and
+    precision = 1 (FP32 narrow phase where it is certain, FP64 on the pairs it
+    flags), the reference's schedule.  Device-resident frames, L2 flushed
+    between timed frames; ms/frame and the share of broad pairs flagged for
+    FP64.  A second, 3-frame run of the same layers with a grazing vertical
+    jitter (up to 0.8 gaps: layers cut each other) gives intersecting pairs
+    whose contact points the CPU check compares with FP64.  Returns the JSON
+    block and the last frames' device results for that check."""
+    import scenes
+    out, keep = {}, {}
+    F = args.precision_frames
+    for name, zn, nf in (("as_stated", 0.0, F), ("grazing", 0.8, 3)):
+        faces, frames = scenes.stacked_layers_frames(512, 4, nf, z_noise=zn)
+        T, V = faces.shape[0], frames[0].shape[0]
+        dev = torch.from_numpy(np.stack(frames)).cuda()
+        dfaces = torch.from_numpy(faces).cuda()
+        bvh = bvhcd.LBvh(T, V, enable_restr=True, node_box_fp16=True)
+        front = bvhcd.BvttFront(bvh, cull_adjacent=True, narrow_phase=True, auto_grow=False, precision=1,
+                                **PREC_CAPS[zn])
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        W = min(3, nf - 1)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(nf)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(nf)]
+        flagged = broad = 0
+        for f in range(nf):
+            flush.zero_()
+            starts[f].record(stream)
+            bvhcd.frame(bvh, front, f, 0, dev[f], dfaces, stream=stream, faces_static=f > 0)
+            ends[f].record(stream)
+            if f >= W:
+                st = front.stats(stream)  # outside the events: counts for the flagged share
+                flagged += st["flagged"]
+                broad += st["broad_pairs"]
+        torch.cuda.synchronize()
+        st = front.stats()
+        if st["overflow_any"]:
+            raise RuntimeError(f"precision leg overflow: {st}")
+        ms = float(sum(a.elapsed_time(b) for a, b in zip(starts[W:], ends[W:]))) / (nf - W)
+        out[name] = {"workload": f"4 x 512x512 cloths, {T} triangles, 1e-3 apart, in-plane shear"
+                                 + (", vertical jitter up to 0.8 gaps" if zn else "") + f", {nf} frames",
+                     "value": round(ms, 4), "unit": "ms/frame", "frames_timed": nf - W,
+                     "flagged_fraction": round(flagged / broad, 6) if broad else 0.0,
+                     "pairs_last_frame": [st["broad_pairs"], st["narrow_hits"]]}
+        hits = front.pairs(narrow=True)
+        keep[name] = {"faces": faces, "pos": frames[-1], "broad": front.pairs(), "hits": hits,
+                      "contacts": front.contacts(0)[0] if zn else None,
+                      "dist_pairs": front.pairs() if zn else None, "dists": front.contacts(1)[0] if zn else None}
+        front.close()
+        bvh.close()
+        del dev, dfaces, flush
+        torch.cuda.empty_cache()
+    out["node_records"] = "16 B (FP16, outward-rounded)"
+    out["narrow_phase"] = "fp32 17-axis SAT, fp64 on flagged pairs (precision = 1)"
+    return out, keep
+
+
+def precision_check(keep):
+    """CPU side of the precision leg (the oracle as checker, on the host
+    cores): the last frame's broad set against the sweep-and-prune set of
+    overlapping FP32 boxes and its hits against the exact expansion-arithmetic
+    predicate; on the grazing frame, contact points (segment midpoints) and
+    distances against FP64, relative to each pair's extent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    res = {}
+    for name, k in keep.items():
+        faces, pos = k["faces"], k["pos"]
+        exp = pyoracle.brute_pairs(faces, pos, 1)
+        exact = pyoracle.narrow(exp, faces, pos, exact=True).astype(bool)
+        r = {"broad_equal_bruteforce": bool(np.array_equal(pyoracle.canon_pairs(k["broad"]), exp)),
+             "hits_equal_exact_predicate": bool(np.array_equal(pyoracle.canon_pairs(k["hits"]), exp[exact])),
+             "broad_pairs": int(len(exp)), "hits": int(exact.sum())}
+        if k["contacts"] is not None:
+            def scale(pairs):
+                a, b = pos[faces[pairs[:, 0]]], pos[faces[pairs[:, 1]]]
+                pts = np.concatenate([a, b], axis=1)
+                return (pts.max(axis=1) - pts.min(axis=1)).max(axis=1).astype(np.float64)
+            h = k["hits"]
+            _, con, _ = pyoracle.precision_pairs(h, faces, pos)
+            c = k["contacts"]
+            both = ~np.isnan(con[:, 0]) & ~np.isnan(c[:, 0])
+            e = np.abs(c[both, :3].astype(np.float64) - con[both, :3]).max(axis=1) / scale(h)[both]
+            bp, d = k["dist_pairs"], k["dists"]
+            hit64, _, dist = pyoracle.precision_pairs(bp, faces, pos)
+            sep = ~hit64
+            ed = np.abs(d[sep, 3].astype(np.float64) - dist[sep]) / scale(bp)[sep]
+            r["contact_point_error"] = {"max": float(e.max()) if e.size else 0.0,
+                                        "mean": float(e.mean()) if e.size else 0.0, "points": int(both.sum())}
+            r["distance_error"] = {"max": float(ed.max()) if ed.size else 0.0,
+                                   "mean": float(ed.mean()) if ed.size else 0.0, "pairs": int(sep.sum())}
+            r["zero_distance_equals_fp64_hit"] = bool(np.array_equal(d[:, 3] == 0, hit64))
+        res[name] = r
+    return res
+
+
 def learned_pass(torch, args):
     """The learned scheduler (weights trained on the GPU by learn.py, shipped
     in learned_scheduler.npz) against the reference's heuristic schedule on a
@@ -883,6 +1047,8 @@ def main():
                     help="cloth side in vertices; 512 is the headline workload, smaller sides are for profiling")
     ap.add_argument("--batched-frames", type=int, default=30)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-scheduler leg")
+    ap.add_argument("--no-precision", action="store_true", help="skip the stacked-layer precision leg")
+    ap.add_argument("--precision-frames", type=int, default=50)
     ap.add_argument("--learned-frames", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 3:

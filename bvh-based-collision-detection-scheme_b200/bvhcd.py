@@ -48,7 +48,8 @@ MLP_PARAMS = 5443
 SHAPE_STAGES = ["keep", "prune_int", "prune_ext", "balance", "sprout", "narrow"]
 
 STAGES = ["bvh_build", "bvh_refit", "bvh_restructure", "front_generate", "front_update",
-          "front_keep", "front_balance", "front_reorder", "narrow", "quality", "pure_bvh_cd"]
+          "front_keep", "front_balance", "front_reorder", "narrow", "quality", "pure_bvh_cd",
+          "front_restructure"]
 
 
 class BvhcdError(RuntimeError):

@@ -70,6 +70,11 @@ struct FArgs {
     const float *iexp_in, *xexp_in;
     float *iexp_out, *xexp_out;
     const unsigned *ksel;
+    // an inter front's restructure (k_restr_scan): the traversed BVH's last
+    // restructure -- per internal node a non-zero mark inside a restructured
+    // subtree, per leaf slot its subtree root (0 outside), per root the old
+    // end of its left spine
+    const int *rs_mark, *rs_root, *rs_last;
 };
 
 // A node's box and escape link: from the FP32 record ({lo.xyz, rangex |
@@ -220,14 +225,12 @@ __device__ __forceinline__ int left_child_tagged(const FArgs &a, int d, const fl
 // half of maintainIntLooseIntraFrontsWithLog,
 // BvttFrontPruneSproutKernels.cu:34-56, keepIntLooseIntraFronts,
 // BvttFrontKeepKernels.cu:26-42, and pureBvhSelfCD, BvhCDKernels.cu:30-47):
-// the reference walks the left spine of an internal node by DFS id while the
-// box overlaps, up to the parent of its leftmost leaf; a node that stops
-// overlapping is a front node and is left through its escape link.  Here
-// every step reads one 32-byte record, a leaf's or a node's, and moves to
-// the escape link (a leaf, or a node that does not overlap) or to the left
-// child (an overlapping node): the same visits in the same order, with one
-// loop body for all lanes of a warp and no leaf record read ahead at each
-// spine.
+// walk the left spine of an internal node by DFS id while the box overlaps,
+// up to the parent of its leftmost leaf; a node that stops overlapping is a
+// front node and is left through its escape link.  (A loop body of one
+// record per step for both kinds of node was measured slower: 0.88 against
+// 0.64 ms per generation on the 562,742-triangle scene -- the spine loop
+// keeps consecutive records in a tight dependent chain.)
 template <bool kFront>
 __device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const float4 &plo,
                                          const float4 &phi, const int4 &pf, int st, int stop) {
@@ -239,21 +242,34 @@ __device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const
             atomicOr(a.ctr + C_OVERFLOW, 16u);
             return;
         }
-        const int id = st >> 1;
-        float4 lo, hi;
-        if (st & 1) ldg8(a.lrec + 2 * id, lo, hi);
-        else node_rec(a, id, lo, hi);
-        const bool ov = overlap(lo, hi, plo, phi);
+        int leaf;
+        float4 llo, lhi;
         if (st & 1) {
-            if (ov) emit_pair(a, em, prim, pf, id);
-            if (kFront) emit_ext(a, em, prim, id);
-            st = __float_as_int(hi.w);
-        } else if (!ov) {
-            if (kFront) emit_int(a, em, prim, id);
-            st = __float_as_int(hi.w);
+            leaf = st >> 1;
+            ldg8(a.lrec + 2 * leaf, llo, lhi);
         } else {
-            st = left_child_tagged(a, id, lo);
+            int n = st >> 1;
+            float4 nlo, nhi;
+            node_rec(a, n, nlo, nhi);
+            leaf = node_rangex(a, n, nlo);
+            ldg8(a.lrec + 2 * leaf, llo, lhi);
+            const int last = __float_as_int(llo.w);  // parent of the leftmost leaf
+            bool stopped = false;
+            while (true) {
+                if (!overlap(nlo, nhi, plo, phi)) { stopped = true; break; }
+                if (n >= last) break;
+                ++n;
+                node_rec(a, n, nlo, nhi);
+            }
+            if (stopped) {
+                if (kFront) emit_int(a, em, prim, n);
+                st = __float_as_int(nhi.w);
+                continue;
+            }
         }
+        if (overlap(llo, lhi, plo, phi)) emit_pair(a, em, prim, pf, leaf);
+        if (kFront) emit_ext(a, em, prim, leaf);
+        st = __float_as_int(lhi.w);
     }
 }
 
@@ -376,9 +392,13 @@ __global__ void __launch_bounds__(kB) k_sprout(FArgs a) {
         if (e.x < 0) continue;  // hole
         float4 plo, phi;
         ldg8(a.prec + 2 * e.x, plo, phi);
+        const int node = e.y < 0 ? ~e.y : e.y;
         float4 nlo, nhi;
-        node_rec(a, e.y, nlo, nhi);
-        traverse<kFront>(a, em, e.x, plo, phi, prim_face(a, e.x), left_child_tagged(a, e.y, nlo), __float_as_int(nhi.w));
+        node_rec(a, node, nlo, nhi);
+        // e.y = ~R: the whole restructured subtree R, R itself first (an inter
+        // front's restructure); else below the overlapping node e.y
+        traverse<kFront>(a, em, e.x, plo, phi, prim_face(a, e.x),
+                         e.y < 0 ? (node << 1) : left_child_tagged(a, node, nlo), __float_as_int(nhi.w));
     }
     em_close(a, em);
 }
@@ -441,6 +461,57 @@ __global__ void __launch_bounds__(kB) k_maintain_ext(FArgs a) {
             if (l & 1) continue;  // right child: the parent's left chain handles it
             const int m = prune_up(a, gfa - 1, l >> 1, b.plo[k], b.phi[k]);
             if (m >= 0) emit_int(a, em, prim, m);
+        }
+    }
+    em_close(a, em);
+}
+
+// An inter front after its traversed BVH restructured subtrees
+// (BvttFrontLooseInter::restructure, BvttFrontLooseInter.cu:252-318, with
+// separateInt/ExtLooseInterFrontWithLog, BvttFrontReorderKernels.cu:171-198,
+// filterInt/ExtFrontCnts, FlOrderLog.cu:36-73, and
+// restructureInt/ExtLooseInterFrontWithLog, BvttFrontRestructureKernels.cu:
+// 99-157), in one pass over both fronts.  An entry outside every
+// restructured subtree is valid: an internal one that overlaps goes to the
+// sprout work list, the others are kept as they are (no prune here: a prune
+// could drop an entry whose left sibling's entries are being replaced); an
+// external one is kept and gives its pair.  The entries of a primitive inside
+// a restructured subtree R were a complete cut of R's old subtree, which
+// holds exactly one node of R's old left spine (DFS ids R .. old end) or R's
+// leftmost leaf: that entry becomes the work item (primitive, ~R), which
+// k_sprout<true> traverses from R itself; the others are dropped.
+template <int kU, int kB>
+__global__ void __launch_bounds__(kB) k_restr_scan(FArgs a) {
+    Em em;
+    const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
+    const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
+    const Spread sp = spread<kScanMinPer>(ni + ne);
+    Batch<kU> b, nb;
+    load_ents(a, sp.start, sp.stride, ni, ni + ne, b);
+    for (unsigned q0 = sp.start; q0 < ni + ne; q0 += kU * sp.stride, take_ents(b, nb)) {
+        load_ents(a, q0 + kU * sp.stride, sp.stride, ni, ni + ne, nb);
+        load_recs(a, b);
+#pragma unroll
+        for (int k = 0; k < kU; k++) {
+            if (!b.v[k]) continue;
+            const int prim = b.e[k].x, node = b.e[k].y;
+            if (b.in_int[k]) {
+                if (__ldg(&a.rs_mark[node]) > 0) {
+                    const int R = __ldg(&a.rs_root[node_rangex(a, node, b.nlo[k])]);
+                    if (node <= __ldg(&a.rs_last[R])) emit_work(a, em, make_int2(prim, ~R));
+                    continue;
+                }
+                if (overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k])) emit_work(a, em, b.e[k]);
+                else emit_int(a, em, prim, node);
+                continue;
+            }
+            const int R = __ldg(&a.rs_root[node]);
+            if (R > 0) {
+                if (node == __ldg(&a.nrange[R]).x) emit_work(a, em, make_int2(prim, ~R));
+                continue;
+            }
+            emit_ext(a, em, prim, node);
+            if (overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k])) emit_pair(a, em, prim, prim_face(a, prim), node);
         }
     }
     em_close(a, em);
@@ -1168,6 +1239,7 @@ static FArgs make_args(const LBvh *bvh, const LBvh *trav, unsigned *ctr, const F
     a.iexp_in = a.xexp_in = nullptr;
     a.iexp_out = a.xexp_out = nullptr;
     a.ksel = nullptr;
+    a.rs_mark = a.rs_root = a.rs_last = nullptr;
     return a;
 }
 
@@ -1302,6 +1374,45 @@ bvhcd_status Front::update_kernels(cudaStream_t s) {
     return cuda_status(cudaGetLastError());
 }
 
+// BvttFrontLooseInter::restructure (BvttFrontLooseInter.cu:252-318): the
+// traversed BVH restructured subtrees since this inter front was last made or
+// restructured; valid entries are kept (or sprouted), the entries inside each
+// restructured subtree are replaced by one traversal of the new subtree per
+// primitive (k_restr_scan), then the usual ordering.  The reference also
+// prunes right after; here the next UPDATE does.
+bvhcd_status Front::restructure_inter(cudaStream_t s) {
+    const int T = bvh_->T();
+    unsigned *ctr = counters();
+    FrontLog l = log();
+    FR_TRY(log_clear(l, T, s));
+    FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
+    const int nx = 1 - cur_;
+    a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
+    a.in_int_slot = 2 * cur_; a.in_ext_slot = 2 * cur_ + 1;
+    a.out_int = front_[nx][0].as<int2>(); a.out_ext = front_[nx][1].as<int2>();
+    a.out_int_slot = 2 * nx; a.out_ext_slot = 2 * nx + 1;
+    a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
+    a.pairs = pairs_.as<int2>();
+    a.cap_pairs = (unsigned)pcap_;
+    a.rs_mark = bvh_->rs_intmark();
+    a.rs_root = bvh_->rs_leafroot();
+    a.rs_last = bvh_->rs_oldlast();
+    FR_TRY(cudaMemsetAsync(ctr + 2 * nx, 0, 2 * sizeof(unsigned), s));
+    FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
+    FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
+    {
+        StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_RESTRUCTURE, s);
+        LAUNCH_SCAN(k_restr_scan, shape_[BVHCD_SHAPE_PRUNE_INT], s, a);
+        LAUNCH_ITEM(k_sprout, true, shape_[BVHCD_SHAPE_SPROUT], s, a);
+    }
+    FR_TRY(cudaGetLastError());
+    bvhcd_status st = reorder(s);
+    if (st != BVHCD_OK) return st;
+    seen_epoch_[0] = bvh_->topo_epoch();
+    seen_epoch_[1] = trav()->topo_epoch();
+    return BVHCD_OK;
+}
+
 bvhcd_status Front::prune_sprout(cudaStream_t s) {
     bvhcd_status st = update_kernels(s);
     if (st != BVHCD_OK) return st;
@@ -1425,6 +1536,7 @@ bvhcd_status Front::run(bvhcd_front_op op, cudaStream_t s) {
     case BVHCD_FRONT_UPDATE: return prune_sprout(s);
     case BVHCD_FRONT_REORDER: return balance(s);
     case BVHCD_FRONT_KEEP: return keep(s);
+    case BVHCD_FRONT_RESTRUCTURE: return restructure_inter(s);
     default: return generate(s, false);
     }
 }
@@ -1566,13 +1678,19 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     // front override after a BVH build or restructure (:75-110): the front
     // is regenerated in both cases
     if (bvh_->restr_enabled() && (bvh_->opt_tag() == 2 || bvh_->opt_tag() == 1)) run_op = BVHCD_FRONT_GENERATE;
-    // an inter front's entries name both trees' leaves: after a build or a
-    // restructure of either (the rigid one included, which the reference does
-    // not check) it is regenerated
-    if (inter() && has_front_ && (seen_epoch_[0] != bvh_->topo_epoch() || seen_epoch_[1] != trav_->topo_epoch()) &&
-        run_op != BVHCD_FRONT_PURE_BVH_CD)
-        run_op = BVHCD_FRONT_GENERATE;
-    if (op == BVHCD_FRONT_RESTRUCTURE) run_op = BVHCD_FRONT_GENERATE;
+    // an inter front's entries name both trees' nodes: after a restructure of
+    // the traversed BVH -- the only change of either tree since the front was
+    // last made -- it is restructured (re-sprouted inside the restructured
+    // subtrees, BvttFrontLooseInter.cu:77-83); after any other change of
+    // either tree (a build; the rigid one too, which the reference does not
+    // check) it is regenerated
+    const bool topo_changed =
+        inter() && has_front_ && (seen_epoch_[0] != bvh_->topo_epoch() || seen_epoch_[1] != trav_->topo_epoch());
+    const bool resprout = topo_changed && seen_epoch_[1] == trav_->topo_epoch() &&
+                          seen_epoch_[0] + 1 == bvh_->topo_epoch() && bvh_->rs_epoch() == bvh_->topo_epoch();
+    if (topo_changed && run_op != BVHCD_FRONT_PURE_BVH_CD)
+        run_op = resprout ? BVHCD_FRONT_RESTRUCTURE : BVHCD_FRONT_GENERATE;
+    if (op == BVHCD_FRONT_RESTRUCTURE && !resprout) run_op = BVHCD_FRONT_GENERATE;
     // a front operation needs a front: the first one is generated
     if (!has_front_ && (run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER || run_op == BVHCD_FRONT_KEEP))
         run_op = BVHCD_FRONT_GENERATE;
@@ -1583,8 +1701,8 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     // front is made again
     if (regen && run_op != BVHCD_FRONT_PURE_BVH_CD) run_op = BVHCD_FRONT_GENERATE;
     unsigned *ctr = counters();
-    const bool from_front =
-        run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER || run_op == BVHCD_FRONT_KEEP;
+    const bool from_front = run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER ||
+                            run_op == BVHCD_FRONT_KEEP || run_op == BVHCD_FRONT_RESTRUCTURE;
     k_ovf_roll<<<1, 32, 0, s>>>(ctr, from_front ? kFrontLossBits : 0u); note_launch();
     if (inter() ? (T < 1 || trav_->T() < 1) : T < 2) {
         FR_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned) * 6, s));
@@ -1610,7 +1728,8 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
         // an UPDATE or a balance overwrote the front, or the front this
         // maintain started from had lost entries: start again from a
         // generated front
-        if (run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER || (ovf & (1u | 2u | 16u | 64u)))
+        if (run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER || run_op == BVHCD_FRONT_RESTRUCTURE ||
+            (ovf & (1u | 2u | 16u | 64u)))
             run_op = BVHCD_FRONT_GENERATE;
     }
     last_op_ = run_op;

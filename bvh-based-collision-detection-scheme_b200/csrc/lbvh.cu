@@ -1034,6 +1034,19 @@ __global__ void k_rs_select(int T, const int *__restrict__ leafroot, const unsig
         }
     }
 }
+// For each restructured subtree R (root DFS id R > 0): the DFS id of the old
+// parent of its leftmost leaf, i.e. the end of R's old left spine R, R + 1,
+// ...  Read before the confined rebuild rewrites the links.  A complete cut
+// of the old subtree holds exactly one node of that spine or the leftmost
+// leaf itself, which is what an inter front's restructure keys on.
+__global__ void k_rs_oldlast(int T, const int *__restrict__ leafroot, const float4 *__restrict__ lrec,
+                             int *oldlast) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < T; s += gridDim.x * blockDim.x) {
+        const int R = leafroot[s];
+        if (R > 0 && (s == 0 || leafroot[s - 1] != R)) oldlast[R] = __float_as_int(lrec[2 * (size_t)s].w);
+    }
+}
+
 // updatePrimMap (:68-77), applying the sort permutation: slot task[k]
 // receives the primitive that sorts k-th inside its subtree.
 __global__ void k_rs_gather(int nr, const int *__restrict__ sorted, const int4 *__restrict__ sface,
@@ -1212,7 +1225,7 @@ LBvh::~LBvh() {
                     &code_, &refit_flag_, &keys_, &vals_, &keys2_, &vals2_, &k64_, &k64b_, &metric_,
                     &ulc_, &urc_, &upar_, &urx_, &ury_, &umark_, &ubox_, &uflag_, &posb_, &clen_,
                     &coff_, &dfs_, &ulpar_, &scene_, &partial_, &scratch_, &task_, &tmpface_,
-                    &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &flagbuf_,
+                    &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &rs_oldlast_, &flagbuf_,
                     &ctr_, &scene_of_, &leafscene_, &sbox_, &tiles_, &nrec16_, &split_, &cross_, &topk_,
                     &plan_, &top_, &gbox_, &height_, &llist_, &lhdr_, &tlist_,
                     &thdr_, &llink_, &tlink_, &lexp_, &nexp_, &lexport_, &gext_, &uheight_};
@@ -1331,6 +1344,7 @@ bvhcd_status LBvh::ensure_capacity(int T, int V) {
     BV_TRY(extrange_.reserve(sizeof(int) * (n + 1)));
     BV_TRY(extmark_.reserve(sizeof(int) * (n + 1)));
     BV_TRY(leafroot_.reserve(sizeof(int) * (n + 1)));
+    BV_TRY(rs_oldlast_.reserve(sizeof(int) * (n + 1)));
     BV_TRY(flagbuf_.reserve(sizeof(unsigned) * (n + 1)));
     capT_ = T;
     return BVHCD_OK;
@@ -1690,6 +1704,8 @@ bvhcd_status LBvh::restructure(cudaStream_t s) {
     }
     // 5 per-leaf subtree root
     BV_TRY(scan_i32(extrange_.as<int>(), leafroot_.as<int>(), T + 1, true, nullptr, scratch_.p, s));
+    k_rs_oldlast<<<grid_for(T), kThreads, 0, s>>>(T, leafroot_.as<int>(), lrec_.as<float4>(), rs_oldlast_.as<int>());
+    note_launch();
     // 6-7 keys of the restructured primitives
     bvhcd_status st = scene_box(s);
     if (st != BVHCD_OK) return st;
@@ -1733,6 +1749,7 @@ bvhcd_status LBvh::restructure(cudaStream_t s) {
     BV_TRY(cudaGetLastError());
     opt_tag_ = 1;
     topo_epoch_++;
+    rs_epoch_ = topo_epoch_;  // leafroot_, intmark_ and rs_oldlast_ describe this change
     // a new topology (the refit above saw leaves change slots): the
     // accumulated box motion starts again
     BV_TRY(cudaMemsetAsync(ctr_.as<unsigned>() + C_DELTA, 0, 2 * sizeof(unsigned), s));

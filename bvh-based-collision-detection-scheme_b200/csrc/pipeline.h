@@ -136,6 +136,14 @@ class LBvh {
     // advances whenever the topology (and so the leaf order) changes: build,
     // restructure, state copy
     int topo_epoch() const { return topo_epoch_; }
+    // The last restructure: the topology epoch it produced, and per internal
+    // node a non-zero mark inside a restructured subtree, per leaf slot the
+    // subtree's root (0 outside), per root the old end of its left spine.
+    // Valid while rs_epoch() == topo_epoch().
+    int rs_epoch() const { return rs_epoch_; }
+    const int *rs_intmark() const { return intmark_.as<int>(); }
+    const int *rs_leafroot() const { return leafroot_.as<int>(); }
+    const int *rs_oldlast() const { return rs_oldlast_.as<int>(); }
     // advances whenever the faces (vertex ids) may have changed
     int faces_epoch() const { return faces_epoch_; }
     const float *verts() const { return vptr_; }
@@ -197,6 +205,10 @@ class LBvh {
         ubox_, uflag_, posb_, clen_, coff_, dfs_, ulpar_, scene_, partial_, scratch_, task_, tmpface_;
     // restructure log
     DBuf intrange_, rtroot_, intmark_, extrange_, extmark_, leafroot_, flagbuf_;
+    // old end of each restructured subtree's left spine (see k_rs_oldlast), and
+    // the topology epoch the restructure arrays describe (-1: none)
+    DBuf rs_oldlast_;
+    int rs_epoch_ = -1;
     // batched scenes: S_ scenes, triangle offsets, per-triangle scene id,
     // per-slot scene id, per-scene boxes, box-reduction tiles
     int S_ = 1, ntiles_ = 0, epoch_ = 0, topo_epoch_ = 0, faces_epoch_ = 0;
@@ -276,6 +288,7 @@ class Front {
     bvhcd_status run(bvhcd_front_op op, cudaStream_t s);
     bvhcd_status generate(cudaStream_t s, bool pure);
     bvhcd_status prune_sprout(cudaStream_t s);
+    bvhcd_status restructure_inter(cudaStream_t s);
     bvhcd_status update_kernels(cudaStream_t s);
     bvhcd_status keep(cudaStream_t s);
     bvhcd_status balance(cudaStream_t s);

@@ -285,7 +285,9 @@ typedef enum {
     BVHCD_STAGE_NARROW = 8,
     BVHCD_STAGE_QUALITY = 9,
     BVHCD_STAGE_PURE_BVH_CD = 10,
-    BVHCD_STAGE_COUNT = 11
+    BVHCD_STAGE_FRONT_RESTRUCTURE = 11,  /* an inter front re-sprouting restructured subtrees
+                                            ("broad_phase_restr_front") */
+    BVHCD_STAGE_COUNT = 12
 } bvhcd_stage;
 
 bvhcd_status bvhcd_profile_enable(bvhcd_bvh *bvh, int32_t on);

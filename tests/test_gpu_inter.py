@@ -81,6 +81,8 @@ def test_inter_schedule_matches_brute_force(cuda, lib_built, oracle):
         of, op = _obstacle(8, f)
         rbvh.maintain(bvhcd.BVH_BUILD if f in (0, 9) else bvhcd.BVH_REFIT, op, of, faces_static=f > 0)
         inter.maintain(fr)
+        if f == 4:  # the restructured subtrees are re-sprouted, not the whole front regenerated
+            assert inter.stats()["front_op_run"] == bvhcd.FRONT_RESTRUCTURE
         seen[fr] = seen.get(fr, 0) + 1
         p, h = _check_frame(oracle, inter, cf, cp, of, op, f)
         total += p
@@ -91,6 +93,48 @@ def test_inter_schedule_matches_brute_force(cuda, lib_built, oracle):
     assert total > 0
     for op in (bvhcd.FRONT_GENERATE, bvhcd.FRONT_UPDATE, bvhcd.FRONT_REORDER, bvhcd.FRONT_KEEP):
         assert seen.get(op, 0) > 0, op
+
+
+def test_inter_front_restructure(cuda, lib_built, oracle):
+    """BvttFrontLooseInter::restructure (BvttFrontLooseInter.cu:252-318): the
+    deformable BVH restructures subtrees on several frames while the inter
+    front keeps or updates in between.  The frame after each restructure runs
+    the front restructure (valid entries kept, the restructured subtrees
+    re-sprouted) and every frame equals the brute-force pairs.  Two topology
+    changes between two maintains of the front, or a rebuild, fall back to a
+    regeneration."""
+    bvhcd = lib_built
+    cf, frames = _cloth(56, 16)
+    of, _ = _obstacle(8, 0)
+    dbvh = bvhcd.LBvh(cf.shape[0], frames[0].shape[0], enable_restr=True)
+    rbvh = bvhcd.LBvh(of.shape[0], 2000, enable_restr=False)
+    inter = bvhcd.BvttFront(dbvh, rigid=rbvh, narrow_phase=True, **CAPS)
+    # the intra front over the same BVH consumes the restructure marks each
+    # frame, as in the reference app (keeps only: no quality check adds marks)
+    intra = bvhcd.BvttFront(dbvh, cull_adjacent=True, narrow_phase=False, **CAPS)
+    ops = [bvhcd.FRONT_GENERATE, 4, 4, 4, 4, 2, 4, 4, 2, 4, 4, 4, 4, 3, 4, 4]
+    restr_on = {2, 5, 8, 12}           # frames whose BVH maintain restructures (marks set the frame before)
+    skip_inter = {12}                  # the front is not maintained on frame 12 ...
+    restr_on_13 = True                 # ... and frame 13 restructures again: two changes -> regenerate
+    runs = {}
+    for f, cp in enumerate(frames):
+        dbvh.maintain(bvhcd.BVH_BUILD if f == 0 else bvhcd.BVH_REFIT, cp, cf, faces_static=f > 0)
+        if f in restr_on or (f == 13 and restr_on_13):
+            assert dbvh.opt_tag() == 1, f
+        intra.maintain(bvhcd.FRONT_GENERATE if f == 0 else bvhcd.FRONT_KEEP)
+        of, op = _obstacle(8, f)
+        rbvh.maintain(bvhcd.BVH_BUILD if f == 0 else bvhcd.BVH_REFIT, op, of, faces_static=f > 0)
+        if f not in skip_inter:
+            inter.maintain(ops[f])
+            run = inter.stats()["front_op_run"]
+            runs[f] = run
+            if f in restr_on:
+                assert run == bvhcd.FRONT_RESTRUCTURE, (f, run)
+            _check_frame(oracle, inter, cf, cp, of, op, f)
+        if f + 1 in restr_on or f + 1 == 13:
+            dbvh.request_restructure(pick_roots(dbvh.export(), frac=0.2))
+    assert runs[13] == bvhcd.FRONT_GENERATE, runs
+    assert sum(1 for r in runs.values() if r == bvhcd.FRONT_RESTRUCTURE) == 3, runs
 
 
 def test_inter_every_operation_every_frame(cuda, lib_built, oracle):
