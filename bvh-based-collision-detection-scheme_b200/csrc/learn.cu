@@ -215,61 +215,220 @@ constexpr int oW1 = 0, oB1 = oW1 + kIn * kH, oW2 = oB1 + kH, oB2 = oW2 + kH * kH
               oB3 = oW3 + kH * kOut;
 static_assert(oB3 + kOut == kMlpParams, "parameter layout");
 
-__device__ __forceinline__ float bf(const __nv_bfloat16 *w, int i) { return __bfloat162float(w[i]); }
+// The network runs on the tensor cores: mma.sync m16n8k16 with BF16
+// operands and FP32 accumulation, one warp per tile of 16 rows.  Inputs,
+// activations and back-propagated errors enter each product rounded to BF16
+// (nearest even); accumulation, bias, ReLU, softmax and the loss are FP32.
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// two values as BF16 in one register, the first in the low half
+__device__ __forceinline__ unsigned pack2(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const unsigned *>(&v);
+}
+__device__ __forceinline__ unsigned pack2h(unsigned short lo, unsigned short hi) {
+    return (unsigned)lo | ((unsigned)hi << 16);
+}
 
-// one thread per row: logits and the argmax vote
+// Weights in shared memory as BF16, laid out for the B operands (the two K
+// values a lane reads for one output column are adjacent), rows padded so the
+// lanes of a warp hit distinct banks: w1t[n][k] = W1[k][n], w2t[n][k] =
+// W2[k][n], w3t[c][k] = W3[k][c] (c < 3, zero to 8) for the forward; w2[i][j]
+// = W2[i][j], w3p[j][c] = W3[j][c] (zero past 3) for the back-propagation.
+constexpr int kS16 = 24, kS64 = 72;  // padded row lengths for K = 16 / 64
+struct MlpW {
+    __nv_bfloat16 w1t[kH * kS16];
+    __nv_bfloat16 w2t[kH * kS64];
+    __nv_bfloat16 w2[kH * kS64];
+    __nv_bfloat16 w3t[8 * kS64];
+    __nv_bfloat16 w3p[kH * kS16];
+    float b1[kH], b2[kH], b3[4];
+};
+__device__ void load_mlp_weights(MlpW &w, const __nv_bfloat16 *__restrict__ wq, const float *__restrict__ p) {
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+    for (int i = threadIdx.x; i < kIn * kH; i += blockDim.x) {
+        const int k = i / kH, n = i % kH;
+        w.w1t[n * kS16 + k] = wq[oW1 + i];
+    }
+    for (int i = threadIdx.x; i < kH * kH; i += blockDim.x) {
+        const int k = i / kH, n = i % kH;
+        w.w2t[n * kS64 + k] = wq[oW2 + i];
+        w.w2[k * kS64 + n] = wq[oW2 + i];
+    }
+    for (int i = threadIdx.x; i < 8 * kS64; i += blockDim.x) {
+        const int c = i / kS64, k = i % kS64;
+        w.w3t[i] = (c < kOut && k < kH) ? wq[oW3 + k * kOut + c] : zero;
+    }
+    for (int i = threadIdx.x; i < kH * kS16; i += blockDim.x) {
+        const int j = i / kS16, c = i % kS16;
+        w.w3p[i] = c < kOut ? wq[oW3 + j * kOut + c] : zero;
+    }
+    for (int i = threadIdx.x; i < kH; i += blockDim.x) {
+        w.b1[i] = p[oB1 + i];
+        w.b2[i] = p[oB2 + i];
+    }
+    if (threadIdx.x < 4) w.b3[threadIdx.x] = threadIdx.x < kOut ? p[oB3 + threadIdx.x] : 0.f;
+}
+// B fragment of n-tile nt, k-step kk from a [n][k] array with row length ld
+__device__ __forceinline__ void bfrag(const __nv_bfloat16 *wt, int ld, int nt, int kk, int g, int t, unsigned &b0,
+                                      unsigned &b1) {
+    const __nv_bfloat16 *q = wt + (nt * 8 + g) * ld + kk * 16 + 2 * t;
+    b0 = *reinterpret_cast<const unsigned *>(q);
+    b1 = *reinterpret_cast<const unsigned *>(q + 8);
+}
+
+// Forward of one 16-row tile in a warp: h1, h2 (FP32, after ReLU) and the
+// logits as accumulator fragments (lane g = lane / 4 holds rows g and g + 8,
+// columns 2t, 2t + 1 of each 8-column tile, t = lane % 4).
+struct Fwd {
+    float h1[8][4], h2[8][4], z[4];
+};
+__device__ __forceinline__ void mlp_forward(const MlpW &w, const unsigned (&ax)[4], int g, int t, Fwd &o) {
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        const float b0 = w.b1[nt * 8 + 2 * t], b1 = w.b1[nt * 8 + 2 * t + 1];
+        float c[4] = {b0, b1, b0, b1};
+        unsigned q0, q1;
+        bfrag(w.w1t, kS16, nt, 0, g, t, q0, q1);
+        mma_bf16(c, ax, q0, q1);
+#pragma unroll
+        for (int e = 0; e < 4; e++) o.h1[nt][e] = fmaxf(c[e], 0.f);
+    }
+    unsigned a[4][4];
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {  // accumulator fragments of two column tiles = one A fragment
+        a[kk][0] = pack2(o.h1[2 * kk][0], o.h1[2 * kk][1]);
+        a[kk][1] = pack2(o.h1[2 * kk][2], o.h1[2 * kk][3]);
+        a[kk][2] = pack2(o.h1[2 * kk + 1][0], o.h1[2 * kk + 1][1]);
+        a[kk][3] = pack2(o.h1[2 * kk + 1][2], o.h1[2 * kk + 1][3]);
+    }
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        const float b0 = w.b2[nt * 8 + 2 * t], b1 = w.b2[nt * 8 + 2 * t + 1];
+        float c[4] = {b0, b1, b0, b1};
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+            unsigned q0, q1;
+            bfrag(w.w2t, kS64, nt, kk, g, t, q0, q1);
+            mma_bf16(c, a[kk], q0, q1);
+        }
+#pragma unroll
+        for (int e = 0; e < 4; e++) o.h2[nt][e] = fmaxf(c[e], 0.f);
+    }
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+        a[kk][0] = pack2(o.h2[2 * kk][0], o.h2[2 * kk][1]);
+        a[kk][1] = pack2(o.h2[2 * kk][2], o.h2[2 * kk][3]);
+        a[kk][2] = pack2(o.h2[2 * kk + 1][0], o.h2[2 * kk + 1][1]);
+        a[kk][3] = pack2(o.h2[2 * kk + 1][2], o.h2[2 * kk + 1][3]);
+    }
+    const float c0 = 2 * t < kOut ? w.b3[2 * t] : 0.f, c1 = 2 * t + 1 < kOut ? w.b3[2 * t + 1] : 0.f;
+    o.z[0] = c0; o.z[1] = c1; o.z[2] = c0; o.z[3] = c1;
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+        unsigned q0, q1;
+        bfrag(w.w3t, kS64, 0, kk, g, t, q0, q1);
+        mma_bf16(o.z, a[kk], q0, q1);
+    }
+}
+// A fragment of the inputs of rows r0 + g, r0 + g + 8 (zero past n)
+__device__ __forceinline__ void xfrag(const float *__restrict__ X, int n, int r0, int g, int t, unsigned (&ax)[4]) {
+    float v[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int r = r0 + g + 8 * h;
+        const float *x = X + kIn * (size_t)r;
+        const bool ok = r < n;
+        v[h][0] = ok ? x[2 * t] : 0.f;
+        v[h][1] = ok ? x[2 * t + 1] : 0.f;
+        v[h][2] = ok ? x[2 * t + 8] : 0.f;
+        v[h][3] = ok ? x[2 * t + 9] : 0.f;
+    }
+    ax[0] = pack2(v[0][0], v[0][1]);
+    ax[1] = pack2(v[1][0], v[1][1]);
+    ax[2] = pack2(v[0][2], v[0][3]);
+    ax[3] = pack2(v[1][2], v[1][3]);
+}
+
+// logits and the argmax vote, one warp per 16-row tile
 __global__ void __launch_bounds__(kThreads) k_mlp_infer(int n, const float *__restrict__ X,
                                                         const __nv_bfloat16 *__restrict__ wq,
                                                         const float *__restrict__ p, float *logits, int *vote) {
-    __shared__ float w[kMlpParams];
-    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
-        const bool bias = (i >= oB1 && i < oW2) || (i >= oB2 && i < oW3) || i >= oB3;
-        w[i] = bias ? p[i] : bf(wq, i);
-    }
+    __shared__ __align__(16) MlpW w;
+    load_mlp_weights(w, wq, p);
     __syncthreads();
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        float x[kIn], h1[kH];
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int tile = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tile * 16 < n; tile += warps) {
+        const int r0 = tile * 16;
+        unsigned ax[4];
+        xfrag(X, n, r0, g, t, ax);
+        Fwd o;
+        mlp_forward(w, ax, g, t, o);
+        // column 2 of rows g and g + 8 sits in lane t = 1
+        const float z2a = __shfl_down_sync(0xffffffffu, o.z[0], 1), z2b = __shfl_down_sync(0xffffffffu, o.z[2], 1);
+        if (t == 0) {
 #pragma unroll
-        for (int k = 0; k < kIn; k++) x[k] = X[kIn * (size_t)r + k];
-        for (int j = 0; j < kH; j++) {
-            float a = w[oB1 + j];
+            for (int h = 0; h < 2; h++) {
+                const int r = r0 + g + 8 * h;
+                if (r >= n) continue;
+                const float zz[3] = {o.z[2 * h], o.z[2 * h + 1], h ? z2b : z2a};
+                int best = 0;
 #pragma unroll
-            for (int k = 0; k < kIn; k++) a = fmaf(x[k], w[oW1 + k * kH + j], a);
-            h1[j] = fmaxf(a, 0.f);
+                for (int c = 0; c < kOut; c++) {
+                    if (logits) logits[kOut * (size_t)r + c] = zz[c];
+                    if (zz[c] > zz[best]) best = c;
+                }
+                if (vote) vote[r] = best;
+            }
         }
-        float o[kOut] = {w[oB3], w[oB3 + 1], w[oB3 + 2]};
-        for (int j = 0; j < kH; j++) {
-            float a = w[oB2 + j];
-            for (int k = 0; k < kH; k++) a = fmaf(h1[k], w[oW2 + k * kH + j], a);
-            a = fmaxf(a, 0.f);
-#pragma unroll
-            for (int c = 0; c < kOut; c++) o[c] = fmaf(a, w[oW3 + j * kOut + c], o[c]);
-        }
-        int best = 0;
-#pragma unroll
-        for (int c = 0; c < kOut; c++) {
-            if (logits) logits[kOut * (size_t)r + c] = o[c];
-            if (o[c] > o[best]) best = c;
-        }
-        if (vote) vote[r] = best;
     }
 }
 
 // Minibatch gradient of the class-weighted cross-entropy
 // L = (1/N) sum_r cw[y_r] CE(softmax(logits_r), y_r), accumulated into grad
-// (FP32) and loss.  128 rows per block: thread r (of 128) runs its row's
-// forward and backward into shared memory, then all 256 threads sum the
-// outer products over the block's rows and add them to the global gradient.
+// (FP32) and loss.  128 rows per block, 16 per warp.  Each warp runs the
+// forward and the back-propagation of its rows on the tensor cores (the
+// output error through W3 and W2, masked by the ReLUs), and leaves the BF16
+// inputs, activations and errors of its rows in shared memory; then the
+// block's weight gradients are products over its 128 rows, Actᵀ · Err, again
+// on the tensor cores (44 output tiles of 16 x 8 shared by the 8 warps), and
+// the bias gradients column sums of the errors.
 constexpr int kRows = 128;
-struct GradSmem {  // rows padded by one word: row-per-thread access is conflict-free
-    float w[kMlpParams];
-    float x[kRows][kIn + 1];
-    float h1[kRows][kH + 1];
-    float h2[kRows][kH + 1];
-    float d1[kRows][kH + 1];
-    float d2[kRows][kH + 1];
-    float dl[kRows][kOut];
+struct GradSmem {
+    MlpW w;
+    __nv_bfloat16 x[kRows * kS16];    // inputs, columns 0..15
+    __nv_bfloat16 h1[kRows * kS64];
+    __nv_bfloat16 h2[kRows * kS64];
+    __nv_bfloat16 d1[kRows * kS64];   // errors at the first hidden layer's pre-activations
+    __nv_bfloat16 d2[kRows * kS64];
+    __nv_bfloat16 dl[kRows * kS16];   // errors at the logits, columns 0..2 (zero to 16)
 };
+// one 16 x 8 tile of Actᵀ · Err over the block's rows: rows m0..m0+15 of
+// Actᵀ (feature columns of act), columns n0..n0+7 of err
+__device__ __forceinline__ void wgrad_tile(const __nv_bfloat16 *act, int lda, const __nv_bfloat16 *err, int lde,
+                                           int m0, int n0, int g, int t, float (&c)[4]) {
+    const unsigned short *A = reinterpret_cast<const unsigned short *>(act);
+    const unsigned short *E = reinterpret_cast<const unsigned short *>(err);
+    c[0] = c[1] = c[2] = c[3] = 0.f;
+#pragma unroll 2
+    for (int k0 = 0; k0 < kRows; k0 += 16) {
+        const int ra = k0 + 2 * t;
+        unsigned a[4];
+        a[0] = pack2h(A[ra * lda + m0 + g], A[(ra + 1) * lda + m0 + g]);
+        a[1] = pack2h(A[ra * lda + m0 + g + 8], A[(ra + 1) * lda + m0 + g + 8]);
+        a[2] = pack2h(A[(ra + 8) * lda + m0 + g], A[(ra + 9) * lda + m0 + g]);
+        a[3] = pack2h(A[(ra + 8) * lda + m0 + g + 8], A[(ra + 9) * lda + m0 + g + 8]);
+        const unsigned b0 = pack2h(E[ra * lde + n0 + g], E[(ra + 1) * lde + n0 + g]);
+        const unsigned b1 = pack2h(E[(ra + 8) * lde + n0 + g], E[(ra + 9) * lde + n0 + g]);
+        mma_bf16(c, a, b0, b1);
+    }
+}
 
 __global__ void __launch_bounds__(kThreads) k_mlp_grad(int n, const float *__restrict__ X, const int *__restrict__ y,
                                                        const float *__restrict__ cw, float inv_n,
@@ -277,86 +436,156 @@ __global__ void __launch_bounds__(kThreads) k_mlp_grad(int n, const float *__res
                                                        const float *__restrict__ p, float *grad, float *loss) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GradSmem &sm = *reinterpret_cast<GradSmem *>(smem_raw);
-    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
-        const bool bias = (i >= oB1 && i < oW2) || (i >= oB2 && i < oW3) || i >= oB3;
-        sm.w[i] = bias ? p[i] : bf(wq, i);
-    }
-    const int r0 = blockIdx.x * kRows;
-    const int rows = min(kRows, n - r0);
-    for (int i = threadIdx.x; i < kRows * kIn; i += blockDim.x) {
-        const int r = i / kIn, k = i % kIn;
-        sm.x[r][k] = r < rows ? X[kIn * (size_t)(r0 + r) + k] : 0.f;
-    }
+    load_mlp_weights(sm.w, wq, p);
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+    for (int i = threadIdx.x; i < kRows * kS16; i += blockDim.x) sm.dl[i] = zero;
     __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const int rb = blockIdx.x * kRows;         // the block's first row
+    const int r0 = rb + warp * 16, l0 = warp * 16;  // the warp's first row, globally and in the block
+    unsigned ax[4];
+    xfrag(X, n, r0, g, t, ax);
+    Fwd o;
+    mlp_forward(sm.w, ax, g, t, o);
+    // inputs and activations of the warp's rows, BF16 (what the products read)
+    {
+        unsigned *xs = reinterpret_cast<unsigned *>(sm.x);
+        xs[((l0 + g) * kS16 + 2 * t) >> 1] = ax[0];
+        xs[((l0 + g + 8) * kS16 + 2 * t) >> 1] = ax[1];
+        xs[((l0 + g) * kS16 + 2 * t + 8) >> 1] = ax[2];
+        xs[((l0 + g + 8) * kS16 + 2 * t + 8) >> 1] = ax[3];
+        unsigned *h1s = reinterpret_cast<unsigned *>(sm.h1), *h2s = reinterpret_cast<unsigned *>(sm.h2);
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            h1s[((l0 + g) * kS64 + nt * 8 + 2 * t) >> 1] = pack2(o.h1[nt][0], o.h1[nt][1]);
+            h1s[((l0 + g + 8) * kS64 + nt * 8 + 2 * t) >> 1] = pack2(o.h1[nt][2], o.h1[nt][3]);
+            h2s[((l0 + g) * kS64 + nt * 8 + 2 * t) >> 1] = pack2(o.h2[nt][0], o.h2[nt][1]);
+            h2s[((l0 + g + 8) * kS64 + nt * 8 + 2 * t) >> 1] = pack2(o.h2[nt][2], o.h2[nt][3]);
+        }
+    }
+    // softmax cross-entropy of rows g and g + 8 in lane t = 0; their errors
+    // at the logits (zero for rows past n), BF16 into shared memory
+    const float z2a = __shfl_down_sync(0xffffffffu, o.z[0], 1), z2b = __shfl_down_sync(0xffffffffu, o.z[2], 1);
     float my_loss = 0.f;
-    if (threadIdx.x < kRows) {
-        const int r = threadIdx.x;
-        if (r < rows) {
-            for (int j = 0; j < kH; j++) {
-                float a = sm.w[oB1 + j];
-                for (int k = 0; k < kIn; k++) a = fmaf(sm.x[r][k], sm.w[oW1 + k * kH + j], a);
-                sm.h1[r][j] = fmaxf(a, 0.f);
+    if (t == 0) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int r = r0 + g + 8 * h;
+            const float zz[3] = {o.z[2 * h], o.z[2 * h + 1], h ? z2b : z2a};
+            float d[3] = {0.f, 0.f, 0.f};
+            if (r < n) {
+                const float m = fmaxf(zz[0], fmaxf(zz[1], zz[2]));
+                float e[kOut], s = 0.f;
+#pragma unroll
+                for (int c = 0; c < kOut; c++) {
+                    e[c] = expf(zz[c] - m);
+                    s += e[c];
+                }
+                const int lab = y[r];
+                const float wt = cw[lab] * inv_n;
+                my_loss += wt * (logf(s) + m - zz[lab]);
+#pragma unroll
+                for (int c = 0; c < kOut; c++) d[c] = wt * (e[c] / s - (c == lab ? 1.f : 0.f));
             }
-            float o[kOut] = {sm.w[oB3], sm.w[oB3 + 1], sm.w[oB3 + 2]};
-            for (int j = 0; j < kH; j++) {
-                float a = sm.w[oB2 + j];
-                for (int k = 0; k < kH; k++) a = fmaf(sm.h1[r][k], sm.w[oW2 + k * kH + j], a);
-                a = fmaxf(a, 0.f);
-                sm.h2[r][j] = a;
-                for (int c = 0; c < kOut; c++) o[c] = fmaf(a, sm.w[oW3 + j * kOut + c], o[c]);
+#pragma unroll
+            for (int c = 0; c < kOut; c++) sm.dl[(l0 + g + 8 * h) * kS16 + c] = __float2bfloat16_rn(d[c]);
+        }
+    }
+    __syncwarp();
+    // errors at the second hidden layer: (dl · W3ᵀ) masked by h2 > 0
+    unsigned adl[4];
+    {
+        const unsigned *dls = reinterpret_cast<const unsigned *>(sm.dl);
+        adl[0] = dls[((l0 + g) * kS16 + 2 * t) >> 1];
+        adl[1] = dls[((l0 + g + 8) * kS16 + 2 * t) >> 1];
+        adl[2] = dls[((l0 + g) * kS16 + 2 * t + 8) >> 1];
+        adl[3] = dls[((l0 + g + 8) * kS16 + 2 * t + 8) >> 1];
+    }
+    float d2[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        unsigned q0, q1;
+        bfrag(sm.w.w3p, kS16, nt, 0, g, t, q0, q1);
+        mma_bf16(c, adl, q0, q1);
+#pragma unroll
+        for (int e = 0; e < 4; e++) d2[nt][e] = o.h2[nt][e] > 0.f ? c[e] : 0.f;
+    }
+    unsigned a[4][4];
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+        a[kk][0] = pack2(d2[2 * kk][0], d2[2 * kk][1]);
+        a[kk][1] = pack2(d2[2 * kk][2], d2[2 * kk][3]);
+        a[kk][2] = pack2(d2[2 * kk + 1][0], d2[2 * kk + 1][1]);
+        a[kk][3] = pack2(d2[2 * kk + 1][2], d2[2 * kk + 1][3]);
+    }
+    {
+        unsigned *d2s = reinterpret_cast<unsigned *>(sm.d2);
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+            d2s[((l0 + g) * kS64 + 16 * kk + 2 * t) >> 1] = a[kk][0];
+            d2s[((l0 + g + 8) * kS64 + 16 * kk + 2 * t) >> 1] = a[kk][1];
+            d2s[((l0 + g) * kS64 + 16 * kk + 8 + 2 * t) >> 1] = a[kk][2];
+            d2s[((l0 + g + 8) * kS64 + 16 * kk + 8 + 2 * t) >> 1] = a[kk][3];
+        }
+    }
+    // errors at the first hidden layer: (d2 · W2ᵀ) masked by h1 > 0
+    {
+        unsigned *d1s = reinterpret_cast<unsigned *>(sm.d1);
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+                unsigned q0, q1;
+                bfrag(sm.w.w2, kS64, nt, kk, g, t, q0, q1);
+                mma_bf16(c, a[kk], q0, q1);
             }
-            const float m = fmaxf(o[0], fmaxf(o[1], o[2]));
-            float e[kOut], z = 0.f;
-            for (int c = 0; c < kOut; c++) {
-                e[c] = expf(o[c] - m);
-                z += e[c];
-            }
-            const int lab = y[r0 + r];
-            const float wt = cw[lab] * inv_n;
-            my_loss = wt * (logf(z) + m - o[lab]);
-            for (int c = 0; c < kOut; c++) sm.dl[r][c] = wt * (e[c] / z - (c == lab ? 1.f : 0.f));
-            for (int j = 0; j < kH; j++) {
-                float g = 0.f;
-                for (int c = 0; c < kOut; c++) g = fmaf(sm.dl[r][c], sm.w[oW3 + j * kOut + c], g);
-                sm.d2[r][j] = sm.h2[r][j] > 0.f ? g : 0.f;
-            }
-            for (int k = 0; k < kH; k++) {
-                float g = 0.f;
-                for (int j = 0; j < kH; j++) g = fmaf(sm.d2[r][j], sm.w[oW2 + k * kH + j], g);
-                sm.d1[r][k] = sm.h1[r][k] > 0.f ? g : 0.f;
-            }
-        } else {
-            for (int j = 0; j < kH; j++) sm.h1[r][j] = sm.h2[r][j] = sm.d1[r][j] = sm.d2[r][j] = 0.f;
-            for (int c = 0; c < kOut; c++) sm.dl[r][c] = 0.f;
+#pragma unroll
+            for (int e = 0; e < 4; e++) c[e] = o.h1[nt][e] > 0.f ? c[e] : 0.f;
+            d1s[((l0 + g) * kS64 + nt * 8 + 2 * t) >> 1] = pack2(c[0], c[1]);
+            d1s[((l0 + g + 8) * kS64 + nt * 8 + 2 * t) >> 1] = pack2(c[2], c[3]);
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
-        float g = 0.f;
-        if (i < oB1) {
-            const int k = i / kH, j = i % kH;
-            for (int r = 0; r < kRows; r++) g = fmaf(sm.x[r][k], sm.d1[r][j], g);
-        } else if (i < oW2) {
-            const int j = i - oB1;
-            for (int r = 0; r < kRows; r++) g += sm.d1[r][j];
-        } else if (i < oB2) {
-            const int k = (i - oW2) / kH, j = (i - oW2) % kH;
-            for (int r = 0; r < kRows; r++) g = fmaf(sm.h1[r][k], sm.d2[r][j], g);
-        } else if (i < oW3) {
-            const int j = i - oB2;
-            for (int r = 0; r < kRows; r++) g += sm.d2[r][j];
-        } else if (i < oB3) {
-            const int j = (i - oW3) / kOut, c = (i - oW3) % kOut;
-            for (int r = 0; r < kRows; r++) g = fmaf(sm.h2[r][j], sm.dl[r][c], g);
+    // weight gradients: tiles 0..7 of dW1 (16 x 64), 8..39 of dW2 (64 x 64),
+    // 40..43 of dW3 (64 x 3, padded to 8 columns)
+    for (int tile = warp; tile < 44; tile += kThreads / 32) {
+        float c[4];
+        int base, ld, m0, n0, ncol;
+        if (tile < 8) {
+            m0 = 0; n0 = tile * 8;
+            wgrad_tile(sm.x, kS16, sm.d1, kS64, m0, n0, g, t, c);
+            base = oW1; ld = kH; ncol = kH;
+        } else if (tile < 40) {
+            m0 = ((tile - 8) >> 3) * 16; n0 = ((tile - 8) & 7) * 8;
+            wgrad_tile(sm.h1, kS64, sm.d2, kS64, m0, n0, g, t, c);
+            base = oW2; ld = kH; ncol = kH;
         } else {
-            const int c = i - oB3;
-            for (int r = 0; r < kRows; r++) g += sm.dl[r][c];
+            m0 = (tile - 40) * 16; n0 = 0;
+            wgrad_tile(sm.h2, kS64, sm.dl, kS16, m0, n0, g, t, c);
+            base = oW3; ld = kOut; ncol = kOut;
         }
-        atomicAdd(grad + i, g);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int row = m0 + g + ((e >> 1) << 3), col = n0 + 2 * t + (e & 1);
+            if (col < ncol) atomicAdd(grad + base + row * ld + col, c[e]);
+        }
+    }
+    // bias gradients: column sums of the BF16 errors
+    for (int i = threadIdx.x; i < kH + kH + kOut; i += blockDim.x) {
+        const __nv_bfloat16 *src;
+        int ld, col, dst;
+        if (i < kH) { src = sm.d1; ld = kS64; col = i; dst = oB1 + i; }
+        else if (i < 2 * kH) { src = sm.d2; ld = kS64; col = i - kH; dst = oB2 + col; }
+        else { src = sm.dl; ld = kS16; col = i - 2 * kH; dst = oB3 + col; }
+        float gsum = 0.f;
+        for (int r = 0; r < kRows; r++) gsum += __bfloat162float(src[r * ld + col]);
+        atomicAdd(grad + dst, gsum);
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) my_loss += __shfl_xor_sync(0xffffffffu, my_loss, o);
-    if ((threadIdx.x & 31) == 0 && my_loss != 0.f) atomicAdd(loss, my_loss);
+    for (int o2 = 16; o2 > 0; o2 >>= 1) my_loss += __shfl_xor_sync(0xffffffffu, my_loss, o2);
+    if (lane == 0 && my_loss != 0.f) atomicAdd(loss, my_loss);
 }
 
 // Adam on the FP32 master weights (Kingma & Ba), then the BF16 copy.
