@@ -40,7 +40,8 @@ EXPORTED = [
     "bvhcd_learner_create", "bvhcd_learner_destroy", "bvhcd_learner_set_params", "bvhcd_learner_get_params",
     "bvhcd_learner_frame", "bvhcd_learner_observe", "bvhcd_learner_cut", "bvhcd_learner_features",
     "bvhcd_learner_work", "bvhcd_mlp_gradient", "bvhcd_mlp_train", "bvhcd_mlp_predict",
-    "bvhcd_learner_set_decide_every", "bvhcd_front_contacts", "bvhcd_debug_fail_alloc",
+    "bvhcd_learner_set_decide_every", "bvhcd_front_contacts", "bvhcd_debug_fail_alloc", "bvhcd_front_contacts64",
+    "bvhcd_learner_set_front_cycle",
 ]
 
 MLP_PARAMS = 5443
@@ -170,6 +171,7 @@ def lib():
             "bvhcd_front_copy_state": (ctypes.c_int, [vp, vp, vp]),
             "bvhcd_front_contacts": (ctypes.c_int, [vp, i32, vp, i64, ctypes.POINTER(i64), ctypes.POINTER(i64),
                                                     i32, vp]),
+            "bvhcd_front_contacts64": (ctypes.c_int, [vp, i32, vp, i64, ctypes.POINTER(i64), i32, vp]),
             "bvhcd_learner_create": (ctypes.c_int, [vp, vp, i32, ctypes.POINTER(vp)]),
             "bvhcd_learner_destroy": (ctypes.c_int, [vp]),
             "bvhcd_learner_set_params": (ctypes.c_int, [vp, vp]),
@@ -178,6 +180,7 @@ def lib():
                                                    ctypes.POINTER(i32), vp]),
             "bvhcd_learner_observe": (ctypes.c_int, [vp, i32, i32, vp]),
             "bvhcd_learner_set_decide_every": (ctypes.c_int, [vp, i32]),
+            "bvhcd_learner_set_front_cycle": (ctypes.c_int, [vp, i32]),
             "bvhcd_learner_cut": (ctypes.c_int, [vp, vp, i32, ctypes.POINTER(i32), vp]),
             "bvhcd_learner_features": (ctypes.c_int, [vp, vp, i32, ctypes.POINTER(i32), vp]),
             "bvhcd_learner_work": (ctypes.c_int, [vp, vp, vp, i32, vp]),
@@ -517,6 +520,17 @@ class BvttFront:
                                           ctypes.byref(fl), 0, _stream_ptr(stream)), "contacts")
         return out[:n.value], int(fl.value)
 
+    def contacts64(self, which: int = 0, stream=None) -> np.ndarray:
+        """contacts() computed and returned in FP64: (n, 4) float64."""
+        n = ctypes.c_int64()
+        st = lib().bvhcd_front_contacts64(self._h, int(which), None, 0, ctypes.byref(n), 0, _stream_ptr(stream))
+        if st not in (0, 3):
+            _check(st, "contacts64")
+        out = np.zeros((max(n.value, 1), 4), np.float64)
+        _check(lib().bvhcd_front_contacts64(self._h, int(which), out.ctypes.data, n.value, ctypes.byref(n), 0,
+                                            _stream_ptr(stream)), "contacts64")
+        return out[:n.value]
+
     def shapes(self) -> dict:
         """Launch shape per front stage: {stage: (entries per thread step, threads per block)}."""
         sh = LaunchShapes()
@@ -670,6 +684,10 @@ class Learner:
 
     def set_decide_every(self, frames: int):
         _check(lib().bvhcd_learner_set_decide_every(self._h, int(frames)), "decide every")
+
+    def set_front_cycle(self, frames: int):
+        """0: keep the front between decisions; c: the reference's front cycle of c frames."""
+        _check(lib().bvhcd_learner_set_front_cycle(self._h, int(frames)), "front cycle")
 
     def set_params(self, params):
         p = np.ascontiguousarray(params, dtype=np.float32)

@@ -262,7 +262,13 @@ bvhcd_status bvhcd_frame(bvhcd_bvh *bvh, bvhcd_front *front, int32_t frame, int3
 bvhcd_status bvhcd_front_contacts(bvhcd_front *front, int32_t which, float *out, int64_t cap, int64_t *count,
                                   int64_t *flagged, int32_t out_on_device, void *stream) {
     if (!front) return BVHCD_INVALID_ARG;
-    return front->impl.contacts(which, out, cap, count, flagged, out_on_device != 0, as_stream(stream));
+    return front->impl.contacts(which, out, cap, count, flagged, out_on_device != 0, false, as_stream(stream));
+}
+
+bvhcd_status bvhcd_front_contacts64(bvhcd_front *front, int32_t which, double *out, int64_t cap, int64_t *count,
+                                    int32_t out_on_device, void *stream) {
+    if (!front) return BVHCD_INVALID_ARG;
+    return front->impl.contacts(which, out, cap, count, nullptr, out_on_device != 0, true, as_stream(stream));
 }
 
 bvhcd_status bvhcd_front_pairs_async(bvhcd_front *front, int32_t which, int32_t *host_out, int64_t cap,
@@ -334,6 +340,12 @@ bvhcd_status bvhcd_learner_frame(bvhcd_learner *l, const bvhcd_scene *scene, int
                                  int32_t *front_op, void *stream) {
     if (!l || !scene) return BVHCD_INVALID_ARG;
     return l->impl.frame(*scene, frame, as_stream(stream), bvh_tag, front_op);
+}
+
+bvhcd_status bvhcd_learner_set_front_cycle(bvhcd_learner *l, int32_t frames) {
+    if (!l || frames < 0) return BVHCD_INVALID_ARG;
+    l->impl.set_front_cycle(frames);
+    return BVHCD_OK;
 }
 
 bvhcd_status bvhcd_learner_set_decide_every(bvhcd_learner *l, int32_t frames) {

@@ -973,10 +973,13 @@ __global__ void __launch_bounds__(kB) k_narrow_prec(const int2 *__restrict__ pai
 // kPrec, ill-conditioned cases are evaluated in FP64: nearly parallel planes
 // (sin^2 of their angle below 1e-6) for contact points, distances below a
 // thousandth of the pair's size for distances.
-template <bool kDist, bool kPrec>
+template <bool kDist, bool kPrec, bool kF64>
 __global__ void k_contacts(const int2 *__restrict__ list, const unsigned *__restrict__ count, unsigned cap,
-                           const int *__restrict__ faces, const float *__restrict__ verts, float4 *out,
+                           const int *__restrict__ faces, const float *__restrict__ verts, void *out_,
                            unsigned *nflag) {
+    // kF64: FP64 arithmetic and FP64 results (double4 per item); else float4
+    // results, FP64 arithmetic in the precision mode and FP32 otherwise
+    constexpr bool kD = kPrec || kF64;
     const unsigned n = min(*count, cap);
     unsigned fl = 0;
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -988,24 +991,29 @@ __global__ void k_contacts(const int2 *__restrict__ list, const unsigned *__rest
             P[k] = prec::V<float>{a.x, a.y, a.z};
             Q[k] = prec::V<float>{b.x, b.y, b.z};
         }
-        float4 r;
-        if (!kDist) {
-            float o[4], cond = 0.f;
-            int st = prec::contact_point(P, Q, o, &cond);
-            if (kPrec && (st != 1 || cond < 1e-6f)) {
-                prec::V<double> Pd[3], Qd[3];
-                for (int k = 0; k < 3; k++) {
-                    Pd[k] = prec::V<double>{P[k].x, P[k].y, P[k].z};
-                    Qd[k] = prec::V<double>{Q[k].x, Q[k].y, Q[k].z};
-                }
-                double od[4], cd = 0.0;
-                st = prec::contact_point(Pd, Qd, od, &cd);
-                for (int k = 0; k < 4; k++) o[k] = (float)od[k];
-                ++fl;
+        prec::V<double> Pd[3], Qd[3];
+        if (kD)
+            for (int k = 0; k < 3; k++) {
+                Pd[k] = prec::V<double>{P[k].x, P[k].y, P[k].z};
+                Qd[k] = prec::V<double>{Q[k].x, Q[k].y, Q[k].z};
             }
-            r = st == 1 ? make_float4(o[0], o[1], o[2], o[3]) : make_float4(__int_as_float(0x7fc00000),
-                                                                          __int_as_float(0x7fc00000),
-                                                                          __int_as_float(0x7fc00000), 0.f);
+        double r[4];
+        if (!kDist) {
+            int st;
+            if (kD) {
+                double cd = 0.0;
+                st = prec::contact_point(Pd, Qd, r, &cd);
+                ++fl;
+            } else {
+                float o[4], cond = 0.f;
+                st = prec::contact_point(P, Q, o, &cond);
+                for (int k = 0; k < 4; k++) r[k] = o[k];
+            }
+            if (st != 1) {
+                const double nan = __longlong_as_double(0x7ff8000000000000ll);
+                r[0] = r[1] = r[2] = nan;
+                r[3] = 0.0;
+            }
         } else {
             // intersecting pairs are at distance 0 (decided as the narrow phase decides)
             int hit;
@@ -1021,26 +1029,18 @@ __global__ void k_contacts(const int2 *__restrict__ list, const unsigned *__rest
                 hit = tritri_sat32(v3{P[0].x, P[0].y, P[0].z}, v3{P[1].x, P[1].y, P[1].z}, v3{P[2].x, P[2].y, P[2].z},
                                    v3{Q[0].x, Q[0].y, Q[0].z}, v3{Q[1].x, Q[1].y, Q[1].z}, v3{Q[2].x, Q[2].y, Q[2].z});
             }
-            float d = hit ? 0.f : prec::tri_distance(P, Q, 1.17549435e-38f);
-            if (kPrec && !hit) {
-                float size = 0.f;
-                for (int k = 0; k < 3; k++) {
-                    const prec::V<float> e = P[k] - Q[k];
-                    size = fmaxf(size, fabsf(e.x) + fabsf(e.y) + fabsf(e.z));
-                }
-                if (d < 1e-3f * size) {
-                    prec::V<double> Pd[3], Qd[3];
-                    for (int k = 0; k < 3; k++) {
-                        Pd[k] = prec::V<double>{P[k].x, P[k].y, P[k].z};
-                        Qd[k] = prec::V<double>{Q[k].x, Q[k].y, Q[k].z};
-                    }
-                    d = (float)prec::tri_distance(Pd, Qd, 2.2250738585072014e-308);
-                    ++fl;
-                }
+            double d = 0.0;
+            if (!hit && kD) {
+                d = prec::tri_distance(Pd, Qd, 2.2250738585072014e-308);
+                ++fl;
+            } else if (!hit) {
+                d = prec::tri_distance(P, Q, 1.17549435e-38f);
             }
-            r = make_float4(0.f, 0.f, 0.f, d);
+            r[0] = r[1] = r[2] = 0.0;
+            r[3] = d;
         }
-        out[q] = r;
+        if (kF64) static_cast<double4 *>(out_)[q] = make_double4(r[0], r[1], r[2], r[3]);
+        else static_cast<float4 *>(out_)[q] = make_float4((float)r[0], (float)r[1], (float)r[2], (float)r[3]);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) fl += __shfl_xor_sync(0xffffffffu, fl, o);
@@ -2036,8 +2036,8 @@ bvhcd_status Front::proximity(const float *pos, double h, bvhcd_proximity *out, 
 
 // Contact points of the hits (which = 0) or distances of the broad pairs
 // (which = 1), in the order bvhcd_front_pairs returns them.
-bvhcd_status Front::contacts(int which, float *out, int64_t cap, int64_t *count, int64_t *flagged, bool out_dev,
-                             cudaStream_t s) {
+bvhcd_status Front::contacts(int which, void *out, int64_t cap, int64_t *count, int64_t *flagged, bool out_dev,
+                             bool f64, cudaStream_t s) {
     if (which < 0 || which > 1 || cap < 0 || inter() || bvh_->box_input()) return BVHCD_INVALID_ARG;
     const int2 *list = hits_.as<int2>();
     unsigned *ctr = counters();
@@ -2048,17 +2048,30 @@ bvhcd_status Front::contacts(int which, float *out, int64_t cap, int64_t *count,
         list = outbuf_.as<int2>();
         cnt = ctr + C_COMPACT;
     }
-    FR_TRY(cbuf_.reserve(sizeof(float4) * (size_t)(pcap_ > 0 ? pcap_ : 1) + 16));
-    float4 *res = cbuf_.as<float4>();
-    unsigned *nflag = reinterpret_cast<unsigned *>(res + (pcap_ > 0 ? pcap_ : 1));
+    const size_t item = f64 ? sizeof(double4) : sizeof(float4);
+    const size_t nres = (size_t)(pcap_ > 0 ? pcap_ : 1);
+    FR_TRY(cbuf_.reserve(item * nres + 16));
+    void *res = cbuf_.p;
+    unsigned *nflag = reinterpret_cast<unsigned *>(static_cast<char *>(cbuf_.p) + item * nres);
     FR_TRY(cudaMemsetAsync(nflag, 0, sizeof(unsigned), s));
     const int *faces = bvh_->faces();
     const float *verts = bvh_->verts();
-    const unsigned g = RESIDENT((k_contacts<false, false>));
-    if (which == 0 && cfg_.precision) k_contacts<false, true><<<g, kThreads, 0, s>>>(list, cnt, (unsigned)pcap_, faces, verts, res, nflag);
-    else if (which == 0) k_contacts<false, false><<<g, kThreads, 0, s>>>(list, cnt, (unsigned)pcap_, faces, verts, res, nflag);
-    else if (cfg_.precision) k_contacts<true, true><<<g, kThreads, 0, s>>>(list, cnt, (unsigned)pcap_, faces, verts, res, nflag);
-    else k_contacts<true, false><<<g, kThreads, 0, s>>>(list, cnt, (unsigned)pcap_, faces, verts, res, nflag);
+    const unsigned g = RESIDENT((k_contacts<false, false, false>));
+    const unsigned pc = (unsigned)pcap_;
+    const bool pr = cfg_.precision != 0;
+#define KC(D, P, F) k_contacts<D, P, F><<<g, kThreads, 0, s>>>(list, cnt, pc, faces, verts, res, nflag)
+    if (f64) {
+        if (which == 0) KC(false, false, true);
+        else if (pr) KC(true, true, true);
+        else KC(true, false, true);
+    } else if (which == 0) {
+        if (pr) KC(false, true, false);
+        else KC(false, false, false);
+    } else {
+        if (pr) KC(true, true, false);
+        else KC(true, false, false);
+    }
+#undef KC
     note_launch();
     FR_TRY(cudaGetLastError());
     unsigned h[C_NUM], hf = 0;
@@ -2071,7 +2084,7 @@ bvhcd_status Front::contacts(int which, float *out, int64_t cap, int64_t *count,
     if (flagged) *flagged = hf;
     int64_t m = n < cap ? n : cap;
     if (out && m > 0) {
-        FR_TRY(cudaMemcpyAsync(out, res, sizeof(float4) * (size_t)m,
+        FR_TRY(cudaMemcpyAsync(out, res, item * (size_t)m,
                                out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
         FR_TRY(cudaStreamSynchronize(s));
     }

@@ -928,10 +928,10 @@ void Learner::poll() {
 }
 
 // The learned frame: apply a completed decision, BVH refit (a restructure
-// when a decision marked subtrees; a build on the first frame), the front op
-// of the reference's cycle -- or GENERATE after a build or restructure, or
-// when a decision voted it -- then, every decide_every frames, the next
-// decision (queued, applied in a later frame).
+// when a decision marked subtrees; a build on the first frame), KEEP or the
+// front op of the reference's cycle when one is set -- or GENERATE after a
+// build or restructure, or when a decision voted it -- then, every
+// decide_every frames, the next decision (queued, applied in a later frame).
 bvhcd_status Learner::frame(const bvhcd_scene &scene, int32_t frame_no, cudaStream_t s, int32_t *bvh_op_run,
                             int32_t *front_op_run) {
     if (frame_no < 0) return BVHCD_INVALID_ARG;
@@ -949,10 +949,10 @@ bvhcd_status Learner::frame(const bvhcd_scene &scene, int32_t frame_no, cudaStre
         since_build_++;
     }
     bvhcd_front_op fop;
-    const int k = frame_no % 6;
+    const int k = front_cycle_ ? frame_no % front_cycle_ : 1;
     if (rebuilt || regen_pending_ || !front_->has_front()) fop = BVHCD_FRONT_GENERATE;
-    else if (k == 0) fop = BVHCD_FRONT_UPDATE;
-    else if (k == 5) fop = BVHCD_FRONT_REORDER;
+    else if (front_cycle_ && k == 0) fop = BVHCD_FRONT_UPDATE;
+    else if (front_cycle_ && k == front_cycle_ - 1) fop = BVHCD_FRONT_REORDER;
     else fop = BVHCD_FRONT_KEEP;
     st = front_->maintain(fop, s);
     if (st != BVHCD_OK) return st;

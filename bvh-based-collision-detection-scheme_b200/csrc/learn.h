@@ -37,6 +37,7 @@ class Learner {
     bvhcd_status decide_async(cudaStream_t s);
     void poll();
     void set_decide_every(int k) { decide_every_ = k > 0 ? k : 1; }
+    void set_front_cycle(int c) { front_cycle_ = c > 0 ? c : 0; }
     long long decisions_applied() const { return decisions_applied_; }
     bvhcd_status frame(const bvhcd_scene &scene, int32_t frame_no, cudaStream_t s, int32_t *bvh_tag,
                        int32_t *front_op_run);
@@ -56,6 +57,7 @@ class Learner {
     double regen_threshold_ = 0.5, last_regen_share_ = 0.0;
     int last_restructure_ = 0;
     int decide_every_ = 3, tree_epoch_ = 0, pending_epoch_ = -1;
+    int front_cycle_ = 0;  // 0: keep between decisions; c: the reference's front cycle of c frames
     bool pending_ = false;
     long long decisions_applied_ = 0;
     cudaEvent_t ev_ = nullptr;

@@ -238,8 +238,8 @@ class Front {
     bvhcd_status export_front(int which, int32_t *out, int64_t cap, int64_t *count, cudaStream_t s);
     bvhcd_status proximity(const float *pos, double thickness, bvhcd_proximity *out, int64_t cap, int64_t *count,
                            bool out_dev, cudaStream_t s);
-    bvhcd_status contacts(int which, float *out, int64_t cap, int64_t *count, int64_t *flagged, bool out_dev,
-                          cudaStream_t s);
+    bvhcd_status contacts(int which, void *out, int64_t cap, int64_t *count, int64_t *flagged, bool out_dev,
+                          bool f64, cudaStream_t s);
     bvhcd_status device_results(const int32_t **hits, const int64_t **counts);
     bvhcd_status pairs_async(int which, int32_t *host_out, int64_t cap, int64_t *host_count, cudaStream_t s);
 

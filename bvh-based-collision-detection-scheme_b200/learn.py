@@ -5,14 +5,15 @@ the learned scheduler (bvhcd_learner_*, bvhcd_mlp_*).
     python learn.py eval  --weights learned_scheduler.npz (on a GPU)
 
 Traces.  Seeded variants of the cloth-over-sphere workload (wave amplitude
-0.05-0.4, wave frequency 1-6) run under the learned mode's cycle (BVH refit
-every frame, the reference's front cycle, no mandatory rebuild) with random
+0.05-0.4, wave frequency 1-6) run under the learned mode's base policy (BVH
+refit every frame, the front kept, no mandatory rebuild) with random
 exploratory restructures and front regenerations.  At every decision frame
 the learner's features of the cut's subtrees are recorded, and the run is
 forked (bvhcd_bvh_copy_state / bvhcd_front_copy_state) into six branches that
-run the next H frames: refit only; four branches that each restructure one
-quarter of the cut (a quarter stays between 1/8 and 1/2 of the internal
-nodes, so it is a restructure, not a rebuild); a front regeneration.
+run the next H frames (24 by default: an operation has that long to pay
+back): refit only; four branches that each restructure one quarter of the
+cut (a quarter stays between 1/8 and 1/2 of the internal nodes, so it is a
+restructure, not a rebuild); a front regeneration.
 
 Labels.  A branch's cost for a subtree is the branch's measured frame time
 (CUDA events) shared out by the subtree's share of the front entries
@@ -28,13 +29,19 @@ sequences.
 
 Evaluation.  Held-out seeds of a 708x708 cloth over the sphere (about 1 M
 triangles) for 200 frames under the heuristic (the reference's schedule:
-build every 12 frames, front cycle 6, quality-triggered restructuring) and
-under the learned scheduler, frame by frame: device time per frame and the
-broad and narrow pair sets, which must be equal.
+build every 12 frames, front cycle 6, quality-triggered restructuring), under
+the learned scheduler, and under two schedules without the network: the
+reference's front cycle with the BVH refit every frame ("cycle"), and the
+learned mode's base policy alone, refit and keep ("keep"); frame by frame:
+device time per frame and the broad and narrow pair sets, which must be
+equal.  The host's garbage collector is off while a sequence is timed (a
+collection between a frame's launches would stall the GPU inside the frame's
+events).
 """
 from __future__ import annotations
 
 import argparse
+import gc
 import hashlib
 import json
 import os
@@ -51,6 +58,11 @@ import scenes  # noqa: E402
 
 WEIGHTS = os.path.join(HERE, "learned_scheduler.npz")
 N_BRANCH_QUARTERS = 4
+
+
+def base_front_op(f: int) -> int:
+    """The learned mode's front operation between decisions: keep."""
+    return bvhcd.FRONT_KEEP
 
 
 def cycle_front_op(f: int) -> int:
@@ -111,7 +123,7 @@ def record_sequence(torch, seed, n, frames, amplitude, freq, H, stride, smax, ex
         main.bvh.maintain(bvhcd.BVH_REFIT, pos[f], faces)
         tag = main.bvh.opt_tag()
         regen = tag in (1, 2) or explore <= act < 2 * explore
-        fop = bvhcd.FRONT_GENERATE if regen else cycle_front_op(f)
+        fop = bvhcd.FRONT_GENERATE if regen else base_front_op(f)
         main.front.maintain(fop)
         lrn.observe(tag in (1, 2), fop == bvhcd.FRONT_GENERATE)
         if f % stride:
@@ -138,7 +150,7 @@ def record_sequence(torch, seed, n, frames, amplitude, freq, H, stride, smax, ex
             op_ms = 0.0
             for h in range(1, H + 1):
                 g = f + h
-                fop_b = bvhcd.FRONT_GENERATE if (b == 1 + N_BRANCH_QUARTERS and h == 1) else cycle_front_op(g)
+                fop_b = bvhcd.FRONT_GENERATE if (b == 1 + N_BRANCH_QUARTERS and h == 1) else base_front_op(g)
                 ev[0].record()
                 pipe.bvh.maintain(bvhcd.BVH_REFIT, pos[g], faces)
                 pipe.front.maintain(fop_b)
@@ -259,8 +271,8 @@ def evaluate(torch, weights, n, frames, seed, check_every=1, decide_every=3):
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * frames)]
     out = {}
     digests = {}
-    for mode in ("heuristic", "learned", "cycle"):
-        bvh = bvhcd.LBvh(T, V, enable_restr=mode != "cycle")
+    for mode in ("heuristic", "learned", "cycle", "keep"):
+        bvh = bvhcd.LBvh(T, V, enable_restr=mode in ("heuristic", "learned"))
         front = bvhcd.BvttFront(bvh, *caps, cull_adjacent=True, narrow_phase=True)
         lrn = None
         if mode == "learned":
@@ -268,13 +280,17 @@ def evaluate(torch, weights, n, frames, seed, check_every=1, decide_every=3):
             lrn.set_params(w["params"])
             lrn.set_decide_every(decide_every)
         tags, ops, dig = [], [], []
+        torch.cuda.synchronize()
+        gc.collect()
+        gc.disable()
         for f in range(frames):
             ev[2 * f].record()
             if mode == "heuristic":
                 bvhcd.frame(bvh, front, f, 0, dpos[f], dfaces, faces_static=f > 0)
-            elif mode == "cycle":
+            elif mode in ("cycle", "keep"):
                 bvh.maintain(bvhcd.BVH_BUILD if f == 0 else bvhcd.BVH_REFIT, dpos[f], dfaces, faces_static=f > 0)
-                front.maintain(bvhcd.FRONT_GENERATE if f == 0 else cycle_front_op(f))
+                front.maintain(bvhcd.FRONT_GENERATE if f == 0 else
+                               (cycle_front_op(f) if mode == "cycle" else base_front_op(f)))
             else:
                 tag, op = lrn.frame(dpos[f], dfaces, f)
             ev[2 * f + 1].record()
@@ -286,9 +302,10 @@ def evaluate(torch, weights, n, frames, seed, check_every=1, decide_every=3):
             if f % check_every == 0:
                 dig.append((_digest(front.pairs()), _digest(front.pairs(narrow=True))))
         torch.cuda.synchronize()
+        gc.enable()
         ms = [ev[2 * f].elapsed_time(ev[2 * f + 1]) for f in range(frames)]
         st = front.stats()
-        assert st["overflow"] == 0, st
+        assert st["overflow_any"] == 0, st
         out[mode] = {"total_ms": round(float(sum(ms)), 3), "mean_ms": round(float(np.mean(ms)), 4),
                      "p50_ms": round(float(np.median(ms)), 4), "p99_ms": round(float(np.percentile(ms, 99)), 4),
                      "builds": int(sum(1 for f, t in enumerate(tags)
@@ -300,10 +317,12 @@ def evaluate(torch, weights, n, frames, seed, check_every=1, decide_every=3):
             lrn.close()
         front.close()
         bvh.close()
-    out["pairs_equal"] = digests["heuristic"] == digests["learned"] == digests["cycle"]
+    out["pairs_equal"] = digests["heuristic"] == digests["learned"] == digests["cycle"] == digests["keep"]
     out["frames_checked"] = len(digests["heuristic"])
     out["speedup"] = round(out["heuristic"]["total_ms"] / out["learned"]["total_ms"], 4)
     out["speedup_cycle"] = round(out["heuristic"]["total_ms"] / out["cycle"]["total_ms"], 4)
+    out["speedup_keep"] = round(out["heuristic"]["total_ms"] / out["keep"]["total_ms"], 4)
+    out["learned_vs_cycle"] = round(out["cycle"]["total_ms"] / out["learned"]["total_ms"], 4)
     out["decide_every"] = decide_every
     out["workload"] = f"cloth {n}x{n} over icosphere, {T} triangles, {frames} frames, seed {seed}"
     return out
@@ -327,7 +346,7 @@ def main():
     t.add_argument("--budget-s", type=float, default=900.0)
     t.add_argument("--n", type=int, default=256)
     t.add_argument("--frames", type=int, default=72)
-    t.add_argument("--horizon", type=int, default=6)
+    t.add_argument("--horizon", type=int, default=24)
     t.add_argument("--stride", type=int, default=2)
     t.add_argument("--smax", type=int, default=256)
     t.add_argument("--explore", type=float, default=0.08)

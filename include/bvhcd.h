@@ -398,13 +398,18 @@ bvhcd_status bvhcd_obj_read(const char *path, float *pos, int32_t vcap, int32_t 
  * them, the midpoint (x, y, z) and length (w) of the two triangles'
  * intersection segment (NaN point for coplanar pairs); which = 1: for every
  * broad-phase pair, in the order of bvhcd_front_pairs(which = 0), the distance
- * between the two triangles (w; 0 for intersecting pairs).  FP32; with
- * precision = 1, FP64 for nearly parallel planes (contacts) and for distances
- * below a thousandth of the pair's size.  out: 4 floats per item (host, or
- * device with out_on_device); flagged (may be NULL) receives how many items
- * were computed in FP64.  Synchronises `stream`. */
+ * between the two triangles (w; 0 for intersecting pairs).  Computed in FP32,
+ * or in FP64 with precision = 1; written as FP32.  out: 4 floats per item
+ * (host, or device with out_on_device); flagged (may be NULL) receives how
+ * many items were computed in FP64.  Synchronises `stream`. */
 bvhcd_status bvhcd_front_contacts(bvhcd_front *front, int32_t which, float *out, int64_t cap, int64_t *count,
                                   int64_t *flagged, int32_t out_on_device, void *stream);
+/* The same computed and written in FP64: 4 doubles per item.  FP32 results
+ * carry the FP32 rounding of absolute coordinates -- half an ulp of a
+ * coordinate near 1 is about 1e-5 of a 2e-3 triangle -- which this form does
+ * not. */
+bvhcd_status bvhcd_front_contacts64(bvhcd_front *front, int32_t which, double *out, int64_t cap, int64_t *count,
+                                    int32_t out_on_device, void *stream);
 
 /* ---- State copies.  No counterpart in the reference.  dst becomes a copy of
  * src -- tree, restructure log, counters, fronts, pairs and their host-side
@@ -447,15 +452,20 @@ bvhcd_status bvhcd_learner_destroy(bvhcd_learner *learner);
 bvhcd_status bvhcd_learner_set_params(bvhcd_learner *learner, const float *params);
 bvhcd_status bvhcd_learner_get_params(const bvhcd_learner *learner, float *params);
 /* One learned frame: BVH refit (build on frame 0; a restructure when a
- * decision marked subtrees), the front op of the reference's cycle (UPDATE at
- * frame % 6 == 0, REORDER at 5, KEEP otherwise) or GENERATE after a rebuild or
- * a regenerate vote.  Every `decide_every` frames (default 3) it queues a
+ * decision marked subtrees), then KEEP -- or, with a front cycle of c > 0
+ * frames set (bvhcd_learner_set_front_cycle), the reference's cycle (UPDATE at
+ * frame % c == 0, REORDER at c - 1, KEEP otherwise) -- or GENERATE after a
+ * rebuild or a regenerate vote.  Every `decide_every` frames (default 3) it queues a
  * decision -- features, votes, marks and counts on the device, an event --
  * and the first frame that finds the event complete applies it; the host never
  * waits for it.  A decision voted on a tree that has changed since is dropped.
  * bvh_tag receives the reference's opt tag (0 refit, 1 restructure, 2 build),
  * front_op the op run; either may be NULL. */
 bvhcd_status bvhcd_learner_set_decide_every(bvhcd_learner *learner, int32_t frames);
+/* The front operations between decisions: 0 (the default) keeps the front
+ * until a vote or a tree change regenerates it; c > 0 runs the reference's
+ * front cycle of c frames (BvttFrontSettings.h:49 uses 6). */
+bvhcd_status bvhcd_learner_set_front_cycle(bvhcd_learner *learner, int32_t frames);
 bvhcd_status bvhcd_learner_frame(bvhcd_learner *learner, const bvhcd_scene *scene, int32_t frame,
                                  int32_t *bvh_tag, int32_t *front_op, void *stream);
 /* Trace recording under another schedule: after each frame's maintains, tell

@@ -62,6 +62,7 @@ def test_learned_frames_keep_exact_pairs(cuda, lib_built, oracle, cloth_c1, bias
     T, V = faces.shape[0], frames[0].shape[0]
     bvh, front, lrn = _learner(lib_built, T, V)
     lrn.set_decide_every(2)
+    lrn.set_front_cycle(6)  # the reference's front cycle between decisions (the default keeps)
     rng = np.random.default_rng(11)
     if bias is None:
         p = rng.normal(0, 0.3, m.N_PARAMS).astype(np.float32)

@@ -161,17 +161,21 @@ def test_stacked_layers_full_size_against_exact_predicate(cuda, lib_built, oracl
         assert np.array_equal(hits, exp[exact]), f
     print(f"z_noise {z_noise}: {len(broad)} broad pairs, {len(hits)} hits, {st['flagged']} flagged")
     if z_noise:
+        # FP64 results (bvhcd_front_contacts64): FP32 results would carry the FP32 rounding of
+        # coordinates near 1, about 1.5e-5 of these 2e-3 triangles, whatever the arithmetic
         h = front.pairs(narrow=True)
-        c, _ = front.contacts(0)
+        c = front.contacts64(0)
         _, con, _ = oracle.precision_pairs(h, faces, frames[2])
-        both = ~np.isnan(con[:, 0]) & ~np.isnan(c[:, 0])
+        assert np.array_equal(np.isnan(c[:, 0]), np.isnan(con[:, 0]))
+        both = ~np.isnan(con[:, 0])
         assert both.sum() > 0.9 * len(h)
-        e = np.abs(c[both, :3].astype(np.float64) - con[both, :3]).max(axis=1) / _scale(faces, frames[2], h)[both]
+        e = np.abs(c[both, :3] - con[both, :3]).max(axis=1) / _scale(faces, frames[2], h)[both]
         assert float(e.max()) <= 1e-5, float(e.max())
         bp = front.pairs()
-        d, _ = front.contacts(1)
+        d = front.contacts64(1)
         hit64, _, dist = oracle.precision_pairs(bp, faces, frames[2])
         assert np.array_equal(d[:, 3] == 0, hit64)
         dd = ~hit64
-        ed = np.abs(d[dd, 3].astype(np.float64) - dist[dd]) / _scale(faces, frames[2], bp)[dd]
+        ed = np.abs(d[dd, 3] - dist[dd]) / _scale(faces, frames[2], bp)[dd]
         assert float(ed.max()) <= 1e-5, float(ed.max())
+        print(f"contact points / distances against FP64: {float(e.max()):.2e} / {float(ed.max()):.2e} of the extent")
