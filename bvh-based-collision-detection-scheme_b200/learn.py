@@ -307,6 +307,7 @@ def evaluate(torch, weights, n, frames, seed, check_every=1, decide_every=3):
         st = front.stats()
         assert st["overflow_any"] == 0, st
         out[mode] = {"total_ms": round(float(sum(ms)), 3), "mean_ms": round(float(np.mean(ms)), 4),
+                     "slowest_frames": [[int(f), round(float(ms[f]), 3)] for f in np.argsort(ms)[::-1][:3]],
                      "p50_ms": round(float(np.median(ms)), 4), "p99_ms": round(float(np.percentile(ms, 99)), 4),
                      "builds": int(sum(1 for f, t in enumerate(tags)
                                        if t == 2 or (mode == "heuristic" and f % 12 == 0))),
