@@ -568,6 +568,9 @@ __device__ __forceinline__ float box_depth(const float4 &alo, const float4 &ahi,
 // tiles and from the overlap list) and the internal list into the test list.
 constexpr int kSelPer = 8;
 constexpr unsigned kKeepTile = kSelPer * kThreads;  // 2048 entries per tile summary
+inline size_t keep_tiles(int64_t cap_int, int64_t cap_ext) {
+    return (size_t)((cap_int + cap_ext + kKeepTile - 1) / kKeepTile) + 1;
+}
 
 // dense appends (the converged lanes that append together take consecutive
 // slots, so nothing is reserved unused: the selected keep runs few entries
@@ -1277,6 +1280,13 @@ bvhcd_status Front::init() {
     FR_TRY(iexp_.reserve(sizeof(float) * (size_t)fcap_[0]));
     FR_TRY(xexp_.reserve(sizeof(float) * (size_t)fcap_[1]));
     FR_TRY(ksel_.reserve(sizeof(unsigned) * (size_t)(fcap_[0] + fcap_[1])));
+    // the keep's lists of overlapping entries (external: at most one pair
+    // each; internal: at most the internal front) and its tile summaries
+    for (int k = 0; k < 2; k++) {
+        FR_TRY(kl_sp_[k].reserve(sizeof(int4) * (size_t)pcap_));
+        FR_TRY(kl_al_[k].reserve(sizeof(unsigned) * (size_t)fcap_[0]));
+    }
+    FR_TRY(tsum_.reserve(sizeof(unsigned) * keep_tiles(fcap_[0], fcap_[1])));
     FR_TRY(counts64_.reserve(sizeof(int64_t) * 2));
     FR_TRY(fctr_.reserve(sizeof(unsigned) * C_NUM));
     FR_TRY(cudaMemset(fctr_.p, 0, sizeof(unsigned) * C_NUM));
@@ -1550,18 +1560,7 @@ bvhcd_status Front::keep(cudaStream_t s) {
     const bool expiries = !inter() && !cfg_.precision && !bvh_->tree().nrec16;
     if (exp_epoch_ != bvh_->topo_epoch() || exp_faces_ != bvh_->faces_epoch()) exp_valid_ = false;
     if (expiries) {
-        // the lists of overlapping entries (external: at most one pair each;
-        // internal: at most the internal front) and the tile summaries
-        const size_t tiles = (size_t)((fcap_[0] + fcap_[1] + kKeepTile - 1) / kKeepTile) + 1;
-        if (kl_sp_[0].bytes < sizeof(int4) * (size_t)pcap_ || kl_al_[0].bytes < sizeof(unsigned) * (size_t)fcap_[0] ||
-            tsum_.bytes < sizeof(unsigned) * tiles) {
-            for (int k = 0; k < 2; k++) {
-                FR_TRY(kl_sp_[k].reserve(sizeof(int4) * (size_t)pcap_));
-                FR_TRY(kl_al_[k].reserve(sizeof(unsigned) * (size_t)fcap_[0]));
-            }
-            FR_TRY(tsum_.reserve(sizeof(unsigned) * tiles));
-            exp_valid_ = false;
-        }
+        const size_t tiles = keep_tiles(fcap_[0], fcap_[1]);
         const int pin = keep_par_, pout = 1 - keep_par_;
         a.motion = bvh_->counters() + C_MOTION;
         a.iexp_out = iexp_.as<float>();
@@ -1756,8 +1755,9 @@ bvhcd_status Front::grow_from(const unsigned *h, cudaStream_t s) {
     // Every grown buffer is allocated before the handle changes: if one
     // allocation fails the others are released and the front keeps its old,
     // consistent buffers (no capacity ever exceeds the buffer behind it).
-    DBuf nf[2][2], nwork, niexp, nxexp, nksel, npairs, nhits;
-    DBuf *tmp[] = {&nf[0][0], &nf[0][1], &nf[1][0], &nf[1][1], &nwork, &niexp, &nxexp, &nksel, &npairs, &nhits};
+    DBuf nf[2][2], nwork, niexp, nxexp, nksel, npairs, nhits, nsp[2], nal[2], ntsum;
+    DBuf *tmp[] = {&nf[0][0], &nf[0][1], &nf[1][0], &nf[1][1], &nwork, &niexp, &nxexp, &nksel, &npairs, &nhits,
+                   &nsp[0], &nsp[1], &nal[0], &nal[1], &ntsum};
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < 2 && e == cudaSuccess; k++)
         for (int set = 0; set < 2 && gf[k] && e == cudaSuccess; set++) e = nf[set][k].reserve(sizeof(int2) * (size_t)nc[k]);
@@ -1768,6 +1768,11 @@ bvhcd_status Front::grow_from(const unsigned *h, cudaStream_t s) {
     if (e == cudaSuccess && (gf[0] || gf[1])) e = nksel.reserve(sizeof(unsigned) * (size_t)(nc[0] + nc[1]));
     if (e == cudaSuccess && gp) e = npairs.reserve(sizeof(int2) * (size_t)npc);
     if (e == cudaSuccess && gp) e = nhits.reserve(sizeof(int2) * (size_t)npc);
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+        if (gp) e = nsp[k].reserve(sizeof(int4) * (size_t)npc);
+        if (e == cudaSuccess && gf[0]) e = nal[k].reserve(sizeof(unsigned) * (size_t)nc[0]);
+    }
+    if (e == cudaSuccess && (gf[0] || gf[1])) e = ntsum.reserve(sizeof(unsigned) * keep_tiles(nc[0], nc[1]));
     // the current front survives in set cur_: copied into its grown buffers
     for (int k = 0; k < 2 && e == cudaSuccess; k++)
         if (gf[k]) e = cudaMemcpyAsync(nf[cur_][k].p, front_[cur_][k].p, sizeof(int2) * (size_t)fcap_[k],
@@ -1793,12 +1798,20 @@ bvhcd_status Front::grow_from(const unsigned *h, cudaStream_t s) {
         swap_in(iexp_, niexp);
     }
     if (gf[1]) swap_in(xexp_, nxexp);
-    if (gf[0] || gf[1]) swap_in(ksel_, nksel);
+    if (gf[0] || gf[1]) {
+        swap_in(ksel_, nksel);
+        swap_in(tsum_, ntsum);
+    }
+    for (int k = 0; k < 2; k++) {
+        if (gp) swap_in(kl_sp_[k], nsp[k]);
+        if (gf[0]) swap_in(kl_al_[k], nal[k]);
+    }
     if (gp) {
         swap_in(pairs_, npairs);
         swap_in(hits_, nhits);
         pcap_ = npc;
     }
+    if (gp || gf[0] || gf[1]) exp_valid_ = false;  // the keep's lists start again
     return BVHCD_OK;
 }
 
