@@ -54,7 +54,7 @@ bool same_state(const bvhcd::LBvh::HostState &a, const bvhcd::LBvh::HostState &b
 }
 bool same_state(const bvhcd::Front::HostState &a, const bvhcd::Front::HostState &b) {
     return a.cur == b.cur && a.last_op == b.last_op && a.has_front == b.has_front && a.int_swapped == b.int_swapped &&
-           a.log_counted == b.log_counted && a.exp_valid == b.exp_valid && a.keep_par == b.keep_par;
+           a.log_counted == b.log_counted && a.exp_valid == b.exp_valid;
 }
 }  // namespace
 

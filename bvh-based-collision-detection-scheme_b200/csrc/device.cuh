@@ -62,9 +62,7 @@ enum CounterSlot {
     C_INT1 = 2, C_EXT1 = 3,   // front sizes, buffer set 1
     C_PAIRS = 4, C_HITS = 5,
     C_OVERFLOW = 6,           // bit0 int front, bit1 ext front, bit2 pairs, bit3 hits,
-                              // bit4 traversal bound hit, bit5 sprout work list, bit6 the
-                              // input front had lost entries, bit7 the keep's lists of
-                              // overlapping entries
+                              // bit4 traversal bound hit, bit5 sprout work list
     C_RT_SUBTREES = 7, C_RT_INTNODES = 8,
     C_KSEL = 9,               // keep: front entries selected for a test (the rest wait on their expiries)
     C_WORK = 10,              // overlapping internal entries queued for traversal
@@ -79,9 +77,7 @@ enum CounterSlot {
     C_NF_ACC = 19,            // BVH: non-finite input seen by the blocks of the running check
     C_NONFINITE = 20,         // BVH: 1 when the last maintain's input held a NaN or infinite coordinate
     C_NF_DONE = 21,           // BVH: blocks of the build-time finiteness check finished
-    C_KL0 = 22,               // keep lists k = 0, 1: C_KL0 + 2k overlapping external entries kept with
-                              // their overlap expiry, C_KL0 + 2k + 1 overlapping internal entries
-    C_NUM = 26
+    C_NUM = 22
 };
 
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }

@@ -70,17 +70,6 @@ struct FArgs {
     const float *iexp_in, *xexp_in;
     float *iexp_out, *xexp_out;
     const unsigned *ksel;
-    // The keep's bookkeeping of overlapping entries (with expiries): the
-    // external ones as {prim, leaf, index, overlap expiry bits} records (sp),
-    // the internal ones as indices (al), each read from one list and written to
-    // the other; per tile of kKeepTile entries the smallest waiting expiry (tsum)
-    const int4 *sp_in;
-    int4 *sp_out;
-    const unsigned *al_in;
-    unsigned *al_out;
-    int sp_in_slot, sp_out_slot, al_in_slot, al_out_slot;
-    unsigned cap_sp, cap_al;
-    unsigned *tsum;
     // an inter front's restructure (k_restr_scan): the traversed BVH's last
     // restructure -- per internal node a non-zero mark inside a restructured
     // subtree, per leaf slot its subtree root (0 outside), per root the old
@@ -543,98 +532,38 @@ __device__ __forceinline__ float box_gap(const float4 &alo, const float4 &ahi, c
     return fmaxf(g, fmaxf(__fsub_rd(blo.z, ahi.z), __fsub_rd(alo.z, bhi.z)));
 }
 
-// The overlap of two intersecting boxes along their least overlapping axis,
-// rounded down: they keep overlapping while each moves by less than half of it.
-__device__ __forceinline__ float box_depth(const float4 &alo, const float4 &ahi, const float4 &blo,
-                                           const float4 &bhi) {
-    float p = __fsub_rd(fminf(ahi.x, bhi.x), fmaxf(alo.x, blo.x));
-    p = fminf(p, __fsub_rd(fminf(ahi.y, bhi.y), fmaxf(alo.y, blo.y)));
-    return fminf(p, __fsub_rd(fminf(ahi.z, bhi.z), fmaxf(alo.z, blo.z)));
-}
-
-// Keep-time bookkeeping.  Every entry is in one of four states, decided by
-// its last test:
-//   separated    expiry e = M + gap / 2 >= 0 in the per-entry array; waits
-//                while the motion stays below e (a tile of kKeepTile entries
-//                keeps the smallest such e, so most tiles are not read);
-//   adjacent     external entry of two triangles sharing a vertex: expiry
-//                FLT_MAX, never gives a pair while the faces stay;
-//   overlapping external: -1 in the array and a record {prim, leaf, index,
-//                M + depth / 2} in the overlap list: its pair is emitted from
-//                the list without a test while the motion stays below;
-//   overlapping internal: -1 in the array and its index in the internal
-//                list: tested and traversed below every keep.
-// A selecting keep turns the due entries (expiry reached, from the touched
-// tiles and from the overlap list) and the internal list into the test list.
+// The entries whose expiry the motion has reached, as a list of indices into
+// [0, F_int + F_ext).  The expiries are read as a stream and nothing else of a
+// waiting entry is touched.  A block takes tiles of kSelPer x 256 entries,
+// each warp kSelPer runs of 32: ballots count a warp's picks, a block scan in
+// shared memory places the warps, one atomic per tile reserves its run.
 constexpr int kSelPer = 8;
-constexpr unsigned kKeepTile = kSelPer * kThreads;  // 2048 entries per tile summary
-inline size_t keep_tiles(int64_t cap_int, int64_t cap_ext) {
-    return (size_t)((cap_int + cap_ext + kKeepTile - 1) / kKeepTile) + 1;
-}
-
-// dense appends (the converged lanes that append together take consecutive
-// slots, so nothing is reserved unused: the selected keep runs few entries
-// per lane, where chunks would leave holes in most slots)
-template <typename V>
-__device__ __forceinline__ bool put_dense_v(V *buf, unsigned *ctr, unsigned cap, const V &v, unsigned *ovf,
-                                            unsigned bit) {
-    cg::coalesced_group g = cg::coalesced_threads();
-    unsigned b = 0;
-    if (g.thread_rank() == 0) b = atomicAdd(ctr, g.size());
-    const unsigned slot = g.shfl(b, 0) + g.thread_rank();
-    if (slot < cap) {
-        buf[slot] = v;
-        return true;
-    }
-    atomicOr(ovf, bit);
-    return false;
-}
-
-__device__ __forceinline__ void put_dense(int2 *buf, unsigned *ctr, unsigned cap, const int2 &v, unsigned *ovf,
-                                          unsigned bit) {
-    put_dense_v(buf, ctr, cap, v, ovf, bit);
-}
-
-// The separated entries whose expiry the motion has reached, from the tiles
-// whose summary it has reached, as indices into [0, F_int + F_ext).  A block
-// takes a tile (kSelPer runs of 32 per warp): ballots count a warp's picks, a
-// block scan places the warps, one atomic reserves the tile's run; the tile's
-// summary becomes the smallest expiry still waiting in it (the tested
-// entries add theirs back in the scan).
 __global__ void __launch_bounds__(kThreads) k_keep_select(FArgs a, unsigned *list, unsigned *count) {
-    __shared__ unsigned wsum[kThreads / 32], tbase, smin;
+    __shared__ unsigned wsum[kThreads / 32], tbase;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     const unsigned total = ni + ne;
     const float M = __uint_as_float(*a.motion);
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (unsigned t0 = blockIdx.x * kKeepTile; t0 < total; t0 += gridDim.x * kKeepTile) {
-        const unsigned tile = t0 / kKeepTile;
-        if (M < __uint_as_float(a.tsum[tile])) continue;  // nothing in this tile is due (block-uniform)
-        if (threadIdx.x == 0) smin = 0x7f800000u;          // +inf
+    constexpr unsigned kTile = kSelPer * kThreads;
+    for (unsigned t0 = blockIdx.x * kTile; t0 < total; t0 += gridDim.x * kTile) {
         float ex[kSelPer];
 #pragma unroll
         for (int r = 0; r < kSelPer; r++) {  // every load of the tile in flight at once
             const unsigned q = t0 + (warp * kSelPer + r) * 32u + lane;
-            ex[r] = q >= total ? -1.f : q < ni ? __ldcs(a.iexp_in + q) : __ldcs(a.xexp_in + (q - ni));
+            ex[r] = q >= total ? 0.f : q < ni ? __ldcs(a.iexp_in + q) : __ldcs(a.xexp_in + (q - ni));
         }
         unsigned m[kSelPer], n = 0;
-        float wait = 3.402823466e+38f * 2.f;  // +inf
 #pragma unroll
         for (int r = 0; r < kSelPer; r++) {
-            // separated or adjacent entries only (the overlapping ones are listed
-            // apart); past the end nothing is picked, whatever the motion
-            const bool sep = ex[r] >= 0.f;
-            const bool due = sep && !(M < ex[r]);
-            if (sep && !due) wait = fminf(wait, ex[r]);
-            m[r] = __ballot_sync(0xffffffffu, due);
+            // past the end nothing is picked, whatever the motion (an infinite
+            // input coordinate makes it infinite)
+            const unsigned q = t0 + (warp * kSelPer + r) * 32u + lane;
+            m[r] = __ballot_sync(0xffffffffu, q < total && !(M < ex[r]));
             n += __popc(m[r]);
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) wait = fminf(wait, __shfl_xor_sync(0xffffffffu, wait, o));
         if (lane == 0) wsum[warp] = n;
         __syncthreads();
-        if (lane == 0) atomicMin(&smin, __float_as_uint(wait));  // non-negative: bit order
         if (threadIdx.x == 0) {
             unsigned s = 0;
             for (int w = 0; w < kThreads / 32; w++) {
@@ -651,45 +580,22 @@ __global__ void __launch_bounds__(kThreads) k_keep_select(FArgs a, unsigned *lis
             if ((m[r] >> lane) & 1u) list[pos + __popc(m[r] & ((1u << lane) - 1u))] = t0 + (warp * kSelPer + r) * 32u + lane;
             pos += __popc(m[r]);
         }
-        if (threadIdx.x == 0) a.tsum[tile] = smin;
-        __syncthreads();  // wsum, tbase and smin are reused by the next tile
+        __syncthreads();  // wsum and tbase are reused by the next tile
     }
 }
 
-// The overlap list: a record whose overlap expiry the motion has not reached
-// gives its pair at once and stays listed; the others join the test list,
-// with every entry of the internal list.
-__global__ void __launch_bounds__(kThreads) k_keep_lists(FArgs a, unsigned *list, unsigned *count, unsigned cap) {
-    const unsigned nsp = min(a.ctr[a.sp_in_slot], a.cap_sp);
-    const unsigned nal = min(a.ctr[a.al_in_slot], a.cap_al);
-    const float M = __uint_as_float(*a.motion);
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < nsp + nal; i += gridDim.x * blockDim.x) {
-        if (i >= nsp) {
-            put_dense_v(list, count, cap, __ldg(a.al_in + (i - nsp)), a.ctr + C_OVERFLOW, 128u);
-            continue;
-        }
-        const int4 r = __ldcs(a.sp_in + i);
-        if (M < __int_as_float(r.w)) {
-            put_dense_v(a.pairs, a.ctr + C_PAIRS, a.cap_pairs, make_int2(r.x, r.y), a.ctr + C_OVERFLOW, 4u);
-            put_dense_v(a.sp_out, a.ctr + a.sp_out_slot, a.cap_sp, r, a.ctr + C_OVERFLOW, 128u);
-        } else {
-            put_dense_v(list, count, cap, (unsigned)r.z, a.ctr + C_OVERFLOW, 128u);
-        }
-    }
-}
-
-// the waiting expiry e of entry q joins its tile's summary (a full keep's
-// lanes hold consecutive entries: one atomic per tile and warp)
-__device__ __forceinline__ void tile_wait(unsigned *tsum, unsigned q, float e, bool warp_runs) {
-    if (!warp_runs) {
-        atomicMin(tsum + q / kKeepTile, __float_as_uint(e));
-        return;
-    }
-    const unsigned mask = __activemask();
-    const unsigned tile = q / kKeepTile;
-    const unsigned peers = __match_any_sync(mask, tile);
-    const unsigned v = __reduce_min_sync(peers, __float_as_uint(e));
-    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicMin(tsum + tile, v);
+// An emission without per-lane chunks: the converged lanes that emit at the
+// same time take consecutive slots with one atomic, so nothing is reserved
+// unused (the selected keep runs few entries per lane, where chunks would
+// leave holes in most slots).
+__device__ __forceinline__ void put_dense(int2 *buf, unsigned *ctr, unsigned cap, const int2 &v, unsigned *ovf,
+                                          unsigned bit) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned b = 0;
+    if (g.thread_rank() == 0) b = atomicAdd(ctr, g.size());
+    const unsigned slot = g.shfl(b, 0) + g.thread_rank();
+    if (slot < cap) buf[slot] = v;
+    else atomicOr(ovf, bit);
 }
 
 // keepIntLooseIntraFronts / keepExtLooseIntraFronts (BvttFrontKeepKernels.cu:11-58)
@@ -714,18 +620,10 @@ __global__ void __launch_bounds__(kB) k_keep_scan(FArgs a) {
         for (int k = 0; k < kU; k++) {
             if (!b.v[k]) continue;
             const bool ov = overlap(b.nlo[k], b.nhi[k], b.plo[k], b.phi[k]);
-            const unsigned q = b.qi[k];
             if (b.in_int[k]) {
-                if (a.iexp_out) {
-                    if (ov) {
-                        a.iexp_out[q] = -1.f;
-                        put_dense_v(a.al_out, a.ctr + a.al_out_slot, a.cap_al, q, a.ctr + C_OVERFLOW, 128u);
-                    } else {
-                        const float e = __fadd_rd(M, __fmul_rd(box_gap(b.plo[k], b.phi[k], b.nlo[k], b.nhi[k]), 0.5f));
-                        a.iexp_out[q] = e;
-                        tile_wait(a.tsum, q, e, !a.ksel);
-                    }
-                }
+                if (a.iexp_out)
+                    a.iexp_out[b.qi[k]] =
+                        ov ? -1.f : __fadd_rd(M, __fmul_rd(box_gap(b.plo[k], b.phi[k], b.nlo[k], b.nhi[k]), 0.5f));
                 if (ov) {
                     if (a.ksel) put_dense(a.work, a.ctr + C_WORK, a.cap_work, b.e[k], a.ctr + C_OVERFLOW, 32u);
                     else emit_work(a, em, b.e[k]);
@@ -738,19 +636,12 @@ __global__ void __launch_bounds__(kB) k_keep_scan(FArgs a) {
             }
             // (faces are read only for overlapping entries; a separated one waits on its gap)
             const bool adj = ov && a.cull && covertex(prim_face(a, b.e[k].x), __ldg(&a.sface[b.e[k].y]));
-            if (adj) {
-                a.xexp_out[q - ni] = 3.402823466e+38f;
-            } else if (ov) {
-                a.xexp_out[q - ni] = -1.f;
-                const float eo = __fadd_rd(M, __fmul_rd(box_depth(b.plo[k], b.phi[k], b.nlo[k], b.nhi[k]), 0.5f));
-                put_dense_v(a.sp_out, a.ctr + a.sp_out_slot, a.cap_sp,
-                            make_int4(b.e[k].x, b.e[k].y, (int)q, __float_as_int(eo)), a.ctr + C_OVERFLOW, 128u);
+            a.xexp_out[b.qi[k] - ni] =
+                adj ? 3.402823466e+38f
+                    : (ov ? -1.f : __fadd_rd(M, __fmul_rd(box_gap(b.plo[k], b.phi[k], b.nlo[k], b.nhi[k]), 0.5f)));
+            if (ov && !adj) {
                 if (a.ksel) put_dense(a.pairs, a.ctr + C_PAIRS, a.cap_pairs, b.e[k], a.ctr + C_OVERFLOW, 4u);
                 else chunk_put(a.pairs, a.ctr + C_PAIRS, a.cap_pairs, em.pr, b.e[k], a.ctr + C_OVERFLOW, 4u);
-            } else {
-                const float e = __fadd_rd(M, __fmul_rd(box_gap(b.plo[k], b.phi[k], b.nlo[k], b.nhi[k]), 0.5f));
-                a.xexp_out[q - ni] = e;
-                tile_wait(a.tsum, q, e, !a.ksel);
             }
         }
     }
@@ -1185,7 +1076,7 @@ __global__ void k_pair_scatter(const int2 *__restrict__ pairs, const int4 *__res
 // incomplete too; a generation starts clean.
 // The carried bits are joined by bit 6, which says that this maintain's own
 // results (pairs, hits) are incomplete because its input front was.
-constexpr unsigned kFrontLossBits = 1u | 2u | 16u | 32u | 64u | 128u;
+constexpr unsigned kFrontLossBits = 1u | 2u | 16u | 32u | 64u;
 __global__ void k_ovf_roll(unsigned *ctr, unsigned carry) {
     if (threadIdx.x == 0) {
         const unsigned o = ctr[C_OVERFLOW];
@@ -1249,8 +1140,7 @@ Front::~Front() {
         for (auto &b : set) b.release();
     DBuf *bufs[] = {&pairs_, &hits_, &outbuf_, &work_, &intcnt_, &extcnt_, &intbeg_, &extbeg_, &intback_,
                     &extback_, &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_, &fctr_, &rcur_,
-                    &pxbuf_, &pxout_, &iexp_, &xexp_, &ksel_, &kl_sp_[0], &kl_sp_[1], &kl_al_[0], &kl_al_[1],
-                    &tsum_};
+                    &pxbuf_, &pxout_, &iexp_, &xexp_, &ksel_};
     for (DBuf *b : bufs) b->release();
     for (int k = 0; k < kSnap; k++)
         if (snap_ev_[k]) cudaEventDestroy(snap_ev_[k]);
@@ -1280,13 +1170,6 @@ bvhcd_status Front::init() {
     FR_TRY(iexp_.reserve(sizeof(float) * (size_t)fcap_[0]));
     FR_TRY(xexp_.reserve(sizeof(float) * (size_t)fcap_[1]));
     FR_TRY(ksel_.reserve(sizeof(unsigned) * (size_t)(fcap_[0] + fcap_[1])));
-    // the keep's lists of overlapping entries (external: at most one pair
-    // each; internal: at most the internal front) and its tile summaries
-    for (int k = 0; k < 2; k++) {
-        FR_TRY(kl_sp_[k].reserve(sizeof(int4) * (size_t)pcap_));
-        FR_TRY(kl_al_[k].reserve(sizeof(unsigned) * (size_t)fcap_[0]));
-    }
-    FR_TRY(tsum_.reserve(sizeof(unsigned) * keep_tiles(fcap_[0], fcap_[1])));
     FR_TRY(counts64_.reserve(sizeof(int64_t) * 2));
     FR_TRY(fctr_.reserve(sizeof(unsigned) * C_NUM));
     FR_TRY(cudaMemset(fctr_.p, 0, sizeof(unsigned) * C_NUM));
@@ -1356,10 +1239,6 @@ static FArgs make_args(const LBvh *bvh, const LBvh *trav, unsigned *ctr, const F
     a.iexp_in = a.xexp_in = nullptr;
     a.iexp_out = a.xexp_out = nullptr;
     a.ksel = nullptr;
-    a.sp_in = nullptr; a.sp_out = nullptr; a.al_in = nullptr; a.al_out = nullptr;
-    a.sp_in_slot = C_KL0; a.al_in_slot = C_KL0 + 1; a.sp_out_slot = C_KL0 + 2; a.al_out_slot = C_KL0 + 3;
-    a.cap_sp = a.cap_al = 0;
-    a.tsum = nullptr;
     a.rs_mark = a.rs_root = a.rs_last = nullptr;
     return a;
 }
@@ -1560,37 +1439,16 @@ bvhcd_status Front::keep(cudaStream_t s) {
     const bool expiries = !inter() && !cfg_.precision && !bvh_->tree().nrec16;
     if (exp_epoch_ != bvh_->topo_epoch() || exp_faces_ != bvh_->faces_epoch()) exp_valid_ = false;
     if (expiries) {
-        const size_t tiles = keep_tiles(fcap_[0], fcap_[1]);
-        const int pin = keep_par_, pout = 1 - keep_par_;
         a.motion = bvh_->counters() + C_MOTION;
         a.iexp_out = iexp_.as<float>();
         a.xexp_out = xexp_.as<float>();
-        a.sp_out = kl_sp_[pout].as<int4>();
-        a.al_out = kl_al_[pout].as<unsigned>();
-        a.sp_out_slot = C_KL0 + 2 * pout;
-        a.al_out_slot = C_KL0 + 2 * pout + 1;
-        a.cap_sp = (unsigned)pcap_;
-        a.cap_al = (unsigned)fcap_[0];
-        a.tsum = tsum_.as<unsigned>();
-        FR_TRY(cudaMemsetAsync(ctr + C_KL0 + 2 * pout, 0, 2 * sizeof(unsigned), s));
         if (exp_valid_) {
             a.iexp_in = iexp_.as<float>();
             a.xexp_in = xexp_.as<float>();
-            a.sp_in = kl_sp_[pin].as<int4>();
-            a.al_in = kl_al_[pin].as<unsigned>();
-            a.sp_in_slot = C_KL0 + 2 * pin;
-            a.al_in_slot = C_KL0 + 2 * pin + 1;
             FR_TRY(cudaMemsetAsync(ctr + C_KSEL, 0, sizeof(unsigned), s));
             k_keep_select<<<RESIDENT(k_keep_select), kThreads, 0, s>>>(a, ksel_.as<unsigned>(), ctr + C_KSEL);
             note_launch();
-            k_keep_lists<<<RESIDENT(k_keep_lists), kThreads, 0, s>>>(
-                a, ksel_.as<unsigned>(), ctr + C_KSEL, (unsigned)(ksel_.bytes / sizeof(unsigned)));
-            note_launch();
             a.ksel = ksel_.as<unsigned>();
-        } else {
-            // every tile summary starts high (3.4e38 as bytes 0x7f): the full
-            // keep lowers it to the smallest waiting expiry
-            FR_TRY(cudaMemsetAsync(tsum_.p, 0x7f, sizeof(unsigned) * tiles, s));
         }
     }
     last_keep_sel_ = a.ksel != nullptr;
@@ -1599,7 +1457,6 @@ bvhcd_status Front::keep(cudaStream_t s) {
         exp_valid_ = true;
         exp_epoch_ = bvh_->topo_epoch();
         exp_faces_ = bvh_->faces_epoch();
-        keep_par_ ^= 1;
     }
     LAUNCH_ITEM(k_sprout, false, shape_[BVHCD_SHAPE_SPROUT], s, a);
     return cuda_status(cudaGetLastError());
@@ -1755,9 +1612,8 @@ bvhcd_status Front::grow_from(const unsigned *h, cudaStream_t s) {
     // Every grown buffer is allocated before the handle changes: if one
     // allocation fails the others are released and the front keeps its old,
     // consistent buffers (no capacity ever exceeds the buffer behind it).
-    DBuf nf[2][2], nwork, niexp, nxexp, nksel, npairs, nhits, nsp[2], nal[2], ntsum;
-    DBuf *tmp[] = {&nf[0][0], &nf[0][1], &nf[1][0], &nf[1][1], &nwork, &niexp, &nxexp, &nksel, &npairs, &nhits,
-                   &nsp[0], &nsp[1], &nal[0], &nal[1], &ntsum};
+    DBuf nf[2][2], nwork, niexp, nxexp, nksel, npairs, nhits;
+    DBuf *tmp[] = {&nf[0][0], &nf[0][1], &nf[1][0], &nf[1][1], &nwork, &niexp, &nxexp, &nksel, &npairs, &nhits};
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < 2 && e == cudaSuccess; k++)
         for (int set = 0; set < 2 && gf[k] && e == cudaSuccess; set++) e = nf[set][k].reserve(sizeof(int2) * (size_t)nc[k]);
@@ -1768,11 +1624,6 @@ bvhcd_status Front::grow_from(const unsigned *h, cudaStream_t s) {
     if (e == cudaSuccess && (gf[0] || gf[1])) e = nksel.reserve(sizeof(unsigned) * (size_t)(nc[0] + nc[1]));
     if (e == cudaSuccess && gp) e = npairs.reserve(sizeof(int2) * (size_t)npc);
     if (e == cudaSuccess && gp) e = nhits.reserve(sizeof(int2) * (size_t)npc);
-    for (int k = 0; k < 2 && e == cudaSuccess; k++) {
-        if (gp) e = nsp[k].reserve(sizeof(int4) * (size_t)npc);
-        if (e == cudaSuccess && gf[0]) e = nal[k].reserve(sizeof(unsigned) * (size_t)nc[0]);
-    }
-    if (e == cudaSuccess && (gf[0] || gf[1])) e = ntsum.reserve(sizeof(unsigned) * keep_tiles(nc[0], nc[1]));
     // the current front survives in set cur_: copied into its grown buffers
     for (int k = 0; k < 2 && e == cudaSuccess; k++)
         if (gf[k]) e = cudaMemcpyAsync(nf[cur_][k].p, front_[cur_][k].p, sizeof(int2) * (size_t)fcap_[k],
@@ -1798,20 +1649,12 @@ bvhcd_status Front::grow_from(const unsigned *h, cudaStream_t s) {
         swap_in(iexp_, niexp);
     }
     if (gf[1]) swap_in(xexp_, nxexp);
-    if (gf[0] || gf[1]) {
-        swap_in(ksel_, nksel);
-        swap_in(tsum_, ntsum);
-    }
-    for (int k = 0; k < 2; k++) {
-        if (gp) swap_in(kl_sp_[k], nsp[k]);
-        if (gf[0]) swap_in(kl_al_[k], nal[k]);
-    }
+    if (gf[0] || gf[1]) swap_in(ksel_, nksel);
     if (gp) {
         swap_in(pairs_, npairs);
         swap_in(hits_, nhits);
         pcap_ = npc;
     }
-    if (gp || gf[0] || gf[1]) exp_valid_ = false;  // the keep's lists start again
     return BVHCD_OK;
 }
 
@@ -1886,7 +1729,7 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
         // maintain started from had lost entries: start again from a
         // generated front
         if (run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER || run_op == BVHCD_FRONT_RESTRUCTURE ||
-            (ovf & (1u | 2u | 16u | 64u | 128u)))
+            (ovf & (1u | 2u | 16u | 64u)))
             run_op = BVHCD_FRONT_GENERATE;
     }
     last_op_ = run_op;
@@ -2088,8 +1931,7 @@ bvhcd_status Front::pairs(int which, int32_t *out, int64_t cap, int64_t *count, 
                                out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
     FR_TRY(cudaStreamSynchronize(s));
     // lost pairs or hits, or a front (this maintain's input or its traversals) that lost entries
-    if (h[C_OVERFLOW] & (which ? (4u | 8u | 16u | 32u | 64u | 128u) : (4u | 16u | 32u | 64u | 128u)))
-        return BVHCD_CAPACITY_EXCEEDED;
+    if (h[C_OVERFLOW] & (which ? (4u | 8u | 16u | 32u | 64u) : (4u | 16u | 32u | 64u))) return BVHCD_CAPACITY_EXCEEDED;
     return n > cap ? BVHCD_CAPACITY_EXCEEDED : BVHCD_OK;
 }
 

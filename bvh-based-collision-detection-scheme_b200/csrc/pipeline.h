@@ -248,16 +248,14 @@ class Front {
     // sets an odd number of times; log_counted: the log's per-node counts
     // describe the current front (a balance leaves only its begins valid).
     struct HostState {
-        int cur, last_op, exp_epoch, exp_faces, keep_par;
+        int cur, last_op, exp_epoch, exp_faces;
         bool has_front, int_swapped, log_counted, exp_valid;
     };
     HostState host_state() const {
-        return HostState{cur_, last_op_, exp_epoch_, exp_faces_, keep_par_, has_front_, int_swapped_, log_counted_,
-                         exp_valid_};
+        return HostState{cur_, last_op_, exp_epoch_, exp_faces_, has_front_, int_swapped_, log_counted_, exp_valid_};
     }
     void set_host_state(const HostState &h) {
         cur_ = h.cur;
-        keep_par_ = h.keep_par;
         last_op_ = h.last_op;
         exp_epoch_ = h.exp_epoch;
         exp_faces_ = h.exp_faces;
@@ -329,11 +327,6 @@ class Front {
     // the tree's topology changes or new faces arrive; ksel_: the entries a
     // keep selects for a test
     DBuf iexp_, xexp_, ksel_;
-    // the keep's two lists of overlapping entries ({prim, leaf, index, overlap
-    // expiry} external records; internal indices), read from keep_par_ and
-    // written to the other, and the tile summaries of waiting expiries
-    DBuf kl_sp_[2], kl_al_[2], tsum_;
-    int keep_par_ = 0;
     bool exp_valid_ = false, last_keep_sel_ = false;
     int exp_epoch_ = -1, exp_faces_ = -1;
     bool quality_check_ = true;
