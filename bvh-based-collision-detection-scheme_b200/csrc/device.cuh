@@ -77,7 +77,8 @@ enum CounterSlot {
     C_NF_ACC = 19,            // BVH: non-finite input seen by the blocks of the running check
     C_NONFINITE = 20,         // BVH: 1 when the last maintain's input held a NaN or infinite coordinate
     C_NF_DONE = 21,           // BVH: blocks of the build-time finiteness check finished
-    C_NUM = 22
+    C_NARROW_DONE = 22,       // narrow phase: blocks finished (the last one writes the 64-bit counts)
+    C_NUM = 23
 };
 
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }

@@ -533,52 +533,80 @@ __device__ __forceinline__ float box_gap(const float4 &alo, const float4 &ahi, c
 }
 
 // The entries whose expiry the motion has reached, as a list of indices into
-// [0, F_int + F_ext).  The expiries are read as a stream and nothing else of a
-// waiting entry is touched.  A block takes tiles of kSelPer x 256 entries,
-// each warp kSelPer runs of 32: ballots count a warp's picks, a block scan in
-// shared memory places the warps, one atomic per tile reserves its run.
-constexpr int kSelPer = 8;
+// [0, F_int + F_ext), in index order.  The expiries are read as a stream of
+// 16-byte loads and nothing else of a waiting entry is touched.  The two
+// arrays are tiled apart (a tile starts on a 16-byte boundary of its own
+// array): a block takes tiles of 2048 entries, a warp two runs of 128, a lane
+// four consecutive entries per run.  A warp scan places each lane's picks in
+// its warp, a block scan in shared memory places the warps, one atomic per
+// tile reserves the tile's run of the list.
+constexpr int kSelRuns = 2;  // (the list positions below are written for two)
+constexpr unsigned kSelTile = kSelRuns * 4 * kThreads;
 __global__ void __launch_bounds__(kThreads) k_keep_select(FArgs a, unsigned *list, unsigned *count) {
     __shared__ unsigned wsum[kThreads / 32], tbase;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
-    const unsigned total = ni + ne;
+    const unsigned nti = (ni + kSelTile - 1) / kSelTile, ntiles = nti + (ne + kSelTile - 1) / kSelTile;
     const float M = __uint_as_float(*a.motion);
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr unsigned kTile = kSelPer * kThreads;
-    for (unsigned t0 = blockIdx.x * kTile; t0 < total; t0 += gridDim.x * kTile) {
-        float ex[kSelPer];
+    for (unsigned k = blockIdx.x; k < ntiles; k += gridDim.x) {
+        const bool ext = k >= nti;
+        const float *src = ext ? a.xexp_in : a.iexp_in;
+        const unsigned n = ext ? ne : ni;
+        const unsigned qoff = ext ? ni : 0u;
+        const unsigned base = (ext ? k - nti : k) * kSelTile + warp * (kSelRuns * 128u) + lane * 4u;
+        float4 ex[kSelRuns];
 #pragma unroll
-        for (int r = 0; r < kSelPer; r++) {  // every load of the tile in flight at once
-            const unsigned q = t0 + (warp * kSelPer + r) * 32u + lane;
-            ex[r] = q >= total ? 0.f : q < ni ? __ldcs(a.iexp_in + q) : __ldcs(a.xexp_in + (q - ni));
+        for (int r = 0; r < kSelRuns; r++) {  // every load of the tile in flight at once
+            const unsigned i = base + r * 128u;
+            if (i + 4u <= n) {
+                ex[r] = __ldcs(reinterpret_cast<const float4 *>(src + i));
+            } else {
+                ex[r].x = i < n ? __ldcs(src + i) : 0.f;
+                ex[r].y = i + 1u < n ? __ldcs(src + i + 1u) : 0.f;
+                ex[r].z = i + 2u < n ? __ldcs(src + i + 2u) : 0.f;
+                ex[r].w = 0.f;
+            }
         }
-        unsigned m[kSelPer], n = 0;
+        // picks per lane and run (past the end nothing is picked, whatever
+        // the motion: an infinite input coordinate makes it infinite)
+        unsigned bits[kSelRuns], packed = 0;
 #pragma unroll
-        for (int r = 0; r < kSelPer; r++) {
-            // past the end nothing is picked, whatever the motion (an infinite
-            // input coordinate makes it infinite)
-            const unsigned q = t0 + (warp * kSelPer + r) * 32u + lane;
-            m[r] = __ballot_sync(0xffffffffu, q < total && !(M < ex[r]));
-            n += __popc(m[r]);
+        for (int r = 0; r < kSelRuns; r++) {
+            const unsigned i = base + r * 128u;
+            bits[r] = ((i < n && !(M < ex[r].x)) ? 1u : 0u) | ((i + 1u < n && !(M < ex[r].y)) ? 2u : 0u) |
+                      ((i + 2u < n && !(M < ex[r].z)) ? 4u : 0u) | ((i + 3u < n && !(M < ex[r].w)) ? 8u : 0u);
+            packed += (unsigned)__popc(bits[r]) << (16 * r);
         }
-        if (lane == 0) wsum[warp] = n;
+        // both runs' counts scanned at once, one per half-word
+        unsigned incl = packed;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o) incl += u;
+        }
+        const unsigned wtot = __shfl_sync(0xffffffffu, incl, 31);
+        const unsigned excl = incl - packed;
+        if (lane == 0) wsum[warp] = (wtot & 0xffffu) + (wtot >> 16);
         __syncthreads();
         if (threadIdx.x == 0) {
-            unsigned s = 0;
+            unsigned acc = 0;
             for (int w = 0; w < kThreads / 32; w++) {
                 const unsigned c = wsum[w];
-                wsum[w] = s;
-                s += c;
+                wsum[w] = acc;
+                acc += c;
             }
-            tbase = s ? atomicAdd(count, s) : 0u;
+            tbase = acc ? atomicAdd(count, acc) : 0u;
         }
         __syncthreads();
-        unsigned pos = tbase + wsum[warp];
+        unsigned pos[kSelRuns] = {tbase + wsum[warp] + (excl & 0xffffu),
+                                  tbase + wsum[warp] + (wtot & 0xffffu) + (excl >> 16)};
 #pragma unroll
-        for (int r = 0; r < kSelPer; r++) {
-            if ((m[r] >> lane) & 1u) list[pos + __popc(m[r] & ((1u << lane) - 1u))] = t0 + (warp * kSelPer + r) * 32u + lane;
-            pos += __popc(m[r]);
+        for (int r = 0; r < kSelRuns; r++) {
+            const unsigned q = qoff + base + r * 128u;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if ((bits[r] >> j) & 1u) list[pos[r]++] = q + j;
         }
         __syncthreads();  // wsum and tbase are reused by the next tile
     }
@@ -897,6 +925,22 @@ __device__ __forceinline__ v3 vload(const float *v, int i) {
     return {__ldg(p), __ldg(p + 1), __ldg(p + 2)};
 }
 
+// The block of the narrow phase that finishes last writes the valid pair and
+// hit counts as 64-bit values (the counts the C ABI exports) and clears the
+// finish counter for the next launch.
+__device__ __forceinline__ void narrow_done(unsigned *ctr, unsigned cap_pairs, unsigned cap_hits, int64_t *out) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(ctr + C_NARROW_DONE, 1u) == gridDim.x - 1) {
+            __threadfence();
+            out[0] = min(__ldcg(ctr + C_PAIRS_VALID), cap_pairs);
+            out[1] = min(__ldcg(ctr + C_HITS), cap_hits);
+            ctr[C_NARROW_DONE] = 0u;
+        }
+    }
+}
+
 // simpleNarrowPhase (Mine/collision/narrow_phase/narrow_phase.cu:8-24):
 // keeps the pairs whose triangles intersect, as original triangle ids, and
 // counts the valid broad-phase pairs (the pair list has holes).  Without
@@ -908,7 +952,8 @@ template <bool kTest, int kB>
 __global__ void __launch_bounds__(kB) k_narrow(const int2 *__restrict__ pairs, const int4 *__restrict__ psface,
                                                      const float *__restrict__ pverts, const int4 *__restrict__ sface,
                                                      const float *__restrict__ verts, int leaf_first, unsigned *ctr,
-                                                     unsigned cap_pairs, int2 *hits, unsigned cap_hits) {
+                                                     unsigned cap_pairs, int2 *hits, unsigned cap_hits,
+                                                     int64_t *counts64) {
     const unsigned n = min(ctr[C_PAIRS], cap_pairs);
     unsigned valid = 0;
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -925,6 +970,7 @@ __global__ void __launch_bounds__(kB) k_narrow(const int2 *__restrict__ pairs, c
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) valid += __shfl_xor_sync(0xffffffffu, valid, o);
     if ((threadIdx.x & 31) == 0 && valid) atomicAdd(ctr + C_PAIRS_VALID, valid);
+    narrow_done(ctr, cap_pairs, cap_hits, counts64);
 }
 
 // The precision mode's narrow phase: the FP32 test decides where it is
@@ -933,7 +979,8 @@ __global__ void __launch_bounds__(kB) k_narrow(const int2 *__restrict__ pairs, c
 template <bool kUnused, int kB>
 __global__ void __launch_bounds__(kB) k_narrow_prec(const int2 *__restrict__ pairs, const int4 *__restrict__ sface,
                                                      const float *__restrict__ verts, unsigned *ctr,
-                                                     unsigned cap_pairs, int2 *hits, unsigned cap_hits) {
+                                                     unsigned cap_pairs, int2 *hits, unsigned cap_hits,
+                                                     int64_t *counts64) {
     const unsigned n = min(ctr[C_PAIRS], cap_pairs);
     unsigned valid = 0, flagged = 0;
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -965,6 +1012,7 @@ __global__ void __launch_bounds__(kB) k_narrow_prec(const int2 *__restrict__ pai
         if (valid) atomicAdd(ctr + C_PAIRS_VALID, valid);
         if (flagged) atomicAdd(ctr + C_FLAGGED, flagged);
     }
+    narrow_done(ctr, cap_pairs, cap_hits, counts64);
 }
 
 // Contact points of hits (kDist false: midpoint xyz and length of the
@@ -1077,12 +1125,16 @@ __global__ void k_pair_scatter(const int2 *__restrict__ pairs, const int4 *__res
 // The carried bits are joined by bit 6, which says that this maintain's own
 // results (pairs, hits) are incomplete because its input front was.
 constexpr unsigned kFrontLossBits = 1u | 2u | 16u | 32u | 64u;
-__global__ void k_ovf_roll(unsigned *ctr, unsigned carry) {
+// Lane k < C_NUM also zeroes counter k when bit k of `zero` is set (the
+// maintain's first attempt starts its stage and narrow-phase counters here
+// instead of in a memset each).
+__global__ void k_ovf_roll(unsigned *ctr, unsigned carry, unsigned zero) {
     if (threadIdx.x == 0) {
         const unsigned o = ctr[C_OVERFLOW];
         ctr[C_OVF_STICKY] |= o;
         ctr[C_OVERFLOW] = (o & carry) ? ((o & carry) | 64u) : 0u;
     }
+    if (threadIdx.x < C_NUM && ((zero >> threadIdx.x) & 1u)) ctr[threadIdx.x] = 0u;
 }
 
 __global__ void k_counts64(const unsigned *__restrict__ ctr, unsigned cap_pairs, unsigned cap_hits,
@@ -1432,8 +1484,10 @@ bvhcd_status Front::keep(cudaStream_t s) {
     a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
     a.pairs = pairs_.as<int2>();
     a.cap_pairs = (unsigned)pcap_;
-    FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
-    FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
+    if (!zeroed_) {
+        FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
+        FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
+    }
     // expiries: an intra front over FP32 node boxes (an inter front's
     // primitives move with another tree; FP16 boxes move by their rounding too)
     const bool expiries = !inter() && !cfg_.precision && !bvh_->tree().nrec16;
@@ -1445,7 +1499,7 @@ bvhcd_status Front::keep(cudaStream_t s) {
         if (exp_valid_) {
             a.iexp_in = iexp_.as<float>();
             a.xexp_in = xexp_.as<float>();
-            FR_TRY(cudaMemsetAsync(ctr + C_KSEL, 0, sizeof(unsigned), s));
+            if (!zeroed_) FR_TRY(cudaMemsetAsync(ctr + C_KSEL, 0, sizeof(unsigned), s));
             k_keep_select<<<RESIDENT(k_keep_select), kThreads, 0, s>>>(a, ksel_.as<unsigned>(), ctr + C_KSEL);
             note_launch();
             a.ksel = ksel_.as<unsigned>();
@@ -1511,21 +1565,24 @@ bvhcd_status Front::balance(cudaStream_t s) {
 bvhcd_status Front::narrow(cudaStream_t s, bool test) {
     StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_NARROW, s);
     unsigned *ctr = counters();
-    FR_TRY(cudaMemsetAsync(ctr + C_HITS, 0, sizeof(unsigned), s));
-    FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));
+    if (!zeroed_) {
+        FR_TRY(cudaMemsetAsync(ctr + C_HITS, 0, sizeof(unsigned), s));
+        FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));
+        FR_TRY(cudaMemsetAsync(ctr + C_FLAGGED, 0, sizeof(unsigned), s));
+    }
     const Shape sh = shape_[BVHCD_SHAPE_NARROW];
-    FR_TRY(cudaMemsetAsync(ctr + C_FLAGGED, 0, sizeof(unsigned), s));
+    int64_t *c64 = counts64_.as<int64_t>();
     if (test && cfg_.precision)
         LAUNCH_ITEM(k_narrow_prec, true, sh, s, pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
-                    (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_);
+                    (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_, c64);
     else if (test)
         LAUNCH_ITEM(k_narrow, true, sh, s, pairs_.as<int2>(), trav()->tree().sface, trav()->verts(),
                     bvh_->tree().sface, bvh_->verts(), inter() ? 1 : 0, ctr, (unsigned)pcap_, hits_.as<int2>(),
-                    (unsigned)pcap_);
+                    (unsigned)pcap_, c64);
     else
         LAUNCH_ITEM(k_narrow, false, sh, s, pairs_.as<int2>(), trav()->tree().sface, trav()->verts(),
                     bvh_->tree().sface, bvh_->verts(), inter() ? 1 : 0, ctr, (unsigned)pcap_, hits_.as<int2>(),
-                    (unsigned)pcap_);
+                    (unsigned)pcap_, c64);
     return cuda_status(cudaGetLastError());
 }
 
@@ -1703,7 +1760,11 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     unsigned *ctr = counters();
     const bool from_front = run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER ||
                             run_op == BVHCD_FRONT_KEEP || run_op == BVHCD_FRONT_RESTRUCTURE;
-    k_ovf_roll<<<1, 32, 0, s>>>(ctr, from_front ? kFrontLossBits : 0u); note_launch();
+    // the first attempt's keep and narrow-phase counters start at zero here
+    const unsigned zero = (1u << C_HITS) | (1u << C_PAIRS_VALID) | (1u << C_FLAGGED) |
+                          (run_op == BVHCD_FRONT_KEEP ? (1u << C_PAIRS) | (1u << C_WORK) | (1u << C_KSEL) : 0u);
+    static_assert(C_NUM <= 32, "counter slots zeroed by lane");
+    k_ovf_roll<<<1, 32, 0, s>>>(ctr, from_front ? kFrontLossBits : 0u, zero); note_launch();
     if (inter() ? (T < 1 || trav_->T() < 1) : T < 2) {
         FR_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned) * 6, s));
         FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));
@@ -1716,9 +1777,10 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     // emission overflows because outputs go to the other set, except for the
     // reorder scatter, which is checked before it runs.
     for (int attempt = 0; attempt < 4; attempt++) {
+        zeroed_ = attempt == 0;
         st = run(run_op, s);
-        if (st != BVHCD_OK) return st;
-        st = narrow(s, cfg_.narrow_phase != 0);  // without the test it only counts the pairs
+        if (st == BVHCD_OK) st = narrow(s, cfg_.narrow_phase != 0);  // without the test it only counts the pairs
+        zeroed_ = false;
         if (st != BVHCD_OK) return st;
         if (cfg_.auto_grow != 1) break;
         unsigned ovf = 0;
@@ -1733,7 +1795,6 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
             run_op = BVHCD_FRONT_GENERATE;
     }
     last_op_ = run_op;
-    k_counts64<<<1, 32, 0, s>>>(ctr, (unsigned)pcap_, (unsigned)pcap_, counts64_.as<int64_t>()); note_launch();
     FR_TRY(cudaGetLastError());
     return cfg_.auto_grow == 2 ? deferred_snapshot(s) : BVHCD_OK;
 }

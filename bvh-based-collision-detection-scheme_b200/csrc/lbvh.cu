@@ -245,6 +245,17 @@ struct Climb {
     int *uheight;  // node height (leaves 0), for the refit plan
 };
 
+// Arrival at a parent: an exchange with acquire-release semantics at device
+// scope.  The first child to arrive leaves its tagged reference (+1, so that
+// 0 means nobody yet) and stops; the second gets that reference back, and
+// the release by the first makes the data it wrote before (its box, range,
+// chain position, height) visible to the second's loads.
+__device__ __forceinline__ unsigned arrive_exch(unsigned *p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.exch.acq_rel.gpu.b32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Bottom-up construction (buildIntNodes, LBvhBuildKernels.cu:135-172; with
 // kSeg the confined rebuild of restrIntNodes,
 // Mine/collision/lbvh/LBvhRestructureKernels.cu:122-166, over the listed
@@ -253,6 +264,12 @@ struct Climb {
 // indexed by split.  The second thread to reach a node merges the child
 // boxes, records its height and posb = distance from the bottom of its left
 // chain and, at a chain top, the chain length of the chain's leftmost leaf.
+//
+// A thread carries the node it stands for in registers (tagged reference
+// node << 1 or leaf << 1 | 1, box, leaf range, posb, height) and writes the
+// node's results before it arrives at the parent; the second arrival loads
+// only the sibling's box and the two of its fields it needs, all at once.  One
+// exchange per level orders everything (the uflag words start at 0).
 template <bool kSeg>
 __global__ void __launch_bounds__(kThreads) k_climb(int T, int n, const int *__restrict__ leaves,
                                                     const int *__restrict__ seg,
@@ -263,70 +280,66 @@ __global__ void __launch_bounds__(kThreads) k_climb(int T, int n, const int *__r
         const int idx = (kSeg && leaves) ? leaves[k] : k;
         const int sub = kSeg ? seg[idx] : 0;
         int l = idx - 1, r = idx, bd = 0;
-        bool mark;
+        bool right;  // the node is the right child of its parent
         if (kSeg) bd = ((l < 0 || seg[l] != sub) ? 2 : 0) | ((r == T - 1 || seg[r + 1] != sub) ? 1 : 0);
-        if (bd) mark = bd & 1;
-        else mark = (l >= 0) && (metric[l] < metric[r]);
-        int cur = mark ? l : r;
+        if (bd) right = bd & 1;
+        else right = (l >= 0) && (metric[l] < metric[r]);
+        int cur = right ? l : r;  // the parent split
         c.ulpar[idx] = cur;
-        if (mark) {
-            c.urc[cur] = idx;
-            c.ury[cur] = idx;
-            c.clen[idx] = 0;
-            __threadfence();
-            atomicOr(&c.umark[cur], 2u);
-        } else {
-            c.ulc[cur] = idx;
-            c.urx[cur] = idx;
-            __threadfence();
-            atomicOr(&c.umark[cur], 1u);
-        }
-        __threadfence();
-        while (atomicAdd(&c.uflag[cur], 1u) == 1u) {
-            __threadfence();
-            const unsigned m = __ldcg(&c.umark[cur]) & 3u;
-            const int lc = __ldcg(&c.ulc[cur]), rc = __ldcg(&c.urc[cur]);
-            const int rx = __ldcg(&c.urx[cur]), ry = __ldcg(&c.ury[cur]);
-            float4 alo, ahi, blo, bhi;
-            if (m & 1u) { alo = __ldcg(&lrec[2 * lc]); ahi = __ldcg(&lrec[2 * lc + 1]); }
-            else        { alo = __ldcg(&c.ubox[2 * lc]); ahi = __ldcg(&c.ubox[2 * lc + 1]); }
-            if (m & 2u) { blo = __ldcg(&lrec[2 * rc]); bhi = __ldcg(&lrec[2 * rc + 1]); }
-            else        { blo = __ldcg(&c.ubox[2 * rc]); bhi = __ldcg(&c.ubox[2 * rc + 1]); }
-            c.ubox[2 * cur] = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.f);
-            c.ubox[2 * cur + 1] = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.f);
-            const int pb = (m & 1u) ? 0 : __ldcg(&c.posb[lc]) + 1;
+        if (right) c.clen[idx] = 0;
+        int ref = (idx << 1) | 1, rx = idx, ry = idx, pb = 0, h = 0;
+        float4 lo = __ldg(&lrec[2 * idx]), hi = __ldg(&lrec[2 * idx + 1]);
+        while (true) {
+            const unsigned old = arrive_exch(&c.uflag[cur], (unsigned)ref + 1u);
+            if (old == 0u) break;  // first arrival: the sibling's thread goes on
+            const int sref = (int)old - 1, sib = sref >> 1;
+            float4 slo, shi;
+            int sbound = sib, spb = 0, sh = 0;
+            if (sref & 1) {
+                slo = __ldcg(&lrec[2 * sib]);
+                shi = __ldcg(&lrec[2 * sib + 1]);
+            } else {
+                slo = __ldcg(&c.ubox[2 * sib]);
+                shi = __ldcg(&c.ubox[2 * sib + 1]);
+                sbound = right ? __ldcg(&c.urx[sib]) : __ldcg(&c.ury[sib]);
+                spb = __ldcg(&c.posb[sib]);
+                sh = __ldcg(&c.uheight[sib]);
+            }
+            const int lref = right ? sref : ref, rref = right ? ref : sref;
+            const unsigned m = (unsigned)(lref & 1) | ((unsigned)(rref & 1) << 1);
+            const int nrx = right ? sbound : rx, nry = right ? ry : sbound;
+            lo = make_float4(fminf(lo.x, slo.x), fminf(lo.y, slo.y), fminf(lo.z, slo.z), 0.f);
+            hi = make_float4(fmaxf(hi.x, shi.x), fmaxf(hi.y, shi.y), fmaxf(hi.z, shi.z), 0.f);
+            pb = (m & 1u) ? 0 : (right ? spb : pb) + 1;
+            h = 1 + max(h, sh);
+            c.ulc[cur] = lref >> 1;
+            c.urc[cur] = rref >> 1;
+            c.urx[cur] = nrx;
+            c.ury[cur] = nry;
+            c.ubox[2 * cur] = lo;
+            c.ubox[2 * cur + 1] = hi;
             c.posb[cur] = pb;
-            c.uheight[cur] = 1 + max((m & 1u) ? 0 : __ldcg(&c.uheight[lc]), (m & 2u) ? 0 : __ldcg(&c.uheight[rc]));
+            c.uheight[cur] = h;
+            rx = nrx;
+            ry = nry;
             l = rx - 1;
             r = ry;
             if (kSeg) bd = ((l < 0 || seg[l] != sub) ? 2 : 0) | ((r == T - 1 || seg[r + 1] != sub) ? 1 : 0);
             const bool is_root = kSeg ? (bd == 3) : (l + 1 == 0 && r == T - 1);
             if (is_root) {
                 c.upar[cur] = -1;
-                const bool right = (kSeg && prev_topo) ? ((prev_topo[sub].w & 4) != 0) : false;
-                c.umark[cur] = m | (right ? 4u : 0u);
+                const bool rflag = (kSeg && prev_topo) ? ((prev_topo[sub].w & 4) != 0) : false;
+                c.umark[cur] = m | (rflag ? 4u : 0u);
                 c.clen[rx] = pb + 1;
                 break;
             }
-            if (bd) mark = bd & 1;
-            else mark = (l >= 0) && (metric[l] < metric[r]);
-            const int par = mark ? l : r;
+            if (bd) right = bd & 1;
+            else right = (l >= 0) && (metric[l] < metric[r]);
+            const int par = right ? l : r;
             c.upar[cur] = par;
-            if (mark) {
-                c.urc[par] = cur;
-                c.ury[par] = r;
-                c.umark[cur] = m | 4u;
-                c.clen[rx] = pb + 1;
-                __threadfence();
-                atomicAnd(&c.umark[par], ~2u);
-            } else {
-                c.ulc[par] = cur;
-                c.urx[par] = l + 1;
-                c.umark[cur] = m;
-                __threadfence();
-                atomicAnd(&c.umark[par], ~1u);
-            }
-            __threadfence();
+            c.umark[cur] = m | (right ? 4u : 0u);
+            if (right) c.clen[rx] = pb + 1;
+            ref = cur << 1;
             cur = par;
         }
     }

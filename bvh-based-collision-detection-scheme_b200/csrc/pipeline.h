@@ -328,6 +328,9 @@ class Front {
     // keep selects for a test
     DBuf iexp_, xexp_, ksel_;
     bool exp_valid_ = false, last_keep_sel_ = false;
+    // the running stage and narrow phase find their counters zeroed already
+    // (the maintain's first attempt zeroes them in its prologue)
+    bool zeroed_ = false;
     int exp_epoch_ = -1, exp_faces_ = -1;
     bool quality_check_ = true;
     DBuf front_[2][2];  // [set][0 int, 1 ext] int2 entries

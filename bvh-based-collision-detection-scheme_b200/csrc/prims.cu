@@ -187,6 +187,132 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const K *keys, co
     }
 }
 
+// All passes in one cooperative launch (one CTA per SM, every CTA resident):
+// CTA b owns the b-th slice of the keys; per pass it counts its slice's
+// digits, a grid barrier, then every CTA reads all slices' counts (the
+// digit's global offset plus the counts of the slices before its own), ranks
+// its keys stably (rounds of 1024 in index order, warp match ranks, per-warp
+// counts) and scatters them; a grid barrier ends the pass.  No look-back and
+// no launch per step: 2 barriers per pass.
+constexpr int kCoopThreads = 1024;
+constexpr int kCoopWarps = kCoopThreads / 32;
+
+// Grid barrier k (0, 1, ...) of the launch: the arrival counter (zeroed before
+// the launch) reaches (k + 1) x gridDim.x.  The wait is bounded: a CTA that
+// gives up raises *err and goes on (the sort's result is then not used).
+__device__ __forceinline__ void coop_barrier(unsigned *bar, unsigned k, unsigned *err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        const unsigned goal = (k + 1u) * gridDim.x;
+        unsigned v = 0;
+        for (long long it = 0; it < (1ll << 26); it++) {
+            asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+            if (v >= goal) break;
+        }
+        if (v < goal) atomicOr(err, 1u);
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kCoopThreads, 1) k_sort_coop(unsigned *keys, int *vals, unsigned *keys_alt,
+                                                                int *vals_alt, int n, int passes,
+                                                                unsigned *counts, unsigned *bar, unsigned *err) {
+    __shared__ unsigned s_cnt[256], s_base[256], s_run[256];
+    __shared__ unsigned short s_w[kCoopWarps][256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int per = (n + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int lo = min(n, (int)blockIdx.x * per), hi = min(n, lo + per);
+    unsigned *ks = keys, *kd = keys_alt;
+    int *vs = vals, *vd = vals_alt;
+    unsigned k = 0;  // barriers passed
+    for (int p = 0; p < passes; p++, ks = (p & 1) ? keys_alt : keys, kd = (p & 1) ? keys : keys_alt,
+             vs = (p & 1) ? vals_alt : vals, vd = (p & 1) ? vals : vals_alt) {
+        const int shift = 8 * p;
+        if (threadIdx.x < 256) s_cnt[threadIdx.x] = 0u;
+        __syncthreads();
+        for (int i = lo + threadIdx.x; i < hi; i += kCoopThreads) atomicAdd(&s_cnt[(__ldcg(ks + i) >> shift) & 255u], 1u);
+        __syncthreads();
+        if (threadIdx.x < 256) __stcg(counts + (size_t)blockIdx.x * 256 + threadIdx.x, s_cnt[threadIdx.x]);
+        coop_barrier(bar, k++, err);
+        // digit d: its global offset (all slices' counts of smaller digits)
+        // and the counts of the slices before this one; four threads per
+        // digit, each over every fourth slice
+        if (threadIdx.x < 256) {
+            s_cnt[threadIdx.x] = 0u;
+            s_run[threadIdx.x] = 0u;
+        }
+        __syncthreads();
+        {
+            const unsigned d = threadIdx.x & 255u;
+            unsigned tot = 0, before = 0;
+#pragma unroll 8
+            for (unsigned b = threadIdx.x >> 8; b < gridDim.x; b += kCoopThreads / 256) {
+                const unsigned c = __ldcg(counts + (size_t)b * 256 + d);
+                tot += c;
+                before += b < blockIdx.x ? c : 0u;
+            }
+            atomicAdd(&s_cnt[d], tot);
+            atomicAdd(&s_run[d], before);
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {  // exclusive scan of the 256 digit totals by one warp
+            unsigned v[8], acc = 0;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                v[j] = s_cnt[lane * 8 + j];
+                acc += v[j];
+            }
+            unsigned incl = acc;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned u = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += u;
+            }
+            unsigned ex = incl - acc;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                s_base[lane * 8 + j] = ex;
+                ex += v[j];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 256) s_run[threadIdx.x] += s_base[threadIdx.x];
+        // stable ranks, 1024 keys per round in index order
+        for (int r0 = lo; r0 < hi; r0 += kCoopThreads) {
+            for (int x = threadIdx.x; x < kCoopWarps * 256; x += kCoopThreads) (&s_w[0][0])[x] = 0;
+            __syncthreads();
+            const int i = r0 + threadIdx.x;
+            const bool valid = i < hi;
+            const unsigned key = valid ? __ldcg(ks + i) : 0u;
+            const int val = valid ? __ldcg(vs + i) : 0;
+            const unsigned d = valid ? ((key >> shift) & 255u) : 256u;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const unsigned lrank = __popc(peers & lt);
+            if (valid && lrank == 0) s_w[w][d] = (unsigned short)__popc(peers);
+            __syncthreads();
+            if (valid) {
+                unsigned pos = s_run[d] + lrank;
+                for (int q = 0; q < w; q++) pos += s_w[q][d];
+                kd[pos] = key;
+                vd[pos] = val;
+            }
+            __syncthreads();
+            if (threadIdx.x < 256) {
+                unsigned add = 0;
+#pragma unroll 8
+                for (int q = 0; q < kCoopWarps; q++) add += s_w[q][threadIdx.x];
+                s_run[threadIdx.x] += add;
+            }
+            __syncthreads();  // s_w is cleared by the next round
+        }
+        coop_barrier(bar, k++, err);
+    }
+}
+
 template <typename K>
 cudaError_t sort_impl(K *keys, int *vals, K *keys_alt, int *vals_alt, int64_t n, int key_bits,
                       void *scratch, cudaStream_t s) {
@@ -214,6 +340,44 @@ cudaError_t sort_impl(K *keys, int *vals, K *keys_alt, int *vals_alt, int64_t n,
     return cudaGetLastError();
 }
 
+// The cooperative sort of 32-bit keys when every CTA fits at once and the
+// scratch holds the per-slice counts (n at least 1024 keys per SM, so each
+// slice is at least one round); false: use the launch-per-step sort.  Not
+// inside a stream capture.
+bool sort_coop_u32(unsigned *keys, int *vals, unsigned *keys_alt, int *vals_alt, int64_t n, int key_bits,
+                   void *scratch, size_t scratch_bytes, cudaStream_t s, cudaError_t *err_out) {
+    static int sms = -1;
+    if (sms < 0) {
+        int dev = 0, coop = 0, nb = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sort_coop, kCoopThreads, 0);
+        if (!coop || nb < 1) sms = 0;
+    }
+    if (sms <= 0 || n < (int64_t)sms * kCoopThreads || n > INT32_MAX) return false;
+    if ((size_t)sms * 256 * sizeof(unsigned) + 256 > scratch_bytes) return false;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+    unsigned *counts = reinterpret_cast<unsigned *>(scratch);
+    unsigned *bar = counts + (size_t)sms * 256;  // barrier counter, then the timeout flag
+    cudaError_t e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s);
+    if (e == cudaSuccess) {
+        int nn = (int)n, passes = (key_bits + 7) / 8;
+        unsigned *errp = bar + 1;
+        void *args[] = {&keys, &vals, &keys_alt, &vals_alt, &nn, &passes, &counts, &bar, &errp};
+        e = cudaLaunchCooperativeKernel((const void *)k_sort_coop, dim3(sms), dim3(kCoopThreads), args, 0, s);
+        note_launch();
+        if (e == cudaSuccess && (passes & 1)) {
+            e = cudaMemcpyAsync(keys, keys_alt, sizeof(unsigned) * (size_t)n, cudaMemcpyDeviceToDevice, s);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(vals, vals_alt, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s);
+        }
+    }
+    *err_out = e;
+    return true;
+}
+
 }  // namespace
 
 size_t scan_scratch_bytes(int64_t n) {
@@ -237,6 +401,8 @@ size_t sort_scratch_bytes(int64_t n) {
 
 cudaError_t radix_sort_u32(unsigned *keys, int *vals, unsigned *keys_alt, int *vals_alt, int64_t n,
                            int key_bits, void *scratch, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    if (sort_coop_u32(keys, vals, keys_alt, vals_alt, n, key_bits, scratch, sort_scratch_bytes(n), s, &e)) return e;
     return sort_impl<unsigned>(keys, vals, keys_alt, vals_alt, n, key_bits, scratch, s);
 }
 cudaError_t radix_sort_u64(unsigned long long *keys, int *vals, unsigned long long *keys_alt,
