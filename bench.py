@@ -74,6 +74,12 @@ class ClockSampler:
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi's start-up (driver attach, first query) can hold the
+            # launch path for milliseconds: the timed region starts after its
+            # first sample has arrived
+            t_end = time.perf_counter() + 5.0
+            while not self.rows and time.perf_counter() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
         except FileNotFoundError:
             self.proc = None
         return self

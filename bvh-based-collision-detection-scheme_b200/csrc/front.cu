@@ -1307,9 +1307,7 @@ static cudaError_t log_clear(const FrontLog &l, int T, cudaStream_t s) {
 
 // FlOrderLog::prepare (FlOrderLog.cu:7-12): begins from counts
 static cudaError_t log_prepare(const FrontLog &l, int T, void *scratch, cudaStream_t s) {
-    cudaError_t e = scan_u32(l.intcnt, l.intbeg, T + 1, false, nullptr, scratch, s);
-    if (e == cudaSuccess) e = scan_u32(l.extcnt, l.extbeg, T + 1, false, nullptr, scratch, s);
-    return e;
+    return scan2_u32(l.intcnt, l.intbeg, l.extcnt, l.extbeg, T + 1, scratch, s);
 }
 
 bvhcd_status Front::reorder(cudaStream_t s) {

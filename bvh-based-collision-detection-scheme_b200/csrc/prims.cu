@@ -44,6 +44,26 @@ __device__ __forceinline__ T block_excl_scan(T v, T &total) {
     return r;
 }
 
+// Grid barrier k (0, 1, ...) of the launch: the arrival counter (zeroed before
+// the launch) reaches (k + 1) x gridDim.x.  The wait is bounded: a CTA that
+// gives up raises *err and goes on (the sort's result is then not used).
+__device__ __forceinline__ void coop_barrier(unsigned *bar, unsigned k, unsigned *err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        const unsigned goal = (k + 1u) * gridDim.x;
+        unsigned v = 0;
+        for (long long it = 0; it < (1ll << 26); it++) {
+            asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+            if (v >= goal) break;
+        }
+        if (v < goal) atomicOr(err, 1u);
+        __threadfence();
+    }
+    __syncthreads();
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kScanThreads) k_tile_sums(const T *in, int64_t n, T *sums) {
     int64_t base = (int64_t)blockIdx.x * kScanTile;
@@ -196,26 +216,6 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const K *keys, co
 // no launch per step: 2 barriers per pass.
 constexpr int kCoopThreads = 1024;
 constexpr int kCoopWarps = kCoopThreads / 32;
-
-// Grid barrier k (0, 1, ...) of the launch: the arrival counter (zeroed before
-// the launch) reaches (k + 1) x gridDim.x.  The wait is bounded: a CTA that
-// gives up raises *err and goes on (the sort's result is then not used).
-__device__ __forceinline__ void coop_barrier(unsigned *bar, unsigned k, unsigned *err) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(bar, 1u);
-        const unsigned goal = (k + 1u) * gridDim.x;
-        unsigned v = 0;
-        for (long long it = 0; it < (1ll << 26); it++) {
-            asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
-            if (v >= goal) break;
-        }
-        if (v < goal) atomicOr(err, 1u);
-        __threadfence();
-    }
-    __syncthreads();
-}
 
 __global__ void __launch_bounds__(kCoopThreads, 1) k_sort_coop(unsigned *keys, int *vals, unsigned *keys_alt,
                                                                 int *vals_alt, int n, int passes,
@@ -378,6 +378,127 @@ bool sort_coop_u32(unsigned *keys, int *vals, unsigned *keys_alt, int *vals_alt,
     return true;
 }
 
+// One or two scans in one cooperative launch: every CTA sums its tiles
+// (2048 values), a grid barrier, then every CTA adds the sums of the tiles
+// before its own (one load per thread and a block reduction) and writes its
+// tiles' scan.  Replaces the three launches of the tile-sum scan.
+struct CoopScan {
+    const unsigned *in;
+    unsigned *out;
+    int64_t n;
+    unsigned *total;  // device, may be null
+    int inclusive;
+    unsigned tiles;   // ceil(n / kScanTile)
+};
+
+template <int NT>
+__device__ __forceinline__ unsigned block_sum(unsigned v) {
+    __shared__ unsigned s_w[NT / 32];
+    v = warp_incl_scan(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 31) s_w[w] = v;
+    __syncthreads();
+    unsigned t = 0;
+#pragma unroll
+    for (int q = 0; q < NT / 32; q++) t += s_w[q];
+    __syncthreads();
+    return t;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_coop(CoopScan a, CoopScan b, unsigned *sums, unsigned *bar,
+                                                             unsigned *err) {
+    const unsigned ntot = a.tiles + b.tiles;
+    for (unsigned t = blockIdx.x; t < ntot; t += gridDim.x) {
+        const CoopScan &j = t < a.tiles ? a : b;
+        const int64_t base = (int64_t)(t < a.tiles ? t : t - a.tiles) * kScanTile;
+        unsigned acc = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            const int64_t i = base + k * kScanThreads + threadIdx.x;
+            if (i < j.n) acc += j.in[i];
+        }
+        acc = block_sum<kScanThreads>(acc);
+        if (threadIdx.x == 0) __stcg(sums + t, acc);
+    }
+    coop_barrier(bar, 0u, err);
+    for (unsigned t = blockIdx.x; t < ntot; t += gridDim.x) {
+        const bool first = t < a.tiles;
+        const CoopScan &j = first ? a : b;
+        const unsigned t0 = first ? 0u : a.tiles, lt = t - t0;
+        // the sums of this job's tiles before this one
+        unsigned before = 0;
+        for (unsigned q = threadIdx.x; q < lt; q += kScanThreads) before += __ldcg(sums + t0 + q);
+        before = block_sum<kScanThreads>(before);
+        const int64_t base = (int64_t)lt * kScanTile;
+        __shared__ unsigned sv[kScanTile];
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            const int64_t i = base + k * kScanThreads + threadIdx.x;
+            sv[k * kScanThreads + threadIdx.x] = i < j.n ? j.in[i] : 0u;
+        }
+        __syncthreads();
+        unsigned v[kScanItems], acc = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            v[k] = sv[threadIdx.x * kScanItems + k];
+            acc += v[k];
+        }
+        unsigned tot;
+        unsigned ex = block_excl_scan<unsigned, kScanThreads>(acc, tot) + before;
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            sv[threadIdx.x * kScanItems + k] = j.inclusive ? ex + v[k] : ex;
+            ex += v[k];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            const int64_t i = base + k * kScanThreads + threadIdx.x;
+            if (i < j.n) j.out[i] = sv[k * kScanThreads + threadIdx.x];
+        }
+        if (threadIdx.x == 0 && j.total && lt + 1 == j.tiles) *j.total = before + tot;
+        __syncthreads();  // sv is the next tile's
+    }
+}
+
+// The cooperative form of one or two scans when it applies (not inside a
+// stream capture; every CTA resident; the scratch of a scan of the longer
+// input holds both jobs' tile sums); false: use the three-launch form.
+bool scan_coop(const CoopScan &a, const CoopScan &b, void *scratch, size_t scratch_bytes, cudaStream_t s,
+               cudaError_t *err_out) {
+    static int resident = -1;
+    if (resident < 0) {
+        int dev = 0, coop = 0, nb = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_scan_coop, kScanThreads, 0);
+        resident = coop ? nb * sms : 0;
+    }
+    const unsigned ntot = a.tiles + b.tiles;
+    if (resident <= 0 || ntot < 2) return false;
+    if ((size_t)ntot * sizeof(unsigned) + 16 > scratch_bytes) return false;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+    unsigned *sums = reinterpret_cast<unsigned *>(scratch);
+    unsigned *bar = sums + ntot;  // barrier counter, then the timeout flag
+    cudaError_t e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s);
+    if (e == cudaSuccess) {
+        CoopScan ja = a, jb = b;
+        unsigned *errp = bar + 1;
+        void *args[] = {&ja, &jb, &sums, &bar, &errp};
+        const unsigned grid = ntot < (unsigned)resident ? ntot : (unsigned)resident;
+        e = cudaLaunchCooperativeKernel((const void *)k_scan_coop, dim3(grid), dim3(kScanThreads), args, 0, s);
+        note_launch();
+    }
+    *err_out = e;
+    return true;
+}
+
+inline CoopScan coop_job(const unsigned *in, unsigned *out, int64_t n, bool inclusive, unsigned *total) {
+    return CoopScan{in, out, n, total, inclusive ? 1 : 0, (unsigned)((n + kScanTile - 1) / kScanTile)};
+}
+
 }  // namespace
 
 size_t scan_scratch_bytes(int64_t n) {
@@ -387,11 +508,29 @@ size_t scan_scratch_bytes(int64_t n) {
 
 cudaError_t scan_u32(const unsigned *in, unsigned *out, int64_t n, bool inclusive, unsigned *total,
                      void *scratch, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    if (n > 0 && n <= INT32_MAX &&
+        scan_coop(coop_job(in, out, n, inclusive, total), coop_job(nullptr, nullptr, 0, false, nullptr), scratch,
+                  scan_scratch_bytes(n), s, &e))
+        return e;
     return scan_impl<unsigned>(in, out, n, inclusive, total, scratch, s);
 }
+// (two's complement: the sums of int32 values are those of their bit patterns)
 cudaError_t scan_i32(const int *in, int *out, int64_t n, bool inclusive, int *total, void *scratch,
                      cudaStream_t s) {
-    return scan_impl<int>(in, out, n, inclusive, total, scratch, s);
+    return scan_u32(reinterpret_cast<const unsigned *>(in), reinterpret_cast<unsigned *>(out), n, inclusive,
+                    reinterpret_cast<unsigned *>(total), scratch, s);
+}
+cudaError_t scan2_u32(const unsigned *in_a, unsigned *out_a, const unsigned *in_b, unsigned *out_b, int64_t n,
+                      void *scratch, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    if (n > 0 && n <= INT32_MAX &&
+        scan_coop(coop_job(in_a, out_a, n, false, nullptr), coop_job(in_b, out_b, n, false, nullptr), scratch,
+                  scan_scratch_bytes(n), s, &e))
+        return e;
+    e = scan_impl<unsigned>(in_a, out_a, n, false, nullptr, scratch, s);
+    if (e == cudaSuccess) e = scan_impl<unsigned>(in_b, out_b, n, false, nullptr, scratch, s);
+    return e;
 }
 
 size_t sort_scratch_bytes(int64_t n) {

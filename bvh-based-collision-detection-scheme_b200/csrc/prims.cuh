@@ -18,6 +18,9 @@ cudaError_t scan_u32(const unsigned *in, unsigned *out, int64_t n, bool inclusiv
                      void *scratch, cudaStream_t s);
 cudaError_t scan_i32(const int *in, int *out, int64_t n, bool inclusive, int *total, void *scratch,
                      cudaStream_t s);
+// Two exclusive scans of n elements each (scratch as for one scan of n).
+cudaError_t scan2_u32(const unsigned *in_a, unsigned *out_a, const unsigned *in_b, unsigned *out_b, int64_t n,
+                      void *scratch, cudaStream_t s);
 
 // Stable LSD radix sort of (key, value) pairs; keys_alt / vals_alt are
 // ping-pong buffers of the same size.  Sorts bits [0, key_bits).  The sorted
