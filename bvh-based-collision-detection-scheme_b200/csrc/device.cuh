@@ -81,6 +81,15 @@ enum CounterSlot {
     C_NUM = 23
 };
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialisation may start while the previous kernel of the stream runs; it
+// waits here before it touches anything that kernel (or one before it)
+// writes, and every such kernel waits before it ends, so completion stays in
+// stream order.  Without the launch attribute the wait returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// lets the next kernel (launched with the attribute) start before this one ends
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
 __device__ __forceinline__ float4 ldcg4(const float4 *p) { return __ldcg(p); }
 // A 32-byte record {lo, hi} (32-byte aligned, read-only for the kernel's

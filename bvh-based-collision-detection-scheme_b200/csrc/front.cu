@@ -8,6 +8,7 @@
 // capacity before writing.
 #include <climits>
 #include <cstdlib>
+#include <utility>
 
 #include <cuda_fp16.h>
 
@@ -385,6 +386,7 @@ __device__ __forceinline__ void take_ents(Batch<kU> &dst, const Batch<kU> &src) 
 // BvttFrontReorderKernels.cu:43-62, without).
 template <bool kFront, int kB>
 __global__ void __launch_bounds__(kB) k_sprout(FArgs a) {
+    pdl_wait();
     Em em;
     const unsigned n = min(a.ctr[C_WORK], a.cap_work);
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -407,6 +409,7 @@ __global__ void __launch_bounds__(kB) k_sprout(FArgs a) {
 // non-overlapping entries are pruned here, overlapping ones go to k_sprout<true>.
 template <int kU, int kB>
 __global__ void __launch_bounds__(kB) k_maintain_int_scan(FArgs a) {
+    pdl_wait();
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const Spread sp = spread<kScanMinPer>(ni);
@@ -433,6 +436,7 @@ __global__ void __launch_bounds__(kB) k_maintain_int_scan(FArgs a) {
 // maintainExtLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:60-93)
 template <int kU, int kB>
 __global__ void __launch_bounds__(kB) k_maintain_ext(FArgs a) {
+    pdl_wait();
     Em em;
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     const Spread sp = spread<kScanMinPer>(ne);
@@ -482,6 +486,7 @@ __global__ void __launch_bounds__(kB) k_maintain_ext(FArgs a) {
 // k_sprout<true> traverses from R itself; the others are dropped.
 template <int kU, int kB>
 __global__ void __launch_bounds__(kB) k_restr_scan(FArgs a) {
+    pdl_wait();
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
@@ -547,17 +552,15 @@ __global__ void __launch_bounds__(kThreads) k_keep_select(FArgs a, unsigned *lis
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
     const unsigned nti = (ni + kSelTile - 1) / kSelTile, ntiles = nti + (ne + kSelTile - 1) / kSelTile;
-    const float M = __uint_as_float(*a.motion);
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (unsigned k = blockIdx.x; k < ntiles; k += gridDim.x) {
+    float4 ex[kSelRuns];
+    auto load_tile = [&](unsigned k) {  // every load of the tile in flight at once
         const bool ext = k >= nti;
         const float *src = ext ? a.xexp_in : a.iexp_in;
         const unsigned n = ext ? ne : ni;
-        const unsigned qoff = ext ? ni : 0u;
         const unsigned base = (ext ? k - nti : k) * kSelTile + warp * (kSelRuns * 128u) + lane * 4u;
-        float4 ex[kSelRuns];
 #pragma unroll
-        for (int r = 0; r < kSelRuns; r++) {  // every load of the tile in flight at once
+        for (int r = 0; r < kSelRuns; r++) {
             const unsigned i = base + r * 128u;
             if (i + 4u <= n) {
                 ex[r] = __ldcs(reinterpret_cast<const float4 *>(src + i));
@@ -568,6 +571,19 @@ __global__ void __launch_bounds__(kThreads) k_keep_select(FArgs a, unsigned *lis
                 ex[r].w = 0.f;
             }
         }
+    };
+    // the front sizes and the expiries come from earlier maintains: the first
+    // tile is loaded before the wait for the kernels just before (the refit
+    // that accumulates the motion, the prologue that zeroes the count)
+    if (blockIdx.x < ntiles) load_tile(blockIdx.x);
+    pdl_wait();
+    const float M = __uint_as_float(*a.motion);
+    for (unsigned k = blockIdx.x; k < ntiles; k += gridDim.x) {
+        const bool ext = k >= nti;
+        const unsigned n = ext ? ne : ni;
+        const unsigned qoff = ext ? ni : 0u;
+        const unsigned base = (ext ? k - nti : k) * kSelTile + warp * (kSelRuns * 128u) + lane * 4u;
+        if (k != blockIdx.x) load_tile(k);
         // picks per lane and run (past the end nothing is picked, whatever
         // the motion: an infinite input coordinate makes it infinite)
         unsigned bits[kSelRuns], packed = 0;
@@ -633,6 +649,7 @@ __device__ __forceinline__ void put_dense(int2 *buf, unsigned *ctr, unsigned cap
 // expiry.
 template <int kU, int kB>
 __global__ void __launch_bounds__(kB) k_keep_scan(FArgs a) {
+    pdl_wait();
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
@@ -682,6 +699,7 @@ __global__ void __launch_bounds__(kB) k_keep_scan(FArgs a) {
 // and are traversed by k_sprout<false>.
 template <int kU, int kB>
 __global__ void __launch_bounds__(kB) k_balance_scan(FArgs a) {
+    pdl_wait();
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
@@ -954,6 +972,7 @@ __global__ void __launch_bounds__(kB) k_narrow(const int2 *__restrict__ pairs, c
                                                      const float *__restrict__ verts, int leaf_first, unsigned *ctr,
                                                      unsigned cap_pairs, int2 *hits, unsigned cap_hits,
                                                      int64_t *counts64) {
+    pdl_wait();
     const unsigned n = min(ctr[C_PAIRS], cap_pairs);
     unsigned valid = 0;
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -981,6 +1000,7 @@ __global__ void __launch_bounds__(kB) k_narrow_prec(const int2 *__restrict__ pai
                                                      const float *__restrict__ verts, unsigned *ctr,
                                                      unsigned cap_pairs, int2 *hits, unsigned cap_hits,
                                                      int64_t *counts64) {
+    pdl_wait();
     const unsigned n = min(ctr[C_PAIRS], cap_pairs);
     unsigned valid = 0, flagged = 0;
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -1129,6 +1149,10 @@ constexpr unsigned kFrontLossBits = 1u | 2u | 16u | 32u | 64u;
 // maintain's first attempt starts its stage and narrow-phase counters here
 // instead of in a memset each).
 __global__ void k_ovf_roll(unsigned *ctr, unsigned carry, unsigned zero) {
+    // the next kernel may start at once (it waits for this one); this one
+    // waits for the kernel before it, so completion stays in order
+    pdl_release();
+    pdl_wait();
     if (threadIdx.x == 0) {
         const unsigned o = ctr[C_OVERFLOW];
         ctr[C_OVF_STICKY] |= o;
@@ -1155,6 +1179,28 @@ unsigned resident_blocks(const void *kernel, int block = kThreads) {
 
 }  // namespace
 
+// A launch, with programmatic stream serialisation when `pdl` (the kernel
+// then waits with pdl_wait before it reads what earlier kernels wrote).
+template <typename... KArgs, typename... Args>
+void launch_k(bool pdl, void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+              Args &&...args) {
+    if (!pdl) {
+        k<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+
 // One resident wave of blocks (blocks per SM at this kernel's occupancy x SM
 // count): the grid-stride kernels then run without a tail wave.
 #define RESIDENT(K) ([]() { static unsigned g_ = 0; if (!g_) g_ = resident_blocks((const void *)(K)); return g_; }())
@@ -1162,7 +1208,7 @@ unsigned resident_blocks(const void *kernel, int block = kThreads) {
     ([]() { static unsigned g_ = 0; if (!g_) g_ = resident_blocks((const void *)(K), B); return g_; }())
 // Front scans in a launch shape: entries per thread step (1, 2, 4) x threads
 // per block (128, 256, 512).
-#define SCAN_AT(KERNEL, U, B, S, ARG) KERNEL<U, B><<<RESIDENT_B((KERNEL<U, B>), B), B, 0, S>>>(ARG)
+#define SCAN_AT(KERNEL, U, B, S, ARG) launch_k(pdl_, KERNEL<U, B>, RESIDENT_B((KERNEL<U, B>), B), B, 0, S, ARG)
 #define SCAN_U(KERNEL, U, B, S, ARG)                 \
     do {                                             \
         if ((U) == 1) SCAN_AT(KERNEL, 1, B, S, ARG); \
@@ -1177,7 +1223,7 @@ unsigned resident_blocks(const void *kernel, int block = kThreads) {
         note_launch();                                             \
     } while (0)
 // Per-item kernels (sprout, narrow phase) in a block size.
-#define ITEM_AT(KERNEL, F, B, S, ...) KERNEL<F, B><<<RESIDENT_B((KERNEL<F, B>), B), B, 0, S>>>(__VA_ARGS__)
+#define ITEM_AT(KERNEL, F, B, S, ...) launch_k(pdl_, KERNEL<F, B>, RESIDENT_B((KERNEL<F, B>), B), B, 0, S, __VA_ARGS__)
 #define LAUNCH_ITEM(KERNEL, F, SH, S, ...)                                \
     do {                                                                  \
         if ((SH).b == 128) ITEM_AT(KERNEL, F, 128, S, __VA_ARGS__);         \
@@ -1498,7 +1544,8 @@ bvhcd_status Front::keep(cudaStream_t s) {
             a.iexp_in = iexp_.as<float>();
             a.xexp_in = xexp_.as<float>();
             if (!zeroed_) FR_TRY(cudaMemsetAsync(ctr + C_KSEL, 0, sizeof(unsigned), s));
-            k_keep_select<<<RESIDENT(k_keep_select), kThreads, 0, s>>>(a, ksel_.as<unsigned>(), ctr + C_KSEL);
+            launch_k(pdl_, k_keep_select, RESIDENT(k_keep_select), kThreads, 0, s, a, ksel_.as<unsigned>(),
+                     ctr + C_KSEL);
             note_launch();
             a.ksel = ksel_.as<unsigned>();
         }
@@ -1762,7 +1809,16 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     const unsigned zero = (1u << C_HITS) | (1u << C_PAIRS_VALID) | (1u << C_FLAGGED) |
                           (run_op == BVHCD_FRONT_KEEP ? (1u << C_PAIRS) | (1u << C_WORK) | (1u << C_KSEL) : 0u);
     static_assert(C_NUM <= 32, "counter slots zeroed by lane");
-    k_ovf_roll<<<1, 32, 0, s>>>(ctr, from_front ? kFrontLossBits : 0u, zero); note_launch();
+    // kernels of this maintain may start before the one before them ends
+    // (programmatic dependent launch), except inside a stream capture
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    FR_TRY(cudaStreamIsCapturing(s, &cs));
+    struct PdlScope {
+        bool &on;
+        ~PdlScope() { on = false; }
+    } pdl_scope{pdl_};
+    pdl_ = cs == cudaStreamCaptureStatusNone;
+    launch_k(pdl_, k_ovf_roll, 1u, 32u, 0, s, ctr, from_front ? kFrontLossBits : 0u, zero); note_launch();
     if (inter() ? (T < 1 || trav_->T() < 1) : T < 2) {
         FR_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned) * 6, s));
         FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));

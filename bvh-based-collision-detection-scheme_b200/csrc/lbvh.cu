@@ -943,6 +943,9 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
     }
     __syncthreads();
     if (!last) return;
+    // the kernel after the refit may start now (a front maintain's first
+    // kernels wait for the refit's end before they read what it writes)
+    pdl_release();
     __threadfence();
     refit_top(g, nrec, sb, sofs);
     if (threadIdx.x == 0) {

@@ -331,6 +331,9 @@ class Front {
     // the running stage and narrow phase find their counters zeroed already
     // (the maintain's first attempt zeroes them in its prologue)
     bool zeroed_ = false;
+    // the front scans, sprouts and narrow phase of the running maintain are
+    // launched with programmatic stream serialisation
+    bool pdl_ = false;
     int exp_epoch_ = -1, exp_faces_ = -1;
     bool quality_check_ = true;
     DBuf front_[2][2];  // [set][0 int, 1 ext] int2 entries
