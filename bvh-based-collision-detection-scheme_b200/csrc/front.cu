@@ -1236,8 +1236,8 @@ void launch_k(bool pdl, void (*k)(KArgs...), unsigned grid, unsigned block, size
 Front::~Front() {
     for (auto &set : front_)
         for (auto &b : set) b.release();
-    DBuf *bufs[] = {&pairs_, &hits_, &outbuf_, &work_, &intcnt_, &extcnt_, &intbeg_, &extbeg_, &intback_,
-                    &extback_, &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_, &fctr_, &rcur_,
+    DBuf *bufs[] = {&pairs_, &hits_, &outbuf_, &work_, &logcnt_, &intbeg_, &extbeg_,
+                    &snapshot_, &scratch_, &counts64_, &cbuf_, &cflag_, &cscratch_, &fctr_, &rcur_,
                     &pxbuf_, &pxout_, &iexp_, &xexp_, &ksel_};
     for (DBuf *b : bufs) b->release();
     for (int k = 0; k < kSnap; k++)
@@ -1277,21 +1277,16 @@ bvhcd_status Front::init() {
 bvhcd_status Front::ensure_node_capacity(int T) {
     if (T <= capT_) return BVHCD_OK;
     size_t n = (size_t)T + 2;
-    FR_TRY(intcnt_.reserve(sizeof(unsigned) * n));
-    FR_TRY(extcnt_.reserve(sizeof(unsigned) * n));
+    FR_TRY(logcnt_.reserve(sizeof(unsigned) * 4 * n));
     FR_TRY(intbeg_.reserve(sizeof(unsigned) * n));
     FR_TRY(extbeg_.reserve(sizeof(unsigned) * n));
-    FR_TRY(intback_.reserve(sizeof(unsigned) * n));
-    FR_TRY(extback_.reserve(sizeof(unsigned) * n));
     FR_TRY(snapshot_.reserve(sizeof(float) * n));
     FR_TRY(scratch_.reserve(scan_scratch_bytes((int64_t)n)));
     FR_TRY(rcur_.reserve(sizeof(unsigned) * 2 * reorder_groups(T)));
-    FR_TRY(cudaMemset(intcnt_.p, 0, sizeof(unsigned) * n));
-    FR_TRY(cudaMemset(extcnt_.p, 0, sizeof(unsigned) * n));
+    FR_TRY(cudaMemset(logcnt_.p, 0, sizeof(unsigned) * 4 * n));
+    logn_ = n;
     FR_TRY(cudaMemset(intbeg_.p, 0, sizeof(unsigned) * n));
     FR_TRY(cudaMemset(extbeg_.p, 0, sizeof(unsigned) * n));
-    FR_TRY(cudaMemset(intback_.p, 0, sizeof(unsigned) * n));
-    FR_TRY(cudaMemset(extback_.p, 0, sizeof(unsigned) * n));
     FR_TRY(cudaMemset(snapshot_.p, 0, sizeof(float) * n));
     capT_ = T;
     return BVHCD_OK;
@@ -1299,12 +1294,13 @@ bvhcd_status Front::ensure_node_capacity(int T) {
 
 FrontLog Front::log() const {
     FrontLog l;
-    l.intcnt = intcnt_.as<unsigned>();
-    l.extcnt = extcnt_.as<unsigned>();
+    unsigned *c = logcnt_.as<unsigned>();
+    l.intcnt = c;
+    l.extcnt = c + logn_;
+    l.intback = c + 2 * logn_;
+    l.extback = c + 3 * logn_;
     l.intbeg = intbeg_.as<unsigned>();
     l.extbeg = extbeg_.as<unsigned>();
-    l.intback = intback_.as<unsigned>();
-    l.extback = extback_.as<unsigned>();
     return l;
 }
 
@@ -1341,14 +1337,9 @@ static FArgs make_args(const LBvh *bvh, const LBvh *trav, unsigned *ctr, const F
     return a;
 }
 
-// log clear (FlOrderLog.cpp clear): counts and back counts, T+1 entries
-static cudaError_t log_clear(const FrontLog &l, int T, cudaStream_t s) {
-    size_t n = sizeof(unsigned) * (size_t)(T + 1);
-    cudaError_t e = cudaMemsetAsync(l.intcnt, 0, n, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(l.extcnt, 0, n, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(l.intback, 0, n, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(l.extback, 0, n, s);
-    return e;
+// log clear (FlOrderLog.cpp clear): counts and back counts, one memset
+cudaError_t Front::log_clear(cudaStream_t s) const {
+    return cudaMemsetAsync(logcnt_.p, 0, sizeof(unsigned) * 4 * logn_, s);
 }
 
 // FlOrderLog::prepare (FlOrderLog.cu:7-12): begins from counts
@@ -1393,18 +1384,18 @@ bvhcd_status Front::generate(cudaStream_t s, bool pure) {
     FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
     a.pairs = pairs_.as<int2>();
     a.cap_pairs = (unsigned)pcap_;
-    FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
+    if (!zeroed_) FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
     if (pure) {
         StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_PURE_BVH_CD, s);
         k_generate<false><<<grid_for(a.inter ? a.nprim : T), kThreads, 0, s>>>(a); note_launch();
         return cuda_status(cudaGetLastError());
     }
-    FR_TRY(log_clear(l, T, s));
+    FR_TRY(log_clear(s));
     const int nx = 1 - cur_;
     a.out_int = front_[nx][0].as<int2>(); a.out_ext = front_[nx][1].as<int2>();
     a.out_int_slot = 2 * nx; a.out_ext_slot = 2 * nx + 1;
     a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
-    FR_TRY(cudaMemsetAsync(ctr + 2 * nx, 0, 2 * sizeof(unsigned), s));
+    if (!zeroed_) FR_TRY(cudaMemsetAsync(ctr + 2 * nx, 0, 2 * sizeof(unsigned), s));
     {
         StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_GENERATE, s);
         k_generate<true><<<grid_for(a.inter ? a.nprim : T), kThreads, 0, s>>>(a); note_launch();
@@ -1448,7 +1439,7 @@ bvhcd_status Front::update_kernels(cudaStream_t s) {
     const int T = bvh_->T();
     unsigned *ctr = counters();
     FrontLog l = log();
-    FR_TRY(log_clear(l, T, s));
+    FR_TRY(log_clear(s));
     FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
     const int nx = 1 - cur_;
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
@@ -1458,9 +1449,11 @@ bvhcd_status Front::update_kernels(cudaStream_t s) {
     a.cap_int = (unsigned)fcap_[0]; a.cap_ext = (unsigned)fcap_[1];
     a.pairs = pairs_.as<int2>();
     a.cap_pairs = (unsigned)pcap_;
-    FR_TRY(cudaMemsetAsync(ctr + 2 * nx, 0, 2 * sizeof(unsigned), s));
-    FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
-    FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
+    if (!zeroed_) {
+        FR_TRY(cudaMemsetAsync(ctr + 2 * nx, 0, 2 * sizeof(unsigned), s));
+        FR_TRY(cudaMemsetAsync(ctr + C_PAIRS, 0, sizeof(unsigned), s));
+        FR_TRY(cudaMemsetAsync(ctr + C_WORK, 0, sizeof(unsigned), s));
+    }
     {
         StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_FRONT_UPDATE, s);
         LAUNCH_SCAN(k_maintain_int_scan, shape_[BVHCD_SHAPE_PRUNE_INT], s, a);
@@ -1480,7 +1473,7 @@ bvhcd_status Front::restructure_inter(cudaStream_t s) {
     const int T = bvh_->T();
     unsigned *ctr = counters();
     FrontLog l = log();
-    FR_TRY(log_clear(l, T, s));
+    FR_TRY(log_clear(s));
     FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
     const int nx = 1 - cur_;
     a.in_int = front_[cur_][0].as<int2>(); a.in_ext = front_[cur_][1].as<int2>();
@@ -1575,7 +1568,7 @@ bvhcd_status Front::balance_kernels(cudaStream_t s) {
     // time (BvttFrontLooseIntra.cu:286), which places a second balance's
     // entries over one another; its schedules never run two in a row.
     if (log_counted_) FR_TRY(log_prepare(l, T, scratch_.p, s));
-    FR_TRY(log_clear(l, T, s));
+    FR_TRY(log_clear(s));
     log_counted_ = false;
     exp_valid_ = false;  // the internal front moves
     FArgs a = make_args(bvh_, trav_, counters(), l, cfg_.cull_adjacent, work_);
@@ -1806,8 +1799,12 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     const bool from_front = run_op == BVHCD_FRONT_UPDATE || run_op == BVHCD_FRONT_REORDER ||
                             run_op == BVHCD_FRONT_KEEP || run_op == BVHCD_FRONT_RESTRUCTURE;
     // the first attempt's keep and narrow-phase counters start at zero here
-    const unsigned zero = (1u << C_HITS) | (1u << C_PAIRS_VALID) | (1u << C_FLAGGED) |
-                          (run_op == BVHCD_FRONT_KEEP ? (1u << C_PAIRS) | (1u << C_WORK) | (1u << C_KSEL) : 0u);
+    const unsigned nxs = 1u << (2 * (1 - cur_)) | 1u << (2 * (1 - cur_) + 1);  // the other set's front sizes
+    unsigned zero = (1u << C_HITS) | (1u << C_PAIRS_VALID) | (1u << C_FLAGGED);
+    if (run_op == BVHCD_FRONT_KEEP) zero |= (1u << C_PAIRS) | (1u << C_WORK) | (1u << C_KSEL);
+    if (run_op == BVHCD_FRONT_GENERATE) zero |= (1u << C_PAIRS) | nxs;
+    if (run_op == BVHCD_FRONT_PURE_BVH_CD) zero |= 1u << C_PAIRS;
+    if (run_op == BVHCD_FRONT_UPDATE) zero |= (1u << C_PAIRS) | (1u << C_WORK) | nxs;
     static_assert(C_NUM <= 32, "counter slots zeroed by lane");
     // kernels of this maintain may start before the one before them ends
     // (programmatic dependent launch), except inside a stream capture
@@ -1858,11 +1855,15 @@ bvhcd_status Front::copy_state_from(const Front &src, cudaStream_t s) {
     bvhcd_status st = ensure_node_capacity(src.capT_);
     if (st != BVHCD_OK) return st;
     const DBuf *from[] = {&src.front_[0][0], &src.front_[0][1], &src.front_[1][0], &src.front_[1][1], &src.pairs_,
-                          &src.hits_, &src.work_, &src.intcnt_, &src.extcnt_, &src.intbeg_, &src.extbeg_,
-                          &src.intback_, &src.extback_, &src.snapshot_, &src.counts64_, &src.fctr_};
-    DBuf *to[] = {&front_[0][0], &front_[0][1], &front_[1][0], &front_[1][1], &pairs_, &hits_, &work_, &intcnt_,
-                  &extcnt_, &intbeg_, &extbeg_, &intback_, &extback_, &snapshot_, &counts64_, &fctr_};
+                          &src.hits_, &src.work_, &src.intbeg_, &src.extbeg_,
+                          &src.snapshot_, &src.counts64_, &src.fctr_};
+    DBuf *to[] = {&front_[0][0], &front_[0][1], &front_[1][0], &front_[1][1], &pairs_, &hits_, &work_,
+                  &intbeg_, &extbeg_, &snapshot_, &counts64_, &fctr_};
     for (size_t k = 0; k < sizeof(to) / sizeof(to[0]); k++) FR_TRY(to[k]->copy_from(*from[k], s));
+    // the log sections, src.logn_ words each (this front's are at least as long)
+    for (size_t k = 0; k < 4; k++)
+        FR_TRY(cudaMemcpyAsync(logcnt_.as<unsigned>() + k * logn_, src.logcnt_.as<unsigned>() + k * src.logn_,
+                               sizeof(unsigned) * src.logn_, cudaMemcpyDeviceToDevice, s));
     fcap_[0] = src.fcap_[0];
     fcap_[1] = src.fcap_[1];
     pcap_ = src.pcap_;

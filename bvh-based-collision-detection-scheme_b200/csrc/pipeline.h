@@ -340,7 +340,11 @@ class Front {
     int64_t fcap_[2] = {0, 0};
     DBuf pairs_, hits_, outbuf_, work_, cbuf_, cflag_, cscratch_;
     int64_t pcap_ = 0;
-    DBuf intcnt_, extcnt_, intbeg_, extbeg_, intback_, extback_, snapshot_, scratch_, counts64_;
+    // the per-node counts of the front log in one buffer (one clearing memset):
+    // intcnt, extcnt, intback, extback, logn_ words apart
+    DBuf logcnt_, intbeg_, extbeg_, snapshot_, scratch_, counts64_;
+    size_t logn_ = 0;
+    cudaError_t log_clear(cudaStream_t s) const;
     DBuf rcur_;  // reorder cursors, one per group of 2^kReorderShift nodes and front
     DBuf pxbuf_, pxout_;  // proximity counts / offsets / total; records for a host destination
     // deferred capacity check (auto_grow = 2): counter copies of the last

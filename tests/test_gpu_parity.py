@@ -300,7 +300,9 @@ def test_cloth_over_sphere_full_size(cuda, lib_built, oracle):
     the CPU oracle pipeline alongside.  Every frame: the broad set equals the
     brute-force set of overlapping boxes, the hits equal the FP32 SAT over it,
     sizes / op tags / front operation equal the oracle's; on the frames that
-    change the front, both fronts equal the oracle's as multisets."""
+    change the front, both fronts equal the oracle's as multisets; after the
+    builds, a refit and the restructure the tree equals the oracle's bit for
+    bit."""
     import scenes
     faces, frames = scenes.cloth_over_sphere_frames(512, 14)
     T, V = faces.shape[0], frames[0].shape[0]
@@ -329,6 +331,10 @@ def test_cloth_over_sphere_full_size(cuda, lib_built, oracle):
         if f in (0, 5, 6, 8, 12):
             for which in (0, 1):
                 assert np.array_equal(sorted_rows(front.export(which)), sorted_rows(p.front(which))), (f, which)
+        if f in (0, 1, 8, 12):
+            # builds, a refit and the restructure at full size: the single-launch
+            # sort and scans and the one-exchange climb give the reference's tree
+            _tree_equal(bvh.export(), p.tree())
         if f == 7:
             roots = pick_roots(p.tree())
             bvh.request_restructure(roots)
