@@ -233,7 +233,8 @@ def run_ours(args):
                        "pairs_last_frame": [st["broad_pairs"], st["narrow_hits"]]},
             "wall_s_timed_region": round(wall, 4),
             "per_frame_ms": {"median": round(statistics.median(per), 4), "max": round(max(per), 4),
-                             "min": round(min(per), 4)},
+                             "min": round(min(per), 4),
+                             "slowest": [[W + int(k), round(per[k], 4)] for k in np.argsort(per)[::-1][:3]]},
             "e2e": e2e,
             "gpu_launches": int(launches),
             "roofline": roof,
