@@ -112,6 +112,15 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+def gpu_lead(torch, stream, ms=5.0):
+    """A bounded busy-wait kernel (a clock-cycle count) ahead of a timed loop,
+    outside its events: the host enqueues the first frames while it runs, so a
+    host hiccup early in the loop cannot leave the GPU idle inside a frame's
+    interval.  It changes no frame's work."""
+    with torch.cuda.stream(stream):
+        torch.cuda._sleep(int(ms * 1e-3 * 2.0e9))
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -170,6 +179,7 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
+        gpu_lead(torch, stream)
         for i in range(K):
             f = W + i
             flush.zero_()
@@ -285,6 +295,7 @@ def e2e_pass(bvhcd, torch, pipeline, host, faces, dfaces, flush, stream, W, K, V
     e_starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     e_ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     staged = None
+    gpu_lead(torch, stream)
     for i in range(K):
         f = W + i
         flush.zero_()
