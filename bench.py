@@ -430,6 +430,12 @@ def roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
                 b = stage_bytes(stage, T, V, F_prev, F, U, P, H)
             elif stage == "front_keep":
                 b = stage_bytes(stage, T, V, F, 0, U, P, H)
+                if not times.get("narrow", (0, 0))[1]:
+                    # the keep's last launch ran its narrow phase (one launch with
+                    # the traversals below overlapping entries): its bytes count here
+                    if hits is None:
+                        hits = front.pairs()
+                    b += stage_bytes("narrow", T, V, 0, 0, U, P, H, pairs=hits, faces=faces)
             elif stage == "front_balance":
                 b = stage_bytes(stage, T, V, F, st["int_front"], U, P, H)
             elif stage == "front_reorder":

@@ -56,6 +56,19 @@ struct FrontLog {      // FlOrderLog (Mine/collision/auxiliary/FlOrderLog.h:19-5
     unsigned *extback; // T+1
 };
 
+// The narrow phase's inputs and outputs (front.cu).
+struct NarrowArgs {
+    const int4 *psface;
+    const float *pverts;
+    const int4 *sface;
+    const float *verts;
+    int leaf_first;
+    unsigned *ctr;
+    int2 *hits;
+    unsigned cap_pairs, cap_hits;
+    int64_t *counts64;
+};
+
 // Counters kept on the device so no stage needs a host round trip.
 enum CounterSlot {
     C_INT0 = 0, C_EXT0 = 1,   // front sizes, buffer set 0
@@ -78,7 +91,9 @@ enum CounterSlot {
     C_NONFINITE = 20,         // BVH: 1 when the last maintain's input held a NaN or infinite coordinate
     C_NF_DONE = 21,           // BVH: blocks of the build-time finiteness check finished
     C_NARROW_DONE = 22,       // narrow phase: blocks finished (the last one writes the 64-bit counts)
-    C_NUM = 23
+    C_PAIRS_SCAN = 23,        // keep: the pairs the scan emitted (recorded by its last block)
+    C_SCAN_DONE = 24,         // keep: scan blocks finished
+    C_NUM = 25
 };
 
 // Programmatic dependent launch: a kernel launched with programmatic stream

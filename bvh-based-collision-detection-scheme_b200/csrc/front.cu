@@ -76,6 +76,8 @@ struct FArgs {
     // subtree, per leaf slot its subtree root (0 outside), per root the old
     // end of its left spine
     const int *rs_mark, *rs_root, *rs_last;
+    // keep: the scan's last block records the pair count in C_PAIRS_SCAN
+    int snap_scan;
 };
 
 // A node's box and escape link: from the FP32 record ({lo.xyz, rangex |
@@ -169,9 +171,10 @@ __device__ __forceinline__ void emit_ext(const FArgs &a, Em &em, int prim, int l
     if (chunk_put(a.out_ext, a.ctr + a.out_ext_slot, a.cap_ext, em.fe, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 2u))
         node_add(a.log.extcnt, (unsigned)leaf, leaf);
 }
-__device__ __forceinline__ void emit_pair(const FArgs &a, Em &em, int prim, const int4 &pf, int leaf) {
-    if (a.cull && covertex(pf, __ldg(&a.sface[leaf]))) return;
-    chunk_put(a.pairs, a.ctr + C_PAIRS, a.cap_pairs, em.pr, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 4u);
+// Returns whether the pair was stored (not culled, within the capacity).
+__device__ __forceinline__ bool emit_pair(const FArgs &a, Em &em, int prim, const int4 &pf, int leaf) {
+    if (a.cull && covertex(pf, __ldg(&a.sface[leaf]))) return false;
+    return chunk_put(a.pairs, a.ctr + C_PAIRS, a.cap_pairs, em.pr, make_int2(prim, leaf), a.ctr + C_OVERFLOW, 4u);
 }
 __device__ __forceinline__ void emit_work(const FArgs &a, Em &em, const int2 &e) {
     chunk_put(a.work, a.ctr + C_WORK, a.cap_work, em.wk, e, a.ctr + C_OVERFLOW, 32u);
@@ -232,9 +235,10 @@ __device__ __forceinline__ int left_child_tagged(const FArgs &a, int d, const fl
 // record per step for both kinds of node was measured slower: 0.88 against
 // 0.64 ms per generation on the 562,742-triangle scene -- the spine loop
 // keeps consecutive records in a tight dependent chain.)
-template <bool kFront>
-__device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const float4 &plo,
-                                         const float4 &phi, const int4 &pf, int st, int stop) {
+// An overlapping leaf is passed to on_pair (the pair's emission).
+template <bool kFront, typename PairFn>
+__device__ __forceinline__ void traverse_with(const FArgs &a, Em &em, int prim, const float4 &plo,
+                                              const float4 &phi, int st, int stop, PairFn on_pair) {
     // a valid tree is left after at most 2T - 1 visits; the bound only turns
     // a corrupted tree into an error flag instead of an endless loop
     int guard = 2 * a.T + 2;
@@ -268,10 +272,15 @@ __device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const
                 continue;
             }
         }
-        if (overlap(llo, lhi, plo, phi)) emit_pair(a, em, prim, pf, leaf);
+        if (overlap(llo, lhi, plo, phi)) on_pair(leaf);
         if (kFront) emit_ext(a, em, prim, leaf);
         st = __float_as_int(lhi.w);
     }
+}
+template <bool kFront>
+__device__ __forceinline__ void traverse(const FArgs &a, Em &em, int prim, const float4 &plo,
+                                         const float4 &phi, const int4 &pf, int st, int stop) {
+    traverse_with<kFront>(a, em, prim, plo, phi, st, stop, [&](int leaf) { emit_pair(a, em, prim, pf, leaf); });
 }
 
 __device__ __forceinline__ int4 prim_face(const FArgs &a, int prim) {
@@ -691,6 +700,17 @@ __global__ void __launch_bounds__(kB) k_keep_scan(FArgs a) {
         }
     }
     em_close(a, em);
+    if (a.snap_scan) {  // the last block records the scan's pair count (the keep's tail reads it)
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(a.ctr + C_SCAN_DONE, 1u) == gridDim.x - 1) {
+                __threadfence();
+                a.ctr[C_PAIRS_SCAN] = atomicAdd(a.ctr + C_PAIRS, 0u);
+                a.ctr[C_SCAN_DONE] = 0u;
+            }
+        }
+    }
 }
 
 // balance: reorderIntLooseIntraFrontsWithLog (BvttFrontReorderKernels.cu:27-63)
@@ -966,30 +986,82 @@ __device__ __forceinline__ void narrow_done(unsigned *ctr, unsigned cap_pairs, u
 // primitive's triangle from (psface, pverts), the leaf's from (sface, verts)
 // -- the same mesh for an intra front, the other BVH's for an inter front,
 // whose hits are written leaf first (the reference's inter pair order).
-template <bool kTest, int kB>
-__global__ void __launch_bounds__(kB) k_narrow(const int2 *__restrict__ pairs, const int4 *__restrict__ psface,
-                                                     const float *__restrict__ pverts, const int4 *__restrict__ sface,
-                                                     const float *__restrict__ verts, int leaf_first, unsigned *ctr,
-                                                     unsigned cap_pairs, int2 *hits, unsigned cap_hits,
-                                                     int64_t *counts64) {
-    pdl_wait();
-    const unsigned n = min(ctr[C_PAIRS], cap_pairs);
-    unsigned valid = 0;
-    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        int2 p = pairs[q];
-        if (p.x < 0) continue;  // hole
-        ++valid;
-        if (!kTest) continue;
-        int4 a = __ldg(&psface[p.x]), b = __ldg(&sface[p.y]);
-        if (tritri_sat32(vload(pverts, a.x), vload(pverts, a.y), vload(pverts, a.z), vload(verts, b.x),
-                         vload(verts, b.y), vload(verts, b.z)))
-            emit(hits, ctr + C_HITS, cap_hits, leaf_first ? make_int2(b.w, a.w) : make_int2(a.w, b.w),
-                 ctr + C_OVERFLOW, 8u);
-    }
+// The triangles of a pair (traversing primitive, leaf): the primitive's from
+// (psface, pverts), the leaf's from (sface, verts) -- the same mesh for an
+// intra front, the other BVH's for an inter front, whose hits are written
+// leaf first (the reference's inter pair order).
+__device__ __forceinline__ void narrow_test(const NarrowArgs &n, const int2 &p) {
+    const int4 a = __ldg(&n.psface[p.x]), b = __ldg(&n.sface[p.y]);
+    if (tritri_sat32(vload(n.pverts, a.x), vload(n.pverts, a.y), vload(n.pverts, a.z), vload(n.verts, b.x),
+                     vload(n.verts, b.y), vload(n.verts, b.z)))
+        emit(n.hits, n.ctr + C_HITS, n.cap_hits, n.leaf_first ? make_int2(b.w, a.w) : make_int2(a.w, b.w),
+             n.ctr + C_OVERFLOW, 8u);
+}
+__device__ __forceinline__ void count_valid(unsigned *ctr, unsigned valid) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) valid += __shfl_xor_sync(0xffffffffu, valid, o);
     if ((threadIdx.x & 31) == 0 && valid) atomicAdd(ctr + C_PAIRS_VALID, valid);
-    narrow_done(ctr, cap_pairs, cap_hits, counts64);
+}
+
+template <bool kTest, int kB>
+__global__ void __launch_bounds__(kB) k_narrow(const int2 *__restrict__ pairs, NarrowArgs na) {
+    pdl_wait();
+    const unsigned n = min(na.ctr[C_PAIRS], na.cap_pairs);
+    unsigned valid = 0;
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int2 p = pairs[q];
+        if (p.x < 0) continue;  // hole
+        ++valid;
+        if (kTest) narrow_test(na, p);
+    }
+    count_valid(na.ctr, valid);
+    narrow_done(na.ctr, na.cap_pairs, na.cap_hits, na.counts64);
+}
+
+// The end of a keep, sprout and narrow phase in one launch.  The first
+// blocks run the traversals below the overlapping internal entries (the
+// sprout half of keepIntLooseIntraFronts, BvttFrontKeepKernels.cu:21-42)
+// and test each pair they emit at once; the other blocks test the pairs the
+// keep scan emitted, [0, the count its last block recorded).  The pair list
+// is the same as with k_sprout followed by k_narrow (the scan's pairs, then
+// the traversals'), and so are the hits and counts.
+template <bool kTest, int kB>
+__global__ void __launch_bounds__(kB) k_keep_tail(FArgs a, NarrowArgs na) {
+    pdl_wait();
+    Em em;
+    unsigned valid = 0;
+    const unsigned nwork = min(a.ctr[C_WORK], a.cap_work);
+    const unsigned na_blocks = min((nwork + kB - 1) / kB, gridDim.x - 1u);
+    if (blockIdx.x < na_blocks) {
+        for (unsigned q = blockIdx.x * kB + threadIdx.x; q < nwork; q += na_blocks * kB) {
+            const int2 e = a.work[q];
+            if (e.x < 0) continue;  // hole
+            float4 plo, phi;
+            ldg8(a.prec + 2 * e.x, plo, phi);
+            const int node = e.y < 0 ? ~e.y : e.y;  // (as k_sprout: ~R only comes from an inter restructure)
+            float4 nlo, nhi;
+            node_rec(a, node, nlo, nhi);
+            const int4 pf = prim_face(a, e.x);
+            traverse_with<false>(a, em, e.x, plo, phi, e.y < 0 ? (node << 1) : left_child_tagged(a, node, nlo),
+                                 __float_as_int(nhi.w),
+                                 [&](int leaf) {
+                                     if (!emit_pair(a, em, e.x, pf, leaf)) return;
+                                     ++valid;
+                                     if (kTest) narrow_test(na, make_int2(e.x, leaf));
+                                 });
+        }
+        em_close(a, em);
+    } else {
+        const unsigned ns = min(a.ctr[C_PAIRS_SCAN], na.cap_pairs);
+        for (unsigned q = (blockIdx.x - na_blocks) * kB + threadIdx.x; q < ns; q += (gridDim.x - na_blocks) * kB) {
+            const int2 p = a.pairs[q];
+            if (p.x < 0) continue;  // hole
+            ++valid;
+            if (kTest) narrow_test(na, p);
+        }
+    }
+    count_valid(na.ctr, valid);
+    narrow_done(na.ctr, na.cap_pairs, na.cap_hits, na.counts64);
 }
 
 // The precision mode's narrow phase: the FP32 test decides where it is
@@ -1334,6 +1406,7 @@ static FArgs make_args(const LBvh *bvh, const LBvh *trav, unsigned *ctr, const F
     a.iexp_out = a.xexp_out = nullptr;
     a.ksel = nullptr;
     a.rs_mark = a.rs_root = a.rs_last = nullptr;
+    a.snap_scan = 0;
     return a;
 }
 
@@ -1544,11 +1617,26 @@ bvhcd_status Front::keep(cudaStream_t s) {
         }
     }
     last_keep_sel_ = a.ksel != nullptr;
+    a.snap_scan = keep_tail_ ? 1 : 0;
     LAUNCH_SCAN(k_keep_scan, shape_[BVHCD_SHAPE_KEEP], s, a);
     if (expiries) {
         exp_valid_ = true;
         exp_epoch_ = bvh_->topo_epoch();
         exp_faces_ = bvh_->faces_epoch();
+    }
+    if (keep_tail_) {
+        // the narrow phase's counters start at zero (the maintain's prologue
+        // zeroed them on its first attempt)
+        if (!zeroed_) {
+            FR_TRY(cudaMemsetAsync(ctr + C_HITS, 0, sizeof(unsigned), s));
+            FR_TRY(cudaMemsetAsync(ctr + C_PAIRS_VALID, 0, sizeof(unsigned), s));
+            FR_TRY(cudaMemsetAsync(ctr + C_FLAGGED, 0, sizeof(unsigned), s));
+        }
+        // (timed as part of the keep stage)
+        if (cfg_.narrow_phase) LAUNCH_ITEM(k_keep_tail, true, shape_[BVHCD_SHAPE_SPROUT], s, a, narrow_args());
+        else LAUNCH_ITEM(k_keep_tail, false, shape_[BVHCD_SHAPE_SPROUT], s, a, narrow_args());
+        tail_ran_ = true;
+        return cuda_status(cudaGetLastError());
     }
     LAUNCH_ITEM(k_sprout, false, shape_[BVHCD_SHAPE_SPROUT], s, a);
     return cuda_status(cudaGetLastError());
@@ -1600,6 +1688,21 @@ bvhcd_status Front::balance(cudaStream_t s) {
     return BVHCD_OK;
 }
 
+NarrowArgs Front::narrow_args() {
+    NarrowArgs n;
+    n.psface = trav()->tree().sface;
+    n.pverts = trav()->verts();
+    n.sface = bvh_->tree().sface;
+    n.verts = bvh_->verts();
+    n.leaf_first = inter() ? 1 : 0;
+    n.ctr = counters();
+    n.hits = hits_.as<int2>();
+    n.cap_pairs = (unsigned)pcap_;
+    n.cap_hits = (unsigned)pcap_;
+    n.counts64 = counts64_.as<int64_t>();
+    return n;
+}
+
 bvhcd_status Front::narrow(cudaStream_t s, bool test) {
     StageScope prof_scope(bvh_->profiler(), BVHCD_STAGE_NARROW, s);
     unsigned *ctr = counters();
@@ -1614,13 +1717,9 @@ bvhcd_status Front::narrow(cudaStream_t s, bool test) {
         LAUNCH_ITEM(k_narrow_prec, true, sh, s, pairs_.as<int2>(), bvh_->tree().sface, bvh_->verts(), ctr,
                     (unsigned)pcap_, hits_.as<int2>(), (unsigned)pcap_, c64);
     else if (test)
-        LAUNCH_ITEM(k_narrow, true, sh, s, pairs_.as<int2>(), trav()->tree().sface, trav()->verts(),
-                    bvh_->tree().sface, bvh_->verts(), inter() ? 1 : 0, ctr, (unsigned)pcap_, hits_.as<int2>(),
-                    (unsigned)pcap_, c64);
+        LAUNCH_ITEM(k_narrow, true, sh, s, pairs_.as<int2>(), narrow_args());
     else
-        LAUNCH_ITEM(k_narrow, false, sh, s, pairs_.as<int2>(), trav()->tree().sface, trav()->verts(),
-                    bvh_->tree().sface, bvh_->verts(), inter() ? 1 : 0, ctr, (unsigned)pcap_, hits_.as<int2>(),
-                    (unsigned)pcap_, c64);
+        LAUNCH_ITEM(k_narrow, false, sh, s, pairs_.as<int2>(), narrow_args());
     return cuda_status(cudaGetLastError());
 }
 
@@ -1829,8 +1928,14 @@ bvhcd_status Front::maintain(bvhcd_front_op op, cudaStream_t s) {
     // reorder scatter, which is checked before it runs.
     for (int attempt = 0; attempt < 4; attempt++) {
         zeroed_ = attempt == 0;
+        // a keep's sprout and narrow phase run as one launch (not in the
+        // precision mode, whose narrow phase has its own kernel)
+        keep_tail_ = run_op == BVHCD_FRONT_KEEP && !cfg_.precision;
+        tail_ran_ = false;
         st = run(run_op, s);
-        if (st == BVHCD_OK) st = narrow(s, cfg_.narrow_phase != 0);  // without the test it only counts the pairs
+        keep_tail_ = false;
+        // without the test the narrow phase only counts the pairs
+        if (st == BVHCD_OK && !tail_ran_) st = narrow(s, cfg_.narrow_phase != 0);
         zeroed_ = false;
         if (st != BVHCD_OK) return st;
         if (cfg_.auto_grow != 1) break;

@@ -334,6 +334,10 @@ class Front {
     // the front scans, sprouts and narrow phase of the running maintain are
     // launched with programmatic stream serialisation
     bool pdl_ = false;
+    // a KEEP of the running maintain ends in k_keep_tail (its sprout and the
+    // narrow phase in one launch); the maintain then runs no narrow phase
+    bool keep_tail_ = false, tail_ran_ = false;
+    NarrowArgs narrow_args();
     int exp_epoch_ = -1, exp_faces_ = -1;
     bool quality_check_ = true;
     DBuf front_[2][2];  // [set][0 int, 1 ext] int2 entries
