@@ -6,7 +6,9 @@ One step = one frame (BVH maintain + front maintain + narrow phase) through
 the C ABI.  `value` times frames with inputs already resident in HBM;
 `e2e` times the same frames with the vertex upload from pinned host memory
 and the read-back of the contact pairs inside the timed region.  The L2 is
-flushed (256 MB write) between timed frames, outside the frame's events.
+flushed between timed frames, outside the frame's events: a 256 MB write, then
+a 256 MB read that makes the flush write its own dirty lines back
+(--l2-flush dirty: the write alone).
 
 The JSON line also carries "batched": 256 independent scenes (about 9.7M
 triangles) as one forest with graph-launched frames, against the same scenes
@@ -112,6 +114,31 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+class L2Flush:
+    """Between timed frames, outside their events: a 256 MB write (twice the
+    126 MB L2), then -- unless `dirty` -- a 256 MB read of another buffer.
+    The write alone leaves the L2 full of the flush buffer's dirty lines,
+    whose write-back the next frame would pay as its own loads evict them;
+    the read makes the flush write them back itself, so a frame starts with
+    none of its data in L2 and no foreign dirty lines either."""
+
+    N = 256 * 1024 * 1024 // 4
+
+    def __init__(self, torch, dirty=False):
+        self.w = torch.empty(self.N, dtype=torch.float32, device="cuda")
+        self.r = None if dirty else torch.zeros(self.N, dtype=torch.float32, device="cuda")
+        self.desc = ("flushed between frames (256 MB write" +
+                     (")" if dirty else ", then a 256 MB read so the flush's dirty lines leave L2 before the frame)"))
+
+    def __call__(self):
+        self.w.zero_()
+        if self.r is not None:
+            self.r.sum()
+
+
+FLUSH_DIRTY = False  # --l2-flush dirty: the write alone
+
+
 def gpu_lead(torch, stream, ms=5.0):
     """A bounded busy-wait kernel (a clock-cycle count) ahead of a timed loop,
     outside its events: the host enqueues the first frames while it runs, so a
@@ -159,7 +186,7 @@ def run_ours(args):
     host = torch.from_numpy(np.stack(frames)).pin_memory()          # (W+K, V, 3) pinned
     dev = host.to("cuda", non_blocking=False)                       # resident copy for `value`
     dfaces = torch.from_numpy(faces).cuda()
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = L2Flush(torch, FLUSH_DIRTY)
 
     def pipeline():
         bvh = bvhcd.LBvh(T, V, enable_restr=True)
@@ -194,7 +221,7 @@ def run_ours(args):
         gpu_lead(torch, stream)
         for i in range(K):
             f = W + i
-            flush.zero_()
+            flush()
             starts[i].record(stream)
             bvhcd.frame(bvh, front, f, 0, dev[f], dfaces, stream=stream, faces_static=True)
             ends[i].record(stream)
@@ -249,7 +276,7 @@ def run_ours(args):
                        "frames_timed": K, "schedule": "build/12, front cycle 6 (STATIC_MANDATORY, divergent marks)",
                        "restructure": "quality-triggered (enabled)", "adjacency_culling": True,
                        "narrow_phase": "fp32 17-axis SAT",
-                       "l2": "flushed between frames (256 MB write)",
+                       "l2": flush.desc,
                        "parallelism": "replicas" if world > 1 else "single-gpu",
                        "front_sizes_last_frame": [st["int_front"], st["ext_front"]],
                        "pairs_last_frame": [st["broad_pairs"], st["narrow_hits"]]},
@@ -310,7 +337,7 @@ def e2e_pass(bvhcd, torch, pipeline, host, faces, dfaces, flush, stream, W, K, V
     gpu_lead(torch, stream)
     for i in range(K):
         f = W + i
-        flush.zero_()
+        flush()
         e_starts[i].record(stream)
         if staged is None:
             copy.wait_event(e_starts[i])
@@ -414,12 +441,12 @@ def roofline_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
     bvh = bvhcd.LBvh(T, V, enable_restr=True)
     front = bvhcd.BvttFront(bvh, cull_adjacent=True, narrow_phase=True, auto_grow=False, **CAPS)
     bvh.profile(True)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = L2Flush(torch, FLUSH_DIRTY)
     acc = {}   # stage -> [ms, calls, bytes]
     prev = None
     U = 0
     for f in range(W + K):
-        flush.zero_()
+        flush()
         bvhcd.frame(bvh, front, f, 0, dev[f], dfaces, stream=stream, faces_static=f > 0)
         times = bvh.stage_times(reset=True)
         st = front.stats(stream)
@@ -659,7 +686,7 @@ def inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, single):
     intra = bvhcd.BvttFront(cbvh, cull_adjacent=True, narrow_phase=True, auto_grow=False, **CAPS)
     inter = bvhcd.BvttFront(cbvh, rigid=sbvh, narrow_phase=True, auto_grow=False, **CAPS)
     own = bvhcd.BvttFront(sbvh, cull_adjacent=True, narrow_phase=True, auto_grow=False, **CAPS)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = L2Flush(torch, FLUSH_DIRTY)
 
     def frame(f):
         b, fr = bvhcd.schedule(f)
@@ -676,7 +703,7 @@ def inter_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, single):
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     torch.cuda.synchronize()
     for i in range(K):
-        flush.zero_()
+        flush()
         starts[i].record(stream)
         frame(W + i)
         ends[i].record(stream)
@@ -733,7 +760,7 @@ def inter_restructure_timing(bvhcd, torch, cbvh, sbvh, intra, inter, pos, cfaces
     sbvh.maintain(bvhcd.BVH_REFIT, pos[Vc:], sfaces, stream=stream, faces_static=True)
     out = {"bvh_opt_tag": tag}
     for name, op in (("resprout", bvhcd.FRONT_KEEP), ("regenerate", bvhcd.FRONT_GENERATE)):
-        flush.zero_()
+        flush()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         inter.maintain(op, stream=stream)
@@ -760,7 +787,7 @@ def autogrow_pass(bvhcd, torch, dev, dfaces, stream, W, K, T):
     synchronisation) and 1 (grow and replay inside the call: every maintain
     reads the counters back).  The capacities are the bench's, so nothing
     overflows; both give the main loop's pairs."""
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = L2Flush(torch, FLUSH_DIRTY)
     out = {}
     for mode, name in ((2, "deferred"), (1, "sync")):
         bvh = bvhcd.LBvh(T, dev.shape[1], enable_restr=True)
@@ -772,7 +799,7 @@ def autogrow_pass(bvhcd, torch, dev, dfaces, stream, W, K, T):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for i in range(K):
-            flush.zero_()
+            flush()
             starts[i].record(stream)
             bvhcd.frame(bvh, front, W + i, 0, dev[W + i], dfaces, stream=stream, faces_static=True)
             ends[i].record(stream)
@@ -805,7 +832,7 @@ def box_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
         boxes[f, :, 3:] = torch.maximum(a.amax(dim=1), b.amax(dim=1))
     bvh = bvhcd.LBvh(T, 0, enable_restr=True)
     front = bvhcd.BvttFront(bvh, cull_adjacent=True, narrow_phase=False, auto_grow=False, **CAPS)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = L2Flush(torch, FLUSH_DIRTY)
 
     def frame(f):
         b, fr = bvhcd.schedule(f)
@@ -818,7 +845,7 @@ def box_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     torch.cuda.synchronize()
     for i in range(K):
-        flush.zero_()
+        flush()
         starts[i].record(stream)
         frame(W + i)
         ends[i].record(stream)
@@ -872,14 +899,14 @@ def fp16_pass(bvhcd, torch, faces, dev, dfaces, stream, W, K, T):
     frame, timed as `value`, and the last frame's front sizes."""
     bvh = bvhcd.LBvh(T, dev.shape[1], enable_restr=True, node_box_fp16=True)
     front = bvhcd.BvttFront(bvh, cull_adjacent=True, narrow_phase=True, auto_grow=False, **CAPS)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = L2Flush(torch, FLUSH_DIRTY)
     for f in range(W):
         bvhcd.frame(bvh, front, f, 0, dev[f], dfaces, stream=stream, faces_static=f > 0)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     torch.cuda.synchronize()
     for i in range(K):
-        flush.zero_()
+        flush()
         starts[i].record(stream)
         bvhcd.frame(bvh, front, W + i, 0, dev[W + i], dfaces, stream=stream, faces_static=True)
         ends[i].record(stream)
@@ -925,13 +952,13 @@ def precision_pass(bvhcd, torch, stream, args):
         # sized by growing (auto_grow = 1); its time is reported but it only serves the contact check
         front = bvhcd.BvttFront(bvh, cull_adjacent=True, narrow_phase=True, auto_grow=1 if zn else 0, precision=1,
                                 **PREC_CAPS[zn])
-        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        flush = L2Flush(torch, FLUSH_DIRTY)
         W = min(3, nf - 1)
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(nf)]
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(nf)]
         flagged = broad = 0
         for f in range(nf):
-            flush.zero_()
+            flush()
             starts[f].record(stream)
             bvhcd.frame(bvh, front, f, 0, dev[f], dfaces, stream=stream, faces_static=f > 0)
             ends[f].record(stream)
@@ -1089,6 +1116,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--l2-flush", choices=["clean", "dirty"], default="clean",
+                    help="between timed frames: 256 MB write then 256 MB read (clean), or the write alone")
     ap.add_argument("--only-value", action="store_true",
                     help="time the device-resident frames only (no e2e / roofline replay); for profiling")
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
@@ -1103,8 +1132,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global CLOTH
+    global CLOTH, FLUSH_DIRTY
     CLOTH = args.cloth
+    FLUSH_DIRTY = args.l2_flush == "dirty"
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:
         print(json.dumps(out), flush=True)

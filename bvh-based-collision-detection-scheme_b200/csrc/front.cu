@@ -986,10 +986,6 @@ __device__ __forceinline__ void narrow_done(unsigned *ctr, unsigned cap_pairs, u
 // primitive's triangle from (psface, pverts), the leaf's from (sface, verts)
 // -- the same mesh for an intra front, the other BVH's for an inter front,
 // whose hits are written leaf first (the reference's inter pair order).
-// The triangles of a pair (traversing primitive, leaf): the primitive's from
-// (psface, pverts), the leaf's from (sface, verts) -- the same mesh for an
-// intra front, the other BVH's for an inter front, whose hits are written
-// leaf first (the reference's inter pair order).
 __device__ __forceinline__ void narrow_test(const NarrowArgs &n, const int2 &p) {
     const int4 a = __ldg(&n.psface[p.x]), b = __ldg(&n.sface[p.y]);
     if (tritri_sat32(vload(n.pverts, a.x), vload(n.pverts, a.y), vload(n.pverts, a.z), vload(n.verts, b.x),
