@@ -59,9 +59,9 @@ struct FrontLog {      // FlOrderLog (Mine/collision/auxiliary/FlOrderLog.h:19-5
 // The narrow phase's inputs and outputs (front.cu).
 struct NarrowArgs {
     const int4 *psface;
-    const float *pverts;
+    const float4 *pverts;  // positions as 16-byte records (x, y, z, 0)
     const int4 *sface;
-    const float *verts;
+    const float4 *verts;
     int leaf_first;
     unsigned *ctr;
     int2 *hits;

@@ -962,6 +962,10 @@ __device__ __forceinline__ v3 vload(const float *v, int i) {
     const float *p = v + 3 * (size_t)i;
     return {__ldg(p), __ldg(p + 1), __ldg(p + 2)};
 }
+__device__ __forceinline__ v3 vload(const float4 *v, int i) {
+    const float4 p = __ldg(v + i);
+    return {p.x, p.y, p.z};
+}
 
 // The block of the narrow phase that finishes last writes the valid pair and
 // hit counts as 64-bit values (the counts the C ABI exports) and clears the
@@ -1687,9 +1691,9 @@ bvhcd_status Front::balance(cudaStream_t s) {
 NarrowArgs Front::narrow_args() {
     NarrowArgs n;
     n.psface = trav()->tree().sface;
-    n.pverts = trav()->verts();
+    n.pverts = trav()->verts4();
     n.sface = bvh_->tree().sface;
-    n.verts = bvh_->verts();
+    n.verts = bvh_->verts4();
     n.leaf_first = inter() ? 1 : 0;
     n.ctr = counters();
     n.hits = hits_.as<int2>();

@@ -735,6 +735,8 @@ struct RefitTop {
     unsigned *motion;   // accumulated leaf box change (FP32 bits)
     unsigned *nf_acc;   // a block saw a non-finite input coordinate
     unsigned *nonfinite;  // the refit's verdict (written by the last block)
+    float4 *v4;           // the positions as 16-byte records (null for a box scene)
+    int V;
 };
 
 // The crossing nodes, run by the CTA that finished last: a node's slot
@@ -837,6 +839,16 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
     const int L = __ldg(&hdr[0]);
     const int nloc = L >= 0 ? __ldg(&hdr[2 + L]) : 0;
     if (L >= 0 && threadIdx.x <= L + 1) sofs[threadIdx.x] = __ldg(&hdr[1 + threadIdx.x]);
+    // the positions as 16-byte records for the narrow phase: a contiguous
+    // share of the vertices per CTA, read and written coalesced
+    if (g.v4) {
+        const int per = (g.V + (int)gridDim.x - 1) / (int)gridDim.x;
+        const int v1 = min(g.V, (int)blockIdx.x * per + per);
+        for (int v = blockIdx.x * per + threadIdx.x; v < v1; v += kRefitThreads) {
+            const float *x = p.verts + 3 * (size_t)v;
+            g.v4[v] = make_float4(__ldg(x), __ldg(x + 1), __ldg(x + 2), 0.f);
+        }
+    }
     int4 w[kRefitSlots];
     // the largest change of a leaf box coordinate, rounded up: a bound on how
     // far any box of the tree moved (a node's box is a min / max of leaf boxes)
@@ -960,14 +972,24 @@ __global__ void __launch_bounds__(kRefitThreads, 1) k_refit(int T, const int4 *_
 // inline): every coordinate of the n floats (positions, or a box scene's FP32
 // boxes); the last block to finish writes the verdict and clears the
 // accumulator, so the check needs no clearing launch.
-__global__ void __launch_bounds__(kThreads) k_check_finite(int64_t n, const float *__restrict__ x, unsigned *ctr) {
+__global__ void __launch_bounds__(kThreads) k_check_finite(int64_t n, const float *__restrict__ x, unsigned *ctr,
+                                                           float4 *v4) {
     __shared__ unsigned snf;
     __shared__ bool last;
     if (threadIdx.x == 0) snf = 0u;
     __syncthreads();
     bool bad = false;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        bad |= !finite1(__ldg(x + i));
+    if (v4) {  // triangle positions (n = 3 V), also written as 16-byte records
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n / 3;
+             i += (int64_t)gridDim.x * blockDim.x) {
+            const float a = __ldg(x + 3 * i), b = __ldg(x + 3 * i + 1), c = __ldg(x + 3 * i + 2);
+            bad |= !finite1(a) || !finite1(b) || !finite1(c);
+            v4[i] = make_float4(a, b, c, 0.f);
+        }
+    } else {
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            bad |= !finite1(__ldg(x + i));
+    }
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&snf, 1u);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1296,6 +1318,7 @@ bvhcd_status LBvh::init() {
 bvhcd_status LBvh::ensure_capacity(int T, int V) {
     if (V > capV_) {
         BV_TRY(verts_.reserve(sizeof(float) * 3 * (size_t)V));
+        BV_TRY(verts4_.reserve(sizeof(float4) * (size_t)V));
         capV_ = V;
     }
     if (T <= capT_) return BVHCD_OK;
@@ -1559,14 +1582,14 @@ bvhcd_status LBvh::copy_state_from(const LBvh &src, cudaStream_t s) {
     if (&src == this) return BVHCD_OK;
     if (src.cfg_.enable_restr != cfg_.enable_restr || src.cfg_.node_box_fp16 != cfg_.node_box_fp16)
         return BVHCD_INVALID_ARG;
-    const DBuf *from[] = {&src.verts_, &src.faces_, &src.boxes_, &src.nrec_, &src.lrec_, &src.topo_, &src.nrange_, &src.lca_,
+    const DBuf *from[] = {&src.verts_, &src.verts4_, &src.faces_, &src.boxes_, &src.nrec_, &src.lrec_, &src.topo_, &src.nrange_, &src.lca_,
                           &src.sface_, &src.primmap_, &src.code_, &src.refit_flag_, &src.intrange_, &src.rtroot_,
                           &src.intmark_, &src.extrange_, &src.extmark_, &src.leafroot_, &src.ctr_,
                           &src.scene_of_, &src.leafscene_, &src.sbox_, &src.tiles_, &src.scene_, &src.nrec16_,
                           &src.split_, &src.cross_, &src.topk_, &src.plan_, &src.top_,
                           &src.height_, &src.llist_, &src.lhdr_, &src.tlist_, &src.thdr_,
                           &src.llink_, &src.tlink_, &src.lexport_, &src.gext_};
-    DBuf *to[] = {&verts_, &faces_, &boxes_, &nrec_, &lrec_, &topo_, &nrange_, &lca_, &sface_, &primmap_, &code_,
+    DBuf *to[] = {&verts_, &verts4_, &faces_, &boxes_, &nrec_, &lrec_, &topo_, &nrange_, &lca_, &sface_, &primmap_, &code_,
                   &refit_flag_, &intrange_, &rtroot_, &intmark_, &extrange_, &extmark_, &leafroot_, &ctr_,
                   &scene_of_, &leafscene_, &sbox_, &tiles_, &scene_, &nrec16_, &split_, &cross_, &topk_,
                   &plan_, &top_, &height_, &llist_, &lhdr_, &tlist_, &thdr_, &llink_, &tlink_,
@@ -1681,6 +1704,8 @@ bvhcd_status LBvh::refit(cudaStream_t s) {
     g.motion = ctr_.as<unsigned>() + C_MOTION;
     g.nf_acc = ctr_.as<unsigned>() + C_NF_ACC;
     g.nonfinite = ctr_.as<unsigned>() + C_NONFINITE;
+    g.v4 = box_input_ ? nullptr : verts4_.as<float4>();
+    g.V = V_;
     const int nb = (T + kRefitW - 1) / kRefitW;
     k_refit<<<nb, kRefitThreads, kLocalSmem, s>>>(T, sface_.as<int4>(), src(), plan_.as<int4>(), llist_.as<int4>(),
                                                   llink_.as<int2>(), lexport_.as<int4>(), lhdr_.as<int>(),
@@ -1834,7 +1859,8 @@ bvhcd_status LBvh::check_finite(cudaStream_t s) {
     }
     int64_t g = (n + kThreads - 1) / kThreads;
     if (g > kSms * 4) g = kSms * 4;
-    k_check_finite<<<(unsigned)g, kThreads, 0, s>>>(n, x, ctr_.as<unsigned>()); note_launch();
+    k_check_finite<<<(unsigned)g, kThreads, 0, s>>>(n, x, ctr_.as<unsigned>(),
+                                                    box_input_ ? nullptr : verts4_.as<float4>()); note_launch();
     return cuda_status(cudaGetLastError());
 }
 

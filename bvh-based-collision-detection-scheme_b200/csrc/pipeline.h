@@ -147,6 +147,11 @@ class LBvh {
     // advances whenever the faces (vertex ids) may have changed
     int faces_epoch() const { return faces_epoch_; }
     const float *verts() const { return vptr_; }
+    // The positions as 16-byte records (x, y, z, 0), one load per vertex for
+    // the narrow phase's gathers; written by every maintain that reads new
+    // triangle positions (inside the refit, or by the finiteness check ahead
+    // of a build or restructure).
+    const float4 *verts4() const { return verts4_.as<float4>(); }
     const int *faces() const { return fptr_; }
     bool restr_enabled() const { return cfg_.enable_restr != 0; }
 
@@ -190,6 +195,7 @@ class LBvh {
     // owned copies of host input (boxes_: a box scene's FP32 boxes, boxes64_:
     // its FP64 boxes before rounding)
     DBuf verts_, faces_, boxes_, boxes64_;
+    DBuf verts4_;  // 16-byte position records (verts4())
     // tree
     DBuf nrec_, lrec_, topo_, nrange_, lca_, sface_, primmap_, code_, refit_flag_, nrec16_;
     // refit plan (a function of the topology): split of each internal node,
