@@ -187,6 +187,7 @@ def run_ours(args):
     dev = host.to("cuda", non_blocking=False)                       # resident copy for `value`
     dfaces = torch.from_numpy(faces).cuda()
     flush = L2Flush(torch, FLUSH_DIRTY)
+    flush_desc = flush.desc  # (the buffers are released before the JSON line is written)
 
     def pipeline():
         bvh = bvhcd.LBvh(T, V, enable_restr=True)
@@ -276,7 +277,7 @@ def run_ours(args):
                        "frames_timed": K, "schedule": "build/12, front cycle 6 (STATIC_MANDATORY, divergent marks)",
                        "restructure": "quality-triggered (enabled)", "adjacency_culling": True,
                        "narrow_phase": "fp32 17-axis SAT",
-                       "l2": flush.desc,
+                       "l2": flush_desc,
                        "parallelism": "replicas" if world > 1 else "single-gpu",
                        "front_sizes_last_frame": [st["int_front"], st["ext_front"]],
                        "pairs_last_frame": [st["broad_pairs"], st["narrow_hits"]]},
