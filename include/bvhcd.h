@@ -90,7 +90,11 @@ typedef struct {
     int32_t reserved[4];
 } bvhcd_front_config;
 
-/* SceneData{pos, fids} (Mine/world/Scene.h:16-20). */
+/* SceneData{pos, fids} (Mine/world/Scene.h:16-20).  Every maintain that
+ * reads new positions also writes them into the BVH's own 16-byte records
+ * (x, y, z, 0; 16 bytes of device memory per vertex of capacity), which the
+ * FP32 narrow phase reads; the precision mode's narrow phase, the contacts
+ * and the proximity queries read the positions given to the last maintain. */
 typedef struct {
     const float *pos;      /* V x 3 */
     const int32_t *faces;  /* T x 3 vertex ids */
