@@ -826,9 +826,15 @@ __global__ void __launch_bounds__(kReorderThreads) k_reorder(FArgs a, unsigned *
             if (e[j].x == -1) continue;  // hole (a tagged entry is never -1: its index is below 2^31 - 1)
             const unsigned key = (((unsigned)e[j].y >> kReorderShift) << 1) | ((unsigned)e[j].x >> 31);
             unsigned h = (key * 2654435761u) >> kReorderHashShift;
+            // a filled slot keeps its key until the table is cleared, so a plain
+            // load finds the key (most entries: a tile holds far fewer keys than
+            // entries) and only an empty slot needs the compare-and-swap
             for (int probe = 0; probe < kReorderSlots; probe++, h = (h + 1) & (kReorderSlots - 1)) {
-                const unsigned prev = atomicCAS(&skey[h], kEmptyKey, key);
-                if (prev == kEmptyKey) sused[atomicAdd(&nused[par], 1u)] = (unsigned short)h;
+                unsigned prev = *reinterpret_cast<volatile unsigned *>(&skey[h]);
+                if (prev == kEmptyKey) {
+                    prev = atomicCAS(&skey[h], kEmptyKey, key);
+                    if (prev == kEmptyKey) sused[atomicAdd(&nused[par], 1u)] = (unsigned short)h;
+                }
                 if (prev == kEmptyKey || prev == key) break;
             }
             slot[j] = h;
