@@ -416,8 +416,10 @@ __global__ void __launch_bounds__(kB) k_sprout(FArgs a) {
 
 // maintainIntLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:12-57):
 // non-overlapping entries are pruned here, overlapping ones go to k_sprout<true>.
+// Five CTAs of 256 per SM: the scan fits 48 registers without spilling, and
+// the extra warps hide more of its dependent loads (the left-chain walks).
 template <int kU, int kB>
-__global__ void __launch_bounds__(kB) k_maintain_int_scan(FArgs a) {
+__global__ void __launch_bounds__(kB, 1280 / kB) k_maintain_int_scan(FArgs a) {
     pdl_wait();
     Em em;
     const unsigned ni = min(a.ctr[a.in_int_slot], a.cap_int);
