@@ -137,9 +137,17 @@ __device__ __forceinline__ bool covertex(const int4 &a, const int4 &b) {
            (a.y == b.z) | (a.z == b.x) | (a.z == b.y) | (a.z == b.z);
 }
 
+// A vertex in two loads: its 12 bytes start on an 8-byte boundary (x, y as
+// one 8-byte load, then z) or 4 bytes past one (x, then y, z as one 8-byte
+// load); the choice is a select, not a branch, so a warp issues two load
+// instructions whatever its lanes' parities.  Needs only the 4-byte
+// alignment any float array has.
 __device__ __forceinline__ float3 load_vert(const float *v, int i) {
     const float *p = v + 3 * (size_t)i;
-    return make_float3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
+    const bool even = (reinterpret_cast<uintptr_t>(p) & 7u) == 0;
+    const float2 w = __ldg(reinterpret_cast<const float2 *>(even ? p : p + 1));
+    const float s = __ldg(even ? p + 2 : p);
+    return even ? make_float3(w.x, w.y, s) : make_float3(s, w.x, w.y);
 }
 
 // Triangle box: AABB::empty then three combines (Mine/base/Bv.h:27-34,80-84).
