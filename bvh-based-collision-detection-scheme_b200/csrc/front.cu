@@ -445,8 +445,10 @@ __global__ void __launch_bounds__(kB, 1280 / kB) k_maintain_int_scan(FArgs a) {
 }
 
 // maintainExtLooseIntraFrontsWithLog (BvttFrontPruneSproutKernels.cu:60-93)
+// (five CTAs of 256 per SM, as the internal scan: 48 registers with a few
+// bytes of spills, still faster)
 template <int kU, int kB>
-__global__ void __launch_bounds__(kB) k_maintain_ext(FArgs a) {
+__global__ void __launch_bounds__(kB, 1280 / kB) k_maintain_ext(FArgs a) {
     pdl_wait();
     Em em;
     const unsigned ne = min(a.ctr[a.in_ext_slot], a.cap_ext);
