@@ -323,7 +323,10 @@ class Front {
     struct Shape {
         int u, b;
     };
-    Shape shape_[BVHCD_SHAPE_COUNT] = {{2, 256}, {2, 256}, {2, 256}, {2, 256}, {1, 256}, {1, 256}};
+    // default launch shapes (unroll, block) per stage: keep, internal prune,
+    // external prune, balance, sprout, narrow phase; bvhcd_front_set_shapes or
+    // the autotuner replace them
+    Shape shape_[BVHCD_SHAPE_COUNT] = {{2, 256}, {2, 256}, {1, 512}, {2, 256}, {1, 512}, {1, 256}};
     int shape_epoch_ = 0;
     bool has_front_ = false;
     bool int_swapped_ = false;
