@@ -1643,8 +1643,11 @@ bvhcd_status Front::keep(cudaStream_t s) {
             FR_TRY(cudaMemsetAsync(ctr + C_FLAGGED, 0, sizeof(unsigned), s));
         }
         // (timed as part of the keep stage)
-        if (cfg_.narrow_phase) LAUNCH_ITEM(k_keep_tail, true, shape_[BVHCD_SHAPE_SPROUT], s, a, narrow_args());
-        else LAUNCH_ITEM(k_keep_tail, false, shape_[BVHCD_SHAPE_SPROUT], s, a, narrow_args());
+        // (in the keep stage's block size: most of the tail's work is the scan's
+        // pairs, not sprouts)
+        const Shape tail{1, shape_[BVHCD_SHAPE_KEEP].b};
+        if (cfg_.narrow_phase) LAUNCH_ITEM(k_keep_tail, true, tail, s, a, narrow_args());
+        else LAUNCH_ITEM(k_keep_tail, false, tail, s, a, narrow_args());
         tail_ran_ = true;
         return cuda_status(cudaGetLastError());
     }
